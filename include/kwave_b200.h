@@ -1,0 +1,212 @@
+/*
+ * kwave_b200.h -- C ABI of the B200 k-space first-order acoustic time loop.
+ *
+ * This library replaces the time loop of k-Wave's kspaceFirstOrder2D /
+ * kspaceFirstOrder3D (+kwave/+legacy/kspaceFirstOrder3D.m:769-1208,
+ * +kwave/+legacy/kspaceFirstOrder2D.m:712-1044).  The caller runs the
+ * reference's setup (input checking, p0 smoothing, Cartesian->grid sensor
+ * conversion, source scaling, staggered density interpolation) and hands over
+ * exactly the variable set that the reference serialises for its external
+ * native solver at the SaveToDisk hand-off point
+ * (+kwave/+legacy/private/kspaceFirstOrder_saveToDisk.m:46-353,
+ * +kwave/+legacy/kspaceFirstOrder3D.m:669-687), as plain host pointers.
+ *
+ * Conventions
+ *   - Arrays are MATLAB column-major (x fastest), FP32, Nx*Ny*Nz elements.
+ *   - Index arrays are 1-based MATLAB linear indices (as saved by saveToDisk).
+ *   - Signal matrices are column-major [rows x time] like MATLAB's source.p.
+ *   - Every entry point returns kw_status; kw_last_error() gives the message
+ *     of the last failure on the calling thread.  No C++ exception crosses
+ *     the ABI.  The library owns all device memory of a plan.
+ *   - A plan is used by one host thread at a time; plans are independent.
+ */
+#ifndef KWAVE_B200_H
+#define KWAVE_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef int kw_status;
+#define KW_OK              0
+#define KW_ERR_INVALID     1   /* bad argument: mirrors MATLAB error(...) in inputChecking */
+#define KW_ERR_CUDA        2   /* CUDA runtime failure */
+#define KW_ERR_NOMEM       3   /* device allocation failed */
+#define KW_ERR_UNSUPPORTED 4   /* valid reference input this build does not handle */
+#define KW_ERR_TIMEOUT     5   /* a bounded device wait gave up */
+
+#define KW_ABI_VERSION 1
+
+/* sensor.record bit mask (inputChecking.m:340-400 list of record flags) */
+#define KW_REC_P               (1u << 0)
+#define KW_REC_P_MAX           (1u << 1)
+#define KW_REC_P_MIN           (1u << 2)
+#define KW_REC_P_RMS           (1u << 3)
+#define KW_REC_P_MAX_ALL       (1u << 4)
+#define KW_REC_P_MIN_ALL       (1u << 5)
+#define KW_REC_P_FINAL         (1u << 6)
+#define KW_REC_U               (1u << 7)
+#define KW_REC_U_MAX           (1u << 8)
+#define KW_REC_U_MIN           (1u << 9)
+#define KW_REC_U_RMS           (1u << 10)
+#define KW_REC_U_MAX_ALL       (1u << 11)
+#define KW_REC_U_MIN_ALL       (1u << 12)
+#define KW_REC_U_FINAL         (1u << 13)
+#define KW_REC_U_NON_STAGGERED (1u << 14)
+
+/* source modes: saveToDisk.m p_source_mode / u_source_mode */
+#define KW_SOURCE_DIRICHLET              0
+#define KW_SOURCE_ADDITIVE_NO_CORRECTION 1
+#define KW_SOURCE_ADDITIVE               2
+
+/* absorbing_flag: saveToDisk.m (0 lossless, 1 power-law absorbing, 2 stokes) */
+#define KW_LOSSLESS  0
+#define KW_ABSORBING 1
+#define KW_STOKES    2
+
+/* alpha_mode (createAbsorptionVariables.m:37-71) */
+#define KW_ALPHA_NORMAL        0
+#define KW_ALPHA_NO_ABSORPTION 1
+#define KW_ALPHA_NO_DISPERSION 2
+
+/*
+ * One time-varying source field (p, ux, uy or uz).  Mirrors
+ * {p,u}_source_flag / _mode / _many / _index / _input of saveToDisk.m:142-265
+ * plus the labelled-mask signal index of inputChecking.m:853-887.
+ */
+typedef struct kw_source {
+    uint64_t num_time_samples;   /* *_source_flag: signal length, 0 = field absent */
+    int32_t  mode;               /* KW_SOURCE_* */
+    uint64_t num_points;         /* number of source grid points */
+    const uint64_t *index;       /* [num_points] 1-based linear indices, increasing */
+    uint64_t num_signals;        /* rows of input (1 = one signal for all points) */
+    const uint64_t *signal_index;/* [num_points] 1-based row per point, or NULL
+                                    (NULL: row i for point i when num_signals ==
+                                    num_points, row 1 for all when num_signals == 1) */
+    const float *input;          /* [num_signals x num_time_samples], already scaled
+                                    by scaleSourceTerms.m */
+} kw_source;
+
+typedef struct kw_problem {
+    uint32_t abi_version;        /* KW_ABI_VERSION */
+    int32_t  dim;                /* 2 or 3 */
+    uint64_t Nx, Ny, Nz;         /* Nz = 1 in 2D (saveToDisk.m:146-149) */
+    uint64_t Nt;                 /* kgrid.Nt */
+    double   dx, dy, dz, dt;
+    double   c_ref;              /* setSoundSpeedRef.m result */
+
+    /* medium: pointer to N values, or NULL to use the scalar */
+    const float *c0;        double c0_scalar;
+    const float *rho0;      double rho0_scalar;
+    /* staggered densities rho0_sg{x,y,z} (kspaceFirstOrder3D.m:585-601);
+       NULL -> rho0 */
+    const float *rho0_sgx, *rho0_sgy, *rho0_sgz;
+
+    uint64_t pml_x_size, pml_y_size, pml_z_size;
+    double   pml_x_alpha, pml_y_alpha, pml_z_alpha;
+
+    int32_t  use_kspace;         /* 'UsekSpace' (default 1) */
+    int32_t  use_sg;             /* 'UseSG' (default 1) */
+
+    int32_t  nonlinear_flag;
+    const float *BonA;      double BonA_scalar;
+
+    int32_t  absorbing_flag;     /* KW_LOSSLESS / KW_ABSORBING / KW_STOKES */
+    const float *alpha_coeff; double alpha_coeff_scalar;  /* dB/(MHz^y cm) */
+    double   alpha_power;
+    int32_t  alpha_mode;         /* KW_ALPHA_* */
+    double   alpha_sign[2];      /* medium.alpha_sign, {1,1} when absent */
+
+    kw_source p_source;
+    kw_source u_source[3];       /* ux, uy, uz; share mode/index/signal_index */
+    const float *p0_source_input;/* smoothed p0 (N values) or NULL */
+
+    /* sensor (binary mask, find(mask) order); time reversal when
+       time_reversal_input != NULL */
+    uint64_t sensor_num;
+    const uint64_t *sensor_mask_index;  /* [sensor_num] 1-based, increasing */
+    uint64_t record_start_index;        /* >= 1 */
+    uint32_t record;                    /* KW_REC_* mask */
+    const float *time_reversal_input;   /* [sensor_num x Nt] as given (not flipped) */
+
+    /* region kept by *_all and *_final outputs (record.x1_inside...), 1-based
+       inclusive, per axis */
+    uint64_t inside_lo[3], inside_hi[3];
+} kw_problem;
+
+/* Output sizes (createStorageVariables.m:58-88). */
+typedef struct kw_output_desc {
+    uint64_t sensor_num;          /* rows of time-series outputs */
+    uint64_t num_time_points;     /* Nt - record_start_index + 1 */
+    uint64_t inside_shape[3];     /* shape of *_all / *_final outputs */
+    uint64_t grid_shape[3];
+} kw_output_desc;
+
+/* Caller-allocated host buffers; NULL for outputs not recorded. */
+typedef struct kw_outputs {
+    float *p, *p_max, *p_min, *p_rms, *p_max_all, *p_min_all, *p_final;
+    float *u[3], *u_max[3], *u_min[3], *u_rms[3], *u_max_all[3], *u_min_all[3];
+    float *u_final[3], *u_non_staggered[3];
+} kw_outputs;
+
+typedef struct kw_plan kw_plan;
+
+/* Last error message of the calling thread ("" if none). */
+const char *kw_last_error(void);
+
+/* Library / ABI version. */
+int kw_abi_version(void);
+
+/* Validate *problem, upload it and build every operator on the device.
+   Replaces the external binary's read of the HDF5 input file
+   (kspaceFirstOrder3DC.m:530-546). */
+kw_status kw_plan_create(const kw_problem *problem, kw_plan **plan);
+
+/* Sizes of every output of this plan. */
+kw_status kw_plan_outputs(const kw_plan *plan, kw_output_desc *desc);
+
+/* Run the whole time loop and copy the recorded outputs to *out.
+   Synchronous.  Equivalent of running the binary and reading its HDF5
+   outputs (kspaceFirstOrder3DC.m:546-780). */
+kw_status kw_run(kw_plan *plan, kw_outputs *out);
+
+/* Split form of kw_run: kw_run_device leaves every output on the device;
+   kw_copy_outputs copies them to the host.  kw_reset restores the initial
+   state so the plan can run again. */
+kw_status kw_reset(kw_plan *plan);
+kw_status kw_run_device(kw_plan *plan);
+kw_status kw_copy_outputs(kw_plan *plan, kw_outputs *out);
+
+/* Advance the loop by n steps (n <= remaining); used by step-wise callers. */
+kw_status kw_step(kw_plan *plan, uint64_t n);
+
+/* Free every resource of the plan. */
+kw_status kw_plan_destroy(kw_plan *plan);
+
+/*
+ * Kernel timing: when enabled, each launch of the kernel classes selected by
+ * class_mask is bracketed by CUDA events on the plan's stream; kw_get_timing
+ * returns the summed device milliseconds and the launch count for one class.
+ */
+#define KW_KCLASS_ZSTAGE_U   0   /* momentum update + z transforms */
+#define KW_KCLASS_ZSTAGE_R   1   /* mass conservation / equation of state + z transforms */
+#define KW_KCLASS_ZSTAGE_P   2   /* absorbing pressure finish + z transform */
+#define KW_KCLASS_YPASS      3   /* y-axis FFT passes */
+#define KW_KCLASS_XPASS      4   /* x-axis fused forward/operator/inverse passes */
+#define KW_KCLASS_SENSOR     5   /* sensor gather / reduction */
+#define KW_KCLASS_SOURCE     6   /* source scatter / injection */
+#define KW_KCLASS_COUNT      7
+kw_status kw_set_timing(kw_plan *plan, uint32_t class_mask);
+kw_status kw_get_timing(const kw_plan *plan, int kclass, double *total_ms, uint64_t *launches);
+
+/* Device bytes held by the plan. */
+kw_status kw_plan_device_bytes(const kw_plan *plan, uint64_t *bytes);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* KWAVE_B200_H */

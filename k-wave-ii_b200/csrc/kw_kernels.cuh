@@ -1,0 +1,845 @@
+// kw_kernels.cuh -- transform passes and fused physics stages of the k-space loop.
+//
+// Layout in HBM.  Internally every grid is 3-D (N0, N1, N2) with axis 0
+// contiguous (MATLAB column-major x).  A 3-D problem maps (Nx, Ny, Nz) to
+// (N0, N1, N2); a 2-D problem maps (Nx, Ny) to (Nx, 1, Ny) so the same code
+// serves both.  Real fields hold N0*N1*N2 floats.  Spectra are "z-half"
+// spectra: the real-to-complex axis is axis 2, so a spectrum holds
+// N0*N1*N2h complex values, N2h = N2/2 + 1, element (x, y, kz) at
+// x + N0*(y + N1*kz).  Axis 0 stays contiguous in every layout, so every
+// pass reads and writes whole rows of axis 0.
+//
+// One spectral operator application real(ifftn(op .* fftn(f))) is:
+//   z-stage (R2C along axis 2, fused into the kernel that produces f)
+//   y-pass forward (C2C along axis 1)
+//   x-pass: forward C2C along axis 0, multiply by op (and 1/N), inverse C2C
+//   y-pass inverse
+//   z-stage (C2R along axis 2, fused into the kernel that consumes the result)
+//
+// Real-to-complex and complex-to-real along axis 2 pack two neighbouring
+// axis-0 columns into one complex line (z = a + i b) so every line transform
+// is a full complex transform.
+#pragma once
+
+#include "kw_fft.cuh"
+
+namespace kw {
+
+struct Geom {
+    int N0, N1, N2, N2h;
+    long long N;      // N0*N1*N2
+    long long Nh;     // N0*N1*N2h
+    int vec2;         // N0 even: pairs (x, x+1) with x even are 8/16-byte aligned
+};
+
+struct Spec4 { float2 *p[4]; };
+
+// ---- scalar-or-array medium quantity -------------------------------------
+struct Med {
+    const float *arr;
+    float val;
+};
+__device__ __forceinline__ float2 med2(const Med &m, long long gi, bool two, bool vec) {
+    if (!m.arr) return make_float2(m.val, m.val);
+    if (two && vec) return __ldg(reinterpret_cast<const float2 *>(m.arr + gi));
+    return make_float2(__ldg(m.arr + gi), two ? __ldg(m.arr + gi + 1) : 0.f);
+}
+__device__ __forceinline__ float2 ld2(const float *p, long long gi, bool two, bool vec) {
+    if (two && vec) return *reinterpret_cast<const float2 *>(p + gi);
+    return make_float2(p[gi], two ? p[gi + 1] : 0.f);
+}
+__device__ __forceinline__ void st2(float *p, long long gi, float2 v, bool two, bool vec) {
+    if (two && vec) { *reinterpret_cast<float2 *>(p + gi) = v; return; }
+    p[gi] = v.x;
+    if (two) p[gi + 1] = v.y;
+}
+
+// ---- spectral operators ----------------------------------------------------
+enum OpKind { OP_GRAD_POS = 0, OP_GRAD_NEG = 1, OP_NABLA1 = 2, OP_NABLA2 = 3, OP_SRC_KAPPA = 4, OP_IDENT = 5 };
+
+struct OpParams {
+    const float2 *dd_pos[3];   // i k exp(+i k d/2) per axis, FFT order, Hermitian part
+    const float2 *dd_neg[3];   // i k exp(-i k d/2)
+    const float *k2[3];        // k_i^2 per axis, FFT order
+    float kappa_a;             // c_ref * dt / 2
+    int use_kspace;
+    float nabla1_exp, nabla2_exp;  // alpha_power - 2, alpha_power - 1
+    float scale;               // 1 / (N0 N1 N2)
+};
+
+struct OpSet {
+    int n;
+    int kind[3];
+    int axis[3];
+};
+
+__device__ __forceinline__ float pow_k(float km, float e) {
+    // MATLAB: k.^e with inf -> 0 (createAbsorptionVariables.m:40-52)
+    if (km == 0.f) return e > 0.f ? 0.f : (e == 0.f ? 1.f : 0.f);
+    return powf(km, e);
+}
+
+__device__ __forceinline__ float2 eval_op(const OpParams &P, int kind, int axis, int ix, int iy, int iz) {
+    const float k2 = __ldg(P.k2[0] + ix) + __ldg(P.k2[1] + iy) + __ldg(P.k2[2] + iz);
+    const float km = sqrtf(k2);
+    switch (kind) {
+        case OP_GRAD_POS:
+        case OP_GRAD_NEG: {
+            float kap = 1.f;
+            if (P.use_kspace && km > 0.f) {
+                const float a = P.kappa_a * km;
+                kap = sinf(a) / a;
+            }
+            const int i = axis == 0 ? ix : (axis == 1 ? iy : iz);
+            const float2 d = __ldg((kind == OP_GRAD_POS ? P.dd_pos[axis] : P.dd_neg[axis]) + i);
+            return cscale(d, kap * P.scale);
+        }
+        case OP_NABLA1: return make_float2(pow_k(km, P.nabla1_exp) * P.scale, 0.f);
+        case OP_NABLA2: return make_float2(pow_k(km, P.nabla2_exp) * P.scale, 0.f);
+        case OP_SRC_KAPPA: {
+            const float c = P.use_kspace ? cosf(P.kappa_a * km) : 1.f;
+            return make_float2(c * P.scale, 0.f);
+        }
+        default: return make_float2(P.scale, 0.f);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// y-pass: C2C along axis 1 of a spectrum, in place.  Tile = TY consecutive x
+// at one kz; lines interleaved (x fastest) so loads are coalesced rows.
+// grid = (ceil(N0/TY), N2h, nfields)
+// ---------------------------------------------------------------------------
+template <bool INV>
+__global__ void __launch_bounds__(kThreads, 2) k_ypass(Spec4 bufs, Geom g, AxisFFT ax, int TY) {
+    extern __shared__ float2 sm[];
+    float2 *buf = bufs.p[blockIdx.z];
+    const int x0 = blockIdx.x * TY;
+    const long long base = (long long)blockIdx.y * g.N1 * g.N0;
+    const int tot = TY * g.N1;
+    for (int idx = threadIdx.x; idx < tot; idx += kThreads) {
+        const int l = idx % TY, y = idx / TY, x = x0 + l;
+        sm[idx] = x < g.N0 ? buf[base + (long long)y * g.N0 + x] : make_float2(0.f, 0.f);
+    }
+    __syncthreads();
+    fft_tile<INV>(sm, ax, TY, TY, 1, true);
+    for (int idx = threadIdx.x; idx < tot; idx += kThreads) {
+        const int l = idx % TY, y = idx / TY, x = x0 + l;
+        if (x < g.N0) buf[base + (long long)y * g.N0 + x] = sm[idx];
+    }
+}
+
+// ---------------------------------------------------------------------------
+// x-pass: forward C2C along axis 0, operator, inverse C2C, in place.
+// Lines (y, kz) are contiguous rows of N0 complex values.
+//   fanout == 0: field f = blockIdx.z gets operator ops[f]
+//   fanout == 1: field 0 is transformed once and ops[0..n-1] write fields 0..n-1
+// grid = (ceil(N1*N2h / NL), 1, fanout ? 1 : nfields)
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(kThreads, 2) k_xpass(Spec4 bufs, Geom g, AxisFFT ax, int NL, OpParams P,
+                                                     OpSet ops, int fanout) {
+    extern __shared__ float2 sm[];
+    const int N0 = g.N0;
+    const int lines_total = g.N1 * g.N2h;
+    const int line0 = blockIdx.x * NL;
+    const int nl = min(NL, lines_total - line0);
+    const int f = fanout ? 0 : blockIdx.z;
+    float2 *A = sm;
+    float2 *B = sm + NL * N0;
+    const long long off = (long long)line0 * N0;
+    const int tot = nl * N0;
+    {
+        const float2 *in = bufs.p[f] + off;
+        for (int idx = threadIdx.x; idx < tot; idx += kThreads) A[idx] = in[idx];
+    }
+    __syncthreads();
+    fft_tile<false>(A, ax, nl, 1, N0, false);
+    const int nout = fanout ? ops.n : 1;
+    for (int o = 0; o < nout; ++o) {
+        const int oi = fanout ? o : f;
+        float2 *W = fanout ? B : A;
+        for (int idx = threadIdx.x; idx < tot; idx += kThreads) {
+            const int l = idx / N0, ix = idx - l * N0;
+            const int line = line0 + l;
+            const int iy = line % g.N1, iz = line / g.N1;
+            W[idx] = cmul(A[idx], eval_op(P, ops.kind[oi], ops.axis[oi], ix, iy, iz));
+        }
+        __syncthreads();
+        fft_tile<true>(W, ax, nl, 1, N0, false);
+        float2 *out = bufs.p[oi] + off;
+        for (int idx = threadIdx.x; idx < tot; idx += kThreads) out[idx] = W[idx];
+        __syncthreads();
+    }
+}
+
+// ---------------------------------------------------------------------------
+// z-line tile helpers.  A tile is TX = 2*PL consecutive x at one y and every
+// z; packed element (l, z) at s[z*PL + l] holds (f(x0+2l), f(x0+2l+1)).
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void zload_c2r(float2 *s, const float2 *__restrict__ H, const Geom &g, int x0, int y,
+                                          int PL) {
+    const int N2 = g.N2, N0 = g.N0;
+    const int tot = PL * N2;
+    for (int idx = threadIdx.x; idx < tot; idx += kThreads) {
+        const int l = idx % PL, z = idx / PL;
+        int k = z;
+        bool cj = false;
+        if (z >= g.N2h) { k = N2 - z; cj = true; }
+        const int xa = x0 + 2 * l;
+        const float2 *h = H + ((long long)k * g.N1 + y) * N0;
+        float2 A, B;
+        if (g.vec2 && xa + 1 < N0) {
+            const float4 q = *reinterpret_cast<const float4 *>(h + xa);
+            A = make_float2(q.x, q.y);
+            B = make_float2(q.z, q.w);
+        } else {
+            A = xa < N0 ? h[xa] : make_float2(0.f, 0.f);
+            B = xa + 1 < N0 ? h[xa + 1] : make_float2(0.f, 0.f);
+        }
+        if (cj) { A.y = -A.y; B.y = -B.y; }
+        if (k == 0 || 2 * k == N2) { A.y = 0.f; B.y = 0.f; }   // Hermitian projection
+        s[idx] = make_float2(A.x - B.y, A.y + B.x);
+    }
+}
+
+__device__ __forceinline__ void zstore_r2c(const float2 *s, float2 *__restrict__ H, const Geom &g, int x0, int y,
+                                           int PL) {
+    const int N0 = g.N0;
+    const int tot = PL * g.N2h;
+    for (int idx = threadIdx.x; idx < tot; idx += kThreads) {
+        const int l = idx % PL, k = idx / PL;
+        const float2 Zk = s[k * PL + l];
+        const int nk = k == 0 ? 0 : g.N2 - k;
+        const float2 Zn = s[nk * PL + l];
+        const float2 A = make_float2(0.5f * (Zk.x + Zn.x), 0.5f * (Zk.y - Zn.y));
+        const float2 B = make_float2(0.5f * (Zk.y + Zn.y), -0.5f * (Zk.x - Zn.x));
+        const int xa = x0 + 2 * l;
+        float2 *h = H + ((long long)k * g.N1 + y) * N0;
+        if (g.vec2 && xa + 1 < N0) {
+            *reinterpret_cast<float4 *>(h + xa) = make_float4(A.x, A.y, B.x, B.y);
+        } else {
+            if (xa < N0) h[xa] = A;
+            if (xa + 1 < N0) h[xa + 1] = B;
+        }
+    }
+}
+
+__device__ __forceinline__ void zload_real(float2 *s, const float *__restrict__ R, const Geom &g, int x0, int y,
+                                           int PL) {
+    const int tot = PL * g.N2;
+    for (int idx = threadIdx.x; idx < tot; idx += kThreads) {
+        const int l = idx % PL, z = idx / PL;
+        const int xa = x0 + 2 * l;
+        const long long gi = xa + (long long)g.N0 * (y + (long long)g.N1 * z);
+        const bool two = xa + 1 < g.N0;
+        s[idx] = xa < g.N0 ? ld2(R, gi, two, g.vec2) : make_float2(0.f, 0.f);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// source descriptions used inside the fused z-stages
+// ---------------------------------------------------------------------------
+// Dense additive source: field += scale * F, scale = sig[t-1] (one signal
+// for every source point) or 1 (F already holds this step's filtered source).
+struct DenseSrc {
+    const float *F;
+    const float *sig;
+    int T;
+};
+__device__ __forceinline__ bool dense_active(const DenseSrc &d, int t, float &scale) {
+    if (!d.F || t > d.T) return false;
+    scale = d.sig ? __ldg(d.sig + (t - 1)) : 1.f;
+    return true;
+}
+
+// Sparse point source (dirichlet / additive-no-correction), CSR per z-tile.
+struct SparseSrc {
+    const int *off;       // [ntiles + 1], tile = blockIdx.x + gridDim.x * blockIdx.y
+    const int *cell;      // tile-local cell: z * TX + (x - x0)
+    const int *row;       // signal row of the entry
+    const float *sig[3];  // [nsig x T] column-major per field component
+    int T[3];             // signal length per component
+    int nsig, mode;       // mode: 0 dirichlet, 1 additive-no-correction
+};
+
+// Time-reversal overwrite of p on the sensor mask, CSR per z-tile.
+struct TRSrc {
+    const int *off;
+    const int *cell;
+    const int *row;       // sensor row
+    const float *data;    // [M x Nt] as given (not flipped)
+    int M, Nt;
+};
+
+// ---------------------------------------------------------------------------
+// Stage U: momentum conservation (kspaceFirstOrder3D.m:792-803), velocity
+// sources (:806-886) and the forward z-transform of the new velocity.
+// Input spec[f] = z-half spectrum of dd_pos_f kappa p_k after the inverse x/y
+// passes; output spec[f] = z-half spectrum of u_f.
+// grid = (ceil(N0/TX), N1, D); blockIdx.z = velocity component.
+// ---------------------------------------------------------------------------
+struct StageU {
+    Geom g;
+    AxisFFT axz;
+    int PL;
+    Spec4 spec;
+    float *u[3];
+    Med rho_sg_inv[3];
+    const float *pml_sg[3];   // per internal axis
+    float dt;
+    int init;                 // p0 start: u = dt/2 rho_sg_inv grad, no PML, no output spectrum
+    int write_spec;
+    DenseSrc dense[3];
+    SparseSrc sparse;
+    const int *d_t;
+    int comp_axis[3];         // internal axis of velocity component f
+};
+
+__global__ void __launch_bounds__(kThreads, 2) k_stage_u(StageU a) {
+    extern __shared__ float2 sm[];
+    const Geom &g = a.g;
+    const int f = blockIdx.z;
+    const int PL = a.PL, TX = 2 * PL;
+    const int x0 = blockIdx.x * TX, y = blockIdx.y;
+    const int t = *a.d_t;
+    float *u = a.u[f];
+    const int ax = a.comp_axis[f];
+    const float *pmlv = a.pml_sg[ax];
+
+    zload_c2r(sm, a.spec.p[f], g, x0, y, PL);
+    __syncthreads();
+    fft_tile<true>(sm, a.axz, PL, PL, 1, true);
+
+    float dscale = 0.f;
+    const bool dense = dense_active(a.dense[f], t, dscale);
+    const float pml_y = ax == 1 ? __ldg(pmlv + y) : 1.f;
+    const int tot = PL * g.N2;
+    for (int idx = threadIdx.x; idx < tot; idx += kThreads) {
+        const int l = idx % PL, z = idx / PL;
+        const int xa = x0 + 2 * l;
+        if (xa >= g.N0) continue;
+        const bool two = xa + 1 < g.N0;
+        const long long gi = xa + (long long)g.N0 * (y + (long long)g.N1 * z);
+        const float2 gr = sm[idx];
+        const float2 ri = med2(a.rho_sg_inv[f], gi, two, g.vec2);
+        float2 un;
+        if (a.init) {
+            un = make_float2(0.5f * a.dt * ri.x * gr.x, 0.5f * a.dt * ri.y * gr.y);
+        } else {
+            float2 pm;
+            if (ax == 0) pm = make_float2(__ldg(pmlv + xa), two ? __ldg(pmlv + xa + 1) : 1.f);
+            else if (ax == 1) pm = make_float2(pml_y, pml_y);
+            else { const float q = __ldg(pmlv + z); pm = make_float2(q, q); }
+            const float2 uo = ld2(u, gi, two, g.vec2);
+            un.x = pm.x * (pm.x * uo.x - a.dt * ri.x * gr.x);
+            un.y = pm.y * (pm.y * uo.y - a.dt * ri.y * gr.y);
+            if (dense) {
+                const float2 F = ld2(a.dense[f].F, gi, two, g.vec2);
+                un.x = fmaf(dscale, F.x, un.x);
+                un.y = fmaf(dscale, F.y, un.y);
+            }
+        }
+        st2(u, gi, un, two, g.vec2);
+        sm[idx] = make_float2(un.x, two ? un.y : 0.f);
+    }
+    __syncthreads();
+    if (!a.init && a.sparse.off && a.sparse.sig[f] && t <= a.sparse.T[f]) {
+        const int tile = blockIdx.x + gridDim.x * blockIdx.y;
+        const int e0 = a.sparse.off[tile], e1 = a.sparse.off[tile + 1];
+        for (int e = e0 + threadIdx.x; e < e1; e += kThreads) {
+            const int c = a.sparse.cell[e];
+            const int z = c / TX, xl = c - z * TX;
+            const float v = __ldg(a.sparse.sig[f] + a.sparse.row[e] + (long long)a.sparse.nsig * (t - 1));
+            float *slot = reinterpret_cast<float *>(sm + z * PL + (xl >> 1)) + (xl & 1);
+            const float nv = a.sparse.mode == 0 ? v : *slot + v;
+            *slot = nv;
+            u[x0 + xl + (long long)g.N0 * (y + (long long)g.N1 * z)] = nv;
+        }
+        __syncthreads();
+    }
+    if (!a.init && a.write_spec) {
+        fft_tile<false>(sm, a.axz, PL, PL, 1, true);
+        zstore_r2c(sm, a.spec.p[f], g, x0, y, PL);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Stage R: mass conservation (kspaceFirstOrder3D.m:912-927), pressure sources
+// (:930-962) and the equation of state (:965-1019).
+//   lossless / stokes: p complete; output spec[0] = R2C(p)
+//   absorbing: p holds the non-spectral part; outputs R2C(rho0 * sum du) and
+//   R2C(sum rho) for the absorption / dispersion operators
+// Input spec[0..D-1] = z-half spectra of the velocity divergence terms.
+// grid = (ceil(N0/TX), N1, 1)
+// ---------------------------------------------------------------------------
+struct StageR {
+    Geom g;
+    AxisFFT axz;
+    int PL;
+    int D;
+    Spec4 spec;
+    float *rho[3];
+    float *p;
+    Med rho0, c0, BonA, alpha_np;
+    const float *pml[3];      // per internal axis
+    int comp_axis[3];
+    float dt;
+    int nonlinear;
+    int eos;                  // 0 lossless, 1 absorbing, 2 stokes
+    int has_tau, has_eta;
+    float alpha_y;            // power-law exponent used for tau (stokes: 2)
+    float tau_sign;
+    DenseSrc dense;
+    SparseSrc sparse;
+    TRSrc tr;
+    int write_spec;
+    const int *d_t;
+};
+
+__device__ __forceinline__ float tau_of(float anp, float c, float y, float sgn) {
+    // createAbsorptionVariables.m:45 (absorbing) / :84 (stokes, y = 2)
+    return -2.f * anp * powf(c, y - 1.f) * sgn;
+}
+
+__device__ __forceinline__ void apply_tr(float2 *sm, const TRSrc &tr, const Geom &g, int PL, int x0, int y, int t,
+                                         float *rho0_, float *rho1_, float *rho2_, int D, const Med &c0, float *p) {
+    // Dirichlet overwrite of p on the mask with the flipped data for step t+1
+    // (kspaceFirstOrder3D.m:772-788; 2D :715-729) and the matching rho.
+    if (!tr.off) return;
+    const int col = tr.Nt - t - 1;       // flipped column t+1 (1-based) -> original column
+    if (col < 0) return;
+    const int TX = 2 * PL;
+    const int tile = blockIdx.x + gridDim.x * blockIdx.y;
+    const int e0 = tr.off[tile], e1 = tr.off[tile + 1];
+    for (int e = e0 + threadIdx.x; e < e1; e += kThreads) {
+        const int c = tr.cell[e];
+        const int z = c / TX, xl = c - z * TX;
+        const float v = __ldg(tr.data + tr.row[e] + (long long)tr.M * col);
+        const long long gi = x0 + xl + (long long)g.N0 * (y + (long long)g.N1 * z);
+        float *slot = reinterpret_cast<float *>(sm + z * PL + (xl >> 1)) + (xl & 1);
+        *slot = v;
+        p[gi] = v;
+        const float cc = c0.arr ? __ldg(c0.arr + gi) : c0.val;
+        const float r = v / ((float)D * cc * cc);
+        rho0_[gi] = r;
+        rho1_[gi] = r;
+        if (D == 3) rho2_[gi] = r;
+    }
+}
+
+__global__ void __launch_bounds__(kThreads, 2) k_stage_r(StageR a) {
+    extern __shared__ float2 sm[];
+    const Geom &g = a.g;
+    const int PL = a.PL, TX = 2 * PL;
+    const int tot = PL * g.N2;
+    float2 *tile = sm;
+    float2 *acc_old = sm + tot;
+    float2 *acc_rho = sm + 2 * tot;
+    float2 *acc_du = sm + 3 * tot;
+    const int x0 = blockIdx.x * TX, y = blockIdx.y;
+    const int t = *a.d_t;
+    float dscale = 0.f;
+    const bool dense = dense_active(a.dense, t, dscale);
+
+    // sum of rho before the update (nonlinear mass conservation, :921)
+    for (int idx = threadIdx.x; idx < tot; idx += kThreads) {
+        const int l = idx % PL, z = idx / PL;
+        const int xa = x0 + 2 * l;
+        float2 so = make_float2(0.f, 0.f);
+        if (a.nonlinear && xa < g.N0) {
+            const bool two = xa + 1 < g.N0;
+            const long long gi = xa + (long long)g.N0 * (y + (long long)g.N1 * z);
+            for (int i = 0; i < a.D; ++i) {
+                const float2 r = ld2(a.rho[i], gi, two, g.vec2);
+                so.x += r.x;
+                so.y += r.y;
+            }
+        }
+        acc_old[idx] = so;
+        acc_rho[idx] = make_float2(0.f, 0.f);
+        acc_du[idx] = make_float2(0.f, 0.f);
+    }
+    for (int i = 0; i < a.D; ++i) {
+        __syncthreads();
+        zload_c2r(tile, a.spec.p[i], g, x0, y, PL);
+        __syncthreads();
+        fft_tile<true>(tile, a.axz, PL, PL, 1, true);
+        const int ax = a.comp_axis[i];
+        const float *pmlv = a.pml[ax];
+        const float pml_y = ax == 1 ? __ldg(pmlv + y) : 1.f;
+        float *rho = a.rho[i];
+        for (int idx = threadIdx.x; idx < tot; idx += kThreads) {
+            const int l = idx % PL, z = idx / PL;
+            const int xa = x0 + 2 * l;
+            if (xa >= g.N0) continue;
+            const bool two = xa + 1 < g.N0;
+            const long long gi = xa + (long long)g.N0 * (y + (long long)g.N1 * z);
+            const float2 du = tile[idx];
+            float2 coef = med2(a.rho0, gi, two, g.vec2);
+            if (a.nonlinear) {
+                const float2 so = acc_old[idx];
+                coef.x = 2.f * so.x + coef.x;
+                coef.y = 2.f * so.y + coef.y;
+            }
+            float2 pm;
+            if (ax == 0) pm = make_float2(__ldg(pmlv + xa), two ? __ldg(pmlv + xa + 1) : 1.f);
+            else if (ax == 1) pm = make_float2(pml_y, pml_y);
+            else { const float q = __ldg(pmlv + z); pm = make_float2(q, q); }
+            const float2 ro = ld2(rho, gi, two, g.vec2);
+            float2 rn;
+            rn.x = pm.x * (pm.x * ro.x - a.dt * coef.x * du.x);
+            rn.y = pm.y * (pm.y * ro.y - a.dt * coef.y * du.y);
+            if (dense) {
+                const float2 F = ld2(a.dense.F, gi, two, g.vec2);
+                rn.x = fmaf(dscale, F.x, rn.x);
+                rn.y = fmaf(dscale, F.y, rn.y);
+            }
+            st2(rho, gi, rn, two, g.vec2);
+            float2 ar = acc_rho[idx], ad = acc_du[idx];
+            ar.x += rn.x; ar.y += rn.y;
+            ad.x += du.x; ad.y += du.y;
+            acc_rho[idx] = ar;
+            acc_du[idx] = ad;
+        }
+    }
+    __syncthreads();
+    // sparse pressure sources act on every rho component (:930-962)
+    if (a.sparse.off && t <= a.sparse.T[0]) {
+        const int tile_id = blockIdx.x + gridDim.x * blockIdx.y;
+        const int e0 = a.sparse.off[tile_id], e1 = a.sparse.off[tile_id + 1];
+        for (int e = e0 + threadIdx.x; e < e1; e += kThreads) {
+            const int c = a.sparse.cell[e];
+            const int z = c / TX, xl = c - z * TX;
+            const float v = __ldg(a.sparse.sig[0] + a.sparse.row[e] + (long long)a.sparse.nsig * (t - 1));
+            const long long gi = x0 + xl + (long long)g.N0 * (y + (long long)g.N1 * z);
+            float s = 0.f;
+            for (int i = 0; i < a.D; ++i) {
+                const float nv = a.sparse.mode == 0 ? v : a.rho[i][gi] + v;
+                a.rho[i][gi] = nv;
+                s += nv;
+            }
+            float *slot = reinterpret_cast<float *>(acc_rho + z * PL + (xl >> 1)) + (xl & 1);
+            *slot = s;
+        }
+        __syncthreads();
+    }
+    // equation of state
+    const bool absorbing = a.eos == 1;
+    for (int idx = threadIdx.x; idx < tot; idx += kThreads) {
+        const int l = idx % PL, z = idx / PL;
+        const int xa = x0 + 2 * l;
+        float2 pv = make_float2(0.f, 0.f);
+        if (xa < g.N0) {
+            const bool two = xa + 1 < g.N0;
+            const long long gi = xa + (long long)g.N0 * (y + (long long)g.N1 * z);
+            const float2 sr = acc_rho[idx];
+            const float2 c = med2(a.c0, gi, two, g.vec2);
+            const float2 c2 = make_float2(c.x * c.x, c.y * c.y);
+            pv = sr;
+            if (a.eos == 2) {
+                const float2 r0 = med2(a.rho0, gi, two, g.vec2);
+                const float2 an = med2(a.alpha_np, gi, two, g.vec2);
+                const float2 sd = acc_du[idx];
+                pv.x += tau_of(an.x, c.x, 2.f, a.tau_sign) * r0.x * sd.x;
+                pv.y += tau_of(an.y, c.y, 2.f, a.tau_sign) * r0.y * sd.y;
+            }
+            if (a.nonlinear) {
+                const float2 r0 = med2(a.rho0, gi, two, g.vec2);
+                const float2 bn = med2(a.BonA, gi, two, g.vec2);
+                pv.x += bn.x * sr.x * sr.x / (2.f * r0.x);
+                pv.y += bn.y * sr.y * sr.y / (2.f * r0.y);
+            }
+            pv.x *= c2.x;
+            pv.y *= c2.y;
+            st2(a.p, gi, pv, two, g.vec2);
+            if (absorbing && a.has_tau) {
+                const float2 r0 = med2(a.rho0, gi, two, g.vec2);
+                const float2 sd = acc_du[idx];
+                acc_old[idx] = make_float2(r0.x * sd.x, two ? r0.y * sd.y : 0.f);
+            }
+            if (!two) pv.y = 0.f;
+        }
+        tile[idx] = pv;
+    }
+    __syncthreads();
+    if (!absorbing) {
+        apply_tr(tile, a.tr, g, PL, x0, y, t, a.rho[0], a.rho[1], a.rho[2], a.D, a.c0, a.p);
+        __syncthreads();
+        if (a.write_spec) {
+            fft_tile<false>(tile, a.axz, PL, PL, 1, true);
+            zstore_r2c(tile, a.spec.p[0], g, x0, y, PL);
+        }
+        return;
+    }
+    int out = 0;
+    if (a.has_tau) {
+        fft_tile<false>(acc_old, a.axz, PL, PL, 1, true);
+        zstore_r2c(acc_old, a.spec.p[out++], g, x0, y, PL);
+    }
+    if (a.has_eta) {
+        for (int idx = threadIdx.x; idx < tot; idx += kThreads) {
+            const int l = idx % PL;
+            const int xa = x0 + 2 * l;
+            float2 sr = acc_rho[idx];
+            if (xa + 1 >= g.N0) sr.y = 0.f;
+            if (xa >= g.N0) sr.x = 0.f;
+            tile[idx] = sr;
+        }
+        __syncthreads();
+        fft_tile<false>(tile, a.axz, PL, PL, 1, true);
+        zstore_r2c(tile, a.spec.p[out++], g, x0, y, PL);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Stage P: finish the absorbing equation of state (kspaceFirstOrder3D.m:972-979)
+//   p = p_partial + c0^2 (tau A1 - eta A2)
+// with A1 = real(ifftn(nabla1 fftn(rho0 sum du))), A2 = real(ifftn(nabla2 fftn(sum rho))),
+// then the forward z-transform of p.  grid = (ceil(N0/TX), N1, 1)
+// ---------------------------------------------------------------------------
+struct StageP {
+    Geom g;
+    AxisFFT axz;
+    int PL;
+    int D;
+    Spec4 spec;
+    float *p;
+    float *rho[3];
+    Med c0, alpha_np;
+    int has_tau, has_eta;
+    float alpha_y, tau_sign, eta_sign, tan_term;
+    TRSrc tr;
+    int write_spec;
+    const int *d_t;
+};
+
+__global__ void __launch_bounds__(kThreads, 2) k_stage_p(StageP a) {
+    extern __shared__ float2 sm[];
+    const Geom &g = a.g;
+    const int PL = a.PL, TX = 2 * PL;
+    const int tot = PL * g.N2;
+    float2 *tile = sm;
+    float2 *acc = sm + tot;
+    const int x0 = blockIdx.x * TX, y = blockIdx.y;
+    const int t = *a.d_t;
+    for (int idx = threadIdx.x; idx < tot; idx += kThreads) acc[idx] = make_float2(0.f, 0.f);
+    int in = 0;
+    for (int term = 0; term < 2; ++term) {
+        if (term == 0 && !a.has_tau) continue;
+        if (term == 1 && !a.has_eta) continue;
+        __syncthreads();
+        zload_c2r(tile, a.spec.p[in++], g, x0, y, PL);
+        __syncthreads();
+        fft_tile<true>(tile, a.axz, PL, PL, 1, true);
+        for (int idx = threadIdx.x; idx < tot; idx += kThreads) {
+            const int l = idx % PL, z = idx / PL;
+            const int xa = x0 + 2 * l;
+            if (xa >= g.N0) continue;
+            const bool two = xa + 1 < g.N0;
+            const long long gi = xa + (long long)g.N0 * (y + (long long)g.N1 * z);
+            const float2 c = med2(a.c0, gi, two, g.vec2);
+            const float2 an = med2(a.alpha_np, gi, two, g.vec2);
+            const float2 v = tile[idx];
+            float2 ac = acc[idx];
+            if (term == 0) {
+                ac.x += tau_of(an.x, c.x, a.alpha_y, a.tau_sign) * v.x;
+                ac.y += tau_of(an.y, c.y, a.alpha_y, a.tau_sign) * v.y;
+            } else {
+                // eta = 2 alpha c^y tan(pi y / 2)   (createAbsorptionVariables.m:55)
+                ac.x -= 2.f * an.x * powf(c.x, a.alpha_y) * a.tan_term * a.eta_sign * v.x;
+                ac.y -= 2.f * an.y * powf(c.y, a.alpha_y) * a.tan_term * a.eta_sign * v.y;
+            }
+            acc[idx] = ac;
+        }
+    }
+    __syncthreads();
+    for (int idx = threadIdx.x; idx < tot; idx += kThreads) {
+        const int l = idx % PL, z = idx / PL;
+        const int xa = x0 + 2 * l;
+        float2 pv = make_float2(0.f, 0.f);
+        if (xa < g.N0) {
+            const bool two = xa + 1 < g.N0;
+            const long long gi = xa + (long long)g.N0 * (y + (long long)g.N1 * z);
+            const float2 c = med2(a.c0, gi, two, g.vec2);
+            const float2 pp = ld2(a.p, gi, two, g.vec2);
+            const float2 ac = acc[idx];
+            pv.x = fmaf(c.x * c.x, ac.x, pp.x);
+            pv.y = fmaf(c.y * c.y, ac.y, pp.y);
+            st2(a.p, gi, pv, two, g.vec2);
+            if (!two) pv.y = 0.f;
+        }
+        tile[idx] = pv;
+    }
+    __syncthreads();
+    apply_tr(tile, a.tr, g, PL, x0, y, t, a.rho[0], a.rho[1], a.rho[2], a.D, a.c0, a.p);
+    __syncthreads();
+    if (a.write_spec) {
+        fft_tile<false>(tile, a.axz, PL, PL, 1, true);
+        zstore_r2c(tile, a.spec.p[0], g, x0, y, PL);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// plain z-transforms (setup, p0 start, time-reversal start, source filtering)
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(kThreads, 2) k_zr2c(const float *__restrict__ R, float2 *H, Geom g, AxisFFT axz,
+                                                    int PL) {
+    extern __shared__ float2 sm[];
+    const int x0 = blockIdx.x * 2 * PL, y = blockIdx.y;
+    zload_real(sm, R, g, x0, y, PL);
+    __syncthreads();
+    fft_tile<false>(sm, axz, PL, PL, 1, true);
+    zstore_r2c(sm, H, g, x0, y, PL);
+}
+
+__global__ void __launch_bounds__(kThreads, 2) k_zc2r(const float2 *__restrict__ H, float *R, Geom g, AxisFFT axz,
+                                                    int PL) {
+    extern __shared__ float2 sm[];
+    const int x0 = blockIdx.x * 2 * PL, y = blockIdx.y;
+    zload_c2r(sm, H, g, x0, y, PL);
+    __syncthreads();
+    fft_tile<true>(sm, axz, PL, PL, 1, true);
+    const int tot = PL * g.N2;
+    for (int idx = threadIdx.x; idx < tot; idx += kThreads) {
+        const int l = idx % PL, z = idx / PL;
+        const int xa = x0 + 2 * l;
+        if (xa >= g.N0) continue;
+        const bool two = xa + 1 < g.N0;
+        const long long gi = xa + (long long)g.N0 * (y + (long long)g.N1 * z);
+        st2(R, gi, sm[idx], two, g.vec2);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// sensors (kspaceFirstOrder_extractSensorData.m:63-123): gather at the mask
+// and running reductions.  p_rms is accumulated as sum p^2 and finished as
+// sqrt(sum / n), equal to the reference recurrence in exact arithmetic.
+// ---------------------------------------------------------------------------
+struct SensorArgs {
+    int M;
+    const long long *idx;      // 0-based linear indices
+    const float *field[4];     // p, u0, u1, u2
+    float *series[4];          // [M x num_rec] or NULL
+    float *vmax[4], *vmin[4], *vsq[4];
+    int nfield;
+    int record_start;
+    const int *d_t;
+};
+
+__global__ void k_sensor(SensorArgs a) {
+    const int m = blockIdx.x * blockDim.x + threadIdx.x;
+    if (m >= a.M) return;
+    const int t = *a.d_t;
+    const int fi = t - a.record_start;   // 0-based column
+    if (fi < 0) return;
+    const long long gi = a.idx[m];
+    for (int f = 0; f < a.nfield; ++f) {
+        if (!a.field[f]) continue;
+        const float v = a.field[f][gi];
+        if (a.series[f]) a.series[f][m + (long long)a.M * fi] = v;
+        if (a.vmax[f]) a.vmax[f][m] = fi == 0 ? v : fmaxf(a.vmax[f][m], v);
+        if (a.vmin[f]) a.vmin[f][m] = fi == 0 ? v : fminf(a.vmin[f][m], v);
+        if (a.vsq[f]) a.vsq[f][m] = fi == 0 ? v * v : fmaf(v, v, a.vsq[f][m]);
+    }
+}
+
+// running max / min over the inside region (extractSensorData.m:464-569)
+struct RegionArgs {
+    const float *field[4];
+    float *vmax[4], *vmin[4];
+    int nfield;
+    int lo[3], n[3];          // inside region (0-based start, extent) per internal axis
+    Geom g;
+    int record_start;
+    const int *d_t;
+};
+
+__global__ void k_region(RegionArgs a) {
+    const long long tot = (long long)a.n[0] * a.n[1] * a.n[2];
+    const int t = *a.d_t;
+    const int fi = t - a.record_start;
+    if (fi < 0) return;
+    for (long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x; r < tot;
+         r += (long long)gridDim.x * blockDim.x) {
+        const int i0 = r % a.n[0];
+        const long long q = r / a.n[0];
+        const int i1 = q % a.n[1];
+        const int i2 = q / a.n[1];
+        const long long gi = (i0 + a.lo[0]) + (long long)a.g.N0 * ((i1 + a.lo[1]) + (long long)a.g.N1 * (i2 + a.lo[2]));
+        for (int f = 0; f < a.nfield; ++f) {
+            if (!a.field[f]) continue;
+            const float v = a.field[f][gi];
+            if (a.vmax[f]) a.vmax[f][r] = fi == 0 ? v : fmaxf(a.vmax[f][r], v);
+            if (a.vmin[f]) a.vmin[f][r] = fi == 0 ? v : fminf(a.vmin[f][r], v);
+        }
+    }
+}
+
+// copy the inside region of a field into a compact array (p_final, u_final)
+__global__ void k_crop(const float *__restrict__ src, float *dst, Geom g, int lo0, int lo1, int lo2, int n0, int n1,
+                       int n2) {
+    const long long tot = (long long)n0 * n1 * n2;
+    for (long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x; r < tot;
+         r += (long long)gridDim.x * blockDim.x) {
+        const int i0 = r % n0;
+        const long long q = r / n0;
+        const int i1 = q % n1;
+        const int i2 = q / n1;
+        dst[r] = src[(i0 + lo0) + (long long)g.N0 * ((i1 + lo1) + (long long)g.N1 * (i2 + lo2))];
+    }
+}
+
+__global__ void k_rms_finish(float *sq, int M, float inv_n) {
+    const int m = blockIdx.x * blockDim.x + threadIdx.x;
+    if (m < M) sq[m] = sqrtf(sq[m] * inv_n);
+}
+
+// rho_i = p0 / (D c0^2) on every cell (kspaceFirstOrder3D.m:1027-1030)
+__global__ void k_init_rho(const float *__restrict__ p0, Med c0, float *r0, float *r1, float *r2, long long N, int D) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < N; i += (long long)gridDim.x * blockDim.x) {
+        const float c = c0.arr ? c0.arr[i] : c0.val;
+        const float v = p0[i] / ((float)D * c * c);
+        r0[i] = v;
+        r1[i] = v;
+        if (D == 3) r2[i] = v;
+    }
+}
+
+// time-reversal start: p(mask) = data(:, flipped column 1), rho(mask) = p/(D c0^2)
+__global__ void k_tr_start(const long long *idx, int M, const float *data, int Nt, Med c0, float *p, float *r0,
+                           float *r1, float *r2, int D) {
+    const int m = blockIdx.x * blockDim.x + threadIdx.x;
+    if (m >= M) return;
+    const long long gi = idx[m];
+    const float v = data[m + (long long)M * (Nt - 1)];
+    p[gi] = v;
+    const float c = c0.arr ? c0.arr[gi] : c0.val;
+    const float r = v / ((float)D * c * c);
+    r0[gi] = r;
+    r1[gi] = r;
+    if (D == 3) r2[gi] = r;
+}
+
+// final time-reversal assignment p(mask) = data(:, flipped column Nt) (:1211-1213)
+__global__ void k_tr_final(const long long *idx, int M, const float *data, float *p) {
+    const int m = blockIdx.x * blockDim.x + threadIdx.x;
+    if (m < M) p[idx[m]] = data[m];
+}
+
+// source_mat(index) = values(sig_index, t) into a zero field (general additive path)
+__global__ void k_scatter_source(const long long *pos, const int *row, int npts, const float *sig, int nsig,
+                                 float *field, const int *d_t, int T) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= npts) return;
+    const int t = *d_t;
+    if (t > T) return;
+    field[pos[i]] = sig[row[i] + (long long)nsig * (t - 1)];
+}
+
+__global__ void k_set_points(const long long *pos, int npts, float v, float *field) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < npts) field[pos[i]] = v;
+}
+
+__global__ void k_step_advance(int *d_t) { *d_t += 1; }
+
+}  // namespace kw

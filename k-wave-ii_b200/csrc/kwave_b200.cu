@@ -1,0 +1,1200 @@
+// kwave_b200.cu -- host side of the B200 k-space first-order time loop and its C ABI.
+//
+// The entry points declared in include/kwave_b200.h replace the external
+// native solver that k-Wave's kspaceFirstOrder3DC / 3DG / 2DG launch after
+// the MATLAB setup (+kwave/+legacy/kspaceFirstOrder3DC.m:530-546): the same
+// variable set (private/kspaceFirstOrder_saveToDisk.m:46-353) comes in as
+// host pointers, the loop of kspaceFirstOrder3D.m:769-1208 runs on the
+// device, and the sensor outputs come back into caller buffers.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <complex>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "kw_kernels.cuh"
+#include "../../include/kwave_b200.h"
+
+using namespace kw;
+
+namespace {
+
+thread_local std::string g_err;
+
+kw_status fail(kw_status s, const char *fmt, ...) {
+    char buf[1024];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    g_err = buf;
+    return s;
+}
+
+#define KW_CUDA(call)                                                                          \
+    do {                                                                                       \
+        cudaError_t e_ = (call);                                                               \
+        if (e_ != cudaSuccess) {                                                               \
+            return fail(e_ == cudaErrorMemoryAllocation ? KW_ERR_NOMEM : KW_ERR_CUDA,          \
+                        "CUDA error %s at %s:%d (%s)", cudaGetErrorName(e_), __FILE__, __LINE__, \
+                        cudaGetErrorString(e_));                                               \
+        }                                                                                      \
+    } while (0)
+
+#define KW_TRY(call)                   \
+    do {                               \
+        kw_status s_ = (call);         \
+        if (s_ != KW_OK) return s_;    \
+    } while (0)
+
+// --------------------------------------------------------------------------
+// FP64 host precompute
+// --------------------------------------------------------------------------
+bool factorize(int n, std::vector<int> &radix) {
+    radix.clear();
+    while (n % 4 == 0) { radix.push_back(4); n /= 4; }
+    while (n % 2 == 0) { radix.push_back(2); n /= 2; }
+    const int primes[3] = {3, 5, 7};
+    for (int p : primes)
+        while (n % p == 0) { radix.push_back(p); n /= p; }
+    return n == 1 && radix.size() <= (size_t)kMaxStages;
+}
+
+// kWaveGrid.makeDim (kWaveGrid.m:779-797) in FFT order (ifftshift applied)
+std::vector<double> kvec_fft(int n, double d) {
+    std::vector<double> nat(n), out(n);
+    for (int i = 0; i < n; ++i) {
+        const int m = (n % 2 == 0) ? i - n / 2 : i - (n - 1) / 2;
+        nat[i] = (2.0 * M_PI / d) * ((double)m / n);
+    }
+    nat[n / 2] = 0.0;
+    // ifftshift: out[i] = nat[(i + n/2) % n]
+    for (int i = 0; i < n; ++i) out[i] = nat[(i + n / 2) % n];
+    return out;
+}
+
+// getPML.m:52-87
+std::vector<double> get_pml(int n, double d, double dt, double c, int size, double alpha, bool staggered) {
+    std::vector<double> pml(n, 1.0);
+    for (int x = 1; x <= size; ++x) {
+        const double xs = staggered ? x + 0.5 : x;
+        const double left = alpha * (c / d) * std::pow((xs - size - 1) / (0.0 - size), 4);
+        const double right = alpha * (c / d) * std::pow(xs / size, 4);
+        pml[x - 1] = std::exp(-left * dt / 2);
+        pml[n - size + x - 1] = std::exp(-right * dt / 2);
+    }
+    return pml;
+}
+
+// db2neper.m:52
+double db2neper(double a, double y) { return 100.0 * a * std::pow(1e-6 / (2 * M_PI), y) / (20.0 * std::log10(std::exp(1.0))); }
+
+template <typename T>
+kw_status dev_alloc(T **p, size_t count) {
+    *p = nullptr;
+    if (count == 0) return KW_OK;
+    cudaError_t e = cudaMalloc((void **)p, count * sizeof(T));
+    if (e != cudaSuccess) {
+        *p = nullptr;
+        return fail(e == cudaErrorMemoryAllocation ? KW_ERR_NOMEM : KW_ERR_CUDA, "cudaMalloc of %zu bytes failed: %s",
+                    count * sizeof(T), cudaGetErrorString(e));
+    }
+    return KW_OK;
+}
+
+template <typename T>
+kw_status upload(T **p, const T *host, size_t count) {
+    KW_TRY(dev_alloc(p, count));
+    if (count) KW_CUDA(cudaMemcpy(*p, host, count * sizeof(T), cudaMemcpyHostToDevice));
+    return KW_OK;
+}
+
+}  // namespace
+
+// --------------------------------------------------------------------------
+// the plan
+// --------------------------------------------------------------------------
+struct SourceDev {
+    bool present = false;
+    int mode = 0;
+    int T[3] = {0, 0, 0};
+    int nsig = 0;
+    int npts = 0;
+    bool dense_fast = false;      // additive, one signal: rho += s(t) F
+    bool dense_general = false;   // additive, several signals: F_t each step
+    float *sig[3] = {nullptr, nullptr, nullptr};
+    long long *pos = nullptr;     // 0-based linear indices
+    int *row = nullptr;           // 0-based signal row per point
+    float *F = nullptr;           // filtered mask (fast path)
+    float *Ft[3] = {nullptr, nullptr, nullptr};  // filtered source of this step (general path)
+    float *scratch = nullptr;     // zero field holding the scattered source (general path)
+    int *csr_off = nullptr, *csr_cell = nullptr, *csr_row = nullptr;  // sparse modes
+};
+
+struct TimerRec {
+    cudaEvent_t a, b;
+    int cls;
+};
+
+struct kw_plan {
+    kw_problem prob;               // scalars (pointers are not retained)
+    int D = 3;
+    Geom g{};
+    int N[3] = {1, 1, 1};          // internal shape
+    double d[3] = {1, 1, 1};       // internal spacing
+    int comp_axis[3] = {0, 1, 2};
+    int Nt = 0, index_end = 0, record_start = 1, num_rec = 0;
+    bool time_rev = false, p0 = false, absorbing = false, has_tau = false, has_eta = false;
+    cudaStream_t stream = nullptr;
+
+    AxisFFT fft[3]{};
+    float2 *tw[3] = {nullptr, nullptr, nullptr};
+    float2 *dd_pos[3] = {nullptr, nullptr, nullptr}, *dd_neg[3] = {nullptr, nullptr, nullptr};
+    float *k2[3] = {nullptr, nullptr, nullptr};
+    float *pml[3] = {nullptr, nullptr, nullptr}, *pml_sg[3] = {nullptr, nullptr, nullptr};
+    OpParams op{};
+
+    // fields
+    float *p = nullptr, *rho[3] = {nullptr, nullptr, nullptr}, *u[3] = {nullptr, nullptr, nullptr};
+    float2 *spec[4] = {nullptr, nullptr, nullptr, nullptr};
+    float *p0_dev = nullptr;
+    int *d_t = nullptr;
+
+    // medium
+    float *c0_arr = nullptr, *rho0_arr = nullptr, *rsi_arr[3] = {nullptr, nullptr, nullptr};
+    float *bona_arr = nullptr, *anp_arr = nullptr;
+    Med c0{}, rho0{}, rsi[3]{}, bona{}, anp{};
+    float alpha_y = 0, tau_sign = 1, eta_sign = 1, tan_term = 0;
+
+    SourceDev psrc, usrc;
+
+    // tiles
+    int PL_u = 1, PL_r = 1, PL_p = 1, PL_z = 1, TY = 1, NL = 1;
+
+    // sensors / outputs
+    int M = 0;
+    long long *sidx = nullptr;
+    float *tr_data = nullptr;
+    int *tr_off = nullptr, *tr_cell = nullptr, *tr_row = nullptr;
+    uint32_t rec = 0;
+    float *o_series[4] = {nullptr, nullptr, nullptr, nullptr};
+    float *o_max[4] = {nullptr, nullptr, nullptr, nullptr}, *o_min[4] = {nullptr, nullptr, nullptr, nullptr};
+    float *o_sq[4] = {nullptr, nullptr, nullptr, nullptr};
+    float *o_amax[4] = {nullptr, nullptr, nullptr, nullptr}, *o_amin[4] = {nullptr, nullptr, nullptr, nullptr};
+    float *o_tmp = nullptr;        // crop / rms staging
+    int in_lo[3] = {0, 0, 0}, in_n[3] = {1, 1, 1};
+    long long in_count = 1;
+
+    int t = 1;                     // next step to run (1-based)
+    bool started = false;
+
+    // timing
+    uint32_t timing_mask = 0;
+    std::vector<TimerRec> timers;
+    double t_ms[KW_KCLASS_COUNT] = {0};
+    uint64_t t_count[KW_KCLASS_COUNT] = {0};
+
+    std::vector<void *> allocs;
+    size_t bytes = 0;
+};
+
+namespace {
+
+template <typename T>
+kw_status palloc(kw_plan *P, T **p, size_t count) {
+    KW_TRY(dev_alloc(p, count));
+    if (*p) {
+        P->allocs.push_back((void *)*p);
+        P->bytes += count * sizeof(T);
+        cudaError_t e = cudaMemsetAsync(*p, 0, count * sizeof(T), P->stream);
+        if (e != cudaSuccess) return fail(KW_ERR_CUDA, "cudaMemset failed: %s", cudaGetErrorString(e));
+    }
+    return KW_OK;
+}
+
+template <typename T>
+kw_status pupload(kw_plan *P, T **p, const T *host, size_t count) {
+    KW_TRY(palloc(P, p, count));
+    if (count) KW_CUDA(cudaMemcpyAsync(*p, host, count * sizeof(T), cudaMemcpyHostToDevice, P->stream));
+    KW_CUDA(cudaStreamSynchronize(P->stream));
+    return KW_OK;
+}
+
+// ---- timing ---------------------------------------------------------------
+kw_status timer_flush(kw_plan *P) {
+    if (P->timers.empty()) return KW_OK;
+    KW_CUDA(cudaStreamSynchronize(P->stream));
+    for (auto &r : P->timers) {
+        float ms = 0.f;
+        KW_CUDA(cudaEventElapsedTime(&ms, r.a, r.b));
+        P->t_ms[r.cls] += ms;
+        P->t_count[r.cls] += 1;
+        cudaEventDestroy(r.a);
+        cudaEventDestroy(r.b);
+    }
+    P->timers.clear();
+    return KW_OK;
+}
+
+struct Scope {
+    kw_plan *P;
+    int cls;
+    bool on;
+    TimerRec r{};
+    Scope(kw_plan *P_, int cls_) : P(P_), cls(cls_), on((P_->timing_mask >> cls_) & 1u) {
+        if (on) {
+            cudaEventCreate(&r.a);
+            cudaEventCreate(&r.b);
+            r.cls = cls;
+            cudaEventRecord(r.a, P->stream);
+        }
+    }
+    ~Scope() {
+        if (on) {
+            cudaEventRecord(r.b, P->stream);
+            P->timers.push_back(r);
+            if (P->timers.size() > 8192) timer_flush(P);
+        }
+    }
+};
+
+kw_status set_smem(const void *fn, size_t bytes) {
+    if (bytes > 48 * 1024) KW_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+    return KW_OK;
+}
+
+kw_status check_launch() {
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return fail(KW_ERR_CUDA, "kernel launch failed: %s", cudaGetErrorString(e));
+    return KW_OK;
+}
+
+// ---- transform passes -----------------------------------------------------
+kw_status ypass(kw_plan *P, bool inv, Spec4 bufs, int nf) {
+    if (P->g.N1 == 1 || nf == 0) return KW_OK;
+    Scope s(P, KW_KCLASS_YPASS);
+    dim3 grid((P->g.N0 + P->TY - 1) / P->TY, P->g.N2h, nf);
+    size_t sh = (size_t)P->TY * P->g.N1 * sizeof(float2);
+    if (inv) {
+        KW_TRY(set_smem((const void *)k_ypass<true>, sh));
+        k_ypass<true><<<grid, kThreads, sh, P->stream>>>(bufs, P->g, P->fft[1], P->TY);
+    } else {
+        KW_TRY(set_smem((const void *)k_ypass<false>, sh));
+        k_ypass<false><<<grid, kThreads, sh, P->stream>>>(bufs, P->g, P->fft[1], P->TY);
+    }
+    return check_launch();
+}
+
+kw_status xpass(kw_plan *P, Spec4 bufs, OpSet ops, int fanout, int nf) {
+    Scope s(P, KW_KCLASS_XPASS);
+    const int lines = P->g.N1 * P->g.N2h;
+    dim3 grid((lines + P->NL - 1) / P->NL, 1, fanout ? 1 : nf);
+    size_t sh = (size_t)(fanout ? 2 : 1) * P->NL * P->g.N0 * sizeof(float2);
+    KW_TRY(set_smem((const void *)k_xpass, sh));
+    k_xpass<<<grid, kThreads, sh, P->stream>>>(bufs, P->g, P->fft[0], P->NL, P->op, ops, fanout);
+    return check_launch();
+}
+
+kw_status zr2c(kw_plan *P, const float *R, float2 *H) {
+    dim3 grid((P->g.N0 + 2 * P->PL_z - 1) / (2 * P->PL_z), P->g.N1, 1);
+    size_t sh = (size_t)P->PL_z * P->g.N2 * sizeof(float2);
+    KW_TRY(set_smem((const void *)k_zr2c, sh));
+    k_zr2c<<<grid, kThreads, sh, P->stream>>>(R, H, P->g, P->fft[2], P->PL_z);
+    return check_launch();
+}
+
+kw_status zc2r(kw_plan *P, const float2 *H, float *R) {
+    dim3 grid((P->g.N0 + 2 * P->PL_z - 1) / (2 * P->PL_z), P->g.N1, 1);
+    size_t sh = (size_t)P->PL_z * P->g.N2 * sizeof(float2);
+    KW_TRY(set_smem((const void *)k_zc2r, sh));
+    k_zc2r<<<grid, kThreads, sh, P->stream>>>(H, R, P->g, P->fft[2], P->PL_z);
+    return check_launch();
+}
+
+Spec4 specs(kw_plan *P, int a, int b = -1, int c = -1) {
+    Spec4 s{};
+    s.p[0] = P->spec[a];
+    s.p[1] = b >= 0 ? P->spec[b] : nullptr;
+    s.p[2] = c >= 0 ? P->spec[c] : nullptr;
+    s.p[3] = nullptr;
+    return s;
+}
+
+// gradient spectra of p for the next momentum update: spec[0] holds the
+// z-half spectrum of p on entry; spec[0..D-1] hold dd_pos_i kappa p_k after
+// the inverse x and y passes on exit.
+kw_status grad_group(kw_plan *P) {
+    KW_TRY(ypass(P, false, specs(P, 0), 1));
+    OpSet ops{};
+    ops.n = P->D;
+    for (int i = 0; i < P->D; ++i) { ops.kind[i] = OP_GRAD_POS; ops.axis[i] = P->comp_axis[i]; }
+    Spec4 all = specs(P, 0, 1, 2);
+    KW_TRY(xpass(P, all, ops, 1, 1));
+    KW_TRY(ypass(P, true, all, P->D));
+    return KW_OK;
+}
+
+// real(ifftn(source_kappa .* fftn(field))) into out, via spec[3]
+kw_status source_filter(kw_plan *P, const float *field, float *out) {
+    {
+        Scope s(P, KW_KCLASS_SOURCE);
+        KW_TRY(zr2c(P, field, P->spec[3]));
+    }
+    Spec4 b{};
+    b.p[0] = P->spec[3];
+    KW_TRY(ypass(P, false, b, 1));
+    OpSet ops{};
+    ops.n = 1;
+    ops.kind[0] = OP_SRC_KAPPA;
+    KW_TRY(xpass(P, b, ops, 1, 1));
+    KW_TRY(ypass(P, true, b, 1));
+    Scope s(P, KW_KCLASS_SOURCE);
+    KW_TRY(zc2r(P, P->spec[3], out));
+    return KW_OK;
+}
+
+// general additive sources: this step's filtered source field
+kw_status general_source(kw_plan *P, SourceDev &S, int comp, int t) {
+    if (!S.dense_general || t > S.T[comp] || !S.sig[comp]) return KW_OK;
+    {
+        Scope s(P, KW_KCLASS_SOURCE);
+        k_scatter_source<<<(S.npts + 255) / 256, 256, 0, P->stream>>>(S.pos, S.row, S.npts, S.sig[comp], S.nsig,
+                                                                      S.scratch, P->d_t, S.T[comp]);
+        KW_TRY(check_launch());
+    }
+    return source_filter(P, S.scratch, S.Ft[comp]);
+}
+
+DenseSrc dense_of(const SourceDev &S, int comp) {
+    DenseSrc d{};
+    if (S.dense_fast && S.sig[comp]) {
+        d.F = S.F;
+        d.sig = S.sig[comp];
+        d.T = S.T[comp];
+    } else if (S.dense_general && S.sig[comp]) {
+        d.F = S.Ft[comp];
+        d.sig = nullptr;
+        d.T = S.T[comp];
+    }
+    return d;
+}
+
+SparseSrc sparse_of(const SourceDev &S) {
+    SparseSrc s{};
+    if (!S.present || S.dense_fast || S.dense_general) return s;
+    s.off = S.csr_off;
+    s.cell = S.csr_cell;
+    s.row = S.csr_row;
+    for (int i = 0; i < 3; ++i) s.sig[i] = S.sig[i];
+    s.nsig = S.nsig;
+    for (int i = 0; i < 3; ++i) s.T[i] = S.T[i];
+    s.mode = S.mode == KW_SOURCE_DIRICHLET ? 0 : 1;
+    return s;
+}
+
+TRSrc tr_of(kw_plan *P) {
+    TRSrc r{};
+    if (!P->time_rev) return r;
+    r.off = P->tr_off;
+    r.cell = P->tr_cell;
+    r.row = P->tr_row;
+    r.data = P->tr_data;
+    r.M = P->M;
+    r.Nt = P->Nt;
+    return r;
+}
+
+kw_status stage_u(kw_plan *P, int init, int t) {
+    StageU a{};
+    a.g = P->g;
+    a.axz = P->fft[2];
+    a.PL = P->PL_u;
+    for (int i = 0; i < 3; ++i) {
+        a.spec.p[i] = P->spec[i];
+        a.u[i] = P->u[i];
+        a.rho_sg_inv[i] = P->rsi[i];
+        a.pml_sg[i] = P->pml_sg[i];
+        a.comp_axis[i] = P->comp_axis[i];
+        a.dense[i] = dense_of(P->usrc, i);
+    }
+    a.dt = (float)P->prob.dt;
+    a.init = init;
+    a.write_spec = 1;
+    a.sparse = sparse_of(P->usrc);
+    // components without a signal take no sparse input
+    a.d_t = P->d_t;
+    (void)t;
+    Scope s(P, KW_KCLASS_ZSTAGE_U);
+    dim3 grid((P->g.N0 + 2 * a.PL - 1) / (2 * a.PL), P->g.N1, P->D);
+    size_t sh = (size_t)a.PL * P->g.N2 * sizeof(float2);
+    KW_TRY(set_smem((const void *)k_stage_u, sh));
+    k_stage_u<<<grid, kThreads, sh, P->stream>>>(a);
+    return check_launch();
+}
+
+kw_status stage_r(kw_plan *P, int write_spec) {
+    StageR a{};
+    a.g = P->g;
+    a.axz = P->fft[2];
+    a.PL = P->PL_r;
+    a.D = P->D;
+    for (int i = 0; i < 3; ++i) {
+        a.spec.p[i] = P->spec[i];
+        a.rho[i] = P->rho[i];
+        a.pml[i] = P->pml[i];
+        a.comp_axis[i] = P->comp_axis[i];
+    }
+    a.p = P->p;
+    a.rho0 = P->rho0;
+    a.c0 = P->c0;
+    a.BonA = P->bona;
+    a.alpha_np = P->anp;
+    a.dt = (float)P->prob.dt;
+    a.nonlinear = P->prob.nonlinear_flag ? 1 : 0;
+    a.eos = P->prob.absorbing_flag;
+    a.has_tau = P->has_tau;
+    a.has_eta = P->has_eta;
+    a.alpha_y = P->alpha_y;
+    a.tau_sign = P->tau_sign;
+    a.dense = dense_of(P->psrc, 0);
+    a.sparse = sparse_of(P->psrc);
+    a.tr = P->absorbing ? TRSrc{} : tr_of(P);
+    a.write_spec = write_spec;
+    a.d_t = P->d_t;
+    Scope s(P, KW_KCLASS_ZSTAGE_R);
+    dim3 grid((P->g.N0 + 2 * a.PL - 1) / (2 * a.PL), P->g.N1, 1);
+    size_t sh = (size_t)4 * a.PL * P->g.N2 * sizeof(float2);
+    KW_TRY(set_smem((const void *)k_stage_r, sh));
+    k_stage_r<<<grid, kThreads, sh, P->stream>>>(a);
+    return check_launch();
+}
+
+kw_status stage_p(kw_plan *P, int write_spec) {
+    StageP a{};
+    a.g = P->g;
+    a.axz = P->fft[2];
+    a.PL = P->PL_p;
+    a.D = P->D;
+    for (int i = 0; i < 3; ++i) {
+        a.spec.p[i] = P->spec[i];
+        a.rho[i] = P->rho[i];
+    }
+    a.p = P->p;
+    a.c0 = P->c0;
+    a.alpha_np = P->anp;
+    a.has_tau = P->has_tau;
+    a.has_eta = P->has_eta;
+    a.alpha_y = P->alpha_y;
+    a.tau_sign = P->tau_sign;
+    a.eta_sign = P->eta_sign;
+    a.tan_term = P->tan_term;
+    a.tr = tr_of(P);
+    a.write_spec = write_spec;
+    a.d_t = P->d_t;
+    Scope s(P, KW_KCLASS_ZSTAGE_P);
+    dim3 grid((P->g.N0 + 2 * a.PL - 1) / (2 * a.PL), P->g.N1, 1);
+    size_t sh = (size_t)2 * a.PL * P->g.N2 * sizeof(float2);
+    KW_TRY(set_smem((const void *)k_stage_p, sh));
+    k_stage_p<<<grid, kThreads, sh, P->stream>>>(a);
+    return check_launch();
+}
+
+kw_status sensors(kw_plan *P, int t) {
+    if (P->time_rev || t < P->record_start) return KW_OK;
+    if (P->M > 0) {
+        SensorArgs a{};
+        a.M = P->M;
+        a.idx = P->sidx;
+        a.nfield = 1 + P->D;
+        a.field[0] = P->p;
+        for (int i = 0; i < P->D; ++i) a.field[1 + i] = P->u[i];
+        for (int f = 0; f < 4; ++f) {
+            a.series[f] = P->o_series[f];
+            a.vmax[f] = P->o_max[f];
+            a.vmin[f] = P->o_min[f];
+            a.vsq[f] = P->o_sq[f];
+        }
+        bool any = false;
+        for (int f = 0; f < 4; ++f) any = any || a.series[f] || a.vmax[f] || a.vmin[f] || a.vsq[f];
+        if (any) {
+            Scope s(P, KW_KCLASS_SENSOR);
+            a.record_start = P->record_start;
+            a.d_t = P->d_t;
+            k_sensor<<<(P->M + 255) / 256, 256, 0, P->stream>>>(a);
+            KW_TRY(check_launch());
+        }
+    }
+    bool any_all = false;
+    for (int f = 0; f < 4; ++f) any_all = any_all || P->o_amax[f] || P->o_amin[f];
+    if (any_all) {
+        RegionArgs r{};
+        r.nfield = 1 + P->D;
+        r.field[0] = P->p;
+        for (int i = 0; i < P->D; ++i) r.field[1 + i] = P->u[i];
+        for (int f = 0; f < 4; ++f) {
+            r.vmax[f] = P->o_amax[f];
+            r.vmin[f] = P->o_amin[f];
+        }
+        for (int a = 0; a < 3; ++a) {
+            r.lo[a] = P->in_lo[a];
+            r.n[a] = P->in_n[a];
+        }
+        r.g = P->g;
+        r.record_start = P->record_start;
+        r.d_t = P->d_t;
+        Scope s(P, KW_KCLASS_SENSOR);
+        const long long blocks = std::min<long long>((P->in_count + 255) / 256, 148 * 16);
+        k_region<<<(int)blocks, 256, 0, P->stream>>>(r);
+        KW_TRY(check_launch());
+    }
+    return KW_OK;
+}
+
+// ---- start of the loop ------------------------------------------------------
+kw_status zero_state(kw_plan *P) {
+    const size_t N = (size_t)P->g.N, Nh = (size_t)P->g.Nh;
+    KW_CUDA(cudaMemsetAsync(P->p, 0, N * sizeof(float), P->stream));
+    for (int i = 0; i < P->D; ++i) {
+        KW_CUDA(cudaMemsetAsync(P->rho[i], 0, N * sizeof(float), P->stream));
+        KW_CUDA(cudaMemsetAsync(P->u[i], 0, N * sizeof(float), P->stream));
+    }
+    for (int i = 0; i < 4; ++i)
+        if (P->spec[i]) KW_CUDA(cudaMemsetAsync(P->spec[i], 0, Nh * sizeof(float2), P->stream));
+    const int one = 1;
+    KW_CUDA(cudaMemcpyAsync(P->d_t, &one, sizeof(int), cudaMemcpyHostToDevice, P->stream));
+    P->t = 1;
+    P->started = false;
+    return KW_OK;
+}
+
+kw_status start(kw_plan *P) {
+    if (P->time_rev) {
+        // kspaceFirstOrder3D.m:772-788 at t = 1
+        k_tr_start<<<(P->M + 255) / 256, 256, 0, P->stream>>>(P->sidx, P->M, P->tr_data, P->Nt, P->c0, P->p,
+                                                              P->rho[0], P->rho[1], P->rho[2], P->D);
+        KW_TRY(check_launch());
+        KW_TRY(zr2c(P, P->p, P->spec[0]));
+        KW_TRY(grad_group(P));
+    }
+    P->started = true;
+    return KW_OK;
+}
+
+// one time step t (1-based); steps counted on the device by d_t as well
+kw_status run_step(kw_plan *P) {
+    const int t = P->t;
+    const bool need_grad = t < P->index_end;
+    if (t == 1 && P->p0) {
+        // p0 initial condition (kspaceFirstOrder3D.m:1023-1040): the first
+        // step's update is overwritten, so the state is set directly.
+        KW_CUDA(cudaMemcpyAsync(P->p, P->p0_dev, (size_t)P->g.N * sizeof(float), cudaMemcpyDeviceToDevice, P->stream));
+        k_init_rho<<<1024, 256, 0, P->stream>>>(P->p0_dev, P->c0, P->rho[0], P->rho[1], P->rho[2], P->g.N, P->D);
+        KW_TRY(check_launch());
+        KW_TRY(zr2c(P, P->p, P->spec[0]));
+        KW_TRY(grad_group(P));
+        KW_TRY(stage_u(P, 1, t));
+    } else {
+        for (int c = 0; c < P->D; ++c) KW_TRY(general_source(P, P->usrc, c, t));
+        KW_TRY(stage_u(P, 0, t));
+        // divergence: real(ifftn(dd_neg_i kappa fftn(u_i)))
+        Spec4 all = specs(P, 0, 1, 2);
+        KW_TRY(ypass(P, false, all, P->D));
+        OpSet ops{};
+        ops.n = P->D;
+        for (int i = 0; i < P->D; ++i) { ops.kind[i] = OP_GRAD_NEG; ops.axis[i] = P->comp_axis[i]; }
+        KW_TRY(xpass(P, all, ops, 0, P->D));
+        KW_TRY(ypass(P, true, all, P->D));
+        KW_TRY(general_source(P, P->psrc, 0, t));
+        if (!P->absorbing) {
+            KW_TRY(stage_r(P, need_grad ? 1 : 0));
+        } else {
+            KW_TRY(stage_r(P, 0));
+            const int nabs = (P->has_tau ? 1 : 0) + (P->has_eta ? 1 : 0);
+            if (nabs) {
+                Spec4 ab = specs(P, 0, 1);
+                KW_TRY(ypass(P, false, ab, nabs));
+                OpSet o2{};
+                o2.n = nabs;
+                int k = 0;
+                if (P->has_tau) o2.kind[k++] = OP_NABLA1;
+                if (P->has_eta) o2.kind[k++] = OP_NABLA2;
+                KW_TRY(xpass(P, ab, o2, 0, nabs));
+                KW_TRY(ypass(P, true, ab, nabs));
+            }
+            KW_TRY(stage_p(P, need_grad ? 1 : 0));
+        }
+        if (need_grad) KW_TRY(grad_group(P));
+    }
+    KW_TRY(sensors(P, t));
+    k_step_advance<<<1, 1, 0, P->stream>>>(P->d_t);
+    KW_TRY(check_launch());
+    P->t += 1;
+    return KW_OK;
+}
+
+// CSR of points per z-tile of width TX = 2*PL (tile = x/TX + ntx*y)
+kw_status build_csr(kw_plan *P, const std::vector<long long> &pos, const std::vector<int> &row, int PL, int **off,
+                    int **cell, int **rowd) {
+    const int TX = 2 * PL;
+    const int ntx = (P->g.N0 + TX - 1) / TX;
+    const int ntiles = ntx * P->g.N1;
+    std::vector<int> cnt(ntiles + 1, 0);
+    std::vector<int> tile_of(pos.size()), cell_of(pos.size());
+    for (size_t i = 0; i < pos.size(); ++i) {
+        const long long gi = pos[i];
+        const int x = (int)(gi % P->g.N0);
+        const long long q = gi / P->g.N0;
+        const int y = (int)(q % P->g.N1);
+        const int z = (int)(q / P->g.N1);
+        tile_of[i] = x / TX + ntx * y;
+        cell_of[i] = z * TX + (x % TX);
+        cnt[tile_of[i] + 1]++;
+    }
+    for (int i = 0; i < ntiles; ++i) cnt[i + 1] += cnt[i];
+    std::vector<int> fill(cnt.begin(), cnt.end() - 1), cells(pos.size()), rows(pos.size());
+    for (size_t i = 0; i < pos.size(); ++i) {
+        const int k = fill[tile_of[i]]++;
+        cells[k] = cell_of[i];
+        rows[k] = row[i];
+    }
+    KW_TRY(pupload(P, off, cnt.data(), cnt.size()));
+    KW_TRY(pupload(P, cell, cells.data(), cells.size()));
+    KW_TRY(pupload(P, rowd, rows.data(), rows.size()));
+    return KW_OK;
+}
+
+kw_status setup_source(kw_plan *P, SourceDev &S, const kw_source *src, int ncomp, int PL) {
+    // src[0..ncomp-1] share mode, points and signal index (u_mask is shared)
+    int first = -1;
+    for (int c = 0; c < ncomp; ++c)
+        if (src[c].num_time_samples > 0) { first = c; break; }
+    if (first < 0) return KW_OK;
+    const kw_source &s0 = src[first];
+    S.present = true;
+    S.mode = s0.mode;
+    if (S.mode < 0 || S.mode > 2) return fail(KW_ERR_INVALID, "source mode must be 0 (dirichlet), 1 (additive-no-correction) or 2 (additive)");
+    S.npts = (int)s0.num_points;
+    if (S.npts <= 0 || !s0.index) return fail(KW_ERR_INVALID, "source mask must have at least one element set to 1.");
+    std::vector<long long> pos(S.npts);
+    for (int i = 0; i < S.npts; ++i) {
+        const uint64_t v = s0.index[i];
+        if (v < 1 || v > (uint64_t)P->g.N) return fail(KW_ERR_INVALID, "source index %llu outside the grid", (unsigned long long)v);
+        if (i > 0 && v <= s0.index[i - 1]) return fail(KW_ERR_INVALID, "source indices must be increasing (find(mask) order)");
+        pos[i] = (long long)v - 1;
+    }
+    S.nsig = (int)s0.num_signals;
+    std::vector<int> row(S.npts);
+    for (int i = 0; i < S.npts; ++i) {
+        if (s0.signal_index) {
+            const uint64_t r = s0.signal_index[i];
+            if (r < 1 || r > (uint64_t)S.nsig) return fail(KW_ERR_INVALID, "source signal index out of range");
+            row[i] = (int)r - 1;
+        } else if (S.nsig == 1) {
+            row[i] = 0;
+        } else if (S.nsig == S.npts) {
+            row[i] = i;
+        } else {
+            return fail(KW_ERR_INVALID, "The number of time series in the source must match the number of source elements in the mask.");
+        }
+    }
+    bool one_row = true;
+    for (int i = 1; i < S.npts; ++i) one_row = one_row && row[i] == row[0];
+    const bool fast = S.mode == KW_SOURCE_ADDITIVE && one_row;
+    for (int c = 0; c < ncomp; ++c) {
+        if (src[c].num_time_samples == 0) continue;
+        if (src[c].num_signals != s0.num_signals || !src[c].input)
+            return fail(KW_ERR_INVALID, "velocity source components must share the mask and the number of signals");
+        S.T[c] = (int)std::min<uint64_t>(src[c].num_time_samples, (uint64_t)P->Nt);
+        if (fast) {
+            // one signal drives every point: keep that row only
+            std::vector<float> h(S.T[c]);
+            for (int tt = 0; tt < S.T[c]; ++tt) h[tt] = src[c].input[row[0] + (size_t)S.nsig * tt];
+            KW_TRY(pupload(P, &S.sig[c], h.data(), h.size()));
+        } else {
+            const size_t cnt = (size_t)S.nsig * src[c].num_time_samples;
+            KW_TRY(pupload(P, &S.sig[c], src[c].input, cnt));
+        }
+    }
+    KW_TRY(pupload(P, &S.pos, pos.data(), pos.size()));
+    KW_TRY(pupload(P, &S.row, row.data(), row.size()));
+    const size_t N = (size_t)P->g.N;
+    if (S.mode == KW_SOURCE_ADDITIVE) {
+        if (fast) {
+            // rho += s(t) real(ifftn(source_kappa fftn(mask))) -- the source
+            // matrix is s(t) times the mask, so filtering the mask once is the
+            // same linear operation (kspaceFirstOrder3D.m:941-952)
+            S.dense_fast = true;
+            KW_TRY(palloc(P, &S.F, N));
+            float *m = nullptr;
+            KW_TRY(dev_alloc(&m, N));
+            KW_CUDA(cudaMemsetAsync(m, 0, N * sizeof(float), P->stream));
+            k_set_points<<<(S.npts + 255) / 256, 256, 0, P->stream>>>(S.pos, S.npts, 1.0f, m);
+            KW_TRY(check_launch());
+            kw_status st = source_filter(P, m, S.F);
+            cudaStreamSynchronize(P->stream);
+            cudaFree(m);
+            KW_TRY(st);
+        } else {
+            S.dense_general = true;
+            KW_TRY(palloc(P, &S.scratch, N));
+            for (int c = 0; c < ncomp; ++c)
+                if (S.sig[c]) KW_TRY(palloc(P, &S.Ft[c], N));
+        }
+    } else {
+        KW_TRY(build_csr(P, pos, row, PL, &S.csr_off, &S.csr_cell, &S.csr_row));
+    }
+    return KW_OK;
+}
+
+int choose_pl(int cap, int N0, int N1, int N2) {
+    int pl = std::max(1, std::min(16, cap / N2));
+    // keep at least two blocks per SM where the grid allows it
+    while (pl > 1 && (long long)((N0 + 2 * pl - 1) / (2 * pl)) * N1 < 2 * 148) pl /= 2;
+    return pl;
+}
+
+kw_status create(const kw_problem *pr, kw_plan *P) {
+    if (!pr) return fail(KW_ERR_INVALID, "problem is NULL");
+    if (pr->abi_version != KW_ABI_VERSION) return fail(KW_ERR_INVALID, "abi_version %u, library expects %d", pr->abi_version, KW_ABI_VERSION);
+    P->prob = *pr;
+    const kw_problem &q = *pr;
+    if (q.dim != 2 && q.dim != 3) return fail(KW_ERR_INVALID, "dim must be 2 or 3");
+    P->D = q.dim;
+    const uint64_t shp[3] = {q.Nx, q.Ny, q.dim == 3 ? q.Nz : 1};
+    for (int a = 0; a < q.dim; ++a)
+        if (shp[a] < 2 || shp[a] > 4096) return fail(KW_ERR_UNSUPPORTED, "grid size %llu along axis %d outside 2..4096", (unsigned long long)shp[a], a);
+    if (q.dim == 3 && q.Nz < 2) return fail(KW_ERR_INVALID, "Nz must be >= 2 in 3D");
+    if (q.Nt < 1) return fail(KW_ERR_INVALID, "Nt must be a positive integer.");
+    if (!(q.dt > 0)) return fail(KW_ERR_INVALID, "dt must be positive.");
+    if (!(q.dx > 0) || !(q.dy > 0) || (q.dim == 3 && !(q.dz > 0))) return fail(KW_ERR_INVALID, "grid spacing must be positive");
+    const uint64_t pmls[3] = {q.pml_x_size, q.pml_y_size, q.pml_z_size};
+    const double pmla[3] = {q.pml_x_alpha, q.pml_y_alpha, q.pml_z_alpha};
+    for (int a = 0; a < q.dim; ++a)
+        if (pmls[a] * 2 > shp[a]) return fail(KW_ERR_INVALID, "The size of the PML must be smaller than the size of the grid.");
+    if (q.absorbing_flag < 0 || q.absorbing_flag > 2) return fail(KW_ERR_INVALID, "absorbing_flag must be 0, 1 or 2");
+    if (q.absorbing_flag == KW_ABSORBING) {
+        if (!(q.alpha_power >= 0 && q.alpha_power < 3)) return fail(KW_ERR_INVALID, "medium.alpha_power must be a real number between 0 and 3.");
+        if (q.alpha_power == 1 && q.alpha_mode != KW_ALPHA_NO_DISPERSION)
+            return fail(KW_ERR_INVALID, "The power law dispersion term in the equation of state is not valid for medium.alpha_power = 1.");
+    }
+    if (q.record_start_index < 1 || q.record_start_index > q.Nt) return fail(KW_ERR_INVALID, "sensor.record_start_index must be between 1 and the number of time steps.");
+
+    // internal geometry: 2D (Nx, Ny) -> (Nx, 1, Ny)
+    const double sp[3] = {q.dx, q.dy, q.dz};
+    int phys_of_int[3];
+    if (q.dim == 3) {
+        for (int a = 0; a < 3; ++a) { P->N[a] = (int)shp[a]; P->d[a] = sp[a]; phys_of_int[a] = a; }
+        P->comp_axis[0] = 0; P->comp_axis[1] = 1; P->comp_axis[2] = 2;
+    } else {
+        P->N[0] = (int)shp[0]; P->d[0] = sp[0]; phys_of_int[0] = 0;
+        P->N[1] = 1; P->d[1] = 1.0; phys_of_int[1] = -1;
+        P->N[2] = (int)shp[1]; P->d[2] = sp[1]; phys_of_int[2] = 1;
+        P->comp_axis[0] = 0; P->comp_axis[1] = 2; P->comp_axis[2] = 1;
+    }
+    Geom &g = P->g;
+    g.N0 = P->N[0]; g.N1 = P->N[1]; g.N2 = P->N[2];
+    g.N2h = g.N2 / 2 + 1;
+    g.N = (long long)g.N0 * g.N1 * g.N2;
+    g.Nh = (long long)g.N0 * g.N1 * g.N2h;
+    g.vec2 = (g.N0 % 2 == 0) ? 1 : 0;
+    if (g.N > (1LL << 31) - 1) return fail(KW_ERR_UNSUPPORTED, "grid larger than 2^31 cells");
+
+    P->Nt = (int)q.Nt;
+    P->time_rev = q.time_reversal_input != nullptr;
+    P->index_end = P->time_rev ? P->Nt - 1 : P->Nt;
+    P->record_start = (int)q.record_start_index;
+    P->num_rec = P->Nt - P->record_start + 1;
+    P->p0 = q.p0_source_input != nullptr;
+    if (P->p0 && q.p_source.num_time_samples > 0) return fail(KW_ERR_INVALID, "source.p0 and source.p can't be defined in the same simulation.");
+    P->absorbing = q.absorbing_flag == KW_ABSORBING;
+
+    KW_CUDA(cudaStreamCreateWithFlags(&P->stream, cudaStreamNonBlocking));
+
+    // FFT plans and operator tables (FP64 -> FP32)
+    for (int a = 0; a < 3; ++a) {
+        const int n = P->N[a];
+        std::vector<int> rad;
+        if (!factorize(n, rad)) return fail(KW_ERR_UNSUPPORTED, "grid size %d has a prime factor above 7", n);
+        AxisFFT &f = P->fft[a];
+        f.n = n;
+        f.nstages = (int)rad.size();
+        for (size_t s = 0; s < rad.size(); ++s) f.radix[s] = rad[s];
+        std::vector<float2> tw(n);
+        for (int m = 0; m < n; ++m) {
+            const double ang = -2.0 * M_PI * (double)m / n;
+            tw[m] = make_float2((float)std::cos(ang), (float)std::sin(ang));
+        }
+        KW_TRY(pupload(P, &P->tw[a], tw.data(), tw.size()));
+        f.tw = P->tw[a];
+
+        std::vector<float2> dp(n), dn(n);
+        std::vector<float> k2(n);
+        std::vector<float> pml(n, 1.f), pmlsg(n, 1.f);
+        if (phys_of_int[a] >= 0) {
+            const int pa = phys_of_int[a];
+            const std::vector<double> k = kvec_fft(n, P->d[a]);
+            std::vector<std::complex<double>> cp(n), cn(n);
+            for (int i = 0; i < n; ++i) {
+                const std::complex<double> ik(0.0, k[i]);
+                if (q.use_sg) {
+                    cp[i] = ik * std::exp(std::complex<double>(0.0, k[i] * P->d[a] / 2));
+                    cn[i] = ik * std::exp(std::complex<double>(0.0, -k[i] * P->d[a] / 2));
+                } else {
+                    cp[i] = ik;
+                    cn[i] = ik;
+                }
+                k2[i] = (float)(k[i] * k[i]);
+            }
+            // Hermitian part: real(ifftn(op X)) for real input X equals the
+            // inverse transform of (op(k) + conj(op(-k)))/2 times X
+            for (int i = 0; i < n; ++i) {
+                const int j = (n - i) % n;
+                const std::complex<double> hp = 0.5 * (cp[i] + std::conj(cp[j]));
+                const std::complex<double> hn = 0.5 * (cn[i] + std::conj(cn[j]));
+                dp[i] = make_float2((float)hp.real(), (float)hp.imag());
+                dn[i] = make_float2((float)hn.real(), (float)hn.imag());
+            }
+            const std::vector<double> pr1 = get_pml(n, P->d[a], q.dt, q.c_ref, (int)pmls[pa], pmla[pa], false);
+            const std::vector<double> pr2 = get_pml(n, P->d[a], q.dt, q.c_ref, (int)pmls[pa], pmla[pa], q.use_sg != 0);
+            for (int i = 0; i < n; ++i) { pml[i] = (float)pr1[i]; pmlsg[i] = (float)pr2[i]; }
+        } else {
+            for (int i = 0; i < n; ++i) { dp[i] = make_float2(0, 0); dn[i] = make_float2(0, 0); k2[i] = 0.f; }
+        }
+        KW_TRY(pupload(P, &P->dd_pos[a], dp.data(), dp.size()));
+        KW_TRY(pupload(P, &P->dd_neg[a], dn.data(), dn.size()));
+        KW_TRY(pupload(P, &P->k2[a], k2.data(), k2.size()));
+        KW_TRY(pupload(P, &P->pml[a], pml.data(), pml.size()));
+        KW_TRY(pupload(P, &P->pml_sg[a], pmlsg.data(), pmlsg.size()));
+        P->op.dd_pos[a] = P->dd_pos[a];
+        P->op.dd_neg[a] = P->dd_neg[a];
+        P->op.k2[a] = P->k2[a];
+    }
+    P->op.kappa_a = (float)(q.c_ref * q.dt / 2.0);
+    P->op.use_kspace = q.use_kspace ? 1 : 0;
+    P->op.nabla1_exp = (float)(q.alpha_power - 2.0);
+    P->op.nabla2_exp = (float)(q.alpha_power - 1.0);
+    P->op.scale = (float)(1.0 / (double)g.N);
+
+    // tiles
+    P->PL_u = choose_pl(kCap, g.N0, g.N1, g.N2);
+    P->PL_z = P->PL_u;
+    P->PL_r = choose_pl(kCap / 2, g.N0, g.N1, g.N2);
+    P->PL_p = choose_pl(kCap, g.N0, g.N1, g.N2);
+    if (g.N2 > kCap / 2) return fail(KW_ERR_UNSUPPORTED, "axis length %d above %d", g.N2, kCap / 2);
+    {
+        int ty = 1;
+        while (ty * 2 <= 32 && ty * 2 * g.N1 <= kCap) ty *= 2;
+        P->TY = ty;
+        P->NL = std::max(1, kCap / g.N0);
+        const int lines = g.N1 * g.N2h;
+        if (P->NL > lines) P->NL = lines;
+        while (P->NL > 1 && (lines + P->NL - 1) / P->NL < 2 * 148) P->NL /= 2;
+    }
+
+    const size_t N = (size_t)g.N, Nh = (size_t)g.Nh;
+    KW_TRY(palloc(P, &P->d_t, 1));
+    KW_TRY(palloc(P, &P->p, N));
+    for (int i = 0; i < P->D; ++i) {
+        KW_TRY(palloc(P, &P->rho[i], N));
+        KW_TRY(palloc(P, &P->u[i], N));
+    }
+    const int nspec = 4;
+    for (int i = 0; i < nspec; ++i) KW_TRY(palloc(P, &P->spec[i], Nh));
+
+    // medium
+    double cmin = 1e300;
+    if (q.c0) {
+        KW_TRY(pupload(P, &P->c0_arr, q.c0, N));
+        P->c0.arr = P->c0_arr;
+        for (size_t i = 0; i < N; ++i) cmin = std::min(cmin, (double)q.c0[i]);
+    } else {
+        P->c0.val = (float)q.c0_scalar;
+        cmin = q.c0_scalar;
+    }
+    if (!(cmin > 0)) return fail(KW_ERR_INVALID, "medium.sound_speed must be positive");
+    if (q.rho0) {
+        KW_TRY(pupload(P, &P->rho0_arr, q.rho0, N));
+        P->rho0.arr = P->rho0_arr;
+    } else {
+        P->rho0.val = (float)q.rho0_scalar;
+        if (!(q.rho0_scalar > 0)) return fail(KW_ERR_INVALID, "medium.density must be positive");
+    }
+    const float *sg[3] = {q.rho0_sgx, q.rho0_sgy, q.rho0_sgz};
+    for (int c = 0; c < P->D; ++c) {
+        const float *src = sg[c] ? sg[c] : q.rho0;
+        if (src) {
+            std::vector<float> inv(N);
+            for (size_t i = 0; i < N; ++i) inv[i] = (float)(1.0 / (double)src[i]);
+            KW_TRY(pupload(P, &P->rsi_arr[c], inv.data(), N));
+            P->rsi[c].arr = P->rsi_arr[c];
+        } else {
+            P->rsi[c].val = (float)(1.0 / q.rho0_scalar);
+        }
+    }
+    if (q.nonlinear_flag) {
+        if (q.BonA) {
+            KW_TRY(pupload(P, &P->bona_arr, q.BonA, N));
+            P->bona.arr = P->bona_arr;
+        } else {
+            P->bona.val = (float)q.BonA_scalar;
+        }
+    }
+    if (q.absorbing_flag != KW_LOSSLESS) {
+        const double y = q.absorbing_flag == KW_STOKES ? 2.0 : q.alpha_power;
+        P->alpha_y = (float)y;
+        if (q.alpha_coeff) {
+            std::vector<float> a(N);
+            for (size_t i = 0; i < N; ++i) a[i] = (float)db2neper(q.alpha_coeff[i], y);
+            KW_TRY(pupload(P, &P->anp_arr, a.data(), N));
+            P->anp.arr = P->anp_arr;
+        } else {
+            P->anp.val = (float)db2neper(q.alpha_coeff_scalar, y);
+        }
+        const double s0 = q.alpha_sign[0], s1 = q.alpha_sign[1];
+        P->tau_sign = (float)(s0 > 0 ? 1 : (s0 < 0 ? -1 : 0));
+        P->eta_sign = (float)(s1 > 0 ? 1 : (s1 < 0 ? -1 : 0));
+        if (q.absorbing_flag == KW_ABSORBING) {
+            P->has_tau = q.alpha_mode != KW_ALPHA_NO_ABSORPTION;
+            P->has_eta = q.alpha_mode != KW_ALPHA_NO_DISPERSION;
+            P->tan_term = (float)std::tan(M_PI * q.alpha_power / 2.0);
+        }
+    }
+    if (P->p0) KW_TRY(pupload(P, &P->p0_dev, q.p0_source_input, N));
+
+    // sources
+    KW_TRY(setup_source(P, P->psrc, &q.p_source, 1, P->PL_r));
+    KW_TRY(setup_source(P, P->usrc, q.u_source, P->D, P->PL_u));
+
+    // sensors
+    P->rec = q.record;
+    P->M = (int)q.sensor_num;
+    if (P->M > 0) {
+        if (!q.sensor_mask_index) return fail(KW_ERR_INVALID, "sensor_mask_index is NULL");
+        std::vector<long long> idx(P->M);
+        for (int m = 0; m < P->M; ++m) {
+            const uint64_t v = q.sensor_mask_index[m];
+            if (v < 1 || v > (uint64_t)g.N) return fail(KW_ERR_INVALID, "sensor index %llu outside the grid", (unsigned long long)v);
+            if (m > 0 && v <= q.sensor_mask_index[m - 1]) return fail(KW_ERR_INVALID, "sensor indices must be increasing (find(mask) order)");
+            idx[m] = (long long)v - 1;
+        }
+        KW_TRY(pupload(P, &P->sidx, idx.data(), idx.size()));
+        if (P->time_rev) {
+            KW_TRY(pupload(P, &P->tr_data, q.time_reversal_input, (size_t)P->M * P->Nt));
+            std::vector<int> rows(P->M);
+            for (int m = 0; m < P->M; ++m) rows[m] = m;
+            const int PLf = P->absorbing ? P->PL_p : P->PL_r;
+            KW_TRY(build_csr(P, idx, rows, PLf, &P->tr_off, &P->tr_cell, &P->tr_row));
+        }
+    } else if (P->time_rev) {
+        return fail(KW_ERR_INVALID, "time reversal needs a sensor mask");
+    }
+    // inside region per internal axis
+    {
+        int lo[3] = {0, 0, 0}, n[3] = {P->N[0], P->N[1], P->N[2]};
+        for (int a = 0; a < 3; ++a) {
+            const int pa = phys_of_int[a];
+            if (pa < 0) continue;
+            const uint64_t l = q.inside_lo[pa], h = q.inside_hi[pa];
+            if (l == 0 && h == 0) continue;
+            if (l < 1 || h < l || h > (uint64_t)P->N[a]) return fail(KW_ERR_INVALID, "inside region out of range on axis %d", pa);
+            lo[a] = (int)l - 1;
+            n[a] = (int)(h - l + 1);
+        }
+        for (int a = 0; a < 3; ++a) { P->in_lo[a] = lo[a]; P->in_n[a] = n[a]; }
+        P->in_count = (long long)n[0] * n[1] * n[2];
+    }
+    const bool tr = P->time_rev;
+    const size_t ser = (size_t)P->M * P->num_rec;
+    if (!tr && P->M > 0) {
+        if (P->rec & KW_REC_P) KW_TRY(palloc(P, &P->o_series[0], ser));
+        if (P->rec & KW_REC_P_MAX) KW_TRY(palloc(P, &P->o_max[0], P->M));
+        if (P->rec & KW_REC_P_MIN) KW_TRY(palloc(P, &P->o_min[0], P->M));
+        if (P->rec & KW_REC_P_RMS) KW_TRY(palloc(P, &P->o_sq[0], P->M));
+        for (int i = 0; i < P->D; ++i) {
+            if (P->rec & KW_REC_U) KW_TRY(palloc(P, &P->o_series[1 + i], ser));
+            if (P->rec & KW_REC_U_MAX) KW_TRY(palloc(P, &P->o_max[1 + i], P->M));
+            if (P->rec & KW_REC_U_MIN) KW_TRY(palloc(P, &P->o_min[1 + i], P->M));
+            if (P->rec & KW_REC_U_RMS) KW_TRY(palloc(P, &P->o_sq[1 + i], P->M));
+        }
+    }
+    if (P->rec & KW_REC_U_NON_STAGGERED) return fail(KW_ERR_UNSUPPORTED, "sensor.record 'u_non_staggered' is not built yet");
+    if (!tr) {
+        if (P->rec & KW_REC_P_MAX_ALL) KW_TRY(palloc(P, &P->o_amax[0], P->in_count));
+        if (P->rec & KW_REC_P_MIN_ALL) KW_TRY(palloc(P, &P->o_amin[0], P->in_count));
+        for (int i = 0; i < P->D; ++i) {
+            if (P->rec & KW_REC_U_MAX_ALL) KW_TRY(palloc(P, &P->o_amax[1 + i], P->in_count));
+            if (P->rec & KW_REC_U_MIN_ALL) KW_TRY(palloc(P, &P->o_amin[1 + i], P->in_count));
+        }
+    }
+    KW_TRY(palloc(P, &P->o_tmp, std::max<size_t>(std::max<size_t>(P->in_count, P->M), 1)));
+    KW_CUDA(cudaStreamSynchronize(P->stream));
+    KW_TRY(zero_state(P));
+    return KW_OK;
+}
+
+kw_status copy_dev(kw_plan *P, float *dst, const float *src, size_t n) {
+    if (!dst || !src || n == 0) return KW_OK;
+    KW_CUDA(cudaMemcpyAsync(dst, src, n * sizeof(float), cudaMemcpyDeviceToHost, P->stream));
+    return KW_OK;
+}
+
+kw_status crop_out(kw_plan *P, float *dst, const float *field) {
+    if (!dst) return KW_OK;
+    k_crop<<<std::min<long long>((P->in_count + 255) / 256, 148 * 16), 256, 0, P->stream>>>(
+        field, P->o_tmp, P->g, P->in_lo[0], P->in_lo[1], P->in_lo[2], P->in_n[0], P->in_n[1], P->in_n[2]);
+    KW_TRY(check_launch());
+    KW_TRY(copy_dev(P, dst, P->o_tmp, P->in_count));
+    KW_CUDA(cudaStreamSynchronize(P->stream));
+    return KW_OK;
+}
+
+kw_status rms_out(kw_plan *P, float *dst, const float *sq) {
+    if (!dst || !sq) return KW_OK;
+    const int done = std::max(0, std::min(P->t - 1, P->Nt) - P->record_start + 1);
+    KW_CUDA(cudaMemcpyAsync(P->o_tmp, sq, (size_t)P->M * sizeof(float), cudaMemcpyDeviceToDevice, P->stream));
+    k_rms_finish<<<(P->M + 255) / 256, 256, 0, P->stream>>>(P->o_tmp, P->M, done > 0 ? 1.f / done : 0.f);
+    KW_TRY(check_launch());
+    KW_TRY(copy_dev(P, dst, P->o_tmp, P->M));
+    KW_CUDA(cudaStreamSynchronize(P->stream));
+    return KW_OK;
+}
+
+kw_status run_steps(kw_plan *P, uint64_t n) {
+    if (!P->started) KW_TRY(start(P));
+    for (uint64_t k = 0; k < n && P->t <= P->index_end; ++k) KW_TRY(run_step(P));
+    if (P->time_rev && P->t > P->index_end) {
+        k_tr_final<<<(P->M + 255) / 256, 256, 0, P->stream>>>(P->sidx, P->M, P->tr_data, P->p);
+        KW_TRY(check_launch());
+    }
+    return KW_OK;
+}
+
+}  // namespace
+
+// --------------------------------------------------------------------------
+// C ABI
+// --------------------------------------------------------------------------
+extern "C" {
+
+const char *kw_last_error(void) { return g_err.c_str(); }
+
+int kw_abi_version(void) { return KW_ABI_VERSION; }
+
+kw_status kw_plan_create(const kw_problem *problem, kw_plan **plan) {
+    if (!plan) return fail(KW_ERR_INVALID, "plan pointer is NULL");
+    *plan = nullptr;
+    kw_plan *P = new (std::nothrow) kw_plan();
+    if (!P) return fail(KW_ERR_NOMEM, "host allocation failed");
+    kw_status s = create(problem, P);
+    if (s != KW_OK) {
+        std::string keep = g_err;
+        kw_plan_destroy(P);
+        g_err = keep;
+        return s;
+    }
+    *plan = P;
+    g_err.clear();
+    return KW_OK;
+}
+
+kw_status kw_plan_outputs(const kw_plan *P, kw_output_desc *d) {
+    if (!P || !d) return fail(KW_ERR_INVALID, "NULL argument");
+    d->sensor_num = (uint64_t)P->M;
+    d->num_time_points = (uint64_t)P->num_rec;
+    const int D = P->D;
+    if (D == 3) {
+        for (int a = 0; a < 3; ++a) { d->inside_shape[a] = P->in_n[a]; d->grid_shape[a] = P->N[a]; }
+    } else {
+        d->inside_shape[0] = P->in_n[0]; d->inside_shape[1] = P->in_n[2]; d->inside_shape[2] = 1;
+        d->grid_shape[0] = P->N[0]; d->grid_shape[1] = P->N[2]; d->grid_shape[2] = 1;
+    }
+    return KW_OK;
+}
+
+kw_status kw_reset(kw_plan *P) {
+    if (!P) return fail(KW_ERR_INVALID, "plan is NULL");
+    return zero_state(P);
+}
+
+kw_status kw_step(kw_plan *P, uint64_t n) {
+    if (!P) return fail(KW_ERR_INVALID, "plan is NULL");
+    KW_TRY(run_steps(P, n));
+    KW_CUDA(cudaStreamSynchronize(P->stream));
+    return KW_OK;
+}
+
+kw_status kw_run_device(kw_plan *P) {
+    if (!P) return fail(KW_ERR_INVALID, "plan is NULL");
+    if (P->t != 1 || P->started) KW_TRY(zero_state(P));
+    KW_TRY(run_steps(P, (uint64_t)P->index_end));
+    KW_CUDA(cudaStreamSynchronize(P->stream));
+    return KW_OK;
+}
+
+kw_status kw_copy_outputs(kw_plan *P, kw_outputs *o) {
+    if (!P || !o) return fail(KW_ERR_INVALID, "NULL argument");
+    const size_t ser = (size_t)P->M * P->num_rec;
+    KW_TRY(copy_dev(P, o->p, P->o_series[0], ser));
+    KW_TRY(copy_dev(P, o->p_max, P->o_max[0], P->M));
+    KW_TRY(copy_dev(P, o->p_min, P->o_min[0], P->M));
+    KW_TRY(rms_out(P, o->p_rms, P->o_sq[0]));
+    KW_TRY(copy_dev(P, o->p_max_all, P->o_amax[0], P->in_count));
+    KW_TRY(copy_dev(P, o->p_min_all, P->o_amin[0], P->in_count));
+    if ((P->rec & KW_REC_P_FINAL) || P->time_rev) KW_TRY(crop_out(P, o->p_final, P->p));
+    for (int i = 0; i < P->D; ++i) {
+        KW_TRY(copy_dev(P, o->u[i], P->o_series[1 + i], ser));
+        KW_TRY(copy_dev(P, o->u_max[i], P->o_max[1 + i], P->M));
+        KW_TRY(copy_dev(P, o->u_min[i], P->o_min[1 + i], P->M));
+        KW_TRY(rms_out(P, o->u_rms[i], P->o_sq[1 + i]));
+        KW_TRY(copy_dev(P, o->u_max_all[i], P->o_amax[1 + i], P->in_count));
+        KW_TRY(copy_dev(P, o->u_min_all[i], P->o_amin[1 + i], P->in_count));
+        if (P->rec & KW_REC_U_FINAL) KW_TRY(crop_out(P, o->u_final[i], P->u[i]));
+    }
+    KW_CUDA(cudaStreamSynchronize(P->stream));
+    return KW_OK;
+}
+
+kw_status kw_run(kw_plan *P, kw_outputs *o) {
+    KW_TRY(kw_run_device(P));
+    return kw_copy_outputs(P, o);
+}
+
+kw_status kw_plan_destroy(kw_plan *P) {
+    if (!P) return KW_OK;
+    if (P->stream) cudaStreamSynchronize(P->stream);
+    for (auto &r : P->timers) { cudaEventDestroy(r.a); cudaEventDestroy(r.b); }
+    for (void *a : P->allocs) cudaFree(a);
+    if (P->stream) cudaStreamDestroy(P->stream);
+    delete P;
+    return KW_OK;
+}
+
+kw_status kw_set_timing(kw_plan *P, uint32_t mask) {
+    if (!P) return fail(KW_ERR_INVALID, "plan is NULL");
+    KW_TRY(timer_flush(P));
+    P->timing_mask = mask;
+    for (int c = 0; c < KW_KCLASS_COUNT; ++c) { P->t_ms[c] = 0; P->t_count[c] = 0; }
+    return KW_OK;
+}
+
+kw_status kw_get_timing(const kw_plan *Pc, int cls, double *ms, uint64_t *n) {
+    kw_plan *P = const_cast<kw_plan *>(Pc);
+    if (!P || cls < 0 || cls >= KW_KCLASS_COUNT) return fail(KW_ERR_INVALID, "bad argument");
+    KW_TRY(timer_flush(P));
+    if (ms) *ms = P->t_ms[cls];
+    if (n) *n = P->t_count[cls];
+    return KW_OK;
+}
+
+kw_status kw_plan_device_bytes(const kw_plan *P, uint64_t *bytes) {
+    if (!P || !bytes) return fail(KW_ERR_INVALID, "NULL argument");
+    *bytes = P->bytes;
+    return KW_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,718 @@
+"""kspaceFirstOrder2D / kspaceFirstOrder3D on the B200 library.
+
+The Python side plays the role MATLAB plays in the reference's native
+hand-off (+kwave/+legacy/kspaceFirstOrder3DC.m:530-546): it runs the setup of
++kwave/+legacy/private/kspaceFirstOrder_inputChecking.m -- option parsing,
+equation-of-state selection, reference sound speed, sensor and source
+parsing, p0 smoothing, PML expansion, find(mask) indices, source scaling and
+the staggered density interpolation of kspaceFirstOrder3D.m:585-607 -- and
+hands the resulting variable set (private/kspaceFirstOrder_saveToDisk.m) to
+the C ABI.  The time loop itself runs only on the GPU; if the library is
+missing the call raises.
+
+Inputs follow the MATLAB API: ``medium``, ``source`` and ``sensor`` are
+structs given as dicts or attribute objects with the MATLAB field names, and
+the optional inputs use the MATLAB names (``PMLSize=...``, ``Smooth=...``).
+Arrays are indexed ``a[x, y, z]`` like MATLAB ``a(x, y, z)``.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+
+import numpy as np
+
+from . import _abi
+from .helpers import cart2grid, reorderBinarySensorData, smooth
+from .kgrid import kWaveGrid
+
+RECORD_FLAGS = ("p", "p_max", "p_min", "p_rms", "p_max_all", "p_min_all", "p_final",
+                "u", "u_max", "u_min", "u_rms", "u_max_all", "u_min_all", "u_final",
+                "u_non_staggered", "I", "I_avg")
+
+# optional inputs (private/kspaceFirstOrder_checkOptionalInputs.m:35-481)
+_KNOWN_OPTIONS = {
+    "CartInterp", "CreateLog", "DataCast", "DataRecast", "DisplayMask", "LogScale", "MeshPlot",
+    "MovieArgs", "MovieName", "MovieType", "MovieProfile", "PlotFreq", "PlotLayout", "PlotPML",
+    "PlotScale", "PlotSim", "PMLAlpha", "PMLInside", "PMLSize", "RecordMovie", "ScaleSourceTerms",
+    "Smooth", "UsekSpace", "UseSG", "StreamToDisk", "SaveToDisk", "SaveToDiskExit",
+    "HDFCompressionLevel", "MultiAxialPMLRatio", "PMLRange", "RadialSymmetry", "UseFD",
+}
+_DATA_CASTS = {"off", "double", "single", "gsingle", "gdouble", "GPUsingle", "GPUdouble",
+               "gpuArray-single", "gpuArray-double"}
+
+
+class KWaveInputError(ValueError):
+    """Input rejected during setup (the reference raises MATLAB error(...))."""
+
+
+def _field(obj, name, default=None):
+    if obj is None:
+        return default
+    if isinstance(obj, dict):
+        return obj.get(name, default)
+    return getattr(obj, name, default)
+
+
+def _has(obj, name):
+    return _field(obj, name) is not None
+
+
+def _pick(values, dim):
+    """x, y, z values chosen as v(1), v(ceil((end+1)/2)), v(end) from a 1..dim
+    element input (checkOptionalInputs.m:257-330)."""
+    v = list(np.atleast_1d(values))
+    if len(v) > dim:
+        raise KWaveInputError("Optional input must be a 1 or %d element array." % dim)
+    if dim == 2:
+        return [v[0], v[-1]]
+    return [v[0], v[int(math.ceil((len(v) + 1) / 2)) - 1], v[-1]]
+
+
+def _find(mask):
+    """MATLAB find(mask ~= 0): 0-based column-major indices."""
+    return np.flatnonzero(np.asarray(mask).ravel(order="F") != 0)
+
+
+def _f32(a):
+    return np.ascontiguousarray(np.asarray(a, dtype=np.float64).ravel(order="F"), dtype=np.float32)
+
+
+class _Prepared:
+    """Everything the C ABI needs, plus what the post-processing needs."""
+
+
+def _prepare(dim, kgrid, medium, source, sensor, options):
+    for k in options:
+        if k not in _KNOWN_OPTIONS:
+            raise KWaveInputError("Unknown optional input %r." % k)
+    if kgrid.dim != dim:
+        raise KWaveInputError("kgrid must be %dD for kspaceFirstOrder%dD" % (dim, dim))
+    P = _Prepared()
+    P.dim = dim
+
+    # ---- optional inputs (setDefaults.m:151-170, checkOptionalInputs.m) ----
+    for o in ("StreamToDisk", "SaveToDisk", "SaveToDiskExit", "HDFCompressionLevel"):
+        if options.get(o) not in (None, False):
+            raise KWaveInputError("Optional input %r (HDF5 / disk streaming) is not supported by this solver." % o)
+    for o in ("MultiAxialPMLRatio", "PMLRange", "RadialSymmetry", "UseFD"):
+        if o in options:
+            raise KWaveInputError("Optional input %r is not valid for kspaceFirstOrder%dD." % (o, dim))
+    if options.get("RecordMovie"):
+        raise KWaveInputError("'RecordMovie' needs MATLAB figures; this solver runs headless.")
+    dc = options.get("DataCast", "off")
+    if dc not in _DATA_CASTS:
+        raise KWaveInputError("Invalid input for 'DataCast'.")
+    pml_size = options.get("PMLSize", 20 if dim == 2 else 10)
+    if isinstance(pml_size, str):
+        raise KWaveInputError("'PMLSize' set to 'auto' is not supported by this solver.")
+    pml_size = [int(_round(v)) for v in _pick(pml_size, dim)]
+    pml_alpha = [float(v) for v in _pick(options.get("PMLAlpha", 2.0), dim)]
+    pml_inside = bool(options.get("PMLInside", True))
+    sm = options.get("Smooth", [True, False, False])
+    sm = list(np.atleast_1d(sm))
+    if len(sm) > 3 or not all(isinstance(b, (bool, np.bool_)) for b in sm):
+        raise KWaveInputError("Optional input 'Smooth' must be a 1, 2 or 3 element Boolean array.")
+    smooth_p0, smooth_c0, smooth_rho0 = bool(sm[0]), bool(sm[int(math.ceil((len(sm) + 1) / 2)) - 1]), bool(sm[-1])
+    use_kspace = bool(options.get("UsekSpace", True))
+    use_sg = bool(options.get("UseSG", True))
+    scale_source_terms = bool(options.get("ScaleSourceTerms", True))
+    cart_interp = options.get("CartInterp", "linear")
+    if cart_interp not in ("linear", "nearest"):
+        raise KWaveInputError("Optional input 'CartInterp' must be set to 'linear' or 'nearest'.")
+
+    # ---- medium (inputChecking.m:115-281) ----
+    if medium is None or not _has(medium, "sound_speed"):
+        raise KWaveInputError("The field medium.sound_speed must be defined.")
+    c0 = np.asarray(_field(medium, "sound_speed"), dtype=np.float64)
+    if _has(medium, "density"):
+        rho0 = np.asarray(_field(medium, "density"), dtype=np.float64)
+        user_density = True
+    elif c0.size == 1:
+        rho0 = np.asarray(1.0)
+        user_density = False
+    else:
+        raise KWaveInputError("The field medium.density must be defined.")
+    alpha_mode = _field(medium, "alpha_mode")
+    if alpha_mode is not None and alpha_mode not in ("no_absorption", "no_dispersion", "stokes"):
+        raise KWaveInputError("medium.alpha_mode must be set to 'no_absorption', 'no_dispersion', or 'stokes'.")
+    alpha_coeff = None
+    alpha_power = 0.0
+    if _has(medium, "alpha_coeff") or _has(medium, "alpha_power"):
+        if not _has(medium, "alpha_coeff"):
+            raise KWaveInputError("The field medium.alpha_coeff must be defined.")
+        alpha_coeff = np.asarray(_field(medium, "alpha_coeff"), dtype=np.float64)
+        if alpha_mode == "stokes":
+            eos = "stokes"
+            alpha_power = 2.0
+        else:
+            eos = "absorbing"
+            if not _has(medium, "alpha_power"):
+                raise KWaveInputError("The field medium.alpha_power must be defined.")
+            ap = np.asarray(_field(medium, "alpha_power"), dtype=np.float64)
+            if ap.size != 1:
+                raise KWaveInputError("medium.alpha_power must be scalar.")
+            alpha_power = float(ap)
+            if alpha_power >= 3 or alpha_power < 0:
+                raise KWaveInputError("medium.alpha_power must be a real number between 0 and 3.")
+            if alpha_power == 1 and alpha_mode != "no_dispersion":
+                raise KWaveInputError("The power law dispersion term in the equation of state is not valid "
+                                      "for medium.alpha_power = 1.")
+        if np.any(alpha_coeff < 0):
+            raise KWaveInputError("medium.alpha_coeff must be non-negative and real.")
+        if _has(medium, "alpha_filter"):
+            raise KWaveInputError("medium.alpha_filter is not supported by this solver.")
+    else:
+        eos = "lossless"
+    alpha_sign = [1.0, 1.0]
+    if _has(medium, "alpha_sign"):
+        s = np.asarray(_field(medium, "alpha_sign"), dtype=np.float64).ravel()
+        if s.size != 2:
+            raise KWaveInputError("medium.alpha_sign must be given as a 2 element numerical array.")
+        alpha_sign = [float(s[0]), float(s[1])]
+    nonlinear = _has(medium, "BonA")
+    BonA = np.asarray(_field(medium, "BonA"), dtype=np.float64) if nonlinear else None
+    cref = _field(medium, "sound_speed_ref")
+    if cref is None or (isinstance(cref, str) and cref == "max"):
+        c_ref = float(c0.max())
+    elif isinstance(cref, str) and cref == "min":
+        c_ref = float(c0.min())
+    elif isinstance(cref, str) and cref == "mean":
+        c_ref = float(c0.mean())
+    elif isinstance(cref, str):
+        raise KWaveInputError("Unknown input for medium.sound_speed_ref.")
+    else:
+        c_ref = float(cref)
+
+    # ---- sensor (inputChecking.m:288-672) ----
+    use_sensor = sensor is not None
+    time_rev = use_sensor and _has(sensor, "time_reversal_boundary_data")
+    record_given = use_sensor and _has(sensor, "record")
+    record = set()
+    if use_sensor and _has(sensor, "record_mode"):
+        raise KWaveInputError("sensor.record_mode input has been deprecated.")
+    if record_given:
+        rec = _field(sensor, "record")
+        if isinstance(rec, str):
+            raise KWaveInputError("sensor.record must be given as a cell array, e.g., {'p', 'u'}.")
+        for r in rec:
+            if r not in RECORD_FLAGS:
+                raise KWaveInputError("'%s' is not a valid input for sensor.record." % r)
+        record = set(rec)
+    elif use_sensor:
+        record = {"p"}
+    if time_rev:
+        record = set()
+    for r in ("I", "I_avg", "u_non_staggered"):
+        if r in record:
+            raise KWaveInputError("sensor.record '%s' is not supported by this solver yet." % r)
+    needs_mask = bool(record & {"p", "p_max", "p_min", "p_rms", "u", "u_max", "u_min", "u_rms"})
+    blank = use_sensor and not needs_mask and not time_rev
+    rsi = _field(sensor, "record_start_index", 1) if use_sensor else 1
+    record_start = int(_round(rsi))
+    P.cuboid_list = None
+    P.reorder_index = None
+    mask = None
+    if use_sensor and not blank:
+        if not _has(sensor, "mask"):
+            raise KWaveInputError("The field sensor.mask must be defined.")
+        m = np.asarray(_field(sensor, "mask"), dtype=np.float64)
+        if m.shape == kgrid.shape:
+            if np.any((m != 0) & (m != 1)):
+                raise KWaveInputError("sensor.mask must be a binary grid (numeric values must be 0 or 1).")
+            if not np.any(m):
+                raise KWaveInputError("sensor.mask must be a binary grid with at least one element set to 1.")
+            mask = m
+        elif m.ndim == 2 and m.shape[0] == 2 * dim:
+            if np.any(np.mod(m, 1) != 0):
+                raise KWaveInputError("sensor.mask cuboid corner indices must be integers.")
+            if np.any(m[dim:] - m[:dim] < 0):
+                raise KWaveInputError("sensor.mask cuboid corners must be defined as [x1, y1, ... x2, y2, ...] where x2 => x1.")
+            if np.any(m < 1) or any(np.any(m[[a, a + dim]] > kgrid.shape[a]) for a in range(dim)):
+                raise KWaveInputError("sensor.mask cuboid corners must be within the grid.")
+            P.cuboid_list = m.astype(np.int64)
+            mask = np.zeros(kgrid.shape)
+            for c in range(m.shape[1]):
+                sl = tuple(slice(int(m[a, c]) - 1, int(m[a + dim, c])) for a in range(dim))
+                mask[sl] = 1
+        elif m.ndim == 2 and m.shape[0] == dim:
+            if cart_interp == "linear":
+                raise KWaveInputError("Cartesian sensor masks with 'CartInterp' = 'linear' (Delaunay barycentric "
+                                      "interpolation) are not supported yet; use 'CartInterp', 'nearest'.")
+            mask, order_index, reorder_index = cart2grid(kgrid, m)
+            P.reorder_index = None if time_rev else reorder_index
+            P.order_index = order_index
+        else:
+            raise KWaveInputError("Cartesian sensor.mask for a %dD simulation must be given as a %d by N array." % (dim, dim))
+
+    # ---- source (inputChecking.m:713-1220) ----
+    p0 = _field(source, "p0")
+    source_p0 = p0 is not None and np.size(p0) > 0 and np.any(np.asarray(p0) != 0)
+    if source_p0:
+        p0 = np.asarray(p0, dtype=np.float64)
+        if p0.shape != kgrid.shape:
+            raise KWaveInputError("source.p0 must be the same size as the computational grid.")
+    psrc = None
+    if _has(source, "p"):
+        if not _has(source, "p_mask"):
+            raise KWaveInputError("The field source.p_mask must be defined.")
+        pm = np.asarray(_field(source, "p_mask"))
+        if pm.shape != kgrid.shape:
+            raise KWaveInputError("source.p_mask must be the same size as the computational grid.")
+        if not np.any(pm):
+            raise KWaveInputError("source.p_mask must be a binary grid with at least one element set to 1.")
+        if source_p0:
+            raise KWaveInputError("source.p0 and source.p can't be defined in the same simulation.")
+        mode = _field(source, "p_mode", "additive")
+        if mode not in _abi.SOURCE_MODES:
+            raise KWaveInputError("source.p_mode must be set to 'additive', 'additive-no-correction', or 'dirichlet'.")
+        sig = np.atleast_2d(np.asarray(_field(source, "p"), dtype=np.float64))
+        if _has(source, "p_frequency_ref"):
+            raise KWaveInputError("source.p_frequency_ref is not supported by this solver.")
+        psrc = dict(mask=pm, mode=mode, sig=sig)
+    usrc = None
+    ucomp = ["ux", "uy", "uz"][:dim]
+    if any(_has(source, n) for n in ucomp) or _has(source, "u_mask"):
+        if not _has(source, "u_mask"):
+            raise KWaveInputError("The field source.u_mask must be defined.")
+        um = np.asarray(_field(source, "u_mask"))
+        if um.shape != kgrid.shape:
+            raise KWaveInputError("source.u_mask must be the same size as the computational grid.")
+        if not np.any(um):
+            raise KWaveInputError("source.u_mask must be a binary grid with at least one element set to 1.")
+        mode = _field(source, "u_mode", "additive")
+        if mode not in _abi.SOURCE_MODES:
+            raise KWaveInputError("source.u_mode must be set to 'additive', 'additive-no-correction', or 'dirichlet'.")
+        if _has(source, "u_frequency_ref"):
+            raise KWaveInputError("source.u_frequency_ref is not supported by this solver.")
+        sigs = [np.atleast_2d(np.asarray(_field(source, n), dtype=np.float64)) if _has(source, n) else None
+                for n in ucomp]
+        usrc = dict(mask=um, mode=mode, sigs=sigs)
+    if not user_density and (usrc is not None or record & {"u", "u_max", "u_rms"}):
+        raise KWaveInputError("medium.density must be explicitly defined if velocity inputs or outputs are used, "
+                              "even in homogeneous media.")
+    if not user_density and nonlinear:
+        raise KWaveInputError("medium.density must be explicitly defined if medium.BonA is specified.")
+
+    # ---- time (inputChecking.m:1227-1268) ----
+    if kgrid.Nt is None:
+        if time_rev:
+            raise KWaveInputError("kgrid.t_array (Nt and dt) must be defined explicitly in time reversal mode.")
+        if psrc is not None or usrc is not None:
+            raise KWaveInputError("kgrid.t_array (Nt and dt) must be defined explicitly when using a time-varying source.")
+        kgrid.makeTime(c0, 0.3)
+    Nt, dt = int(kgrid.Nt), float(kgrid.dt)
+    if use_sensor and (record_start > Nt or record_start < 1):
+        raise KWaveInputError("sensor.record_start_index must be between 1 and the number of time steps.")
+    if pml_inside and any(2 * pml_size[a] > kgrid.shape[a] for a in range(dim)):
+        raise KWaveInputError("The size of the PML must be smaller than the size of the grid.")
+
+    # ---- smoothing (inputChecking.m:1501-1604) ----
+    if source_p0 and smooth_p0:
+        p0 = smooth(p0, True)
+    if smooth_c0 and c0.ndim == dim and c0.size > 1:
+        c0 = smooth(c0)
+    if smooth_rho0 and rho0.ndim == dim and rho0.size > 1:
+        rho0 = smooth(rho0)
+
+    # ---- grid expansion when the PML is outside (expandGridMatrices.m) ----
+    shape = kgrid.shape
+    spacing = kgrid.spacing
+    if not pml_inside:
+        def grow(a, edge):
+            pad = [(s, s) for s in pml_size]
+            return np.pad(a, pad, mode="edge") if edge else np.pad(a, pad)
+        shape = tuple(shape[a] + 2 * pml_size[a] for a in range(dim))
+        if c0.size > 1:
+            c0 = grow(c0, True)
+        if rho0.size > 1:
+            rho0 = grow(rho0, True)
+        if alpha_coeff is not None and alpha_coeff.size > 1:
+            alpha_coeff = grow(alpha_coeff, True)
+        if nonlinear and BonA.size > 1:
+            BonA = grow(BonA, True)
+        if source_p0:
+            p0 = grow(p0, False)
+        if psrc is not None:
+            psrc["mask"] = grow(psrc["mask"], False)
+        if usrc is not None:
+            usrc["mask"] = grow(usrc["mask"], False)
+        if mask is not None:
+            mask = grow(mask, False)
+        inside = [(pml_size[a] + 1, shape[a] - pml_size[a]) for a in range(dim)]
+    else:
+        inside = [(1, shape[a]) for a in range(dim)]
+    P.shape = shape
+    N = int(np.prod(shape))
+
+    # ---- indices ----
+    if P.cuboid_list is not None:
+        # sensor_mask_index is the concatenation of each cuboid's find()
+        # (inputChecking.m:1612-1633); the library needs increasing indices,
+        # so the rows are gathered from the union mask afterwards
+        idx_parts = []
+        for c in range(P.cuboid_list.shape[1]):
+            tm = np.zeros(shape)
+            off = [pml_size[a] if not pml_inside else 0 for a in range(dim)]
+            sl = tuple(slice(int(P.cuboid_list[a, c]) - 1 + off[a], int(P.cuboid_list[a + dim, c]) + off[a])
+                       for a in range(dim))
+            tm[sl] = 1
+            idx_parts.append(_find(tm))
+        P.cuboid_rows = idx_parts
+    sensor_idx = _find(mask) if mask is not None else np.zeros(0, dtype=np.int64)
+
+    # ---- source scaling (scaleSourceTerms.m) ----
+    c0_flat = c0.ravel(order="F") if c0.size > 1 else None
+    src_struct = []
+    if psrc is not None:
+        pos = _find(psrc["mask"])
+        labels = np.asarray(psrc["mask"]).ravel(order="F")[pos]
+        sig = psrc["sig"].copy()
+        rows = _signal_rows(psrc["mask"], labels, sig.shape[0], pos.size, "source.p", "source.p_mask")
+        if scale_source_terms:
+            if psrc["mode"] == "dirichlet":
+                for r in range(sig.shape[0]):
+                    cc = c0 if c0_flat is None else c0_flat[pos[r]]
+                    sig[r] = sig[r] / (dim * cc ** 2)
+            else:
+                for r in range(sig.shape[0]):
+                    cc = c0 if c0_flat is None else c0_flat[pos[r]]
+                    sig[r] = sig[r] * (2.0 * dt / (dim * cc * kgrid.dx))
+        src_struct.append(("p", psrc["mode"], pos, rows, [sig]))
+    if usrc is not None:
+        pos = _find(usrc["mask"])
+        labels = np.asarray(usrc["mask"]).ravel(order="F")[pos]
+        sigs = [s.copy() if s is not None else None for s in usrc["sigs"]]
+        nrows = max(s.shape[0] for s in sigs if s is not None) if any(s is not None for s in sigs) else 1
+        rows = _signal_rows(usrc["mask"], labels, nrows, pos.size, "source.ux (etc)", "source.u_mask")
+        if scale_source_terms and usrc["mode"] != "dirichlet":
+            for i, s in enumerate(sigs):
+                if s is None:
+                    continue
+                d = spacing[i]
+                for r in range(s.shape[0]):
+                    cc = c0 if c0_flat is None else c0_flat[pos[r]]
+                    s[r] = s[r] * (2.0 * cc * dt / d)
+        src_struct.append(("u", usrc["mode"], pos, rows, sigs))
+
+    # ---- staggered density (kspaceFirstOrder3D.m:585-607) ----
+    rho_sg = [None] * dim
+    if rho0.ndim == dim and rho0.size > 1 and use_sg:
+        for a in range(dim):
+            r = rho0.copy()
+            lo = [slice(None)] * dim
+            hi = [slice(None)] * dim
+            lo[a] = slice(0, shape[a] - 1)
+            hi[a] = slice(1, shape[a])
+            r[tuple(lo)] = 0.5 * (rho0[tuple(lo)] + rho0[tuple(hi)])
+            rho_sg[a] = r
+
+    # ---- the C problem ----
+    keep = []   # arrays referenced by raw pointers must outlive the call
+
+    def arr(a):
+        if a is None:
+            return _abi.f32p()
+        x = _f32(a)
+        keep.append(x)
+        return _abi.fptr(x)
+
+    def idx_arr(i):
+        x = np.ascontiguousarray(np.asarray(i, dtype=np.uint64) + 1)
+        keep.append(x)
+        return _abi.uptr(x)
+
+    pr = _abi.kw_problem()
+    pr.abi_version = _abi.KW_ABI_VERSION
+    pr.dim = dim
+    pr.Nx = shape[0]
+    pr.Ny = shape[1]
+    pr.Nz = shape[2] if dim == 3 else 1
+    pr.Nt = Nt
+    pr.dx = spacing[0]
+    pr.dy = spacing[1]
+    pr.dz = spacing[2] if dim == 3 else 0.0
+    pr.dt = dt
+    pr.c_ref = c_ref
+    if c0.size > 1:
+        pr.c0 = arr(c0)
+    else:
+        pr.c0_scalar = float(c0)
+    if rho0.size > 1:
+        pr.rho0 = arr(rho0)
+    else:
+        pr.rho0_scalar = float(rho0)
+    if rho_sg[0] is not None:
+        pr.rho0_sgx = arr(rho_sg[0])
+        pr.rho0_sgy = arr(rho_sg[1])
+        if dim == 3:
+            pr.rho0_sgz = arr(rho_sg[2])
+    pr.pml_x_size, pr.pml_y_size = pml_size[0], pml_size[1]
+    pr.pml_z_size = pml_size[2] if dim == 3 else 0
+    pr.pml_x_alpha, pr.pml_y_alpha = pml_alpha[0], pml_alpha[1]
+    pr.pml_z_alpha = pml_alpha[2] if dim == 3 else 0.0
+    pr.use_kspace = int(use_kspace)
+    pr.use_sg = int(use_sg)
+    pr.nonlinear_flag = int(nonlinear)
+    if nonlinear:
+        if BonA.size > 1:
+            pr.BonA = arr(BonA)
+        else:
+            pr.BonA_scalar = float(BonA)
+    pr.absorbing_flag = {"lossless": 0, "absorbing": 1, "stokes": 2}[eos]
+    if alpha_coeff is not None:
+        if alpha_coeff.size > 1:
+            pr.alpha_coeff = arr(alpha_coeff)
+        else:
+            pr.alpha_coeff_scalar = float(alpha_coeff)
+    pr.alpha_power = alpha_power
+    pr.alpha_mode = _abi.ALPHA_MODES.get(alpha_mode if alpha_mode != "stokes" else None, 0)
+    pr.alpha_sign[0], pr.alpha_sign[1] = alpha_sign
+    for kind, mode, pos, rows, sigs in src_struct:
+        targets = [pr.p_source] if kind == "p" else [pr.u_source[i] for i in range(dim)]
+        pos_p = idx_arr(pos)
+        row_p = idx_arr(rows)
+        for tgt, s in zip(targets, sigs):
+            if s is None:
+                continue
+            x = np.ascontiguousarray(s.ravel(order="F"), dtype=np.float32)
+            keep.append(x)
+            tgt.num_time_samples = s.shape[1]
+            tgt.mode = _abi.SOURCE_MODES[mode]
+            tgt.num_points = pos.size
+            tgt.index = pos_p
+            tgt.num_signals = s.shape[0]
+            tgt.signal_index = row_p
+            tgt.input = _abi.fptr(x)
+    if source_p0:
+        pr.p0_source_input = arr(p0)
+    pr.sensor_num = sensor_idx.size
+    if sensor_idx.size:
+        pr.sensor_mask_index = idx_arr(sensor_idx)
+    pr.record_start_index = record_start
+    bits = 0
+    for r in record:
+        bits |= 1 << _abi.REC_BITS[r]
+    pr.record = bits
+    if time_rev:
+        trd = np.atleast_2d(np.asarray(_field(sensor, "time_reversal_boundary_data"), dtype=np.float64))
+        if P.reorder_index is None and getattr(P, "order_index", None) is not None:
+            # Cartesian rows put into find(mask) order (inputChecking.m:640-648)
+            trd = trd[np.argsort(P.order_index, kind="stable")]
+        if trd.shape != (sensor_idx.size, Nt):
+            raise KWaveInputError("sensor.time_reversal_boundary_data must be [num_sensor_points x Nt].")
+        pr.time_reversal_input = arr(trd)
+    for a in range(dim):
+        pr.inside_lo[a] = inside[a][0]
+        pr.inside_hi[a] = inside[a][1]
+
+    P.problem = pr
+    P.keep = keep
+    P.record = record
+    P.record_given = record_given
+    P.time_rev = time_rev
+    P.use_sensor = use_sensor
+    P.M = sensor_idx.size
+    P.Nt = Nt
+    P.record_start = record_start
+    P.inside = inside
+    return P
+
+
+def _round(v):
+    v = float(v)
+    return math.copysign(math.floor(abs(v) + 0.5), v)
+
+
+def _signal_rows(mask, labels, nrows, npts, sname, mname):
+    """0-based signal row of each source point (inputChecking.m:853-887)."""
+    uniq = np.unique(mask)
+    if uniq.size <= 2 and uniq.sum() == 1:
+        if nrows > 1 and nrows != npts:
+            raise KWaveInputError("The number of time series in %s must match the number of source elements in %s."
+                                  % (sname, mname))
+        return np.arange(npts) if nrows > 1 else np.zeros(npts, dtype=np.int64)
+    u = uniq[uniq != 0]
+    if np.any(np.diff(u) != 1) or u[0] != 1:
+        raise KWaveInputError("If using a labelled %s, the source labels must be monotonically increasing and "
+                              "start from 1." % mname)
+    if nrows != u.size:
+        raise KWaveInputError("The number of time series in %s must match the number of labelled source elements "
+                              "in %s." % (sname, mname))
+    return labels.astype(np.int64) - 1
+
+
+class Simulation:
+    """A prepared kspaceFirstOrder run bound to a device plan.
+
+    ``Simulation(dim, kgrid, medium, source, sensor, **options)`` runs the
+    setup and uploads everything; ``run()`` executes the time loop on the GPU
+    and returns what kspaceFirstOrder2D/3D returns.  ``run()`` may be called
+    again (the loop restarts from the initial state).
+    """
+
+    def __init__(self, dim, kgrid, medium, source, sensor, **options):
+        self._lib = _abi.load_library()
+        self.prep = _prepare(dim, kgrid, medium, source, sensor, options)
+        h = C.c_void_p()
+        _abi.check(self._lib.kw_plan_create(C.byref(self.prep.problem), C.byref(h)))
+        self.handle = h
+        self.prep.keep = None    # the library copied everything it needs
+        d = _abi.kw_output_desc()
+        _abi.check(self._lib.kw_plan_outputs(self.handle, C.byref(d)))
+        self.desc = d
+
+    def close(self):
+        if getattr(self, "handle", None):
+            self._lib.kw_plan_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    # -- split API used by benchmarks ---------------------------------------
+    def run_device(self):
+        _abi.check(self._lib.kw_run_device(self.handle))
+
+    def step(self, n):
+        _abi.check(self._lib.kw_step(self.handle, n))
+
+    def reset(self):
+        _abi.check(self._lib.kw_reset(self.handle))
+
+    def set_timing(self, classes):
+        mask = 0
+        for c in classes:
+            mask |= 1 << _abi.KCLASS[c]
+        _abi.check(self._lib.kw_set_timing(self.handle, mask))
+
+    def timing(self, cls):
+        ms = C.c_double()
+        n = C.c_uint64()
+        _abi.check(self._lib.kw_get_timing(self.handle, _abi.KCLASS[cls], C.byref(ms), C.byref(n)))
+        return ms.value, n.value
+
+    def device_bytes(self):
+        b = C.c_uint64()
+        _abi.check(self._lib.kw_plan_device_bytes(self.handle, C.byref(b)))
+        return b.value
+
+    # -- outputs ---------------------------------------------------------------
+    def _alloc_outputs(self):
+        P = self.prep
+        M, T = P.M, P.Nt - P.record_start + 1
+        ins = tuple(int(self.desc.inside_shape[a]) for a in range(P.dim))
+        host = {}
+        o = _abi.kw_outputs()
+        rec = P.record
+
+        def buf(key, shape, slot, idx=None):
+            a = np.zeros(int(np.prod(shape)), dtype=np.float32)
+            host[key] = (a, shape)
+            if idx is None:
+                setattr(o, slot, _abi.fptr(a))
+            else:
+                getattr(o, slot)[idx] = _abi.fptr(a)
+
+        if not P.time_rev:
+            if "p" in rec:
+                buf("p", (M, T), "p")
+            for k in ("p_max", "p_min", "p_rms"):
+                if k in rec:
+                    buf(k, (M,), k)
+            for k in ("p_max_all", "p_min_all"):
+                if k in rec:
+                    buf(k, ins, k)
+            comps = ["ux", "uy", "uz"][:P.dim]
+            for i, n in enumerate(comps):
+                if "u" in rec:
+                    buf(n, (M, T), "u", i)
+                for k in ("max", "min", "rms"):
+                    if "u_" + k in rec:
+                        buf(n + "_" + k, (M,), "u_" + k, i)
+                for k in ("max_all", "min_all"):
+                    if "u_" + k in rec:
+                        buf(n + "_" + k, ins, "u_" + k, i)
+                if "u_final" in rec:
+                    buf(n + "_final", ins, "u_final", i)
+        if "p_final" in rec or P.time_rev:
+            buf("p_final", ins, "p_final")
+        return o, host
+
+    def copy_outputs(self):
+        o, host = self._alloc_outputs()
+        _abi.check(self._lib.kw_copy_outputs(self.handle, C.byref(o)))
+        return self._finish(host)
+
+    def run(self):
+        o, host = self._alloc_outputs()
+        _abi.check(self._lib.kw_run(self.handle, C.byref(o)))
+        return self._finish(host)
+
+    def _finish(self, host):
+        P = self.prep
+        out = {}
+        for k, (a, shape) in host.items():
+            out[k] = a.reshape(shape, order="F")
+        # Cartesian nearest-neighbour reorder (reorderCartData.m)
+        if P.reorder_index is not None:
+            for k in list(out):
+                if k.endswith("_all") or k.endswith("_final"):
+                    continue
+                out[k] = reorderBinarySensorData(out[k], P.reorder_index)
+        if P.cuboid_list is not None:
+            out = self._cuboids(out)
+        if not P.use_sensor:
+            return None
+        if P.time_rev:
+            return out["p_final"]
+        if not P.record_given and P.cuboid_list is None:
+            return out["p"]
+        return out
+
+    def _cuboids(self, out):
+        """Per-cuboid outputs shaped [X, Y, (Z,) T] (reorderCuboidCorners.m)."""
+        P = self.prep
+        all_idx = _find_union(P.cuboid_rows)
+        pos = {v: i for i, v in enumerate(all_idx)}
+        res = []
+        for c, rows in enumerate(P.cuboid_rows):
+            sel = np.array([pos[v] for v in rows], dtype=np.int64)
+            lo = P.cuboid_list[:P.dim, c]
+            hi = P.cuboid_list[P.dim:, c]
+            size = tuple(int(h - l + 1) for l, h in zip(lo, hi))
+            d = {}
+            for k, v in out.items():
+                if k.endswith("_all") or k.endswith("_final"):
+                    d[k] = v
+                elif v.ndim == 2:
+                    d[k] = v[sel].reshape(size + (v.shape[1],), order="F")
+                else:
+                    d[k] = v[sel].reshape(size, order="F")
+            res.append(d)
+        return res
+
+
+def _find_union(parts):
+    return np.unique(np.concatenate(parts))
+
+
+def kspaceFirstOrder2D(kgrid, medium, source, sensor, **options):
+    """2-D drop-in for kspaceFirstOrder2D (+kwave/+legacy/kspaceFirstOrder2D.m)."""
+    with Simulation(2, kgrid, medium, source, sensor, **options) as sim:
+        return sim.run()
+
+
+def kspaceFirstOrder3D(kgrid, medium, source, sensor, **options):
+    """3-D drop-in for kspaceFirstOrder3D (+kwave/+legacy/kspaceFirstOrder3D.m)."""
+    with Simulation(3, kgrid, medium, source, sensor, **options) as sim:
+        return sim.run()

@@ -1,0 +1,849 @@
+"""CPU oracle for the k-space first-order acoustic time loop -- TEST INFRASTRUCTURE ONLY.
+
+This module is the checker, never the product: only ``tests/``,
+``__graft_entry__.smoke()`` and the ``cpu_baseline`` / ``--impl reference`` legs
+of ``bench.py`` may import it.  The shipped library must never route through it.
+
+It is an FP64 NumPy/SciPy restatement of k-Wave's legacy ``kspaceFirstOrder2D``
+and ``kspaceFirstOrder3D`` (MATLAB), written from the reference's semantics:
+
+* time loop, update order and p0 initial condition:
+  ``+kwave/+legacy/kspaceFirstOrder3D.m:769-1208`` and
+  ``+kwave/+legacy/kspaceFirstOrder2D.m:712-1044``;
+* staggered density, PML and k-space operators:
+  ``kspaceFirstOrder3D.m:585-661`` / ``kspaceFirstOrder2D.m:547-611``;
+* input checking and defaults: ``+kwave/+legacy/private/kspaceFirstOrder_inputChecking.m``,
+  ``kspaceFirstOrder_setDefaults.m``;
+* absorption variables: ``private/kspaceFirstOrder_createAbsorptionVariables.m:29-101``;
+* source scaling: ``private/kspaceFirstOrder_scaleSourceTerms.m``;
+* sensor extraction: ``private/kspaceFirstOrder_extractSensorData.m:33-569``;
+* helpers: ``kWaveGrid.m``, ``getPML.m``, ``getWin.m``, ``smooth.m``, ``makeDisc.m``,
+  ``makeBall.m``, ``makeCartCircle.m``, ``cart2grid.m``, ``db2neper.m``,
+  ``private/sinc.m``, ``private/makePixelMap.m``, ``expandMatrix.m``,
+  ``reorderBinarySensorData.m``.
+
+Parity status.  The reference is MATLAB and cannot run in this environment, and
+its tests store no golden vectors.  The oracle is pinned against the
+known-answer recipes that the reference's own tests use (analytic wavenumber
+formula ``+kwave/+tests/+unit/TestGrid.m:135-194``; analytic spectral
+derivatives ``TestFourierCollocation.m:47-300``; plane-wave dimension invariance
+``TestAcousticSolver.m:49-316``; PML interior invariance ``TestSplitFieldPML.m:74-106``)
+and against the closed-form homogeneous lossless solution the reference's
+documentation claims the scheme reproduces (``kspaceFirstOrder3D.m:23-25``).
+MATLAB's own ``fftn`` (FFTW inside the closed MATLAB runtime) is not
+reproducible here, so bit-level agreement with MATLAB output is *parity
+unpinned*; the FFT is ``scipy.fft`` in FP64.
+
+Array convention: NumPy arrays are indexed ``a[x, y, z]`` exactly like MATLAB
+``a(x, y, z)``; MATLAB linear indices (``find``) are column-major, i.e.
+``np.flatnonzero(mask.ravel(order='F'))`` (0-based here).
+"""
+from __future__ import annotations
+
+import math
+import os
+from types import SimpleNamespace
+
+import numpy as np
+import scipy.fft as sfft
+
+_WORKERS = max(1, os.cpu_count() or 1)
+
+
+def fftn(a):
+    return sfft.fftn(a, workers=_WORKERS)
+
+
+def ifftn(a):
+    return sfft.ifftn(a, workers=_WORKERS)
+
+
+# ---------------------------------------------------------------------------
+# kWaveGrid (kWaveGrid.m:342-437 ctor, 588-664 setTime/makeTime, 779-797 makeDim)
+# ---------------------------------------------------------------------------
+
+def make_dim(n, d):
+    """kWaveGrid.makeDim (kWaveGrid.m:779-797): FFT wavenumbers in natural order."""
+    if n % 2 == 0:
+        nx = np.arange(-n // 2, n // 2, dtype=np.float64) / n
+    else:
+        nx = np.arange(-(n - 1) // 2, (n - 1) // 2 + 1, dtype=np.float64) / n
+    nx[n // 2] = 0.0
+    return (2.0 * np.pi / d) * nx
+
+
+class KWaveGrid:
+    """Restatement of ``kWaveGrid`` for 1-3 dimensions (only what the loop uses)."""
+
+    def __init__(self, Nx, dx, Ny=None, dy=None, Nz=None, dz=None):
+        self.Nx, self.dx = int(Nx), float(dx)
+        self.Ny, self.dy = (int(Ny), float(dy)) if Ny is not None else (1, 0.0)
+        self.Nz, self.dz = (int(Nz), float(dz)) if Nz is not None else (1, 0.0)
+        self.dim = 1 + (Ny is not None) + (Nz is not None)
+        self.kx_vec = make_dim(self.Nx, self.dx)
+        self.ky_vec = make_dim(self.Ny, self.dy) if self.dim >= 2 else np.zeros(1)
+        self.kz_vec = make_dim(self.Nz, self.dz) if self.dim >= 3 else np.zeros(1)
+        self.Nt = None
+        self.dt = None
+
+    @property
+    def shape(self):
+        return tuple([self.Nx, self.Ny, self.Nz][: self.dim])
+
+    @property
+    def spacing(self):
+        return [self.dx, self.dy, self.dz][: self.dim]
+
+    def k_vecs(self):
+        return [self.kx_vec, self.ky_vec, self.kz_vec][: self.dim]
+
+    @property
+    def k(self):
+        """|k| on the grid in natural (unshifted) order (kWaveGrid.m:399-433)."""
+        vecs = self.k_vecs()
+        k2 = np.zeros(self.shape)
+        for i, v in enumerate(vecs):
+            k2 = k2 + _axis(v, i, self.dim) ** 2
+        return np.sqrt(k2)
+
+    @property
+    def k_max(self):
+        return min(np.max(np.abs(v)) for v in self.k_vecs())
+
+    def vec(self, axis):
+        """x_vec / y_vec / z_vec (kWaveGrid.m:494-505): Ni*di*ki*di/(2 pi)."""
+        n = [self.Nx, self.Ny, self.Nz][axis]
+        d = self.spacing[axis]
+        return n * d * self.k_vecs()[axis] * d / (2.0 * np.pi)
+
+    @property
+    def size(self):
+        return [n * d for n, d in zip(self.shape, self.spacing)]
+
+    def setTime(self, Nt, dt):
+        if round(Nt) != Nt or Nt <= 0:
+            raise ValueError("Nt must be a positive integer.")
+        if dt <= 0:
+            raise ValueError("dt must be positive.")
+        self.Nt, self.dt = int(Nt), float(dt)
+
+    def makeTime(self, c, cfl=0.3, t_end=None):
+        c = np.asarray(c, dtype=np.float64)
+        c_max, c_min = float(c.max()), float(c.min())
+        if t_end is None:
+            t_end = math.sqrt(sum(s * s for s in self.size)) / c_min
+        self.dt = cfl * min(self.spacing) / c_max
+        self.Nt = int(math.floor(t_end / self.dt)) + 1
+        if math.floor(t_end / self.dt) != math.ceil(t_end / self.dt) and math.fmod(t_end, self.dt) == 0:
+            self.Nt += 1
+        return self.Nt, self.dt
+
+
+def _axis(v, axis, dim):
+    shape = [1] * dim
+    shape[axis] = -1
+    return np.reshape(v, shape)
+
+
+# ---------------------------------------------------------------------------
+# small helpers
+# ---------------------------------------------------------------------------
+
+def sinc(x):
+    """private/sinc.m: sin(x)/x with sinc(0)=1."""
+    x = np.asarray(x, dtype=np.float64)
+    z = x == 0
+    return np.sin(x + np.pi * z) / (x + z) + z
+
+
+def db2neper(alpha, y=1.0):
+    """db2neper.m:52."""
+    return 100.0 * np.asarray(alpha, dtype=np.float64) * (1e-6 / (2 * np.pi)) ** y / (20.0 * np.log10(np.e))
+
+
+def get_pml(n, d, dt, c, pml_size, pml_alpha, staggered):
+    """getPML.m:52-87 (returned as a 1-D vector)."""
+    pml = np.ones(n)
+    if pml_size == 0:
+        return pml
+    x = np.arange(1, pml_size + 1, dtype=np.float64)
+    xs = x + 0.5 if staggered else x
+    left = pml_alpha * (c / d) * ((xs - pml_size - 1) / (0 - pml_size)) ** 4
+    right = pml_alpha * (c / d) * (xs / pml_size) ** 4
+    pml[:pml_size] = np.exp(-left * dt / 2)
+    pml[n - pml_size:] = np.exp(-right * dt / 2)
+    return pml
+
+
+def ifftshift(a):
+    return np.fft.ifftshift(a)
+
+
+def expand_matrix(mat, sizes, edge_val=None):
+    """expandMatrix.m: pad by ``sizes`` on both sides; edge replication when
+    ``edge_val`` is None, else a constant."""
+    pad = [(s, s) for s in sizes]
+    if edge_val is None:
+        return np.pad(mat, pad, mode="edge")
+    return np.pad(mat, pad, mode="constant", constant_values=edge_val)
+
+
+# ---------------------------------------------------------------------------
+# windows and smoothing (getWin.m:104-365, smooth.m:72-137)
+# ---------------------------------------------------------------------------
+
+def _cosine_series(n, N, coeffs):
+    s = coeffs[0] + 0 * n
+    for i in range(1, len(coeffs)):
+        s = s + (-1) ** i * coeffs[i] * np.cos(i * 2 * np.pi * n / (N - 1))
+    return s
+
+
+def get_win_1d(N, wtype, param=None, symmetric=True):
+    N0 = N
+    N = N + (0 if symmetric else 1)
+    n = np.arange(N, dtype=np.float64)
+    if wtype == "Blackman":
+        a = 0.16 if param is None else param
+        win = _cosine_series(n, N, [(1 - a) / 2, 0.5, a / 2])
+    elif wtype == "Hanning":
+        win = 0.5 - 0.5 * np.cos(2 * np.pi * n / (N - 1))
+    elif wtype == "Hamming":
+        win = 0.54 - 0.46 * np.cos(2 * np.pi * n / (N - 1))
+    elif wtype == "Rectangular":
+        win = np.ones(N)
+    elif wtype == "Tukey":
+        a = 0.5 if param is None else param
+        win = np.ones(N)
+        index = np.arange(0, (N - 1) * a / 2 + 1e-12 * 0 + np.finfo(float).eps * 0, 1.0)
+        index = index[index <= (N - 1) * a / 2]
+        pa = a * N
+        win[: len(index)] = 0.5 * (1 + np.cos(2 * np.pi / pa * (index - pa / 2)))
+        win[N - len(index):] = win[: len(index)][::-1]
+    else:
+        raise ValueError("window type not restated: " + wtype)
+    return win[:N0]
+
+
+def get_win(N, wtype="Blackman", rotation=False, symmetric=True, param=None):
+    """getWin.m for 1-3 dimensions ('Rotation' radial windows via interp1)."""
+    N = np.atleast_1d(np.asarray(N, dtype=int))
+    sym = np.broadcast_to(np.atleast_1d(np.asarray(symmetric, dtype=bool)), N.shape)
+    if len(N) == 1:
+        return get_win_1d(int(N[0]), wtype, param, bool(sym[0]))
+    Ne = N + (~sym).astype(int)
+    if rotation:
+        L = int(Ne.max())
+        win_lin = get_win_1d(L, wtype, param, True)
+        radius = (L - 1) / 2
+        ll = np.linspace(-radius, radius, L)
+        axes = [np.linspace(-radius, radius, int(n)) for n in Ne]
+        grids = np.meshgrid(*axes, indexing="ij")
+        r = np.sqrt(sum(g ** 2 for g in grids))
+        r[r > radius] = radius
+        win = np.interp(r, ll, win_lin)
+    else:
+        wins = [get_win_1d(int(n), wtype, param, True) for n in Ne]
+        win = wins[0]
+        for w in wins[1:]:
+            win = np.multiply.outer(win, w)
+    sl = tuple(slice(0, int(n)) for n in N)
+    return win[sl]
+
+
+def smooth(mat, restore_max=False, wtype="Blackman"):
+    """smooth.m:110-137: radially symmetric window filter in k-space."""
+    mat = np.asarray(mat, dtype=np.float64)
+    shape = [s for s in mat.shape if s != 1] if mat.ndim > 1 else list(mat.shape)
+    sym = [bool(s % 2) for s in shape]
+    win = np.abs(get_win(shape, wtype, rotation=True, symmetric=sym))
+    win = np.reshape(win, mat.shape)
+    out = np.real(ifftn(fftn(mat) * ifftshift(win)))
+    if restore_max:
+        out = (np.max(np.abs(mat)) / np.max(np.abs(out))) * out
+    return out
+
+
+# ---------------------------------------------------------------------------
+# geometry helpers (makeDisc.m, makeBall.m, makeCartCircle.m, cart2grid.m)
+# ---------------------------------------------------------------------------
+
+def _pixel_dim(n, shift):
+    if n % 2 == 0:
+        return np.arange(-n // 2, n // 2) if shift == 1 else np.arange(-n // 2 + 1, n // 2 + 1)
+    return np.arange(-(n - 1) // 2, (n - 1) // 2 + 1)
+
+
+def make_disc(Nx, Ny, cx, cy, radius):
+    """makeDisc.m: binary disc, centre (cx, cy) 1-based (0 -> grid centre)."""
+    cx = int(round(cx)) or Nx // 2 + 1
+    cy = int(round(cy)) or Ny // 2 + 1
+    rx, ry = np.meshgrid(_pixel_dim(Nx, 0), _pixel_dim(Ny, 0), indexing="ij")
+    disc = (np.sqrt(rx ** 2 + ry ** 2) <= radius).astype(np.float64)
+    return np.roll(disc, (cx - math.ceil(Nx / 2), cy - math.ceil(Ny / 2)), axis=(0, 1))
+
+
+def make_ball(Nx, Ny, Nz, cx, cy, cz, radius):
+    """makeBall.m (non-binary, ball of ones)."""
+    cx = int(round(cx)) or Nx // 2 + 1
+    cy = int(round(cy)) or Ny // 2 + 1
+    cz = int(round(cz)) or Nz // 2 + 1
+    X, Y, Z = np.meshgrid(np.arange(1, Nx + 1) - cx, np.arange(1, Ny + 1) - cy,
+                          np.arange(1, Nz + 1) - cz, indexing="ij")
+    return ((X ** 2 + Y ** 2 + Z ** 2) <= radius ** 2).astype(np.float64)
+
+
+def make_cart_circle(radius, num_points, center=(0.0, 0.0)):
+    """makeCartCircle.m (full circle)."""
+    angles = np.arange(num_points + 1) * 2 * np.pi / num_points + np.pi / 2
+    angles = angles[:-1]
+    c = np.vstack([radius * np.cos(angles), radius * np.sin(-angles)])
+    c[0] += center[0]
+    c[1] += center[1]
+    return c
+
+
+def _mround(x):
+    """MATLAB round (half away from zero)."""
+    return np.sign(x) * np.floor(np.abs(x) + 0.5)
+
+
+def cart2grid(kgrid, cart):
+    """cart2grid.m:67-194 (nearest grid point).  Returns the binary mask,
+    order_index and reorder_index (both 1-based like MATLAB)."""
+    cart = np.atleast_2d(np.asarray(cart, dtype=np.float64))
+    dim = kgrid.dim
+    idx = []
+    for a in range(dim):
+        v = _mround(cart[a] / kgrid.spacing[a]) + kgrid.shape[a] // 2 + 1
+        if v.max() > kgrid.shape[a] or v.min() < 1:
+            raise ValueError("Cartesian points must lie within the grid defined by kgrid.")
+        idx.append(v.astype(int) - 1)
+    grid = np.zeros(kgrid.shape)
+    for p in range(cart.shape[1]):
+        grid[tuple(i[p] for i in idx)] = p + 1
+    flat = grid.ravel(order="F")
+    reorder_index = flat[flat != 0].astype(int)
+    order_index = np.argsort(reorder_index, kind="stable") + 1
+    mask = (grid != 0).astype(np.float64)
+    return mask, order_index, reorder_index
+
+
+def reorder_binary_sensor_data(data, reorder_index):
+    """reorderBinarySensorData.m: sort rows by reorder_index."""
+    order = np.argsort(reorder_index, kind="stable")
+    return data[order]
+
+
+def tone_burst_hann(sample_freq, signal_freq, num_cycles):
+    """A sine tone burst of ``num_cycles`` cycles sampled at ``sample_freq``,
+    windowed by getWin(N, 'Hanning') (toneBurst.m:102-180 time axis)."""
+    dt = 1.0 / sample_freq
+    tone_length = num_cycles / signal_freq
+    t = np.arange(0.0, tone_length + dt * 1e-9, dt)
+    t = t[t <= tone_length + 1e-15]
+    burst = np.sin(2 * np.pi * signal_freq * t)
+    return burst * get_win_1d(len(burst), "Hanning")
+
+
+# ---------------------------------------------------------------------------
+# the solver
+# ---------------------------------------------------------------------------
+
+RECORD_FLAGS = ("p", "p_max", "p_min", "p_rms", "p_max_all", "p_min_all", "p_final",
+                "u", "u_max", "u_min", "u_rms", "u_max_all", "u_min_all", "u_final",
+                "u_non_staggered", "I", "I_avg")
+
+
+def _get(obj, name, default=None):
+    if obj is None:
+        return default
+    if isinstance(obj, dict):
+        return obj.get(name, default)
+    return getattr(obj, name, default)
+
+
+def _has(obj, name):
+    return _get(obj, name, None) is not None
+
+
+def kspace_first_order(kgrid, medium, source, sensor, **opts):
+    """Restatement of ``kspaceFirstOrder2D`` / ``kspaceFirstOrder3D``.
+
+    ``medium``/``source``/``sensor`` are dicts (or namespaces) with the MATLAB
+    field names.  Options use the MATLAB names: PMLSize, PMLAlpha, PMLInside,
+    Smooth, UsekSpace, UseSG, CartInterp.  Returns what the MATLAB function
+    returns: the ``p`` matrix (M x Nt) when ``sensor.record`` is absent, the
+    ``p_final`` array in time-reversal mode, otherwise a dict of outputs.
+    """
+    dim = kgrid.dim
+    if dim not in (2, 3):
+        raise ValueError("only 2D and 3D are restated")
+    # ---- defaults (setDefaults.m:151-170) ----
+    pml_default = 20 if dim == 2 else 10
+    pml_size = opts.get("PMLSize", pml_default)
+    pml_size = [int(v) for v in np.broadcast_to(np.atleast_1d(pml_size), (dim,))]
+    pml_alpha = [float(v) for v in np.broadcast_to(np.atleast_1d(opts.get("PMLAlpha", 2.0)), (dim,))]
+    pml_inside = bool(opts.get("PMLInside", True))
+    smooth_opt = opts.get("Smooth", [True, False, False])
+    smooth_opt = list(np.broadcast_to(np.atleast_1d(smooth_opt), (3,)))
+    use_kspace = bool(opts.get("UsekSpace", True))
+    use_sg = bool(opts.get("UseSG", True))
+    cart_interp = opts.get("CartInterp", "linear")
+
+    c = np.asarray(_get(medium, "sound_speed"), dtype=np.float64)
+    if _has(medium, "density"):
+        rho0 = np.asarray(_get(medium, "density"), dtype=np.float64)
+    else:
+        rho0 = np.asarray(1.0)
+
+    # ---- equation of state (inputChecking.m:148-281) ----
+    alpha_mode = _get(medium, "alpha_mode")
+    if _has(medium, "alpha_coeff") or _has(medium, "alpha_power"):
+        if alpha_mode == "stokes":
+            eos = "stokes"
+            alpha_power = 2.0
+        else:
+            eos = "absorbing"
+            alpha_power = float(_get(medium, "alpha_power"))
+            if not (0 <= alpha_power < 3):
+                raise ValueError("medium.alpha_power must be a real number between 0 and 3.")
+            if alpha_power == 1 and alpha_mode != "no_dispersion":
+                raise ValueError("alpha_power = 1 needs alpha_mode = 'no_dispersion'")
+        alpha_coeff = np.asarray(_get(medium, "alpha_coeff"), dtype=np.float64)
+    else:
+        eos = "lossless"
+    nonlinear = _has(medium, "BonA")
+    BonA = np.asarray(_get(medium, "BonA"), dtype=np.float64) if nonlinear else None
+
+    # c_ref (setSoundSpeedRef.m:30-49)
+    cref_opt = _get(medium, "sound_speed_ref")
+    if cref_opt is None or cref_opt == "max":
+        c_ref = float(c.max())
+    elif cref_opt == "min":
+        c_ref = float(c.min())
+    elif cref_opt == "mean":
+        c_ref = float(c.mean())
+    else:
+        c_ref = float(cref_opt)
+
+    # ---- sensor (inputChecking.m:288-672) ----
+    use_sensor = sensor is not None
+    time_rev = use_sensor and _has(sensor, "time_reversal_boundary_data")
+    record = set()
+    record_given = use_sensor and _has(sensor, "record")
+    if record_given:
+        for r in _get(sensor, "record"):
+            if r not in RECORD_FLAGS:
+                raise ValueError("'%s' is not a valid input for sensor.record." % r)
+        record = set(_get(sensor, "record"))
+    elif use_sensor and not time_rev:
+        record = {"p"}
+    if time_rev:
+        record = set()
+    needs_mask = bool(record & {"p", "p_max", "p_min", "p_rms", "u", "u_non_staggered",
+                                "u_max", "u_min", "u_rms", "I", "I_avg"})
+    blank_sensor = use_sensor and not needs_mask and not time_rev
+    record_start = int(_mround(_get(sensor, "record_start_index", 1))) if use_sensor else 1
+    reorder_index = None
+    mask = None
+    if use_sensor and not blank_sensor:
+        m = np.asarray(_get(sensor, "mask"), dtype=np.float64)
+        if m.shape == kgrid.shape:
+            mask = m
+        elif m.ndim == 2 and m.shape[0] == dim:
+            if cart_interp != "nearest":
+                raise NotImplementedError("Cartesian 'linear' interpolation is not restated")
+            mask, order_index, reorder_index = cart2grid(kgrid, m)
+        else:
+            raise ValueError("sensor.mask shape not understood")
+
+    # ---- source (inputChecking.m:713-1220) ----
+    p0 = _get(source, "p0")
+    source_p0 = p0 is not None and np.any(np.asarray(p0) != 0)
+    if source_p0:
+        p0 = np.asarray(p0, dtype=np.float64)
+    source_p = 0
+    if _has(source, "p"):
+        sp = np.atleast_2d(np.asarray(_get(source, "p"), dtype=np.float64))
+        p_mask = np.asarray(_get(source, "p_mask"))
+        p_mode = _get(source, "p_mode", "additive")
+        source_p = sp.shape[1]
+        if source_p0:
+            raise ValueError("source.p0 and source.p can't be defined in the same simulation.")
+    u_comps = ["ux", "uy", "uz"][:dim]
+    source_u = [0] * dim
+    su = [None] * dim
+    if any(_has(source, n) for n in u_comps) or _has(source, "u_mask"):
+        u_mask = np.asarray(_get(source, "u_mask"))
+        u_mode = _get(source, "u_mode", "additive")
+        for i, n in enumerate(u_comps):
+            if _has(source, n):
+                su[i] = np.atleast_2d(np.asarray(_get(source, n), dtype=np.float64))
+                source_u[i] = su[i].shape[1]
+
+    # ---- time (inputChecking.m:1227-1268) ----
+    if kgrid.Nt is None:
+        if time_rev or source_p or any(source_u):
+            raise ValueError("kgrid.t_array (Nt and dt) must be defined explicitly")
+        kgrid.makeTime(c, 0.3)
+    Nt, dt = kgrid.Nt, kgrid.dt
+
+    # ---- smoothing (inputChecking.m:1501-1544, 1574-1604) ----
+    if source_p0 and smooth_opt[0]:
+        p0 = smooth(p0, True)
+    if smooth_opt[1] and c.ndim == dim and c.size > 1:
+        c = smooth(c)
+    if smooth_opt[2] and rho0.ndim == dim and rho0.size > 1:
+        rho0 = smooth(rho0)
+
+    # ---- PMLInside = false (expandGridMatrices.m) ----
+    if not pml_inside:
+        kg = KWaveGrid(*sum(([kgrid.shape[a] + 2 * pml_size[a], kgrid.spacing[a]] for a in range(dim)), []))
+        kg.setTime(Nt, dt)
+        kgrid = kg
+        if c.size > 1:
+            c = expand_matrix(c, pml_size)
+        if rho0.size > 1:
+            rho0 = expand_matrix(rho0, pml_size)
+        if eos != "lossless" and alpha_coeff.size > 1:
+            alpha_coeff = expand_matrix(alpha_coeff, pml_size)
+        if nonlinear and BonA.size > 1:
+            BonA = expand_matrix(BonA, pml_size)
+        if source_p0:
+            p0 = expand_matrix(p0, pml_size, 0)
+        if source_p:
+            p_mask = expand_matrix(p_mask, pml_size, 0)
+        if any(source_u):
+            u_mask = expand_matrix(u_mask, pml_size, 0)
+        if mask is not None:
+            mask = expand_matrix(mask, pml_size, 0)
+        inside = [slice(pml_size[a], kgrid.shape[a] - pml_size[a]) for a in range(dim)]
+    else:
+        inside = [slice(0, kgrid.shape[a]) for a in range(dim)]
+    shape = kgrid.shape
+
+    def find(m):
+        return np.flatnonzero(np.asarray(m).ravel(order="F") != 0)
+
+    def gather(field, idx):
+        return field.ravel(order="F")[idx]
+
+    def scatter_set(field, idx, vals):
+        f = field.ravel(order="F").copy()
+        f[idx] = vals
+        return f.reshape(shape, order="F")
+
+    def scatter_add(field, idx, vals):
+        f = field.ravel(order="F").copy()
+        f[idx] = f[idx] + vals
+        return f.reshape(shape, order="F")
+
+    sensor_idx = find(mask) if mask is not None else None
+
+    # source indices / labels
+    def sig_index(msk, nrows):
+        pos = find(msk)
+        vals = np.asarray(msk).ravel(order="F")[pos]
+        uniq = np.unique(msk)
+        if uniq.size <= 2 and uniq.sum() == 1:
+            labelled = False
+            sig = np.arange(pos.size) if nrows > 1 else np.zeros(pos.size, dtype=int)
+        else:
+            labelled = True
+            sig = vals.astype(int) - 1
+        return pos, sig, labelled
+
+    if source_p:
+        p_pos, p_sig, _ = sig_index(p_mask, sp.shape[0])
+    if any(source_u):
+        nrows = max(s.shape[0] for s in su if s is not None)
+        u_pos, u_sig, _ = sig_index(u_mask, nrows)
+
+    # ---- absorption (createAbsorptionVariables.m:29-101) ----
+    kmag = kgrid.k
+    if eos == "absorbing":
+        a_np = db2neper(alpha_coeff, alpha_power)
+        if alpha_mode != "no_absorption":
+            with np.errstate(divide="ignore"):
+                nabla1 = kmag ** (alpha_power - 2)
+            nabla1[np.isinf(nabla1)] = 0
+            nabla1 = ifftshift(nabla1)
+            tau = -2 * a_np * c ** (alpha_power - 1)
+        else:
+            nabla1, tau = 0.0, 0.0
+        if alpha_mode != "no_dispersion":
+            with np.errstate(divide="ignore"):
+                nabla2 = kmag ** (alpha_power - 1)
+            nabla2[np.isinf(nabla2)] = 0
+            nabla2 = ifftshift(nabla2)
+            eta = 2 * a_np * c ** alpha_power * np.tan(np.pi * alpha_power / 2)
+        else:
+            nabla2, eta = 0.0, 0.0
+        if _has(medium, "alpha_sign"):
+            sgn = np.asarray(_get(medium, "alpha_sign"), dtype=np.float64)
+            tau = np.sign(sgn[0]) * tau
+            eta = np.sign(sgn[1]) * eta
+    elif eos == "stokes":
+        a_np = db2neper(alpha_coeff, 2)
+        tau = -2 * a_np * c
+        if _has(medium, "alpha_sign"):
+            tau = np.sign(np.asarray(_get(medium, "alpha_sign"))[0]) * tau
+
+    c0 = c
+    # ---- source scaling (scaleSourceTerms.m) ----
+    if source_p:
+        sp = sp.copy()
+        if p_mode == "dirichlet":
+            if c0.size == 1:
+                sp = sp / (dim * c0 ** 2)
+            else:
+                for r in range(sp.shape[0]):
+                    sp[r] = sp[r] / (dim * c0.ravel(order="F")[p_pos[r]] ** 2)
+        else:
+            if c0.size == 1:
+                sp = sp * (2 * dt / (dim * c0 * kgrid.dx))
+            else:
+                for r in range(sp.shape[0]):
+                    sp[r] = sp[r] * (2 * dt / (dim * c0.ravel(order="F")[p_pos[r]] * kgrid.dx))
+    if any(source_u) and u_mode != "dirichlet":
+        for i in range(dim):
+            if su[i] is None:
+                continue
+            su[i] = su[i].copy()
+            d = kgrid.spacing[i] if i > 0 else kgrid.dx
+            if c0.size == 1:
+                su[i] = su[i] * (2 * c0 * dt / d)
+            else:
+                for r in range(su[i].shape[0]):
+                    su[i][r] = su[i][r] * (2 * c0.ravel(order="F")[u_pos[r]] * dt / d)
+
+    # ---- staggered density (kspaceFirstOrder3D.m:585-607) ----
+    rho_sg_inv = []
+    for a in range(dim):
+        if rho0.ndim == dim and rho0.size > 1 and use_sg:
+            r = rho0.copy()
+            sl_lo = [slice(None)] * dim
+            sl_hi = [slice(None)] * dim
+            sl_lo[a] = slice(0, shape[a] - 1)
+            sl_hi[a] = slice(1, shape[a])
+            r[tuple(sl_lo)] = 0.5 * (rho0[tuple(sl_lo)] + rho0[tuple(sl_hi)])
+            rho_sg_inv.append(1.0 / r)
+        else:
+            rho_sg_inv.append(1.0 / rho0)
+
+    # ---- PML and k-space operators (kspaceFirstOrder3D.m:619-661) ----
+    pml = []
+    pml_sg = []
+    for a in range(dim):
+        pml.append(_axis(get_pml(shape[a], kgrid.spacing[a], dt, c_ref, pml_size[a], pml_alpha[a], False), a, dim))
+        pml_sg.append(_axis(get_pml(shape[a], kgrid.spacing[a], dt, c_ref, pml_size[a], pml_alpha[a], use_sg), a, dim))
+    dd_pos, dd_neg = [], []
+    for a, kv in enumerate(kgrid.k_vecs()):
+        d = kgrid.spacing[a]
+        if use_sg:
+            pos = ifftshift(1j * kv * np.exp(1j * kv * d / 2))
+            neg = ifftshift(1j * kv * np.exp(-1j * kv * d / 2))
+        else:
+            pos = ifftshift(1j * kv)
+            neg = ifftshift(1j * kv)
+        dd_pos.append(_axis(pos, a, dim))
+        dd_neg.append(_axis(neg, a, dim))
+    if use_kspace:
+        kappa = ifftshift(sinc(c_ref * kmag * dt / 2))
+        source_kappa = ifftshift(np.cos(c_ref * kmag * dt / 2))
+    else:
+        kappa = 1.0
+        source_kappa = 1.0
+
+    # ---- storage (createStorageVariables.m) ----
+    num_rec = Nt - record_start + 1
+    out = {}
+    M = sensor_idx.size if sensor_idx is not None else 0
+    if "p" in record:
+        out["p"] = np.zeros((M, num_rec))
+    if "p_rms" in record:
+        out["p_rms"] = np.zeros(M)
+    if "u" in record:
+        for i in range(dim):
+            out[u_comps[i]] = np.zeros((M, num_rec))
+    if "u_non_staggered" in record:
+        for i in range(dim):
+            out[u_comps[i] + "_non_staggered"] = np.zeros((M, num_rec))
+    if "u_rms" in record:
+        for i in range(dim):
+            out[u_comps[i] + "_rms"] = np.zeros(M)
+    shift_neg = None
+    if "u_non_staggered" in record:
+        shift_neg = []
+        for a, kv in enumerate(kgrid.k_vecs()):
+            s = ifftshift(np.exp(-1j * kv * kgrid.spacing[a] / 2)) if use_sg else np.ones(shape[a])
+            shift_neg.append(s)
+
+    # ---- time reversal data ----
+    if time_rev:
+        trd = np.atleast_2d(np.asarray(_get(sensor, "time_reversal_boundary_data"), dtype=np.float64))
+        if reorder_index is not None:
+            # inputChecking.m:640-648: rows re-sorted into find(mask) order
+            trd = trd[np.argsort(order_index, kind="stable")]
+        trd = trd[:, ::-1]
+        index_end = Nt - 1
+    else:
+        index_end = Nt
+
+    # ---- loop ----
+    p = np.zeros(shape)
+    rho = [np.zeros(shape) for _ in range(dim)]
+    u = [np.zeros(shape) for _ in range(dim)]
+    p_k = np.zeros(shape, dtype=complex)
+    c2 = c0 ** 2
+
+    for t in range(1, index_end + 1):
+        if time_rev:
+            p = scatter_set(p, sensor_idx, trd[:, t - 1])
+            p_k = fftn(p)
+            rmod = p / (dim * c2) if dim == 3 else 0.5 * p / c2
+            rmod = np.broadcast_to(rmod, shape)
+            for i in range(dim):
+                rho[i] = scatter_set(rho[i], sensor_idx, gather(np.ascontiguousarray(rmod), sensor_idx))
+
+        # momentum (kspaceFirstOrder3D.m:792-803)
+        for i in range(dim):
+            u[i] = pml_sg[i] * (pml_sg[i] * u[i] - dt * rho_sg_inv[i] * np.real(ifftn(dd_pos[i] * kappa * p_k)))
+
+        # velocity sources (kspaceFirstOrder3D.m:806-886)
+        for i in range(dim):
+            if source_u[i] >= t:
+                rows = u_sig if su[i].shape[0] > 1 else np.zeros_like(u_sig)
+                vals = su[i][rows, t - 1]
+                if u_mode == "dirichlet":
+                    u[i] = scatter_set(u[i], u_pos, vals)
+                elif u_mode == "additive":
+                    smat = scatter_set(np.zeros(shape), u_pos, vals)
+                    u[i] = u[i] + np.real(ifftn(source_kappa * fftn(smat)))
+                else:
+                    u[i] = scatter_add(u[i], u_pos, vals)
+
+        # divergence (kspaceFirstOrder3D.m:907-909)
+        du = [np.real(ifftn(dd_neg[i] * kappa * fftn(u[i]))) for i in range(dim)]
+
+        # mass conservation (kspaceFirstOrder3D.m:912-927)
+        if not nonlinear:
+            for i in range(dim):
+                rho[i] = pml[i] * (pml[i] * rho[i] - dt * rho0 * du[i])
+        else:
+            r0pr = 2 * sum(rho) + rho0
+            for i in range(dim):
+                rho[i] = pml[i] * (pml[i] * rho[i] - dt * r0pr * du[i])
+
+        # pressure sources (kspaceFirstOrder3D.m:930-962)
+        if source_p >= t:
+            vals = sp[p_sig, t - 1]
+            if p_mode == "dirichlet":
+                for i in range(dim):
+                    rho[i] = scatter_set(rho[i], p_pos, vals)
+            elif p_mode == "additive":
+                smat = scatter_set(np.zeros(shape), p_pos, vals)
+                smat = np.real(ifftn(source_kappa * fftn(smat)))
+                for i in range(dim):
+                    rho[i] = rho[i] + smat
+            else:
+                for i in range(dim):
+                    rho[i] = scatter_add(rho[i], p_pos, vals)
+
+        # equation of state (kspaceFirstOrder3D.m:965-1019)
+        srho = sum(rho)
+        sdu = sum(du)
+        if eos == "lossless":
+            p = c2 * srho
+        elif eos == "absorbing":
+            p = c2 * (srho + tau * np.real(ifftn(nabla1 * fftn(rho0 * sdu)))
+                      - eta * np.real(ifftn(nabla2 * fftn(srho))))
+        else:
+            p = c2 * (srho + tau * rho0 * sdu)
+        if nonlinear:
+            p = p + c2 * BonA * srho ** 2 / (2 * rho0)
+        p = np.broadcast_to(p, shape).copy()
+
+        # p0 initial condition (kspaceFirstOrder3D.m:1023-1037)
+        if t == 1 and source_p0:
+            p = p0.copy()
+            for i in range(dim):
+                rho[i] = np.broadcast_to(p0 / (dim * c2), shape).copy()
+            pk0 = fftn(p)
+            for i in range(dim):
+                u[i] = dt * rho_sg_inv[i] * np.real(ifftn(dd_pos[i] * kappa * pk0)) / 2
+                u[i] = np.broadcast_to(u[i], shape).copy()
+
+        p_k = fftn(p)
+
+        # sensors (extractSensorData.m)
+        if use_sensor and not time_rev and t >= record_start:
+            fi = t - record_start + 1
+            if sensor_idx is not None:
+                ps = gather(p, sensor_idx)
+                if "p" in record:
+                    out["p"][:, fi - 1] = ps
+                if "p_max" in record:
+                    out["p_max"] = ps.copy() if fi == 1 else np.maximum(out["p_max"], ps)
+                if "p_min" in record:
+                    out["p_min"] = ps.copy() if fi == 1 else np.minimum(out["p_min"], ps)
+                if "p_rms" in record:
+                    out["p_rms"] = np.sqrt((out["p_rms"] ** 2 * (fi - 1) + ps ** 2) / fi)
+                for i in range(dim):
+                    us = gather(u[i], sensor_idx)
+                    n = u_comps[i]
+                    if "u" in record:
+                        out[n][:, fi - 1] = us
+                    if "u_max" in record:
+                        out[n + "_max"] = us.copy() if fi == 1 else np.maximum(out[n + "_max"], us)
+                    if "u_min" in record:
+                        out[n + "_min"] = us.copy() if fi == 1 else np.minimum(out[n + "_min"], us)
+                    if "u_rms" in record:
+                        out[n + "_rms"] = np.sqrt((out[n + "_rms"] ** 2 * (fi - 1) + us ** 2) / fi)
+                    if "u_non_staggered" in record:
+                        ush = np.real(np.fft.ifft(_axis(shift_neg[i], i, dim) * np.fft.fft(u[i], axis=i), axis=i))
+                        out[n + "_non_staggered"][:, fi - 1] = gather(ush, sensor_idx)
+            ins = tuple(inside)
+            if "p_max_all" in record:
+                out["p_max_all"] = p[ins].copy() if fi == 1 else np.maximum(out["p_max_all"], p[ins])
+            if "p_min_all" in record:
+                out["p_min_all"] = p[ins].copy() if fi == 1 else np.minimum(out["p_min_all"], p[ins])
+            for i in range(dim):
+                n = u_comps[i]
+                if "u_max_all" in record:
+                    out[n + "_max_all"] = u[i][ins].copy() if fi == 1 else np.maximum(out[n + "_max_all"], u[i][ins])
+                if "u_min_all" in record:
+                    out[n + "_min_all"] = u[i][ins].copy() if fi == 1 else np.minimum(out[n + "_min_all"], u[i][ins])
+
+    if time_rev:
+        p = scatter_set(p, sensor_idx, trd[:, index_end])
+        record.add("p_final")
+    ins = tuple(inside)
+    if "p_final" in record:
+        out["p_final"] = p[ins].copy()
+    if "u_final" in record:
+        for i in range(dim):
+            out[u_comps[i] + "_final"] = u[i][ins].copy()
+
+    # Cartesian nearest-neighbour reorder (reorderCartData.m)
+    if reorder_index is not None and not time_rev:
+        for key in list(out.keys()):
+            if key.endswith("_all") or key.endswith("_final"):
+                continue
+            out[key] = reorder_binary_sensor_data(out[key], reorder_index)
+
+    if not use_sensor:
+        return None
+    if time_rev:
+        return out["p_final"]
+    if not record_given:
+        return out["p"]
+    return out
+
+
+def rel_l2(a, b):
+    a = np.asarray(a, dtype=np.float64)
+    b = np.asarray(b, dtype=np.float64)
+    den = np.linalg.norm(b.ravel())
+    return float(np.linalg.norm((a - b).ravel()) / (den if den > 0 else 1.0))
