@@ -1,0 +1,337 @@
+"""Benchmark of the k-space first-order time loop on B200.
+
+Workload (the configuration the headline metric is quoted on): 3-D
+heterogeneous absorbing nonlinear kspaceFirstOrder3D at 256^3, dx = 0.2 mm,
+blob sound speed (1500 m/s + 8 Gaussian blobs), density 1000 + 0.6 (c - 1500),
+alpha_coeff 0.75 dB/(MHz^y cm), alpha_power 1.5, BonA 6, a 64 x 64 plane
+pressure source (additive) driven by a 1 MHz 3-cycle Hann-windowed tone burst
+at 1 MPa, PML 10, CFL 0.3, Nt = 1000, sensor = the central xy-plane plus a
+256-point line along z, recording p and p_max.  Inputs are seeded synthetic
+data.
+
+One bench step is one complete simulation (Nt time steps).  ``value`` is the
+whole-job throughput in Gcell-steps/s with every input resident on the device
+(CUDA events on the library's stream); ``e2e`` is the same metric through the
+public kspaceFirstOrder3D call with host arrays (setup, host->device upload,
+loop and device->host outputs inside the timed region).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+With --gpus N > 1 (launched by torch.distributed.run) each rank runs an
+independent replica on its own GPU: the loop has no exchange between
+simulations, so the job is replicas only (weak scaling).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "k-wave-ii_b200"))
+
+METRIC = "Gcell-steps/s (256³ FP32); served p50/p99 vs plain GPU path at ≤1e-4 rel-L2"
+UNIT = "Gcell-steps/s"
+BYTES_PER_CELL_STEP = 144.0      # 4 B x (6 state reads + 7 state writes + 7 medium + 2 x 8 spectral ops)
+BYTES_PER_CELL_SRC_STEP = 8.0    # one more spectral application on source-active steps
+HBM_FALLBACK_GBS = 6650.0
+
+
+def blob_speed(shape, rng, n_blobs=8, pml=10):
+    c = np.full(shape, 1500.0)
+    axes = [np.arange(s, dtype=np.float64) for s in shape]
+    for _ in range(n_blobs):
+        ctr = [rng.uniform(pml, s - pml) for s in shape]
+        sig = rng.uniform(5.0, 20.0)
+        amp = rng.uniform(-100.0, 200.0)
+        g = [np.exp(-(a - c0) ** 2 / (2 * sig * sig)) for a, c0 in zip(axes, ctr)]
+        c += amp * g[0][:, None, None] * g[1][None, :, None] * g[2][None, None, :]
+    return c
+
+
+def hann_burst(dt, f0=1e6, cycles=3, amp=1e6):
+    n = int(math.floor(cycles / f0 / dt + 1e-9)) + 1
+    t = np.arange(n) * dt
+    w = 0.5 - 0.5 * np.cos(2 * np.pi * np.arange(n) / (n - 1))
+    return amp * np.sin(2 * np.pi * f0 * t) * w
+
+
+def workload(seed=0, N=256, Nt=1000, dx=0.2e-3, pml=10):
+    rng = np.random.default_rng(seed)
+    shape = (N, N, N)
+    c = blob_speed(shape, rng, pml=pml)
+    rho = 1000.0 + 0.6 * (c - 1500.0)
+    medium = {"sound_speed": c, "density": rho, "alpha_coeff": 0.75, "alpha_power": 1.5, "BonA": 6.0}
+    dt = 0.3 * dx / c.max()
+    p_mask = np.zeros(shape)
+    h = N // 2
+    p_mask[pml, h - 32:h + 32, h - 32:h + 32] = 1
+    sig = hann_burst(dt)
+    source = {"p_mask": p_mask, "p": sig[None, :]}
+    sensor_mask = np.zeros(shape)
+    sensor_mask[:, :, h] = 1                   # central xy-plane
+    sensor_mask[3 * N // 4, h, :] = 1          # 256-point line along z
+    sensor = {"mask": sensor_mask, "record": ["p", "p_max"]}
+    return dict(shape=shape, dx=dx, Nt=Nt, dt=dt, medium=medium, source=source, sensor=sensor,
+                options={"PMLSize": pml}, src_len=len(sig))
+
+
+def make_grid(kw, w):
+    g = kw.kWaveGrid(w["shape"][0], w["dx"], w["shape"][1], w["dx"], w["shape"][2], w["dx"])
+    g.setTime(w["Nt"], w["dt"])
+    return g
+
+
+def measured_peak():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return HBM_FALLBACK_GBS, "fallback"
+
+
+class Clocks:
+    """nvidia-smi samples of the SM clock and throttle reasons while running."""
+
+    def __init__(self, device, path):
+        self.path = path
+        self.proc = None
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.f = open(path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(device), "--query-gpu=" + q,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.f.close()
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx.append(float(parts[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower() in ("active", "1"):
+                    reasons.add(n)
+        if not sm:
+            return None
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": float(max(mx)), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def cpu_baseline(w, steps):
+    """The FP64 oracle (NumPy/SciPy, all host cores) on a bounded sample of the
+    same workload: the first ``steps`` time steps."""
+    sys.path.insert(0, ROOT)
+    from oracle import kspace as oracle
+    g = oracle.KWaveGrid(w["shape"][0], w["dx"], w["shape"][1], w["dx"], w["shape"][2], w["dx"])
+    g.setTime(steps, w["dt"])
+    oracle.kspace_first_order(g, w["medium"], w["source"], w["sensor"], **w["options"])
+    secs = oracle.LAST_LOOP_SECONDS
+    cells = float(np.prod(w["shape"]))
+    return {"value": cells * steps / secs / 1e9, "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
+            "sample": "first %d of %d time steps of the 256^3 workload, FP64 NumPy/SciPy oracle "
+                      "(scipy.fft workers=%d); loop time only" % (steps, w["Nt"], os.cpu_count()),
+            "seconds": secs}
+
+
+def dist_setup():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if ws > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    return ws, rank, local
+
+
+def dist_max(x, ws):
+    if ws == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def dist_barrier(ws):
+    if ws > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def run_reference(args, ws, rank):
+    """The reference arm: the reference's CPU implementation of the loop.  MATLAB
+    is not installed, so the FP64 restatement of the reference solver runs on
+    the host cores (kind 'port'); each step is a bounded sample of the
+    workload (its first --cpu-steps time steps)."""
+    if rank != 0:
+        return
+    w = workload(seed=0)
+    sys.path.insert(0, ROOT)
+    for _ in range(args.warmup):
+        cpu_baseline(w, 1)
+    secs = 0.0
+    for _ in range(args.steps):
+        r = cpu_baseline(w, args.cpu_steps)
+        secs += r["seconds"]
+    cells = float(np.prod(w["shape"]))
+    value = cells * args.cpu_steps * args.steps / secs / 1e9
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * secs / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded)", "config": {"workload": "kspaceFirstOrder3D 256^3 absorbing BonA plane source",
+                                                      "step": "first %d time steps" % args.cpu_steps},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
+                             "sample": r["sample"]},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--cpu-steps", type=int, default=3)
+    ap.add_argument("--e2e-steps", type=int, default=2)
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--Nt", type=int, default=1000)
+    ap.add_argument("--N", type=int, default=256)
+    args = ap.parse_args()
+    ws, rank, local = dist_setup()
+    if args.impl == "reference":
+        run_reference(args, ws, rank)
+        if ws > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+        return
+
+    import kwave_b200 as kw
+    w = workload(seed=rank, N=args.N, Nt=args.Nt)
+    opts = dict(w["options"], DeviceNum=local)
+    sim = kw.Simulation(3, make_grid(kw, w), w["medium"], w["source"], w["sensor"], **opts)
+    cells = float(np.prod(w["shape"]))
+    Nt = w["Nt"]
+    dev_gb = sim.device_bytes() / 1e9
+
+    # warm-up (full simulations)
+    sim.run_timed(max(args.warmup, 0)) if args.warmup > 0 else None
+
+    # timed region: K complete simulations, device events on the library stream
+    os.makedirs(os.path.join(ROOT, "gpurun_out"), exist_ok=True)
+    clk = Clocks(local, os.path.join(ROOT, "gpurun_out", "clocks_rank%d.csv" % rank))
+    l0 = sim.launch_count()
+    dist_barrier(ws)
+    ms = sim.run_timed(args.steps)
+    dist_barrier(ws)
+    launches = sim.launch_count() - l0
+    clocks = clk.stop()
+    ms_max = dist_max(ms, ws)
+    value = ws * cells * Nt * args.steps / (ms_max / 1e3) / 1e9
+
+    # kernel classes (separate run with per-launch events; not part of the timed region)
+    sim.set_timing(["zstage_u", "zstage_r", "zstage_p", "ypass", "xpass", "sensor", "source"])
+    sim.run_device()
+    classes = {}
+    tot = 0.0
+    for c in ("zstage_u", "zstage_r", "zstage_p", "ypass", "xpass", "sensor", "source"):
+        t, n = sim.timing(c)
+        classes[c] = {"ms_per_sim": t, "launches_per_sim": n}
+        tot += t
+    for c in classes:
+        classes[c]["share"] = classes[c]["ms_per_sim"] / tot if tot else 0.0
+    sim.set_timing([])
+
+    # roofline for the time step (the unit the bytes-per-cell-step model describes)
+    peak, peak_kind = measured_peak()
+    src_steps = min(w["src_len"], Nt)
+    alg_bytes_per_sim = cells * (BYTES_PER_CELL_STEP * Nt + BYTES_PER_CELL_SRC_STEP * src_steps)
+    achieved = alg_bytes_per_sim / (ms / args.steps / 1e3) / 1e9
+    traffic = None
+    tf = os.path.join(ROOT, "profiles", "step_traffic_256.json")
+    if os.path.exists(tf):
+        try:
+            traffic = json.load(open(tf)).get("dram_bytes_per_step")
+        except Exception:
+            traffic = None
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                "traffic": traffic, "peak_source": peak_kind,
+                "kernel": "one time step of the loop (all its launches)",
+                "alg_bytes_per_cell_step": BYTES_PER_CELL_STEP}
+    sim.close()
+
+    # end to end through the public API with host arrays
+    e2e = None
+    if args.e2e_steps > 0:
+        h2d = d2h = 0
+        t0 = time.perf_counter()
+        for _ in range(args.e2e_steps):
+            with kw.Simulation(3, make_grid(kw, w), w["medium"], w["source"], w["sensor"], **opts) as s2:
+                out = s2.run()
+                h2d = s2.h2d_bytes
+                d2h = int(sum(v.nbytes for v in out.values()))
+        secs = time.perf_counter() - t0
+        secs = dist_max(secs, ws)
+        e2e = {"value": ws * cells * Nt * args.e2e_steps / secs / 1e9, "unit": UNIT,
+               "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "steps": args.e2e_steps,
+               "call": "kwave_b200.Simulation(...).run() == kspaceFirstOrder3D(kgrid, medium, source, sensor)"}
+
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu:
+        try:
+            cpu = cpu_baseline(w, args.cpu_steps)
+            cpu.pop("seconds", None)
+        except Exception as e:  # the baseline is reported, not required
+            cpu = {"error": str(e)}
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+                "data": "synthetic (seeded blob medium; no dataset)",
+                "config": {"workload": "kspaceFirstOrder3D %d^3 heterogeneous absorbing (y=1.5) BonA=6, "
+                                       "64x64 additive plane p source, 1 MHz 3-cycle burst, PML 10, Nt=%d"
+                                       % (args.N, Nt),
+                           "grid": list(w["shape"]), "Nt": Nt, "step": "one complete simulation (Nt time steps)",
+                           "l2": "no flush: inputs larger than L2 (device working set %.2f GB vs 126 MB L2)" % dev_gb,
+                           "parallelism": "replicas x%d" % ws},
+                "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
+                "clocks": clocks, "kernel_classes": classes}
+        print(json.dumps(line), flush=True)
+    if ws > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

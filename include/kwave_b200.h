@@ -135,6 +135,8 @@ typedef struct kw_problem {
     /* region kept by *_all and *_final outputs (record.x1_inside...), 1-based
        inclusive, per axis */
     uint64_t inside_lo[3], inside_hi[3];
+
+    int32_t  device;             /* CUDA device ordinal of the plan ('DeviceNum') */
 } kw_problem;
 
 /* Output sizes (createStorageVariables.m:58-88). */
@@ -204,6 +206,14 @@ kw_status kw_get_timing(const kw_plan *plan, int kclass, double *total_ms, uint6
 
 /* Device bytes held by the plan. */
 kw_status kw_plan_device_bytes(const kw_plan *plan, uint64_t *bytes);
+
+/* Run the whole loop n times back to back (each from the initial state) on
+   the plan's stream between two CUDA events; *device_ms is the elapsed device
+   time.  Outputs of the last run stay on the device. */
+kw_status kw_run_timed(kw_plan *plan, uint32_t n, double *device_ms);
+
+/* Number of kernels the plan has launched since creation. */
+kw_status kw_launch_count(const kw_plan *plan, uint64_t *launches);
 
 #ifdef __cplusplus
 }

@@ -201,6 +201,8 @@ struct kw_plan {
 
     std::vector<void *> allocs;
     size_t bytes = 0;
+    uint64_t launches = 0;
+    int device = 0;
 };
 
 namespace {
@@ -268,9 +270,10 @@ kw_status set_smem(const void *fn, size_t bytes) {
     return KW_OK;
 }
 
-kw_status check_launch() {
+kw_status launched(kw_plan *P) {
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return fail(KW_ERR_CUDA, "kernel launch failed: %s", cudaGetErrorString(e));
+    P->launches += 1;
     return KW_OK;
 }
 
@@ -287,7 +290,7 @@ kw_status ypass(kw_plan *P, bool inv, Spec4 bufs, int nf) {
         KW_TRY(set_smem((const void *)k_ypass<false>, sh));
         k_ypass<false><<<grid, kThreads, sh, P->stream>>>(bufs, P->g, P->fft[1], P->TY);
     }
-    return check_launch();
+    return launched(P);
 }
 
 kw_status xpass(kw_plan *P, Spec4 bufs, OpSet ops, int fanout, int nf) {
@@ -297,7 +300,7 @@ kw_status xpass(kw_plan *P, Spec4 bufs, OpSet ops, int fanout, int nf) {
     size_t sh = (size_t)(fanout ? 2 : 1) * P->NL * P->g.N0 * sizeof(float2);
     KW_TRY(set_smem((const void *)k_xpass, sh));
     k_xpass<<<grid, kThreads, sh, P->stream>>>(bufs, P->g, P->fft[0], P->NL, P->op, ops, fanout);
-    return check_launch();
+    return launched(P);
 }
 
 kw_status zr2c(kw_plan *P, const float *R, float2 *H) {
@@ -305,7 +308,7 @@ kw_status zr2c(kw_plan *P, const float *R, float2 *H) {
     size_t sh = (size_t)P->PL_z * P->g.N2 * sizeof(float2);
     KW_TRY(set_smem((const void *)k_zr2c, sh));
     k_zr2c<<<grid, kThreads, sh, P->stream>>>(R, H, P->g, P->fft[2], P->PL_z);
-    return check_launch();
+    return launched(P);
 }
 
 kw_status zc2r(kw_plan *P, const float2 *H, float *R) {
@@ -313,7 +316,7 @@ kw_status zc2r(kw_plan *P, const float2 *H, float *R) {
     size_t sh = (size_t)P->PL_z * P->g.N2 * sizeof(float2);
     KW_TRY(set_smem((const void *)k_zc2r, sh));
     k_zc2r<<<grid, kThreads, sh, P->stream>>>(H, R, P->g, P->fft[2], P->PL_z);
-    return check_launch();
+    return launched(P);
 }
 
 Spec4 specs(kw_plan *P, int a, int b = -1, int c = -1) {
@@ -365,7 +368,7 @@ kw_status general_source(kw_plan *P, SourceDev &S, int comp, int t) {
         Scope s(P, KW_KCLASS_SOURCE);
         k_scatter_source<<<(S.npts + 255) / 256, 256, 0, P->stream>>>(S.pos, S.row, S.npts, S.sig[comp], S.nsig,
                                                                       S.scratch, P->d_t, S.T[comp]);
-        KW_TRY(check_launch());
+        KW_TRY(launched(P));
     }
     return source_filter(P, S.scratch, S.Ft[comp]);
 }
@@ -434,7 +437,7 @@ kw_status stage_u(kw_plan *P, int init, int t) {
     size_t sh = (size_t)a.PL * P->g.N2 * sizeof(float2);
     KW_TRY(set_smem((const void *)k_stage_u, sh));
     k_stage_u<<<grid, kThreads, sh, P->stream>>>(a);
-    return check_launch();
+    return launched(P);
 }
 
 kw_status stage_r(kw_plan *P, int write_spec) {
@@ -471,7 +474,7 @@ kw_status stage_r(kw_plan *P, int write_spec) {
     size_t sh = (size_t)4 * a.PL * P->g.N2 * sizeof(float2);
     KW_TRY(set_smem((const void *)k_stage_r, sh));
     k_stage_r<<<grid, kThreads, sh, P->stream>>>(a);
-    return check_launch();
+    return launched(P);
 }
 
 kw_status stage_p(kw_plan *P, int write_spec) {
@@ -501,7 +504,7 @@ kw_status stage_p(kw_plan *P, int write_spec) {
     size_t sh = (size_t)2 * a.PL * P->g.N2 * sizeof(float2);
     KW_TRY(set_smem((const void *)k_stage_p, sh));
     k_stage_p<<<grid, kThreads, sh, P->stream>>>(a);
-    return check_launch();
+    return launched(P);
 }
 
 kw_status sensors(kw_plan *P, int t) {
@@ -526,7 +529,7 @@ kw_status sensors(kw_plan *P, int t) {
             a.record_start = P->record_start;
             a.d_t = P->d_t;
             k_sensor<<<(P->M + 255) / 256, 256, 0, P->stream>>>(a);
-            KW_TRY(check_launch());
+            KW_TRY(launched(P));
         }
     }
     bool any_all = false;
@@ -550,7 +553,7 @@ kw_status sensors(kw_plan *P, int t) {
         Scope s(P, KW_KCLASS_SENSOR);
         const long long blocks = std::min<long long>((P->in_count + 255) / 256, 148 * 16);
         k_region<<<(int)blocks, 256, 0, P->stream>>>(r);
-        KW_TRY(check_launch());
+        KW_TRY(launched(P));
     }
     return KW_OK;
 }
@@ -577,7 +580,7 @@ kw_status start(kw_plan *P) {
         // kspaceFirstOrder3D.m:772-788 at t = 1
         k_tr_start<<<(P->M + 255) / 256, 256, 0, P->stream>>>(P->sidx, P->M, P->tr_data, P->Nt, P->c0, P->p,
                                                               P->rho[0], P->rho[1], P->rho[2], P->D);
-        KW_TRY(check_launch());
+        KW_TRY(launched(P));
         KW_TRY(zr2c(P, P->p, P->spec[0]));
         KW_TRY(grad_group(P));
     }
@@ -594,7 +597,7 @@ kw_status run_step(kw_plan *P) {
         // step's update is overwritten, so the state is set directly.
         KW_CUDA(cudaMemcpyAsync(P->p, P->p0_dev, (size_t)P->g.N * sizeof(float), cudaMemcpyDeviceToDevice, P->stream));
         k_init_rho<<<1024, 256, 0, P->stream>>>(P->p0_dev, P->c0, P->rho[0], P->rho[1], P->rho[2], P->g.N, P->D);
-        KW_TRY(check_launch());
+        KW_TRY(launched(P));
         KW_TRY(zr2c(P, P->p, P->spec[0]));
         KW_TRY(grad_group(P));
         KW_TRY(stage_u(P, 1, t));
@@ -632,7 +635,7 @@ kw_status run_step(kw_plan *P) {
     }
     KW_TRY(sensors(P, t));
     k_step_advance<<<1, 1, 0, P->stream>>>(P->d_t);
-    KW_TRY(check_launch());
+    KW_TRY(launched(P));
     P->t += 1;
     return KW_OK;
 }
@@ -734,7 +737,7 @@ kw_status setup_source(kw_plan *P, SourceDev &S, const kw_source *src, int ncomp
             KW_TRY(dev_alloc(&m, N));
             KW_CUDA(cudaMemsetAsync(m, 0, N * sizeof(float), P->stream));
             k_set_points<<<(S.npts + 255) / 256, 256, 0, P->stream>>>(S.pos, S.npts, 1.0f, m);
-            KW_TRY(check_launch());
+            KW_TRY(launched(P));
             kw_status st = source_filter(P, m, S.F);
             cudaStreamSynchronize(P->stream);
             cudaFree(m);
@@ -813,6 +816,13 @@ kw_status create(const kw_problem *pr, kw_plan *P) {
     if (P->p0 && q.p_source.num_time_samples > 0) return fail(KW_ERR_INVALID, "source.p0 and source.p can't be defined in the same simulation.");
     P->absorbing = q.absorbing_flag == KW_ABSORBING;
 
+    P->device = q.device;
+    {
+        int ndev = 0;
+        KW_CUDA(cudaGetDeviceCount(&ndev));
+        if (q.device < 0 || q.device >= ndev) return fail(KW_ERR_INVALID, "device %d not present (%d devices)", q.device, ndev);
+    }
+    KW_CUDA(cudaSetDevice(P->device));
     KW_CUDA(cudaStreamCreateWithFlags(&P->stream, cudaStreamNonBlocking));
 
     // FFT plans and operator tables (FP64 -> FP32)
@@ -1047,7 +1057,7 @@ kw_status crop_out(kw_plan *P, float *dst, const float *field) {
     if (!dst) return KW_OK;
     k_crop<<<std::min<long long>((P->in_count + 255) / 256, 148 * 16), 256, 0, P->stream>>>(
         field, P->o_tmp, P->g, P->in_lo[0], P->in_lo[1], P->in_lo[2], P->in_n[0], P->in_n[1], P->in_n[2]);
-    KW_TRY(check_launch());
+    KW_TRY(launched(P));
     KW_TRY(copy_dev(P, dst, P->o_tmp, P->in_count));
     KW_CUDA(cudaStreamSynchronize(P->stream));
     return KW_OK;
@@ -1058,7 +1068,7 @@ kw_status rms_out(kw_plan *P, float *dst, const float *sq) {
     const int done = std::max(0, std::min(P->t - 1, P->Nt) - P->record_start + 1);
     KW_CUDA(cudaMemcpyAsync(P->o_tmp, sq, (size_t)P->M * sizeof(float), cudaMemcpyDeviceToDevice, P->stream));
     k_rms_finish<<<(P->M + 255) / 256, 256, 0, P->stream>>>(P->o_tmp, P->M, done > 0 ? 1.f / done : 0.f);
-    KW_TRY(check_launch());
+    KW_TRY(launched(P));
     KW_TRY(copy_dev(P, dst, P->o_tmp, P->M));
     KW_CUDA(cudaStreamSynchronize(P->stream));
     return KW_OK;
@@ -1069,8 +1079,13 @@ kw_status run_steps(kw_plan *P, uint64_t n) {
     for (uint64_t k = 0; k < n && P->t <= P->index_end; ++k) KW_TRY(run_step(P));
     if (P->time_rev && P->t > P->index_end) {
         k_tr_final<<<(P->M + 255) / 256, 256, 0, P->stream>>>(P->sidx, P->M, P->tr_data, P->p);
-        KW_TRY(check_launch());
+        KW_TRY(launched(P));
     }
+    return KW_OK;
+}
+
+kw_status use_device(const kw_plan *P) {
+    KW_CUDA(cudaSetDevice(P->device));
     return KW_OK;
 }
 
@@ -1118,11 +1133,13 @@ kw_status kw_plan_outputs(const kw_plan *P, kw_output_desc *d) {
 
 kw_status kw_reset(kw_plan *P) {
     if (!P) return fail(KW_ERR_INVALID, "plan is NULL");
+    KW_TRY(use_device(P));
     return zero_state(P);
 }
 
 kw_status kw_step(kw_plan *P, uint64_t n) {
     if (!P) return fail(KW_ERR_INVALID, "plan is NULL");
+    KW_TRY(use_device(P));
     KW_TRY(run_steps(P, n));
     KW_CUDA(cudaStreamSynchronize(P->stream));
     return KW_OK;
@@ -1130,6 +1147,7 @@ kw_status kw_step(kw_plan *P, uint64_t n) {
 
 kw_status kw_run_device(kw_plan *P) {
     if (!P) return fail(KW_ERR_INVALID, "plan is NULL");
+    KW_TRY(use_device(P));
     if (P->t != 1 || P->started) KW_TRY(zero_state(P));
     KW_TRY(run_steps(P, (uint64_t)P->index_end));
     KW_CUDA(cudaStreamSynchronize(P->stream));
@@ -1138,6 +1156,7 @@ kw_status kw_run_device(kw_plan *P) {
 
 kw_status kw_copy_outputs(kw_plan *P, kw_outputs *o) {
     if (!P || !o) return fail(KW_ERR_INVALID, "NULL argument");
+    KW_TRY(use_device(P));
     const size_t ser = (size_t)P->M * P->num_rec;
     KW_TRY(copy_dev(P, o->p, P->o_series[0], ser));
     KW_TRY(copy_dev(P, o->p_max, P->o_max[0], P->M));
@@ -1166,6 +1185,7 @@ kw_status kw_run(kw_plan *P, kw_outputs *o) {
 
 kw_status kw_plan_destroy(kw_plan *P) {
     if (!P) return KW_OK;
+    cudaSetDevice(P->device);
     if (P->stream) cudaStreamSynchronize(P->stream);
     for (auto &r : P->timers) { cudaEventDestroy(r.a); cudaEventDestroy(r.b); }
     for (void *a : P->allocs) cudaFree(a);
@@ -1188,6 +1208,37 @@ kw_status kw_get_timing(const kw_plan *Pc, int cls, double *ms, uint64_t *n) {
     KW_TRY(timer_flush(P));
     if (ms) *ms = P->t_ms[cls];
     if (n) *n = P->t_count[cls];
+    return KW_OK;
+}
+
+kw_status kw_run_timed(kw_plan *P, uint32_t n, double *device_ms) {
+    if (!P || !device_ms) return fail(KW_ERR_INVALID, "NULL argument");
+    KW_TRY(use_device(P));
+    cudaEvent_t a, b;
+    KW_CUDA(cudaEventCreate(&a));
+    KW_CUDA(cudaEventCreate(&b));
+    KW_CUDA(cudaStreamSynchronize(P->stream));
+    KW_CUDA(cudaEventRecord(a, P->stream));
+    kw_status st = KW_OK;
+    for (uint32_t k = 0; k < n && st == KW_OK; ++k) {
+        st = zero_state(P);
+        if (st == KW_OK) st = run_steps(P, (uint64_t)P->index_end);
+    }
+    cudaEventRecord(b, P->stream);
+    cudaEventSynchronize(b);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, a, b);
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    KW_TRY(st);
+    KW_CUDA(cudaGetLastError());
+    *device_ms = ms;
+    return KW_OK;
+}
+
+kw_status kw_launch_count(const kw_plan *P, uint64_t *launches) {
+    if (!P || !launches) return fail(KW_ERR_INVALID, "NULL argument");
+    *launches = P->launches;
     return KW_OK;
 }
 

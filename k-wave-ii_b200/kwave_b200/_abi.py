@@ -91,6 +91,7 @@ class kw_problem(C.Structure):
         ("time_reversal_input", f32p),
         ("inside_lo", C.c_uint64 * 3),
         ("inside_hi", C.c_uint64 * 3),
+        ("device", C.c_int32),
     ]
 
 
@@ -128,6 +129,8 @@ SYMBOLS = {
     "kw_set_timing": (C.c_int, [C.c_void_p, C.c_uint32]),
     "kw_get_timing": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_uint64)]),
     "kw_plan_device_bytes": (C.c_int, [C.c_void_p, C.POINTER(C.c_uint64)]),
+    "kw_run_timed": (C.c_int, [C.c_void_p, C.c_uint32, C.POINTER(C.c_double)]),
+    "kw_launch_count": (C.c_int, [C.c_void_p, C.POINTER(C.c_uint64)]),
 }
 
 _lib = None

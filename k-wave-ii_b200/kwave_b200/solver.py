@@ -36,7 +36,7 @@ _KNOWN_OPTIONS = {
     "MovieArgs", "MovieName", "MovieType", "MovieProfile", "PlotFreq", "PlotLayout", "PlotPML",
     "PlotScale", "PlotSim", "PMLAlpha", "PMLInside", "PMLSize", "RecordMovie", "ScaleSourceTerms",
     "Smooth", "UsekSpace", "UseSG", "StreamToDisk", "SaveToDisk", "SaveToDiskExit",
-    "HDFCompressionLevel", "MultiAxialPMLRatio", "PMLRange", "RadialSymmetry", "UseFD",
+    "HDFCompressionLevel", "MultiAxialPMLRatio", "PMLRange", "RadialSymmetry", "UseFD", "DeviceNum",
 }
 _DATA_CASTS = {"off", "double", "single", "gsingle", "gdouble", "GPUsingle", "GPUdouble",
                "gpuArray-single", "gpuArray-double"}
@@ -506,8 +506,10 @@ def _prepare(dim, kgrid, medium, source, sensor, options):
         pr.inside_lo[a] = inside[a][0]
         pr.inside_hi[a] = inside[a][1]
 
+    pr.device = int(options.get("DeviceNum", 0))
     P.problem = pr
     P.keep = keep
+    P.h2d_bytes = int(sum(a.nbytes for a in keep))
     P.record = record
     P.record_given = record_given
     P.time_rev = time_rev
@@ -558,6 +560,7 @@ class Simulation:
         _abi.check(self._lib.kw_plan_create(C.byref(self.prep.problem), C.byref(h)))
         self.handle = h
         self.prep.keep = None    # the library copied everything it needs
+        self.h2d_bytes = self.prep.h2d_bytes
         d = _abi.kw_output_desc()
         _abi.check(self._lib.kw_plan_outputs(self.handle, C.byref(d)))
         self.desc = d
@@ -600,6 +603,16 @@ class Simulation:
         n = C.c_uint64()
         _abi.check(self._lib.kw_get_timing(self.handle, _abi.KCLASS[cls], C.byref(ms), C.byref(n)))
         return ms.value, n.value
+
+    def run_timed(self, n):
+        ms = C.c_double()
+        _abi.check(self._lib.kw_run_timed(self.handle, n, C.byref(ms)))
+        return ms.value
+
+    def launch_count(self):
+        n = C.c_uint64()
+        _abi.check(self._lib.kw_launch_count(self.handle, C.byref(n)))
+        return n.value
 
     def device_bytes(self):
         b = C.c_uint64()

@@ -49,6 +49,9 @@ import scipy.fft as sfft
 
 _WORKERS = max(1, os.cpu_count() or 1)
 
+# wall-clock seconds spent in the time loop by the last kspace_first_order call
+LAST_LOOP_SECONDS = 0.0
+
 
 def fftn(a):
     return sfft.fftn(a, workers=_WORKERS)
@@ -698,6 +701,8 @@ def kspace_first_order(kgrid, medium, source, sensor, **opts):
     p_k = np.zeros(shape, dtype=complex)
     c2 = c0 ** 2
 
+    import time as _time
+    _t0 = _time.perf_counter()
     for t in range(1, index_end + 1):
         if time_rev:
             p = scatter_set(p, sensor_idx, trd[:, t - 1])
@@ -816,6 +821,8 @@ def kspace_first_order(kgrid, medium, source, sensor, **opts):
                 if "u_min_all" in record:
                     out[n + "_min_all"] = u[i][ins].copy() if fi == 1 else np.minimum(out[n + "_min_all"], u[i][ins])
 
+    global LAST_LOOP_SECONDS
+    LAST_LOOP_SECONDS = _time.perf_counter() - _t0
     if time_rev:
         p = scatter_set(p, sensor_idx, trd[:, index_end])
         record.add("p_final")
