@@ -215,6 +215,37 @@ kw_status kw_run_timed(kw_plan *plan, uint32_t n, double *device_ms);
 /* Number of kernels the plan has launched since creation. */
 kw_status kw_launch_count(const kw_plan *plan, uint64_t *launches);
 
+/*
+ * Allocation-free staggered spectral gradient.  No counterpart in the
+ * reference: it exists for callers that must not have this library allocate
+ * device memory -- a MEX function working on gpuArray data owned by MATLAB's
+ * memory pool, a PyTorch extension that takes every byte from the
+ * framework's caching allocator, or a service that forbids device
+ * allocation after start-up.
+ *
+ * Computes out = real(ifftn(d_k * kappa * fftn(field))) on the calling
+ * thread's current device, where d_k = i k exp(shift_sign * i k d / 2) along
+ * `axis` (0 = x, 1 = y, 2 = z; shift_sign +1 / -1 / 0 gives the reference's
+ * ddx_k_shift_pos / ddx_k_shift_neg / unstaggered operator,
+ * kspaceFirstOrder3D.m:629-650) and kappa = sinc(c_ref |k| dt / 2) when
+ * use_kspace is non-zero, else 1.  field and out are device pointers to
+ * column-major FP32 grids of shape[0] x shape[1] (x shape[2] in 3-D); they
+ * may alias.  `stream` is a cudaStream_t (NULL: the default stream); the
+ * call returns after the result is written.
+ *
+ * It calls no cudaMalloc or cudaFree.  Its only other device memory is one
+ * file-scope array of 32 MiB, held by every GPU that loads the library until
+ * the process exits; grids whose spectrum and operator tables do not fit
+ * (above about 4.1 million cells) are rejected with KW_ERR_UNSUPPORTED.  The
+ * first call on each device looks up the array's device address with that
+ * device current; make that first call before any stream capture.  Every call
+ * shares the array, so calls that overlap on the GPU (other host threads,
+ * other streams) race; issue them one at a time.
+ */
+kw_status kw_gradient_noalloc(int32_t dim, const uint64_t shape[3], const double spacing[3], int32_t axis,
+                              int32_t shift_sign, double c_ref, double dt, int32_t use_kspace,
+                              const float *field, float *out, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

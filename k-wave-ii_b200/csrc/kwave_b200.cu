@@ -15,6 +15,7 @@
 #include <cstdio>
 #include <cstring>
 #include <string>
+#include <mutex>
 #include <vector>
 
 #include "kw_kernels.cuh"
@@ -1092,6 +1093,48 @@ kw_status use_device(const kw_plan *P) {
 }  // namespace
 
 // --------------------------------------------------------------------------
+// Allocation-free spectral gradient (kw_gradient_noalloc)
+//
+// Some callers cannot let this library call cudaMalloc: a MATLAB MEX function
+// working on gpuArray data whose device memory belongs to MATLAB's pool, a
+// PyTorch extension that must draw every byte from the framework's caching
+// allocator, or a long-running service that forbids device allocation after
+// start-up because an allocation can block, fragment the heap or fail late.
+// kw_gradient_noalloc serves them: the caller passes device input and output
+// buffers, and the only other device memory it touches is the file-scope
+// array below.  That array is part of the module image, so every GPU that
+// loads this library holds it until the process exits.
+// --------------------------------------------------------------------------
+#define KW_NOALLOC_SCRATCH_BYTES ((size_t)32 << 20)
+static __device__ __align__(256) unsigned char g_noalloc_scratch[KW_NOALLOC_SCRATCH_BYTES];
+
+namespace {
+
+constexpr int kMaxDevices = 64;
+void *g_noalloc_base[kMaxDevices] = {nullptr};
+std::mutex g_noalloc_mutex;
+
+// Device address of the scratch array on the current device (resolved once
+// per device; host code may not use the symbol name as a device address).
+kw_status noalloc_base(int dev, void **base) {
+    if (dev < 0 || dev >= kMaxDevices) return fail(KW_ERR_UNSUPPORTED, "device ordinal %d above %d", dev, kMaxDevices);
+    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+    if (!g_noalloc_base[dev]) {
+        void *p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess || !p)
+            return fail(KW_ERR_CUDA, "cudaGetSymbolAddress of the scratch array failed: %s", cudaGetErrorString(e));
+        g_noalloc_base[dev] = p;
+    }
+    *base = g_noalloc_base[dev];
+    return KW_OK;
+}
+
+size_t align256(size_t v) { return (v + 255) & ~(size_t)255; }
+
+}  // namespace
+
+// --------------------------------------------------------------------------
 // C ABI
 // --------------------------------------------------------------------------
 extern "C" {
@@ -1239,6 +1282,127 @@ kw_status kw_run_timed(kw_plan *P, uint32_t n, double *device_ms) {
 kw_status kw_launch_count(const kw_plan *P, uint64_t *launches) {
     if (!P || !launches) return fail(KW_ERR_INVALID, "NULL argument");
     *launches = P->launches;
+    return KW_OK;
+}
+
+kw_status kw_gradient_noalloc(int32_t dim, const uint64_t shape[3], const double spacing[3], int32_t axis,
+                              int32_t shift_sign, double c_ref, double dt, int32_t use_kspace,
+                              const float *field, float *out, void *stream) {
+    if (dim != 2 && dim != 3) return fail(KW_ERR_INVALID, "dim must be 2 or 3");
+    if (!shape || !spacing || !field || !out) return fail(KW_ERR_INVALID, "NULL argument");
+    if (axis < 0 || axis >= dim) return fail(KW_ERR_INVALID, "axis must be 0..dim-1");
+    if (shift_sign != 1 && shift_sign != -1 && shift_sign != 0) return fail(KW_ERR_INVALID, "shift_sign must be +1, -1 or 0");
+    int n[3] = {1, 1, 1};
+    double d[3] = {1, 1, 1};
+    int phys_of_int[3] = {0, -1, 1};
+    if (dim == 3) {
+        for (int a = 0; a < 3; ++a) { n[a] = (int)shape[a]; d[a] = spacing[a]; phys_of_int[a] = a; }
+    } else {
+        n[0] = (int)shape[0]; d[0] = spacing[0];
+        n[2] = (int)shape[1]; d[2] = spacing[1];
+    }
+    for (int a = 0; a < dim; ++a) {
+        if (shape[a] < 2 || shape[a] > 4096) return fail(KW_ERR_UNSUPPORTED, "grid size outside 2..4096");
+        if (!(spacing[a] > 0)) return fail(KW_ERR_INVALID, "grid spacing must be positive");
+    }
+    if (n[2] > kCap / 2) return fail(KW_ERR_UNSUPPORTED, "axis length %d above %d", n[2], kCap / 2);
+    const int iaxis = dim == 3 ? axis : (axis == 0 ? 0 : 2);
+
+    kw_plan P;   // launch context only: no plan memory is allocated
+    P.D = dim;
+    for (int a = 0; a < 3; ++a) { P.N[a] = n[a]; P.d[a] = d[a]; }
+    Geom &g = P.g;
+    g.N0 = n[0]; g.N1 = n[1]; g.N2 = n[2];
+    g.N2h = g.N2 / 2 + 1;
+    g.N = (long long)g.N0 * g.N1 * g.N2;
+    g.Nh = (long long)g.N0 * g.N1 * g.N2h;
+    g.vec2 = (g.N0 % 2 == 0) ? 1 : 0;
+
+    // scratch layout: spectrum, then per-axis twiddles, wavenumbers^2 and the
+    // derivative operator of the requested axis
+    size_t off = 0;
+    const size_t o_spec = off; off = align256(off + (size_t)g.Nh * sizeof(float2));
+    size_t o_tw[3], o_k2[3];
+    for (int a = 0; a < 3; ++a) { o_tw[a] = off; off = align256(off + (size_t)n[a] * sizeof(float2)); }
+    for (int a = 0; a < 3; ++a) { o_k2[a] = off; off = align256(off + (size_t)n[a] * sizeof(float)); }
+    const size_t o_dd = off; off = align256(off + (size_t)n[iaxis] * sizeof(float2));
+    if (off > KW_NOALLOC_SCRATCH_BYTES)
+        return fail(KW_ERR_UNSUPPORTED, "grid needs %zu bytes of scratch; kw_gradient_noalloc is limited to %zu bytes "
+                    "(about 4.1 million cells)", off, (size_t)KW_NOALLOC_SCRATCH_BYTES);
+
+    int dev = 0;
+    KW_CUDA(cudaGetDevice(&dev));
+    void *basev = nullptr;
+    KW_TRY(noalloc_base(dev, &basev));
+    unsigned char *base = (unsigned char *)basev;
+    P.stream = (cudaStream_t)stream;
+
+    for (int a = 0; a < 3; ++a) {
+        std::vector<int> rad;
+        if (!factorize(n[a], rad)) return fail(KW_ERR_UNSUPPORTED, "grid size %d has a prime factor above 7", n[a]);
+        AxisFFT &f = P.fft[a];
+        f.n = n[a];
+        f.nstages = (int)rad.size();
+        for (size_t s2 = 0; s2 < rad.size(); ++s2) f.radix[s2] = rad[s2];
+        std::vector<float2> tw(n[a]);
+        for (int m = 0; m < n[a]; ++m) {
+            const double ang = -2.0 * M_PI * (double)m / n[a];
+            tw[m] = make_float2((float)std::cos(ang), (float)std::sin(ang));
+        }
+        std::vector<float> k2(n[a], 0.f);
+        if (phys_of_int[a] >= 0) {
+            const std::vector<double> k = kvec_fft(n[a], d[a]);
+            for (int i = 0; i < n[a]; ++i) k2[i] = (float)(k[i] * k[i]);
+        }
+        KW_CUDA(cudaMemcpyAsync(base + o_tw[a], tw.data(), tw.size() * sizeof(float2), cudaMemcpyHostToDevice, P.stream));
+        KW_CUDA(cudaMemcpyAsync(base + o_k2[a], k2.data(), k2.size() * sizeof(float), cudaMemcpyHostToDevice, P.stream));
+        f.tw = (const float2 *)(base + o_tw[a]);
+        P.op.k2[a] = (const float *)(base + o_k2[a]);
+        P.op.dd_pos[a] = P.op.dd_neg[a] = (const float2 *)(base + o_dd);
+    }
+    {
+        // i k exp(+-i k d/2) (kspaceFirstOrder3D.m:629-636), Hermitian part
+        const int na = n[iaxis];
+        const double da = d[iaxis];
+        const std::vector<double> k = kvec_fft(na, da);
+        std::vector<std::complex<double>> c(na);
+        for (int i = 0; i < na; ++i)
+            c[i] = std::complex<double>(0.0, k[i]) * std::exp(std::complex<double>(0.0, shift_sign * k[i] * da / 2));
+        std::vector<float2> dd(na);
+        for (int i = 0; i < na; ++i) {
+            const std::complex<double> h = 0.5 * (c[i] + std::conj(c[(na - i) % na]));
+            dd[i] = make_float2((float)h.real(), (float)h.imag());
+        }
+        KW_CUDA(cudaMemcpyAsync(base + o_dd, dd.data(), dd.size() * sizeof(float2), cudaMemcpyHostToDevice, P.stream));
+    }
+    P.op.kappa_a = (float)(c_ref * dt / 2.0);
+    P.op.use_kspace = use_kspace ? 1 : 0;
+    P.op.scale = (float)(1.0 / (double)g.N);
+    P.PL_z = choose_pl(kCap, g.N0, g.N1, g.N2);
+    {
+        int ty = 1;
+        while (ty * 2 <= 32 && ty * 2 * g.N1 <= kCap) ty *= 2;
+        P.TY = ty;
+        P.NL = std::max(1, kCap / g.N0);
+        const int lines = g.N1 * g.N2h;
+        if (P.NL > lines) P.NL = lines;
+        while (P.NL > 1 && (lines + P.NL - 1) / P.NL < 2 * 148) P.NL /= 2;
+    }
+    float2 *spec = (float2 *)(base + o_spec);
+    // the spectrum is fully written by the forward z-transform, so nothing
+    // left in the scratch by an earlier call is read
+    KW_TRY(zr2c(&P, field, spec));
+    Spec4 b{};
+    b.p[0] = spec;
+    KW_TRY(ypass(&P, false, b, 1));
+    OpSet ops{};
+    ops.n = 1;
+    ops.kind[0] = OP_GRAD_POS;
+    ops.axis[0] = iaxis;
+    KW_TRY(xpass(&P, b, ops, 1, 1));
+    KW_TRY(ypass(&P, true, b, 1));
+    KW_TRY(zc2r(&P, spec, out));
+    KW_CUDA(cudaStreamSynchronize(P.stream));
     return KW_OK;
 }
 

@@ -131,6 +131,9 @@ SYMBOLS = {
     "kw_plan_device_bytes": (C.c_int, [C.c_void_p, C.POINTER(C.c_uint64)]),
     "kw_run_timed": (C.c_int, [C.c_void_p, C.c_uint32, C.POINTER(C.c_double)]),
     "kw_launch_count": (C.c_int, [C.c_void_p, C.POINTER(C.c_uint64)]),
+    "kw_gradient_noalloc": (C.c_int, [C.c_int32, C.POINTER(C.c_uint64), C.POINTER(C.c_double), C.c_int32,
+                                      C.c_int32, C.c_double, C.c_double, C.c_int32, C.c_void_p, C.c_void_p,
+                                      C.c_void_p]),
 }
 
 _lib = None
