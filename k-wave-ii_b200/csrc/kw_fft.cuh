@@ -151,6 +151,72 @@ template <bool INV> struct Dft<7, INV> {
     static __device__ __forceinline__ void run(float2 *v) { DftOdd<7, INV>::run(v); }
 };
 
+// Radix-16 and radix-8 DFTs as 4x4 and 4x2 Cooley-Tukey splits in registers:
+// n = N2*n1 + n2, k = k1 + N1*k2; inner DFT over n1, twiddle w_N^(n2 k1),
+// outer DFT over n2.
+__device__ __forceinline__ float c16(int m) {
+    const float t[10] = {1.0f, 0.92387953251128674f, 0.70710678118654752f, 0.38268343236508977f, 0.0f,
+                         -0.38268343236508977f, -0.70710678118654752f, -0.92387953251128674f, -1.0f,
+                         -0.92387953251128674f};
+    return t[m];
+}
+__device__ __forceinline__ float s16(int m) {
+    const float t[10] = {0.0f, 0.38268343236508977f, 0.70710678118654752f, 0.92387953251128674f, 1.0f,
+                         0.92387953251128674f, 0.70710678118654752f, 0.38268343236508977f, 0.0f,
+                         -0.38268343236508977f};
+    return t[m];
+}
+// multiply by exp(-+ 2 pi i m / 16)
+template <bool INV>
+__device__ __forceinline__ float2 w16mul(float2 x, int m) {
+    const float c = c16(m), s = INV ? s16(m) : -s16(m);
+    return make_float2(x.x * c - x.y * s, x.x * s + x.y * c);
+}
+
+template <bool INV> struct Dft<16, INV> {
+    static __device__ __forceinline__ void run(float2 *v) {
+        float2 y[4][4];
+#pragma unroll
+        for (int n2 = 0; n2 < 4; ++n2) {
+            float2 a[4] = {v[n2], v[4 + n2], v[8 + n2], v[12 + n2]};
+            Dft<4, INV>::run(a);
+#pragma unroll
+            for (int k1 = 0; k1 < 4; ++k1) y[n2][k1] = a[k1];
+        }
+#pragma unroll
+        for (int n2 = 1; n2 < 4; ++n2)
+#pragma unroll
+            for (int k1 = 1; k1 < 4; ++k1) {
+                const int m = n2 * k1;
+                y[n2][k1] = (m == 4) ? mul_mi<INV>(y[n2][k1]) : w16mul<INV>(y[n2][k1], m);
+            }
+#pragma unroll
+        for (int k1 = 0; k1 < 4; ++k1) {
+            float2 b[4] = {y[0][k1], y[1][k1], y[2][k1], y[3][k1]};
+            Dft<4, INV>::run(b);
+#pragma unroll
+            for (int k2 = 0; k2 < 4; ++k2) v[k1 + 4 * k2] = b[k2];
+        }
+    }
+};
+
+template <bool INV> struct Dft<8, INV> {
+    static __device__ __forceinline__ void run(float2 *v) {
+        float2 a[4] = {v[0], v[2], v[4], v[6]};
+        float2 b[4] = {v[1], v[3], v[5], v[7]};
+        Dft<4, INV>::run(a);
+        Dft<4, INV>::run(b);
+        b[1] = w16mul<INV>(b[1], 2);
+        b[2] = mul_mi<INV>(b[2]);
+        b[3] = w16mul<INV>(b[3], 6);
+#pragma unroll
+        for (int k1 = 0; k1 < 4; ++k1) {
+            v[k1] = cadd(a[k1], b[k1]);
+            v[k1 + 4] = csub(a[k1], b[k1]);
+        }
+    }
+};
+
 // ---------------------------------------------------------------------------
 // one Stockham stage over a shared-memory tile
 // ---------------------------------------------------------------------------
@@ -219,6 +285,87 @@ __device__ void fft_tile(float2 *s, const AxisFFT &ax, int nl, int es, int ls, b
             default: break;
         }
         Ns *= R;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// compile-time transforms: the axis length N and the tile's line count are
+// template parameters, so every index split, stride and loop count below is a
+// constant.  Radix plan: 16, 8, 4, 2 while they divide, then 3, 5, 7.
+// ---------------------------------------------------------------------------
+__host__ __device__ constexpr int plan_next(int n) {
+    return n % 16 == 0 ? 16 : n % 8 == 0 ? 8 : n % 4 == 0 ? 4 : n % 2 == 0 ? 2 : n % 3 == 0 ? 3
+         : n % 5 == 0 ? 5 : n % 7 == 0 ? 7 : 0;
+}
+__host__ __device__ constexpr bool plan_ok(int n) {
+    return n == 1 ? true : (plan_next(n) == 0 ? false : plan_ok(n / plan_next(n)));
+}
+__host__ __device__ constexpr int pow2_floor(int v) { return v < 2 ? 1 : 2 * pow2_floor(v / 2); }
+
+// padded contiguous line layout: one pad slot after every 16 elements
+template <int N> struct Padded {
+    static constexpr int LS = N + (N + 15) / 16;
+    static __device__ __forceinline__ int at(int l, int i) { return l * LS + i + (i >> 4); }
+};
+
+// One stage; IL: lines interleaved (element (l, i) at s[i*NL + l], consecutive
+// threads take consecutive lines), else padded contiguous lines (consecutive
+// threads take consecutive butterflies of one line).
+template <int R, bool INV, int N, int NS, int NL, bool IL>
+__device__ __forceinline__ void stage_c(float2 *s, const float2 *__restrict__ tw) {
+    constexpr int NB = N / R;
+    constexpr int TOTAL = NB * NL;
+    constexpr int TWS = N / (NS * R);
+    constexpr int MAXB = (TOTAL + kThreads - 1) / kThreads;
+    float2 v[MAXB][R];
+#pragma unroll
+    for (int b = 0; b < MAXB; ++b) {
+        const int g = threadIdx.x + b * kThreads;
+        if (TOTAL % kThreads == 0 || g < TOTAL) {
+            const int l = IL ? g % NL : g / NB;
+            const int j = IL ? g / NL : g % NB;
+            const int k = j % NS;
+#pragma unroll
+            for (int t = 0; t < R; ++t) {
+                const int i = j + t * NB;
+                float2 x = IL ? s[i * NL + l] : s[Padded<N>::at(l, i)];
+                if (NS > 1 && t > 0) {
+                    float2 w = __ldg(tw + t * k * TWS);
+                    if (INV) w.y = -w.y;
+                    x = cmul(x, w);
+                }
+                v[b][t] = x;
+            }
+            Dft<R, INV>::run(v[b]);
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int b = 0; b < MAXB; ++b) {
+        const int g = threadIdx.x + b * kThreads;
+        if (TOTAL % kThreads == 0 || g < TOTAL) {
+            const int l = IL ? g % NL : g / NB;
+            const int j = IL ? g / NL : g % NB;
+            const int k = j % NS;
+            const int base = (j / NS) * NS * R + k;
+#pragma unroll
+            for (int t = 0; t < R; ++t) {
+                const int i = base + t * NS;
+                if (IL) s[i * NL + l] = v[b][t];
+                else s[Padded<N>::at(l, i)] = v[b][t];
+            }
+        }
+    }
+    __syncthreads();
+}
+
+template <int N, int NL, bool INV, bool IL, int REM = N, int NS = 1>
+__device__ __forceinline__ void fft_static(float2 *s, const float2 *__restrict__ tw) {
+    if constexpr (REM > 1) {
+        constexpr int R = plan_next(REM);
+        static_assert(R > 0, "axis length has a prime factor above 7");
+        stage_c<R, INV, N, NS, NL, IL>(s, tw);
+        fft_static<N, NL, INV, IL, REM / R, NS * R>(s, tw);
     }
 }
 

@@ -34,6 +34,15 @@ struct Geom {
 
 struct Spec4 { float2 *p[4]; };
 
+// Tile transform in the interleaved layout (element (l, i) at s[i*nl + l]):
+// compile-time plan when the axis length N is a template argument, the
+// runtime radix loop otherwise (N == 0).
+template <int N, int NL, bool INV>
+__device__ __forceinline__ void tile_fft_il(float2 *s, const AxisFFT &ax, int nl) {
+    if constexpr (N > 0) fft_static<N, NL, INV, true>(s, ax.tw);
+    else fft_tile<INV>(s, ax, nl, nl, 1, true);
+}
+
 // ---- scalar-or-array medium quantity -------------------------------------
 struct Med {
     const float *arr;
@@ -109,22 +118,46 @@ __device__ __forceinline__ float2 eval_op(const OpParams &P, int kind, int axis,
 // at one kz; lines interleaved (x fastest) so loads are coalesced rows.
 // grid = (ceil(N0/TY), N2h, nfields)
 // ---------------------------------------------------------------------------
-template <bool INV>
-__global__ void __launch_bounds__(kThreads, 2) k_ypass(Spec4 bufs, Geom g, AxisFFT ax, int TY) {
+template <bool INV, int N1S, int TYS>
+__global__ void __launch_bounds__(kThreads, 3) k_ypass(Spec4 bufs, Geom g, AxisFFT ax, int TYrt) {
     extern __shared__ float2 sm[];
+    const int N1 = N1S ? N1S : g.N1;
+    const int TY = TYS ? TYS : TYrt;
     float2 *buf = bufs.p[blockIdx.z];
     const int x0 = blockIdx.x * TY;
-    const long long base = (long long)blockIdx.y * g.N1 * g.N0;
-    const int tot = TY * g.N1;
-    for (int idx = threadIdx.x; idx < tot; idx += kThreads) {
-        const int l = idx % TY, y = idx / TY, x = x0 + l;
-        sm[idx] = x < g.N0 ? buf[base + (long long)y * g.N0 + x] : make_float2(0.f, 0.f);
+    const long long base = (long long)blockIdx.y * N1 * g.N0;
+    const bool vec = g.vec2 && (TY % 2 == 0) && (x0 + TY <= g.N0);
+    if (vec) {
+        const int half = TY / 2, tot2 = half * N1;
+#pragma unroll 4
+        for (int q = threadIdx.x; q < tot2; q += kThreads) {
+            const int c2 = q % half, y = q / half;
+            *reinterpret_cast<float4 *>(sm + y * TY + 2 * c2) =
+                *reinterpret_cast<const float4 *>(buf + base + (long long)y * g.N0 + x0 + 2 * c2);
+        }
+    } else {
+        const int tot = TY * N1;
+        for (int idx = threadIdx.x; idx < tot; idx += kThreads) {
+            const int l = idx % TY, y = idx / TY, x = x0 + l;
+            sm[idx] = x < g.N0 ? buf[base + (long long)y * g.N0 + x] : make_float2(0.f, 0.f);
+        }
     }
     __syncthreads();
-    fft_tile<INV>(sm, ax, TY, TY, 1, true);
-    for (int idx = threadIdx.x; idx < tot; idx += kThreads) {
-        const int l = idx % TY, y = idx / TY, x = x0 + l;
-        if (x < g.N0) buf[base + (long long)y * g.N0 + x] = sm[idx];
+    tile_fft_il<N1S, TYS, INV>(sm, ax, TY);
+    if (vec) {
+        const int half = TY / 2, tot2 = half * N1;
+#pragma unroll 4
+        for (int q = threadIdx.x; q < tot2; q += kThreads) {
+            const int c2 = q % half, y = q / half;
+            *reinterpret_cast<float4 *>(buf + base + (long long)y * g.N0 + x0 + 2 * c2) =
+                *reinterpret_cast<const float4 *>(sm + y * TY + 2 * c2);
+        }
+    } else {
+        const int tot = TY * N1;
+        for (int idx = threadIdx.x; idx < tot; idx += kThreads) {
+            const int l = idx % TY, y = idx / TY, x = x0 + l;
+            if (x < g.N0) buf[base + (long long)y * g.N0 + x] = sm[idx];
+        }
     }
 }
 
@@ -135,38 +168,77 @@ __global__ void __launch_bounds__(kThreads, 2) k_ypass(Spec4 bufs, Geom g, AxisF
 //   fanout == 1: field 0 is transformed once and ops[0..n-1] write fields 0..n-1
 // grid = (ceil(N1*N2h / NL), 1, fanout ? 1 : nfields)
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(kThreads, 2) k_xpass(Spec4 bufs, Geom g, AxisFFT ax, int NL, OpParams P,
-                                                     OpSet ops, int fanout) {
+template <int N0S, int NLS>
+__global__ void __launch_bounds__(kThreads, 3) k_xpass(Spec4 bufs, Geom g, AxisFFT ax, int NLrt, OpParams P,
+                                                        OpSet ops, int fanout) {
     extern __shared__ float2 sm[];
-    const int N0 = g.N0;
+    const int N0 = N0S ? N0S : g.N0;
+    const int NL = NLS ? NLS : NLrt;
+    // static sizes use padded contiguous lines; the runtime path plain ones
+    const int LS = N0S ? Padded<N0S>::LS : N0;
+    auto at = [&](int l, int i) { return N0S ? Padded<N0S>::at(l, i) : l * N0 + i; };
     const int lines_total = g.N1 * g.N2h;
     const int line0 = blockIdx.x * NL;
     const int nl = min(NL, lines_total - line0);
     const int f = fanout ? 0 : blockIdx.z;
     float2 *A = sm;
-    float2 *B = sm + NL * N0;
+    float2 *B = sm + NL * LS;
     const long long off = (long long)line0 * N0;
-    const int tot = nl * N0;
     {
         const float2 *in = bufs.p[f] + off;
-        for (int idx = threadIdx.x; idx < tot; idx += kThreads) A[idx] = in[idx];
+        if (N0 % 2 == 0) {
+            const int tot2 = NL * N0 / 2, valid2 = nl * N0 / 2;
+#pragma unroll 4
+            for (int q = threadIdx.x; q < tot2; q += kThreads) {
+                const int e = 2 * q, l = e / N0, i = e - l * N0;
+                float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+                if (q < valid2) v = *reinterpret_cast<const float4 *>(in + e);
+                A[at(l, i)] = make_float2(v.x, v.y);
+                A[at(l, i + 1)] = make_float2(v.z, v.w);
+            }
+        } else {
+            const int tot = NL * N0, valid = nl * N0;
+            for (int e = threadIdx.x; e < tot; e += kThreads) {
+                const int l = e / N0, i = e - l * N0;
+                A[at(l, i)] = e < valid ? in[e] : make_float2(0.f, 0.f);
+            }
+        }
     }
     __syncthreads();
-    fft_tile<false>(A, ax, nl, 1, N0, false);
+    if constexpr (N0S > 0) fft_static<N0S, NLS, false, false>(A, ax.tw);
+    else fft_tile<false>(A, ax, NL, 1, N0, false);
     const int nout = fanout ? ops.n : 1;
     for (int o = 0; o < nout; ++o) {
         const int oi = fanout ? o : f;
         float2 *W = fanout ? B : A;
-        for (int idx = threadIdx.x; idx < tot; idx += kThreads) {
-            const int l = idx / N0, ix = idx - l * N0;
+        const int tot = NL * N0;
+        for (int e = threadIdx.x; e < tot; e += kThreads) {
+            const int l = e / N0, ix = e - l * N0;
             const int line = line0 + l;
             const int iy = line % g.N1, iz = line / g.N1;
-            W[idx] = cmul(A[idx], eval_op(P, ops.kind[oi], ops.axis[oi], ix, iy, iz));
+            const int a = at(l, ix);
+            W[a] = line < lines_total ? cmul(A[a], eval_op(P, ops.kind[oi], ops.axis[oi], ix, iy, iz))
+                                      : make_float2(0.f, 0.f);
         }
         __syncthreads();
-        fft_tile<true>(W, ax, nl, 1, N0, false);
+        if constexpr (N0S > 0) fft_static<N0S, NLS, true, false>(W, ax.tw);
+        else fft_tile<true>(W, ax, NL, 1, N0, false);
         float2 *out = bufs.p[oi] + off;
-        for (int idx = threadIdx.x; idx < tot; idx += kThreads) out[idx] = W[idx];
+        if (N0 % 2 == 0) {
+            const int valid2 = nl * N0 / 2;
+#pragma unroll 4
+            for (int q = threadIdx.x; q < valid2; q += kThreads) {
+                const int e = 2 * q, l = e / N0, i = e - l * N0;
+                const float2 a0 = W[at(l, i)], a1 = W[at(l, i + 1)];
+                *reinterpret_cast<float4 *>(out + e) = make_float4(a0.x, a0.y, a1.x, a1.y);
+            }
+        } else {
+            const int valid = nl * N0;
+            for (int e = threadIdx.x; e < valid; e += kThreads) {
+                const int l = e / N0, i = e - l * N0;
+                out[e] = W[at(l, i)];
+            }
+        }
         __syncthreads();
     }
 }
@@ -175,15 +247,19 @@ __global__ void __launch_bounds__(kThreads, 2) k_xpass(Spec4 bufs, Geom g, AxisF
 // z-line tile helpers.  A tile is TX = 2*PL consecutive x at one y and every
 // z; packed element (l, z) at s[z*PL + l] holds (f(x0+2l), f(x0+2l+1)).
 // ---------------------------------------------------------------------------
+template <int N2S, int PLS>
 __device__ __forceinline__ void zload_c2r(float2 *s, const float2 *__restrict__ H, const Geom &g, int x0, int y,
-                                          int PL) {
-    const int N2 = g.N2, N0 = g.N0;
+                                          int PLrt) {
+    const int N2 = N2S ? N2S : g.N2, N0 = g.N0;
+    const int N2h = N2 / 2 + 1;
+    const int PL = PLS ? PLS : PLrt;
     const int tot = PL * N2;
+#pragma unroll 4
     for (int idx = threadIdx.x; idx < tot; idx += kThreads) {
         const int l = idx % PL, z = idx / PL;
         int k = z;
         bool cj = false;
-        if (z >= g.N2h) { k = N2 - z; cj = true; }
+        if (z >= N2h) { k = N2 - z; cj = true; }
         const int xa = x0 + 2 * l;
         const float2 *h = H + ((long long)k * g.N1 + y) * N0;
         float2 A, B;
@@ -201,14 +277,18 @@ __device__ __forceinline__ void zload_c2r(float2 *s, const float2 *__restrict__ 
     }
 }
 
+template <int N2S, int PLS>
 __device__ __forceinline__ void zstore_r2c(const float2 *s, float2 *__restrict__ H, const Geom &g, int x0, int y,
-                                           int PL) {
+                                           int PLrt) {
     const int N0 = g.N0;
-    const int tot = PL * g.N2h;
+    const int N2 = N2S ? N2S : g.N2;
+    const int PL = PLS ? PLS : PLrt;
+    const int tot = PL * (N2 / 2 + 1);
+#pragma unroll 4
     for (int idx = threadIdx.x; idx < tot; idx += kThreads) {
         const int l = idx % PL, k = idx / PL;
         const float2 Zk = s[k * PL + l];
-        const int nk = k == 0 ? 0 : g.N2 - k;
+        const int nk = k == 0 ? 0 : N2 - k;
         const float2 Zn = s[nk * PL + l];
         const float2 A = make_float2(0.5f * (Zk.x + Zn.x), 0.5f * (Zk.y - Zn.y));
         const float2 B = make_float2(0.5f * (Zk.y + Zn.y), -0.5f * (Zk.x - Zn.x));
@@ -223,9 +303,12 @@ __device__ __forceinline__ void zstore_r2c(const float2 *s, float2 *__restrict__
     }
 }
 
+template <int N2S, int PLS>
 __device__ __forceinline__ void zload_real(float2 *s, const float *__restrict__ R, const Geom &g, int x0, int y,
-                                           int PL) {
-    const int tot = PL * g.N2;
+                                           int PLrt) {
+    const int PL = PLS ? PLS : PLrt;
+    const int tot = PL * (N2S ? N2S : g.N2);
+#pragma unroll 4
     for (int idx = threadIdx.x; idx < tot; idx += kThreads) {
         const int l = idx % PL, z = idx / PL;
         const int xa = x0 + 2 * l;
@@ -294,25 +377,28 @@ struct StageU {
     int comp_axis[3];         // internal axis of velocity component f
 };
 
+template <int N2S, int PLS>
 __global__ void __launch_bounds__(kThreads, 2) k_stage_u(StageU a) {
     extern __shared__ float2 sm[];
     const Geom &g = a.g;
     const int f = blockIdx.z;
-    const int PL = a.PL, TX = 2 * PL;
+    const int PL = PLS ? PLS : a.PL, TX = 2 * PL;
+    const int N2 = N2S ? N2S : g.N2;
     const int x0 = blockIdx.x * TX, y = blockIdx.y;
     const int t = *a.d_t;
     float *u = a.u[f];
     const int ax = a.comp_axis[f];
     const float *pmlv = a.pml_sg[ax];
 
-    zload_c2r(sm, a.spec.p[f], g, x0, y, PL);
+    zload_c2r<N2S, PLS>(sm, a.spec.p[f], g, x0, y, PL);
     __syncthreads();
-    fft_tile<true>(sm, a.axz, PL, PL, 1, true);
+    tile_fft_il<N2S, PLS, true>(sm, a.axz, PL);
 
     float dscale = 0.f;
     const bool dense = dense_active(a.dense[f], t, dscale);
     const float pml_y = ax == 1 ? __ldg(pmlv + y) : 1.f;
-    const int tot = PL * g.N2;
+    const int tot = PL * N2;
+#pragma unroll 2
     for (int idx = threadIdx.x; idx < tot; idx += kThreads) {
         const int l = idx % PL, z = idx / PL;
         const int xa = x0 + 2 * l;
@@ -357,8 +443,8 @@ __global__ void __launch_bounds__(kThreads, 2) k_stage_u(StageU a) {
         __syncthreads();
     }
     if (!a.init && a.write_spec) {
-        fft_tile<false>(sm, a.axz, PL, PL, 1, true);
-        zstore_r2c(sm, a.spec.p[f], g, x0, y, PL);
+        tile_fft_il<N2S, PLS, false>(sm, a.axz, PL);
+        zstore_r2c<N2S, PLS>(sm, a.spec.p[f], g, x0, y, PL);
     }
 }
 
@@ -377,7 +463,8 @@ struct StageR {
     int PL;
     int D;
     Spec4 spec;
-    float *rho[3];
+    float *rho[3];            // values before this step's update
+    float *rho_out[3];        // updated values (double-buffered)
     float *p;
     Med rho0, c0, BonA, alpha_np;
     const float *pml[3];      // per internal axis
@@ -426,11 +513,13 @@ __device__ __forceinline__ void apply_tr(float2 *sm, const TRSrc &tr, const Geom
     }
 }
 
+template <int N2S, int PLS>
 __global__ void __launch_bounds__(kThreads, 2) k_stage_r(StageR a) {
     extern __shared__ float2 sm[];
     const Geom &g = a.g;
-    const int PL = a.PL, TX = 2 * PL;
-    const int tot = PL * g.N2;
+    const int PL = PLS ? PLS : a.PL, TX = 2 * PL;
+    const int N2 = N2S ? N2S : g.N2;
+    const int tot = PL * N2;
     float2 *tile = sm;
     float2 *acc_old = sm + tot;
     float2 *acc_rho = sm + 2 * tot;
@@ -460,13 +549,14 @@ __global__ void __launch_bounds__(kThreads, 2) k_stage_r(StageR a) {
     }
     for (int i = 0; i < a.D; ++i) {
         __syncthreads();
-        zload_c2r(tile, a.spec.p[i], g, x0, y, PL);
+        zload_c2r<N2S, PLS>(tile, a.spec.p[i], g, x0, y, PL);
         __syncthreads();
-        fft_tile<true>(tile, a.axz, PL, PL, 1, true);
+        tile_fft_il<N2S, PLS, true>(tile, a.axz, PL);
         const int ax = a.comp_axis[i];
         const float *pmlv = a.pml[ax];
         const float pml_y = ax == 1 ? __ldg(pmlv + y) : 1.f;
-        float *rho = a.rho[i];
+        const float *rho = a.rho[i];
+        float *rho_new = a.rho_out[i];
         for (int idx = threadIdx.x; idx < tot; idx += kThreads) {
             const int l = idx % PL, z = idx / PL;
             const int xa = x0 + 2 * l;
@@ -493,7 +583,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_stage_r(StageR a) {
                 rn.x = fmaf(dscale, F.x, rn.x);
                 rn.y = fmaf(dscale, F.y, rn.y);
             }
-            st2(rho, gi, rn, two, g.vec2);
+            st2(rho_new, gi, rn, two, g.vec2);
             float2 ar = acc_rho[idx], ad = acc_du[idx];
             ar.x += rn.x; ar.y += rn.y;
             ad.x += du.x; ad.y += du.y;
@@ -513,8 +603,8 @@ __global__ void __launch_bounds__(kThreads, 2) k_stage_r(StageR a) {
             const long long gi = x0 + xl + (long long)g.N0 * (y + (long long)g.N1 * z);
             float s = 0.f;
             for (int i = 0; i < a.D; ++i) {
-                const float nv = a.sparse.mode == 0 ? v : a.rho[i][gi] + v;
-                a.rho[i][gi] = nv;
+                const float nv = a.sparse.mode == 0 ? v : a.rho_out[i][gi] + v;
+                a.rho_out[i][gi] = nv;
                 s += nv;
             }
             float *slot = reinterpret_cast<float *>(acc_rho + z * PL + (xl >> 1)) + (xl & 1);
@@ -562,18 +652,18 @@ __global__ void __launch_bounds__(kThreads, 2) k_stage_r(StageR a) {
     }
     __syncthreads();
     if (!absorbing) {
-        apply_tr(tile, a.tr, g, PL, x0, y, t, a.rho[0], a.rho[1], a.rho[2], a.D, a.c0, a.p);
+        apply_tr(tile, a.tr, g, PL, x0, y, t, a.rho_out[0], a.rho_out[1], a.rho_out[2], a.D, a.c0, a.p);
         __syncthreads();
         if (a.write_spec) {
-            fft_tile<false>(tile, a.axz, PL, PL, 1, true);
-            zstore_r2c(tile, a.spec.p[0], g, x0, y, PL);
+            tile_fft_il<N2S, PLS, false>(tile, a.axz, PL);
+            zstore_r2c<N2S, PLS>(tile, a.spec.p[0], g, x0, y, PL);
         }
         return;
     }
     int out = 0;
     if (a.has_tau) {
-        fft_tile<false>(acc_old, a.axz, PL, PL, 1, true);
-        zstore_r2c(acc_old, a.spec.p[out++], g, x0, y, PL);
+        tile_fft_il<N2S, PLS, false>(acc_old, a.axz, PL);
+        zstore_r2c<N2S, PLS>(acc_old, a.spec.p[out++], g, x0, y, PL);
     }
     if (a.has_eta) {
         for (int idx = threadIdx.x; idx < tot; idx += kThreads) {
@@ -585,8 +675,8 @@ __global__ void __launch_bounds__(kThreads, 2) k_stage_r(StageR a) {
             tile[idx] = sr;
         }
         __syncthreads();
-        fft_tile<false>(tile, a.axz, PL, PL, 1, true);
-        zstore_r2c(tile, a.spec.p[out++], g, x0, y, PL);
+        tile_fft_il<N2S, PLS, false>(tile, a.axz, PL);
+        zstore_r2c<N2S, PLS>(tile, a.spec.p[out++], g, x0, y, PL);
     }
 }
 
@@ -612,11 +702,13 @@ struct StageP {
     const int *d_t;
 };
 
+template <int N2S, int PLS>
 __global__ void __launch_bounds__(kThreads, 2) k_stage_p(StageP a) {
     extern __shared__ float2 sm[];
     const Geom &g = a.g;
-    const int PL = a.PL, TX = 2 * PL;
-    const int tot = PL * g.N2;
+    const int PL = PLS ? PLS : a.PL, TX = 2 * PL;
+    const int N2 = N2S ? N2S : g.N2;
+    const int tot = PL * N2;
     float2 *tile = sm;
     float2 *acc = sm + tot;
     const int x0 = blockIdx.x * TX, y = blockIdx.y;
@@ -627,9 +719,9 @@ __global__ void __launch_bounds__(kThreads, 2) k_stage_p(StageP a) {
         if (term == 0 && !a.has_tau) continue;
         if (term == 1 && !a.has_eta) continue;
         __syncthreads();
-        zload_c2r(tile, a.spec.p[in++], g, x0, y, PL);
+        zload_c2r<N2S, PLS>(tile, a.spec.p[in++], g, x0, y, PL);
         __syncthreads();
-        fft_tile<true>(tile, a.axz, PL, PL, 1, true);
+        tile_fft_il<N2S, PLS, true>(tile, a.axz, PL);
         for (int idx = threadIdx.x; idx < tot; idx += kThreads) {
             const int l = idx % PL, z = idx / PL;
             const int xa = x0 + 2 * l;
@@ -673,32 +765,38 @@ __global__ void __launch_bounds__(kThreads, 2) k_stage_p(StageP a) {
     apply_tr(tile, a.tr, g, PL, x0, y, t, a.rho[0], a.rho[1], a.rho[2], a.D, a.c0, a.p);
     __syncthreads();
     if (a.write_spec) {
-        fft_tile<false>(tile, a.axz, PL, PL, 1, true);
-        zstore_r2c(tile, a.spec.p[0], g, x0, y, PL);
+        tile_fft_il<N2S, PLS, false>(tile, a.axz, PL);
+        zstore_r2c<N2S, PLS>(tile, a.spec.p[0], g, x0, y, PL);
     }
 }
 
 // ---------------------------------------------------------------------------
 // plain z-transforms (setup, p0 start, time-reversal start, source filtering)
 // ---------------------------------------------------------------------------
+template <int N2S, int PLS>
 __global__ void __launch_bounds__(kThreads, 2) k_zr2c(const float *__restrict__ R, float2 *H, Geom g, AxisFFT axz,
-                                                    int PL) {
+                                                    int PLrt) {
     extern __shared__ float2 sm[];
+    const int PL = PLS ? PLS : PLrt;
     const int x0 = blockIdx.x * 2 * PL, y = blockIdx.y;
-    zload_real(sm, R, g, x0, y, PL);
+    zload_real<N2S, PLS>(sm, R, g, x0, y, PL);
     __syncthreads();
-    fft_tile<false>(sm, axz, PL, PL, 1, true);
-    zstore_r2c(sm, H, g, x0, y, PL);
+    tile_fft_il<N2S, PLS, false>(sm, axz, PL);
+    zstore_r2c<N2S, PLS>(sm, H, g, x0, y, PL);
 }
 
+template <int N2S, int PLS>
 __global__ void __launch_bounds__(kThreads, 2) k_zc2r(const float2 *__restrict__ H, float *R, Geom g, AxisFFT axz,
-                                                    int PL) {
+                                                    int PLrt) {
     extern __shared__ float2 sm[];
+    const int PL = PLS ? PLS : PLrt;
+    const int N2 = N2S ? N2S : g.N2;
     const int x0 = blockIdx.x * 2 * PL, y = blockIdx.y;
-    zload_c2r(sm, H, g, x0, y, PL);
+    zload_c2r<N2S, PLS>(sm, H, g, x0, y, PL);
     __syncthreads();
-    fft_tile<true>(sm, axz, PL, PL, 1, true);
-    const int tot = PL * g.N2;
+    tile_fft_il<N2S, PLS, true>(sm, axz, PL);
+    const int tot = PL * N2;
+#pragma unroll 2
     for (int idx = threadIdx.x; idx < tot; idx += kThreads) {
         const int l = idx % PL, z = idx / PL;
         const int xa = x0 + 2 * l;

@@ -1,0 +1,744 @@
+// kw_static.cuh -- register-staged transform passes for compile-time axis lengths.
+//
+// Same algorithms as kw_kernels.cuh (Stockham transforms, fused physics
+// stages), organised so that data crosses shared memory as little as
+// possible:
+//   * the first radix stage of every transform loads its butterfly inputs
+//     straight from global memory (or from registers), the last stage hands
+//     its outputs to a consumer in registers; only the stages in between
+//     exchange through shared memory (one exchange for N <= 256);
+//   * an inverse transform runs the forward radix plan reversed, so the
+//     inverse's last stage and a following forward's first stage own the same
+//     elements in the same thread: "inverse -> physics -> forward" (z-stages)
+//     and "forward -> operator -> inverse" (x-pass) stay in registers.
+#pragma once
+
+#include "kw_kernels.cuh"
+
+namespace kw {
+
+__host__ __device__ constexpr int rs_stages(int n) {
+    int m = 0;
+    while (n > 1) { n /= plan_next(n); ++m; }
+    return m;
+}
+__host__ __device__ constexpr int rs_radix(int n, int s) {
+    for (int k = 0; k < s; ++k) n /= plan_next(n);
+    return plan_next(n);
+}
+
+template <int N, bool INV> struct RPlan {
+    static constexpr int M = rs_stages(N);
+    __host__ __device__ static constexpr int R(int s) { return INV ? rs_radix(N, M - 1 - s) : rs_radix(N, s); }
+    __host__ __device__ static constexpr int NS(int s) {
+        int p = 1;
+        for (int k = 0; k < s; ++k) p *= R(k);
+        return p;
+    }
+};
+
+// element (l, i) of a tile: interleaved lines (i*NL + l) or padded rows
+template <int N, int NL, bool IL>
+__device__ __forceinline__ int tat(int l, int i) {
+    if constexpr (IL) return i * NL + l;
+    else return Padded<N>::at(l, i);
+}
+
+// butterfly g of a stage with NB butterflies per line -> (line, butterfly)
+template <int NB, int NL, bool IL>
+__device__ __forceinline__ void bmap(int g, int &l, int &j) {
+    if constexpr (IL) { l = g % NL; j = g / NL; }
+    else { j = g % NB; l = g / NB; }
+}
+
+// Registers a thread owns after stage S of plan (N, INV): MAXB butterflies of R values.
+template <int N, int NL, bool INV, int S> struct StageShape {
+    static constexpr int R = RPlan<N, INV>::R(S);
+    static constexpr int NB = N / R;
+    static constexpr int TOT = NB * NL;
+    static constexpr int MAXB = (TOT + kThreads - 1) / kThreads;
+};
+// the shape of the registers handed between an inverse's last stage and a
+// forward's first stage (identical by construction)
+template <int N, int NL> using HandShape = StageShape<N, NL, false, 0>;
+
+template <int N, int NL, bool IL, bool INV, int S, class Ld, class St>
+__device__ __forceinline__ void rs_stage(float2 *sm, const float2 *__restrict__ tw, Ld &ld, St &st) {
+    using P = RPlan<N, INV>;
+    using SH = StageShape<N, NL, INV, S>;
+    constexpr int M = P::M, R = SH::R, NS = P::NS(S), NB = SH::NB;
+    constexpr int TOT = SH::TOT, MAXB = SH::MAXB;
+    constexpr int TWS = N / (NS * R);
+    float2 v[MAXB][R];
+#pragma unroll
+    for (int b = 0; b < MAXB; ++b) {
+        const int g = threadIdx.x + b * kThreads;
+        if (TOT % kThreads == 0 || g < TOT) {
+            int l, j;
+            bmap<NB, NL, IL>(g, l, j);
+#pragma unroll
+            for (int t = 0; t < R; ++t) {
+                const int i = j + t * NB;
+                if constexpr (S == 0) v[b][t] = ld(b, t, l, i);
+                else v[b][t] = sm[tat<N, NL, IL>(l, i)];
+            }
+            if constexpr (NS > 1) {
+                const int k = j % NS;
+#pragma unroll
+                for (int t = 1; t < R; ++t) {
+                    float2 w = __ldg(tw + t * k * TWS);
+                    if (INV) w.y = -w.y;
+                    v[b][t] = cmul(v[b][t], w);
+                }
+            }
+            Dft<R, INV>::run(v[b]);
+        }
+    }
+    if constexpr (S == M - 1) {
+#pragma unroll
+        for (int b = 0; b < MAXB; ++b) {
+            const int g = threadIdx.x + b * kThreads;
+            if (TOT % kThreads == 0 || g < TOT) {
+                int l, j;
+                bmap<NB, NL, IL>(g, l, j);
+                const int base = (j / NS) * NS * R + j % NS;
+#pragma unroll
+                for (int t = 0; t < R; ++t) st(b, t, l, base + t * NS, v[b][t]);
+            }
+        }
+    } else {
+        __syncthreads();   // earlier readers of the tile are done
+#pragma unroll
+        for (int b = 0; b < MAXB; ++b) {
+            const int g = threadIdx.x + b * kThreads;
+            if (TOT % kThreads == 0 || g < TOT) {
+                int l, j;
+                bmap<NB, NL, IL>(g, l, j);
+                const int base = (j / NS) * NS * R + j % NS;
+#pragma unroll
+                for (int t = 0; t < R; ++t) sm[tat<N, NL, IL>(l, base + t * NS)] = v[b][t];
+            }
+        }
+        __syncthreads();
+    }
+}
+
+template <int N, int NL, bool IL, bool INV, int S = 0, class Ld, class St>
+__device__ __forceinline__ void rs_fft(float2 *sm, const float2 *__restrict__ tw, Ld &ld, St &st) {
+    rs_stage<N, NL, IL, INV, S>(sm, tw, ld, st);
+    if constexpr (S + 1 < RPlan<N, INV>::M) rs_fft<N, NL, IL, INV, S + 1>(sm, tw, ld, st);
+}
+
+// (line, element) owned by hand-off register (b, t)
+template <int N, int NL, bool IL>
+__device__ __forceinline__ bool hand_pos(int b, int t, int &l, int &i) {
+    using SH = HandShape<N, NL>;
+    const int g = threadIdx.x + b * kThreads;
+    if (!(SH::TOT % kThreads == 0 || g < SH::TOT)) return false;
+    int j;
+    bmap<SH::NB, NL, IL>(g, l, j);
+    i = j + t * SH::NB;
+    return true;
+}
+
+// sinc(a) = sin(a)/a and cos(a) from their Taylor series in a^2 (Horner form).
+// The k-space argument is a = c_ref |k| dt / 2 <= (CFL c_ref / c_max) pi sqrt(3) / 2,
+// below 2.8 for any CFL <= 1; the first omitted terms (a^16/17! and
+// a^18/18!) are then below 1e-7 and 1.7e-8.
+__device__ __forceinline__ float sinc_series(float a2) {
+    // sin(a)/a = sum_n (-1)^n a^(2n) / (2n+1)!, n = 0..7
+    float r = -1.0f / 1307674368000.0f;           // n = 7: -1/15!
+    r = fmaf(r, a2, 1.0f / 6227020800.0f);        // n = 6: +1/13!
+    r = fmaf(r, a2, -1.0f / 39916800.0f);         // n = 5: -1/11!
+    r = fmaf(r, a2, 1.0f / 362880.0f);            // n = 4: +1/9!
+    r = fmaf(r, a2, -1.0f / 5040.0f);             // n = 3: -1/7!
+    r = fmaf(r, a2, 1.0f / 120.0f);               // n = 2: +1/5!
+    r = fmaf(r, a2, -1.0f / 6.0f);                // n = 1: -1/3!
+    r = fmaf(r, a2, 1.0f);                        // n = 0
+    return r;
+}
+__device__ __forceinline__ float cos_series(float a2) {
+    // cos(a) = sum_n (-1)^n a^(2n) / (2n)!, n = 0..8
+    float r = 1.0f / 20922789888000.0f;           // n = 8: +1/16!
+    r = fmaf(r, a2, -1.0f / 87178291200.0f);      // n = 7: -1/14!
+    r = fmaf(r, a2, 1.0f / 479001600.0f);         // n = 6: +1/12!
+    r = fmaf(r, a2, -1.0f / 3628800.0f);          // n = 5: -1/10!
+    r = fmaf(r, a2, 1.0f / 40320.0f);             // n = 4: +1/8!
+    r = fmaf(r, a2, -1.0f / 720.0f);              // n = 3: -1/6!
+    r = fmaf(r, a2, 1.0f / 24.0f);                // n = 2: +1/4!
+    r = fmaf(r, a2, -0.5f);                       // n = 1: -1/2!
+    r = fmaf(r, a2, 1.0f);                        // n = 0
+    return r;
+}
+
+// Tile widths of the compile-time kernels: as many lines as fill one
+// 4096-element tile, so every thread owns one radix-R butterfly.
+__host__ __device__ constexpr int ks_lines(int n) {
+    return pow2_floor(kCap / n) < 64 ? pow2_floor(kCap / n) : 64;
+}
+
+// ---------------------------------------------------------------------------
+// y-pass (C2C along axis 1, in place).  grid = (ceil(N0/TY), N2h, nfields)
+// ---------------------------------------------------------------------------
+template <bool INV, int N1>
+__global__ void __launch_bounds__(kThreads, 3) ks_ypass(Spec4 bufs, Geom g, const float2 *__restrict__ tw) {
+    constexpr int TY = ks_lines(N1);
+    static_assert(RPlan<N1, false>::M >= 2, "in-place pass needs two stages");
+    __shared__ float2 sm[N1 * TY];
+    float2 *buf = bufs.p[blockIdx.z];
+    const int x0 = blockIdx.x * TY;
+    const long long base = (long long)blockIdx.y * N1 * g.N0 + x0;
+    const int N0 = g.N0;
+    auto ld = [&](int, int, int l, int i) -> float2 {
+        return x0 + l < N0 ? buf[base + (long long)i * N0 + l] : make_float2(0.f, 0.f);
+    };
+    auto st = [&](int, int, int l, int i, float2 v) {
+        if (x0 + l < N0) buf[base + (long long)i * N0 + l] = v;
+    };
+    rs_fft<N1, TY, true, INV>(sm, tw, ld, st);
+}
+
+// ---------------------------------------------------------------------------
+// x-pass: forward C2C along axis 0, operator, inverse C2C, in place.
+// grid = (ceil(N1*N2h/NL), 1, fanout ? 1 : nfields)
+// ---------------------------------------------------------------------------
+template <int N0>
+__global__ void __launch_bounds__(kThreads, 3) ks_xpass(Spec4 bufs, Geom g, const float2 *__restrict__ tw,
+                                                         OpParams P, OpSet ops, int fanout) {
+    constexpr int NL = ks_lines(N0);
+    static_assert(RPlan<N0, false>::M >= 2, "in-place pass needs two stages");
+    __shared__ float2 sm[NL * Padded<N0>::LS];
+    __shared__ float kyz2[NL];
+    __shared__ int liy[NL], liz[NL];
+    const int lines_total = g.N1 * g.N2h;
+    const int line0 = blockIdx.x * NL;
+    const int f = fanout ? 0 : blockIdx.z;
+    for (int l = threadIdx.x; l < NL; l += kThreads) {
+        const int line = min(line0 + l, lines_total - 1);
+        const int iy = line % g.N1, iz = line / g.N1;
+        liy[l] = iy;
+        liz[l] = iz;
+        kyz2[l] = __ldg(P.k2[1] + iy) + __ldg(P.k2[2] + iz);
+    }
+    __syncthreads();
+    const float2 *in = bufs.p[f] + (long long)line0 * N0;
+    auto ld = [&](int, int, int l, int i) -> float2 {
+        return line0 + l < lines_total ? in[l * N0 + i] : make_float2(0.f, 0.f);
+    };
+    using SH = StageShape<N0, NL, false, RPlan<N0, false>::M - 1>;   // forward last stage
+    float2 spec[SH::MAXB][SH::R];
+    auto keep = [&](int b, int t, int, int, float2 v) { spec[b][t] = v; };
+    rs_fft<N0, NL, false, false>(sm, tw, ld, keep);
+
+    // common factor of the operator (kappa, |k|^e or cos), times 1/N
+    const int kind0 = ops.kind[f];
+    const bool grad = kind0 == OP_GRAD_POS || kind0 == OP_GRAD_NEG;
+#pragma unroll
+    for (int b = 0; b < SH::MAXB; ++b) {
+        const int gg = threadIdx.x + b * kThreads;
+        if (!(SH::TOT % kThreads == 0 || gg < SH::TOT)) continue;
+        int l, j;
+        bmap<SH::NB, NL, false>(gg, l, j);
+        const float ky = kyz2[l];
+        constexpr int NSL = RPlan<N0, false>::NS(RPlan<N0, false>::M - 1);
+#pragma unroll
+        for (int t = 0; t < SH::R; ++t) {
+            const int ix = j + t * NSL;
+            const float k2 = __ldg(P.k2[0] + ix) + ky;
+            float fac;
+            if (grad) {
+                fac = P.use_kspace ? sinc_series(P.kappa_a * P.kappa_a * k2) : 1.f;
+            } else if (kind0 == OP_NABLA1 || kind0 == OP_NABLA2) {
+                const float e = kind0 == OP_NABLA1 ? P.nabla1_exp : P.nabla2_exp;
+                fac = k2 == 0.f ? (e > 0.f ? 0.f : (e == 0.f ? 1.f : 0.f)) : powf(k2, 0.5f * e);
+            } else if (kind0 == OP_SRC_KAPPA) {
+                fac = P.use_kspace ? cos_series(P.kappa_a * P.kappa_a * k2) : 1.f;
+            } else {
+                fac = 1.f;
+            }
+            spec[b][t] = cscale(spec[b][t], fac * P.scale);
+        }
+    }
+    const int nout = fanout ? ops.n : 1;
+    for (int o = 0; o < nout; ++o) {
+        const int oi = fanout ? o : f;
+        const int axis = ops.axis[oi];
+        const float2 *dd = ops.kind[oi] == OP_GRAD_POS ? P.dd_pos[axis] : P.dd_neg[axis];
+        const bool mul_dd = ops.kind[oi] == OP_GRAD_POS || ops.kind[oi] == OP_GRAD_NEG;
+        float2 *out = bufs.p[oi] + (long long)line0 * N0;
+        auto ld2 = [&](int b, int t, int l, int i) -> float2 {
+            if (!mul_dd) return spec[b][t];
+            const int idx = axis == 0 ? i : (axis == 1 ? liy[l] : liz[l]);
+            return cmul(spec[b][t], __ldg(dd + idx));
+        };
+        auto st2 = [&](int, int, int l, int i, float2 v) {
+            if (line0 + l < lines_total) out[l * N0 + i] = v;
+        };
+        rs_fft<N0, NL, false, true>(sm, tw, ld2, st2);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// z-tiles: TX = 2*PL consecutive x at one y, all z; hand-off register (b, t)
+// holds packed element (l, z) = (f(x0+2l), f(x0+2l+1)).
+// ---------------------------------------------------------------------------
+template <int N2>
+struct ZTile {
+    static constexpr int PL = ks_lines(N2);
+    static constexpr int TX = 2 * PL;
+    using SH = HandShape<N2, PL>;
+};
+
+// packed C2R input: element z of packed line l from the z-half spectrum
+template <int N2>
+__device__ __forceinline__ float2 zpack_load(const float2 *__restrict__ H, const Geom &g, int x0, int y, int l, int z) {
+    constexpr int N2h = N2 / 2 + 1;
+    int k = z;
+    bool cj = false;
+    if (z >= N2h) { k = N2 - z; cj = true; }
+    const int xa = x0 + 2 * l;
+    const float2 *h = H + ((long long)k * g.N1 + y) * g.N0;
+    float2 A, B;
+    if (g.vec2 && xa + 1 < g.N0) {
+        const float4 q = *reinterpret_cast<const float4 *>(h + xa);
+        A = make_float2(q.x, q.y);
+        B = make_float2(q.z, q.w);
+    } else {
+        A = xa < g.N0 ? h[xa] : make_float2(0.f, 0.f);
+        B = xa + 1 < g.N0 ? h[xa + 1] : make_float2(0.f, 0.f);
+    }
+    if (cj) { A.y = -A.y; B.y = -B.y; }
+    if (k == 0 || 2 * k == N2) { A.y = 0.f; B.y = 0.f; }
+    return make_float2(A.x - B.y, A.y + B.x);
+}
+
+// forward transform of the hand-off registers, then unpack and store the
+// z-half spectrum (two real columns per packed line)
+template <int N2, class Hold>
+__device__ __forceinline__ void zforward_store(float2 *sm, const float2 *__restrict__ tw, Hold &hold, float2 *H,
+                                               const Geom &g, int x0, int y) {
+    constexpr int PL = ZTile<N2>::PL;
+    using SL = StageShape<N2, PL, false, RPlan<N2, false>::M - 1>;   // forward last stage
+    float2 outv[SL::MAXB][SL::R];
+    int outi[SL::MAXB];
+    auto ld = [&](int b, int t, int, int) -> float2 { return hold[b][t]; };
+    auto st = [&](int b, int t, int l, int i, float2 v) {
+        outv[b][t] = v;
+        if (t == 0) outi[b] = i * PL + l;   // element i + t*NS of line l sits at outi + t*NS*PL
+    };
+    rs_fft<N2, PL, true, false>(sm, tw, ld, st);
+    __syncthreads();   // every thread has read its last-stage inputs from the tile
+    constexpr int NSL = RPlan<N2, false>::NS(RPlan<N2, false>::M - 1);
+#pragma unroll
+    for (int b = 0; b < SL::MAXB; ++b) {
+        const int gg = threadIdx.x + b * kThreads;
+        if (!(SL::TOT % kThreads == 0 || gg < SL::TOT)) continue;
+#pragma unroll
+        for (int t = 0; t < SL::R; ++t) sm[outi[b] + t * NSL * PL] = outv[b][t];
+    }
+    __syncthreads();
+    zstore_r2c<N2, PL>(sm, H, g, x0, y, PL);
+}
+
+// write hand-off registers into the tile (packed layout z*PL + l)
+template <int N2, class Hold>
+__device__ __forceinline__ void hold_to_smem(float2 *sm, Hold &hold) {
+    constexpr int PL = ZTile<N2>::PL;
+    using SH = typename ZTile<N2>::SH;
+#pragma unroll
+    for (int b = 0; b < SH::MAXB; ++b)
+#pragma unroll
+        for (int t = 0; t < SH::R; ++t) {
+            int l, i;
+            if (hand_pos<N2, PL, true>(b, t, l, i)) sm[i * PL + l] = hold[b][t];
+        }
+}
+template <int N2, class Hold>
+__device__ __forceinline__ void smem_to_hold(const float2 *sm, Hold &hold) {
+    constexpr int PL = ZTile<N2>::PL;
+    using SH = typename ZTile<N2>::SH;
+#pragma unroll
+    for (int b = 0; b < SH::MAXB; ++b)
+#pragma unroll
+        for (int t = 0; t < SH::R; ++t) {
+            int l, i;
+            if (hand_pos<N2, PL, true>(b, t, l, i)) hold[b][t] = sm[i * PL + l];
+        }
+}
+
+// ---------------------------------------------------------------------------
+// Stage U (momentum, velocity sources, forward z-transform of u); see k_stage_u.
+// grid = (ceil(N0/TX), N1, D)
+// ---------------------------------------------------------------------------
+template <int N2>
+__global__ void __launch_bounds__(kThreads, 2) ks_stage_u(StageU a, const float2 *__restrict__ tw) {
+    using ZT = ZTile<N2>;
+    using SH = typename ZT::SH;
+    constexpr int PL = ZT::PL, TX = ZT::TX;
+    static_assert(RPlan<N2, false>::M >= 2, "z-stages need two stages");
+    __shared__ float2 sm[N2 * PL];
+    const Geom &g = a.g;
+    const int f = blockIdx.z;
+    const int x0 = blockIdx.x * TX, y = blockIdx.y;
+    const int t = *a.d_t;
+    float *u = a.u[f];
+    const int ax = a.comp_axis[f];
+    const float *pmlv = a.pml_sg[ax];
+    const float2 *H = a.spec.p[f];
+
+    float2 hold[SH::MAXB][SH::R];
+    auto ld = [&](int, int, int l, int i) -> float2 { return zpack_load<N2>(H, g, x0, y, l, i); };
+    auto st = [&](int b, int tt, int, int, float2 v) { hold[b][tt] = v; };
+    rs_fft<N2, PL, true, true>(sm, tw, ld, st);
+
+    float dscale = 0.f;
+    const bool dense = dense_active(a.dense[f], t, dscale);
+    const float pml_y = ax == 1 ? __ldg(pmlv + y) : 1.f;
+#pragma unroll
+    for (int b = 0; b < SH::MAXB; ++b)
+#pragma unroll
+        for (int tt = 0; tt < SH::R; ++tt) {
+            int l, z;
+            if (!hand_pos<N2, PL, true>(b, tt, l, z)) continue;
+            const int xa = x0 + 2 * l;
+            if (xa >= g.N0) { hold[b][tt] = make_float2(0.f, 0.f); continue; }
+            const bool two = xa + 1 < g.N0;
+            const long long gi = xa + (long long)g.N0 * (y + (long long)g.N1 * z);
+            const float2 gr = hold[b][tt];
+            const float2 ri = med2(a.rho_sg_inv[f], gi, two, g.vec2);
+            float2 un;
+            if (a.init) {
+                un = make_float2(0.5f * a.dt * ri.x * gr.x, 0.5f * a.dt * ri.y * gr.y);
+            } else {
+                float2 pm;
+                if (ax == 0) pm = make_float2(__ldg(pmlv + xa), two ? __ldg(pmlv + xa + 1) : 1.f);
+                else if (ax == 1) pm = make_float2(pml_y, pml_y);
+                else { const float q = __ldg(pmlv + z); pm = make_float2(q, q); }
+                const float2 uo = ld2(u, gi, two, g.vec2);
+                un.x = pm.x * (pm.x * uo.x - a.dt * ri.x * gr.x);
+                un.y = pm.y * (pm.y * uo.y - a.dt * ri.y * gr.y);
+                if (dense) {
+                    const float2 F = ld2(a.dense[f].F, gi, two, g.vec2);
+                    un.x = fmaf(dscale, F.x, un.x);
+                    un.y = fmaf(dscale, F.y, un.y);
+                }
+            }
+            st2(u, gi, un, two, g.vec2);
+            hold[b][tt] = make_float2(un.x, two ? un.y : 0.f);
+        }
+    if (a.init || !a.write_spec) return;
+    if (a.sparse.off && a.sparse.sig[f] && t <= a.sparse.T[f]) {
+        const int tile = blockIdx.x + gridDim.x * blockIdx.y;
+        const int e0 = a.sparse.off[tile], e1 = a.sparse.off[tile + 1];
+        if (e1 > e0) {
+            __syncthreads();
+            hold_to_smem<N2>(sm, hold);
+            __syncthreads();
+            for (int e = e0 + threadIdx.x; e < e1; e += kThreads) {
+                const int c = a.sparse.cell[e];
+                const int z = c / TX, xl = c - z * TX;
+                const float v = __ldg(a.sparse.sig[f] + a.sparse.row[e] + (long long)a.sparse.nsig * (t - 1));
+                float *slot = reinterpret_cast<float *>(sm + z * PL + (xl >> 1)) + (xl & 1);
+                const float nv = a.sparse.mode == 0 ? v : *slot + v;
+                *slot = nv;
+                u[x0 + xl + (long long)g.N0 * (y + (long long)g.N1 * z)] = nv;
+            }
+            __syncthreads();
+            smem_to_hold<N2>(sm, hold);
+        }
+    }
+    zforward_store<N2>(sm, tw, hold, a.spec.p[f], g, x0, y);
+}
+
+// ---------------------------------------------------------------------------
+// Stage R (mass conservation, pressure sources, equation of state); see
+// k_stage_r.  rho is double-buffered: old values are read from a.rho, new
+// values written to a.rho_out, so the nonlinear coefficient
+// 2 * sum(rho_old) + rho0 can be re-read per component instead of held.
+// grid = (ceil(N0/TX), N1, 1)
+// ---------------------------------------------------------------------------
+template <int N2>
+__global__ void __launch_bounds__(kThreads, 2) ks_stage_r(StageR a, const float2 *__restrict__ tw) {
+    using ZT = ZTile<N2>;
+    using SH = typename ZT::SH;
+    constexpr int PL = ZT::PL, TX = ZT::TX;
+    __shared__ float2 sm[N2 * PL];
+    const Geom &g = a.g;
+    const int x0 = blockIdx.x * TX, y = blockIdx.y;
+    const int t = *a.d_t;
+    float dscale = 0.f;
+    const bool dense = dense_active(a.dense, t, dscale);
+
+    float2 acc_r[SH::MAXB][SH::R], acc_d[SH::MAXB][SH::R];
+#pragma unroll
+    for (int b = 0; b < SH::MAXB; ++b)
+#pragma unroll
+        for (int tt = 0; tt < SH::R; ++tt) {
+            acc_r[b][tt] = make_float2(0.f, 0.f);
+            acc_d[b][tt] = make_float2(0.f, 0.f);
+        }
+    for (int i = 0; i < a.D; ++i) {
+        float2 hold[SH::MAXB][SH::R];
+        const float2 *H = a.spec.p[i];
+        auto ld = [&](int, int, int l, int z) -> float2 { return zpack_load<N2>(H, g, x0, y, l, z); };
+        auto st = [&](int b, int tt, int, int, float2 v) { hold[b][tt] = v; };
+        __syncthreads();
+        rs_fft<N2, PL, true, true>(sm, tw, ld, st);
+        const int ax = a.comp_axis[i];
+        const float *pmlv = a.pml[ax];
+        const float pml_y = ax == 1 ? __ldg(pmlv + y) : 1.f;
+        const float *rin = a.rho[i];
+        float *rout = a.rho_out[i];
+#pragma unroll
+        for (int b = 0; b < SH::MAXB; ++b)
+#pragma unroll
+            for (int tt = 0; tt < SH::R; ++tt) {
+                int l, z;
+                if (!hand_pos<N2, PL, true>(b, tt, l, z)) continue;
+                const int xa = x0 + 2 * l;
+                if (xa >= g.N0) continue;
+                const bool two = xa + 1 < g.N0;
+                const long long gi = xa + (long long)g.N0 * (y + (long long)g.N1 * z);
+                const float2 du = hold[b][tt];
+                float2 coef = med2(a.rho0, gi, two, g.vec2);
+                if (a.nonlinear) {
+                    float2 so = make_float2(0.f, 0.f);
+                    for (int q = 0; q < a.D; ++q) {
+                        const float2 r = ld2(a.rho[q], gi, two, g.vec2);
+                        so.x += r.x;
+                        so.y += r.y;
+                    }
+                    coef.x += 2.f * so.x;
+                    coef.y += 2.f * so.y;
+                }
+                float2 pm;
+                if (ax == 0) pm = make_float2(__ldg(pmlv + xa), two ? __ldg(pmlv + xa + 1) : 1.f);
+                else if (ax == 1) pm = make_float2(pml_y, pml_y);
+                else { const float q = __ldg(pmlv + z); pm = make_float2(q, q); }
+                const float2 ro = ld2(rin, gi, two, g.vec2);
+                float2 rn;
+                rn.x = pm.x * (pm.x * ro.x - a.dt * coef.x * du.x);
+                rn.y = pm.y * (pm.y * ro.y - a.dt * coef.y * du.y);
+                if (dense) {
+                    const float2 F = ld2(a.dense.F, gi, two, g.vec2);
+                    rn.x = fmaf(dscale, F.x, rn.x);
+                    rn.y = fmaf(dscale, F.y, rn.y);
+                }
+                st2(rout, gi, rn, two, g.vec2);
+                acc_r[b][tt].x += rn.x;
+                acc_r[b][tt].y += rn.y;
+                acc_d[b][tt].x += du.x;
+                acc_d[b][tt].y += du.y;
+            }
+    }
+    // sparse pressure sources act on every rho component (:930-962)
+    if (a.sparse.off && t <= a.sparse.T[0]) {
+        const int tile = blockIdx.x + gridDim.x * blockIdx.y;
+        const int e0 = a.sparse.off[tile], e1 = a.sparse.off[tile + 1];
+        if (e1 > e0) {
+            __syncthreads();
+            hold_to_smem<N2>(sm, acc_r);
+            __syncthreads();
+            for (int e = e0 + threadIdx.x; e < e1; e += kThreads) {
+                const int c = a.sparse.cell[e];
+                const int z = c / TX, xl = c - z * TX;
+                const float v = __ldg(a.sparse.sig[0] + a.sparse.row[e] + (long long)a.sparse.nsig * (t - 1));
+                const long long gi = x0 + xl + (long long)g.N0 * (y + (long long)g.N1 * z);
+                float s = 0.f;
+                for (int i = 0; i < a.D; ++i) {
+                    const float nv = a.sparse.mode == 0 ? v : a.rho_out[i][gi] + v;
+                    a.rho_out[i][gi] = nv;
+                    s += nv;
+                }
+                *(reinterpret_cast<float *>(sm + z * PL + (xl >> 1)) + (xl & 1)) = s;
+            }
+            __syncthreads();
+            smem_to_hold<N2>(sm, acc_r);
+        }
+    }
+    // equation of state
+    const bool absorbing = a.eos == 1;
+#pragma unroll
+    for (int b = 0; b < SH::MAXB; ++b)
+#pragma unroll
+        for (int tt = 0; tt < SH::R; ++tt) {
+            int l, z;
+            if (!hand_pos<N2, PL, true>(b, tt, l, z)) continue;
+            const int xa = x0 + 2 * l;
+            float2 pv = make_float2(0.f, 0.f);
+            float2 rd = make_float2(0.f, 0.f);
+            if (xa < g.N0) {
+                const bool two = xa + 1 < g.N0;
+                const long long gi = xa + (long long)g.N0 * (y + (long long)g.N1 * z);
+                const float2 sr = acc_r[b][tt];
+                const float2 c = med2(a.c0, gi, two, g.vec2);
+                pv = sr;
+                if (a.eos == 2) {
+                    const float2 r0 = med2(a.rho0, gi, two, g.vec2);
+                    const float2 an = med2(a.alpha_np, gi, two, g.vec2);
+                    const float2 sd = acc_d[b][tt];
+                    pv.x += tau_of(an.x, c.x, 2.f, a.tau_sign) * r0.x * sd.x;
+                    pv.y += tau_of(an.y, c.y, 2.f, a.tau_sign) * r0.y * sd.y;
+                }
+                if (a.nonlinear) {
+                    const float2 r0 = med2(a.rho0, gi, two, g.vec2);
+                    const float2 bn = med2(a.BonA, gi, two, g.vec2);
+                    pv.x += bn.x * sr.x * sr.x / (2.f * r0.x);
+                    pv.y += bn.y * sr.y * sr.y / (2.f * r0.y);
+                }
+                pv.x *= c.x * c.x;
+                pv.y *= c.y * c.y;
+                st2(a.p, gi, pv, two, g.vec2);
+                if (absorbing && a.has_tau) {
+                    const float2 r0 = med2(a.rho0, gi, two, g.vec2);
+                    const float2 sd = acc_d[b][tt];
+                    rd = make_float2(r0.x * sd.x, r0.y * sd.y);
+                }
+                if (!two) { pv.y = 0.f; rd.y = 0.f; acc_r[b][tt].y = 0.f; }
+            } else {
+                acc_r[b][tt] = make_float2(0.f, 0.f);
+            }
+            acc_d[b][tt] = absorbing ? rd : pv;   // reuse as the next forward input
+        }
+    if (!absorbing) {
+        if (a.tr.off) {
+            __syncthreads();
+            hold_to_smem<N2>(sm, acc_d);
+            __syncthreads();
+            apply_tr(sm, a.tr, g, PL, x0, y, t, a.rho_out[0], a.rho_out[1], a.rho_out[2], a.D, a.c0, a.p);
+            __syncthreads();
+            smem_to_hold<N2>(sm, acc_d);
+        }
+        if (a.write_spec) zforward_store<N2>(sm, tw, acc_d, a.spec.p[0], g, x0, y);
+        return;
+    }
+    int out = 0;
+    if (a.has_tau) zforward_store<N2>(sm, tw, acc_d, a.spec.p[out++], g, x0, y);
+    if (a.has_eta) zforward_store<N2>(sm, tw, acc_r, a.spec.p[out++], g, x0, y);
+}
+
+// ---------------------------------------------------------------------------
+// Stage P: p = p_partial + c0^2 (tau A1 - eta A2), time reversal, forward z of p.
+// ---------------------------------------------------------------------------
+template <int N2>
+__global__ void __launch_bounds__(kThreads, 2) ks_stage_p(StageP a, const float2 *__restrict__ tw) {
+    using ZT = ZTile<N2>;
+    using SH = typename ZT::SH;
+    constexpr int PL = ZT::PL, TX = ZT::TX;
+    __shared__ float2 sm[N2 * PL];
+    const Geom &g = a.g;
+    const int x0 = blockIdx.x * TX, y = blockIdx.y;
+    const int t = *a.d_t;
+    float2 acc[SH::MAXB][SH::R];
+#pragma unroll
+    for (int b = 0; b < SH::MAXB; ++b)
+#pragma unroll
+        for (int tt = 0; tt < SH::R; ++tt) acc[b][tt] = make_float2(0.f, 0.f);
+    int in = 0;
+    for (int term = 0; term < 2; ++term) {
+        if (term == 0 && !a.has_tau) continue;
+        if (term == 1 && !a.has_eta) continue;
+        float2 hold[SH::MAXB][SH::R];
+        const float2 *H = a.spec.p[in++];
+        auto ld = [&](int, int, int l, int z) -> float2 { return zpack_load<N2>(H, g, x0, y, l, z); };
+        auto st = [&](int b, int tt, int, int, float2 v) { hold[b][tt] = v; };
+        __syncthreads();
+        rs_fft<N2, PL, true, true>(sm, tw, ld, st);
+#pragma unroll
+        for (int b = 0; b < SH::MAXB; ++b)
+#pragma unroll
+            for (int tt = 0; tt < SH::R; ++tt) {
+                int l, z;
+                if (!hand_pos<N2, PL, true>(b, tt, l, z)) continue;
+                const int xa = x0 + 2 * l;
+                if (xa >= g.N0) continue;
+                const bool two = xa + 1 < g.N0;
+                const long long gi = xa + (long long)g.N0 * (y + (long long)g.N1 * z);
+                const float2 c = med2(a.c0, gi, two, g.vec2);
+                const float2 an = med2(a.alpha_np, gi, two, g.vec2);
+                const float2 v = hold[b][tt];
+                if (term == 0) {
+                    acc[b][tt].x += tau_of(an.x, c.x, a.alpha_y, a.tau_sign) * v.x;
+                    acc[b][tt].y += tau_of(an.y, c.y, a.alpha_y, a.tau_sign) * v.y;
+                } else {
+                    acc[b][tt].x -= 2.f * an.x * powf(c.x, a.alpha_y) * a.tan_term * a.eta_sign * v.x;
+                    acc[b][tt].y -= 2.f * an.y * powf(c.y, a.alpha_y) * a.tan_term * a.eta_sign * v.y;
+                }
+            }
+    }
+#pragma unroll
+    for (int b = 0; b < SH::MAXB; ++b)
+#pragma unroll
+        for (int tt = 0; tt < SH::R; ++tt) {
+            int l, z;
+            if (!hand_pos<N2, PL, true>(b, tt, l, z)) continue;
+            const int xa = x0 + 2 * l;
+            float2 pv = make_float2(0.f, 0.f);
+            if (xa < g.N0) {
+                const bool two = xa + 1 < g.N0;
+                const long long gi = xa + (long long)g.N0 * (y + (long long)g.N1 * z);
+                const float2 c = med2(a.c0, gi, two, g.vec2);
+                const float2 pp = ld2(a.p, gi, two, g.vec2);
+                pv.x = fmaf(c.x * c.x, acc[b][tt].x, pp.x);
+                pv.y = fmaf(c.y * c.y, acc[b][tt].y, pp.y);
+                st2(a.p, gi, pv, two, g.vec2);
+                if (!two) pv.y = 0.f;
+            }
+            acc[b][tt] = pv;
+        }
+    if (a.tr.off) {
+        __syncthreads();
+        hold_to_smem<N2>(sm, acc);
+        __syncthreads();
+        apply_tr(sm, a.tr, g, PL, x0, y, t, a.rho[0], a.rho[1], a.rho[2], a.D, a.c0, a.p);
+        __syncthreads();
+        smem_to_hold<N2>(sm, acc);
+    }
+    if (a.write_spec) zforward_store<N2>(sm, tw, acc, a.spec.p[0], g, x0, y);
+}
+
+// ---------------------------------------------------------------------------
+// plain z-transforms
+// ---------------------------------------------------------------------------
+template <int N2>
+__global__ void __launch_bounds__(kThreads, 2) ks_zr2c(const float *__restrict__ R, float2 *H, Geom g,
+                                                        const float2 *__restrict__ tw) {
+    using ZT = ZTile<N2>;
+    using SH = typename ZT::SH;
+    constexpr int PL = ZT::PL, TX = ZT::TX;
+    __shared__ float2 sm[N2 * PL];
+    const int x0 = blockIdx.x * TX, y = blockIdx.y;
+    float2 hold[SH::MAXB][SH::R];
+#pragma unroll
+    for (int b = 0; b < SH::MAXB; ++b)
+#pragma unroll
+        for (int tt = 0; tt < SH::R; ++tt) {
+            int l, z;
+            hold[b][tt] = make_float2(0.f, 0.f);
+            if (!hand_pos<N2, PL, true>(b, tt, l, z)) continue;
+            const int xa = x0 + 2 * l;
+            if (xa >= g.N0) continue;
+            const long long gi = xa + (long long)g.N0 * (y + (long long)g.N1 * z);
+            hold[b][tt] = ld2(R, gi, xa + 1 < g.N0, g.vec2);
+        }
+    zforward_store<N2>(sm, tw, hold, H, g, x0, y);
+}
+
+template <int N2>
+__global__ void __launch_bounds__(kThreads, 2) ks_zc2r(const float2 *__restrict__ H, float *R, Geom g,
+                                                        const float2 *__restrict__ tw) {
+    using ZT = ZTile<N2>;
+    constexpr int PL = ZT::PL, TX = ZT::TX;
+    __shared__ float2 sm[N2 * PL];
+    const int x0 = blockIdx.x * TX, y = blockIdx.y;
+    auto ld = [&](int, int, int l, int z) -> float2 { return zpack_load<N2>(H, g, x0, y, l, z); };
+    auto st = [&](int, int, int l, int z, float2 v) {
+        const int xa = x0 + 2 * l;
+        if (xa >= g.N0) return;
+        const long long gi = xa + (long long)g.N0 * (y + (long long)g.N1 * z);
+        st2(R, gi, v, xa + 1 < g.N0, g.vec2);
+    };
+    rs_fft<N2, PL, true, true>(sm, tw, ld, st);
+}
+
+}  // namespace kw

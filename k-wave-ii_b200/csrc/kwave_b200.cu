@@ -19,6 +19,7 @@
 #include <vector>
 
 #include "kw_kernels.cuh"
+#include "kw_static.cuh"
 #include "../../include/kwave_b200.h"
 
 using namespace kw;
@@ -162,6 +163,7 @@ struct kw_plan {
 
     // fields
     float *p = nullptr, *rho[3] = {nullptr, nullptr, nullptr}, *u[3] = {nullptr, nullptr, nullptr};
+    float *rho_b[3] = {nullptr, nullptr, nullptr};   // second rho buffer (Stage R writes it, then they swap)
     float2 *spec[4] = {nullptr, nullptr, nullptr, nullptr};
     float *p0_dev = nullptr;
     int *d_t = nullptr;
@@ -176,6 +178,7 @@ struct kw_plan {
 
     // tiles
     int PL_u = 1, PL_r = 1, PL_p = 1, PL_z = 1, TY = 1, NL = 1;
+    bool static_x = false, static_y = false, static_z = false;
 
     // sensors / outputs
     int M = 0;
@@ -279,45 +282,109 @@ kw_status launched(kw_plan *P) {
 }
 
 // ---- transform passes -----------------------------------------------------
+// ---- compile-time tile shapes --------------------------------------------
+// Axis lengths with compile-time kernels; every other length uses the
+// runtime-radix kernels.  Tile shapes of both are shared with the planner.
+#define KW_STATIC_SIZES(X) X(64) X(96) X(128) X(160) X(192) X(256) X(320) X(384) X(512)
+bool is_static(int n) {
+    switch (n) {
+#define KW_CASE(N) case N:
+        KW_STATIC_SIZES(KW_CASE)
+#undef KW_CASE
+        return true;
+        default: return false;
+    }
+}
+template <template <int> class L, typename... A>
+kw_status dispatch(int n, A... args) {
+    switch (n) {
+#define KW_CASE(N) case N: return L<N>::run(args...);
+        KW_STATIC_SIZES(KW_CASE)
+#undef KW_CASE
+        default: return L<0>::run(args...);
+    }
+}
+
+// ---- transform passes -----------------------------------------------------
+template <int N> struct YLaunch {
+    static kw_status run(kw_plan *P, bool inv, Spec4 bufs, int nf) {
+        dim3 grid((P->g.N0 + P->TY - 1) / P->TY, P->g.N2h, nf);
+        if constexpr (N > 0) {
+            if (inv) ks_ypass<true, N><<<grid, kThreads, 0, P->stream>>>(bufs, P->g, P->tw[1]);
+            else ks_ypass<false, N><<<grid, kThreads, 0, P->stream>>>(bufs, P->g, P->tw[1]);
+        } else {
+            size_t sh = (size_t)P->TY * P->g.N1 * sizeof(float2);
+            if (inv) {
+                KW_TRY(set_smem((const void *)k_ypass<true, 0, 0>, sh));
+                k_ypass<true, 0, 0><<<grid, kThreads, sh, P->stream>>>(bufs, P->g, P->fft[1], P->TY);
+            } else {
+                KW_TRY(set_smem((const void *)k_ypass<false, 0, 0>, sh));
+                k_ypass<false, 0, 0><<<grid, kThreads, sh, P->stream>>>(bufs, P->g, P->fft[1], P->TY);
+            }
+        }
+        return launched(P);
+    }
+};
+
 kw_status ypass(kw_plan *P, bool inv, Spec4 bufs, int nf) {
     if (P->g.N1 == 1 || nf == 0) return KW_OK;
     Scope s(P, KW_KCLASS_YPASS);
-    dim3 grid((P->g.N0 + P->TY - 1) / P->TY, P->g.N2h, nf);
-    size_t sh = (size_t)P->TY * P->g.N1 * sizeof(float2);
-    if (inv) {
-        KW_TRY(set_smem((const void *)k_ypass<true>, sh));
-        k_ypass<true><<<grid, kThreads, sh, P->stream>>>(bufs, P->g, P->fft[1], P->TY);
-    } else {
-        KW_TRY(set_smem((const void *)k_ypass<false>, sh));
-        k_ypass<false><<<grid, kThreads, sh, P->stream>>>(bufs, P->g, P->fft[1], P->TY);
-    }
-    return launched(P);
+    return dispatch<YLaunch>(P->static_y ? P->g.N1 : 0, P, inv, bufs, nf);
 }
+
+template <int N> struct XLaunch {
+    static kw_status run(kw_plan *P, Spec4 bufs, OpSet ops, int fanout, int nf) {
+        const int lines = P->g.N1 * P->g.N2h;
+        dim3 grid((lines + P->NL - 1) / P->NL, 1, fanout ? 1 : nf);
+        if constexpr (N > 0) {
+            ks_xpass<N><<<grid, kThreads, 0, P->stream>>>(bufs, P->g, P->tw[0], P->op, ops, fanout);
+        } else {
+            size_t sh = (size_t)(fanout ? 2 : 1) * P->NL * P->g.N0 * sizeof(float2);
+            KW_TRY(set_smem((const void *)k_xpass<0, 0>, sh));
+            k_xpass<0, 0><<<grid, kThreads, sh, P->stream>>>(bufs, P->g, P->fft[0], P->NL, P->op, ops, fanout);
+        }
+        return launched(P);
+    }
+};
 
 kw_status xpass(kw_plan *P, Spec4 bufs, OpSet ops, int fanout, int nf) {
     Scope s(P, KW_KCLASS_XPASS);
-    const int lines = P->g.N1 * P->g.N2h;
-    dim3 grid((lines + P->NL - 1) / P->NL, 1, fanout ? 1 : nf);
-    size_t sh = (size_t)(fanout ? 2 : 1) * P->NL * P->g.N0 * sizeof(float2);
-    KW_TRY(set_smem((const void *)k_xpass, sh));
-    k_xpass<<<grid, kThreads, sh, P->stream>>>(bufs, P->g, P->fft[0], P->NL, P->op, ops, fanout);
-    return launched(P);
+    return dispatch<XLaunch>(P->static_x ? P->g.N0 : 0, P, bufs, ops, fanout, nf);
 }
 
+template <int N> struct ZR2CLaunch {
+    static kw_status run(kw_plan *P, const float *R, float2 *H) {
+        dim3 grid((P->g.N0 + 2 * P->PL_z - 1) / (2 * P->PL_z), P->g.N1, 1);
+        if constexpr (N > 0) {
+            ks_zr2c<N><<<grid, kThreads, 0, P->stream>>>(R, H, P->g, P->tw[2]);
+        } else {
+            size_t sh = (size_t)P->PL_z * P->g.N2 * sizeof(float2);
+            KW_TRY(set_smem((const void *)k_zr2c<0, 0>, sh));
+            k_zr2c<0, 0><<<grid, kThreads, sh, P->stream>>>(R, H, P->g, P->fft[2], P->PL_z);
+        }
+        return launched(P);
+    }
+};
+template <int N> struct ZC2RLaunch {
+    static kw_status run(kw_plan *P, const float2 *H, float *R) {
+        dim3 grid((P->g.N0 + 2 * P->PL_z - 1) / (2 * P->PL_z), P->g.N1, 1);
+        if constexpr (N > 0) {
+            ks_zc2r<N><<<grid, kThreads, 0, P->stream>>>(H, R, P->g, P->tw[2]);
+        } else {
+            size_t sh = (size_t)P->PL_z * P->g.N2 * sizeof(float2);
+            KW_TRY(set_smem((const void *)k_zc2r<0, 0>, sh));
+            k_zc2r<0, 0><<<grid, kThreads, sh, P->stream>>>(H, R, P->g, P->fft[2], P->PL_z);
+        }
+        return launched(P);
+    }
+};
+
 kw_status zr2c(kw_plan *P, const float *R, float2 *H) {
-    dim3 grid((P->g.N0 + 2 * P->PL_z - 1) / (2 * P->PL_z), P->g.N1, 1);
-    size_t sh = (size_t)P->PL_z * P->g.N2 * sizeof(float2);
-    KW_TRY(set_smem((const void *)k_zr2c, sh));
-    k_zr2c<<<grid, kThreads, sh, P->stream>>>(R, H, P->g, P->fft[2], P->PL_z);
-    return launched(P);
+    return dispatch<ZR2CLaunch>(P->static_z ? P->g.N2 : 0, P, R, H);
 }
 
 kw_status zc2r(kw_plan *P, const float2 *H, float *R) {
-    dim3 grid((P->g.N0 + 2 * P->PL_z - 1) / (2 * P->PL_z), P->g.N1, 1);
-    size_t sh = (size_t)P->PL_z * P->g.N2 * sizeof(float2);
-    KW_TRY(set_smem((const void *)k_zc2r, sh));
-    k_zc2r<<<grid, kThreads, sh, P->stream>>>(H, R, P->g, P->fft[2], P->PL_z);
-    return launched(P);
+    return dispatch<ZC2RLaunch>(P->static_z ? P->g.N2 : 0, P, H, R);
 }
 
 Spec4 specs(kw_plan *P, int a, int b = -1, int c = -1) {
@@ -413,6 +480,46 @@ TRSrc tr_of(kw_plan *P) {
     return r;
 }
 
+template <int N> struct ULaunch {
+    static kw_status run(kw_plan *P, StageU a) {
+        dim3 grid((P->g.N0 + 2 * a.PL - 1) / (2 * a.PL), P->g.N1, P->D);
+        if constexpr (N > 0) {
+            ks_stage_u<N><<<grid, kThreads, 0, P->stream>>>(a, P->tw[2]);
+        } else {
+            size_t sh = (size_t)a.PL * P->g.N2 * sizeof(float2);
+            KW_TRY(set_smem((const void *)k_stage_u<0, 0>, sh));
+            k_stage_u<0, 0><<<grid, kThreads, sh, P->stream>>>(a);
+        }
+        return launched(P);
+    }
+};
+template <int N> struct RLaunch {
+    static kw_status run(kw_plan *P, StageR a) {
+        dim3 grid((P->g.N0 + 2 * a.PL - 1) / (2 * a.PL), P->g.N1, 1);
+        if constexpr (N > 0) {
+            ks_stage_r<N><<<grid, kThreads, 0, P->stream>>>(a, P->tw[2]);
+        } else {
+            size_t sh = (size_t)4 * a.PL * P->g.N2 * sizeof(float2);
+            KW_TRY(set_smem((const void *)k_stage_r<0, 0>, sh));
+            k_stage_r<0, 0><<<grid, kThreads, sh, P->stream>>>(a);
+        }
+        return launched(P);
+    }
+};
+template <int N> struct PLaunch {
+    static kw_status run(kw_plan *P, StageP a) {
+        dim3 grid((P->g.N0 + 2 * a.PL - 1) / (2 * a.PL), P->g.N1, 1);
+        if constexpr (N > 0) {
+            ks_stage_p<N><<<grid, kThreads, 0, P->stream>>>(a, P->tw[2]);
+        } else {
+            size_t sh = (size_t)2 * a.PL * P->g.N2 * sizeof(float2);
+            KW_TRY(set_smem((const void *)k_stage_p<0, 0>, sh));
+            k_stage_p<0, 0><<<grid, kThreads, sh, P->stream>>>(a);
+        }
+        return launched(P);
+    }
+};
+
 kw_status stage_u(kw_plan *P, int init, int t) {
     StageU a{};
     a.g = P->g;
@@ -434,11 +541,7 @@ kw_status stage_u(kw_plan *P, int init, int t) {
     a.d_t = P->d_t;
     (void)t;
     Scope s(P, KW_KCLASS_ZSTAGE_U);
-    dim3 grid((P->g.N0 + 2 * a.PL - 1) / (2 * a.PL), P->g.N1, P->D);
-    size_t sh = (size_t)a.PL * P->g.N2 * sizeof(float2);
-    KW_TRY(set_smem((const void *)k_stage_u, sh));
-    k_stage_u<<<grid, kThreads, sh, P->stream>>>(a);
-    return launched(P);
+    return dispatch<ULaunch>(P->static_z ? P->g.N2 : 0, P, a);
 }
 
 kw_status stage_r(kw_plan *P, int write_spec) {
@@ -450,6 +553,7 @@ kw_status stage_r(kw_plan *P, int write_spec) {
     for (int i = 0; i < 3; ++i) {
         a.spec.p[i] = P->spec[i];
         a.rho[i] = P->rho[i];
+        a.rho_out[i] = P->rho_b[i];
         a.pml[i] = P->pml[i];
         a.comp_axis[i] = P->comp_axis[i];
     }
@@ -471,11 +575,9 @@ kw_status stage_r(kw_plan *P, int write_spec) {
     a.write_spec = write_spec;
     a.d_t = P->d_t;
     Scope s(P, KW_KCLASS_ZSTAGE_R);
-    dim3 grid((P->g.N0 + 2 * a.PL - 1) / (2 * a.PL), P->g.N1, 1);
-    size_t sh = (size_t)4 * a.PL * P->g.N2 * sizeof(float2);
-    KW_TRY(set_smem((const void *)k_stage_r, sh));
-    k_stage_r<<<grid, kThreads, sh, P->stream>>>(a);
-    return launched(P);
+    KW_TRY(dispatch<RLaunch>(P->static_z ? P->g.N2 : 0, P, a));
+    for (int i = 0; i < 3; ++i) std::swap(P->rho[i], P->rho_b[i]);   // the new values become current
+    return KW_OK;
 }
 
 kw_status stage_p(kw_plan *P, int write_spec) {
@@ -501,11 +603,7 @@ kw_status stage_p(kw_plan *P, int write_spec) {
     a.write_spec = write_spec;
     a.d_t = P->d_t;
     Scope s(P, KW_KCLASS_ZSTAGE_P);
-    dim3 grid((P->g.N0 + 2 * a.PL - 1) / (2 * a.PL), P->g.N1, 1);
-    size_t sh = (size_t)2 * a.PL * P->g.N2 * sizeof(float2);
-    KW_TRY(set_smem((const void *)k_stage_p, sh));
-    k_stage_p<<<grid, kThreads, sh, P->stream>>>(a);
-    return launched(P);
+    return dispatch<PLaunch>(P->static_z ? P->g.N2 : 0, P, a);
 }
 
 kw_status sensors(kw_plan *P, int t) {
@@ -605,30 +703,35 @@ kw_status run_step(kw_plan *P) {
     } else {
         for (int c = 0; c < P->D; ++c) KW_TRY(general_source(P, P->usrc, c, t));
         KW_TRY(stage_u(P, 0, t));
-        // divergence: real(ifftn(dd_neg_i kappa fftn(u_i)))
-        Spec4 all = specs(P, 0, 1, 2);
-        KW_TRY(ypass(P, false, all, P->D));
-        OpSet ops{};
-        ops.n = P->D;
-        for (int i = 0; i < P->D; ++i) { ops.kind[i] = OP_GRAD_NEG; ops.axis[i] = P->comp_axis[i]; }
-        KW_TRY(xpass(P, all, ops, 0, P->D));
-        KW_TRY(ypass(P, true, all, P->D));
+        // divergence: real(ifftn(dd_neg_i kappa fftn(u_i))).  One field at a
+        // time through its y / x / y passes, so the half spectrum a pass
+        // writes is still in L2 when the next pass reads it.
+        for (int i = 0; i < P->D; ++i) {
+            Spec4 one = specs(P, i);
+            OpSet ops{};
+            ops.n = 1;
+            ops.kind[0] = OP_GRAD_NEG;
+            ops.axis[0] = P->comp_axis[i];
+            KW_TRY(ypass(P, false, one, 1));
+            KW_TRY(xpass(P, one, ops, 0, 1));
+            KW_TRY(ypass(P, true, one, 1));
+        }
         KW_TRY(general_source(P, P->psrc, 0, t));
         if (!P->absorbing) {
             KW_TRY(stage_r(P, need_grad ? 1 : 0));
         } else {
             KW_TRY(stage_r(P, 0));
             const int nabs = (P->has_tau ? 1 : 0) + (P->has_eta ? 1 : 0);
-            if (nabs) {
-                Spec4 ab = specs(P, 0, 1);
-                KW_TRY(ypass(P, false, ab, nabs));
+            int k = 0;
+            for (int term = 0; term < 2; ++term) {
+                if ((term == 0 && !P->has_tau) || (term == 1 && !P->has_eta)) continue;
+                Spec4 one = specs(P, k++);
                 OpSet o2{};
-                o2.n = nabs;
-                int k = 0;
-                if (P->has_tau) o2.kind[k++] = OP_NABLA1;
-                if (P->has_eta) o2.kind[k++] = OP_NABLA2;
-                KW_TRY(xpass(P, ab, o2, 0, nabs));
-                KW_TRY(ypass(P, true, ab, nabs));
+                o2.n = 1;
+                o2.kind[0] = term == 0 ? OP_NABLA1 : OP_NABLA2;
+                KW_TRY(ypass(P, false, one, 1));
+                KW_TRY(xpass(P, one, o2, 0, 1));
+                KW_TRY(ypass(P, true, one, 1));
             }
             KW_TRY(stage_p(P, need_grad ? 1 : 0));
         }
@@ -762,6 +865,38 @@ int choose_pl(int cap, int N0, int N1, int N2) {
     return pl;
 }
 
+void plan_tiles(kw_plan *P) {
+    const Geom &g = P->g;
+    // compile-time kernels where the axis length has one and the grid still
+    // fills one wave of blocks; their tile widths are fixed by ks_lines
+    P->static_z = is_static(g.N2) && (long long)((g.N0 + 2 * ks_lines(g.N2) - 1) / (2 * ks_lines(g.N2))) * g.N1 >= 148;
+    if (P->static_z) {
+        P->PL_u = P->PL_z = P->PL_p = P->PL_r = ks_lines(g.N2);
+    } else {
+        P->PL_u = choose_pl(kCap, g.N0, g.N1, g.N2);
+        P->PL_z = P->PL_u;
+        P->PL_r = choose_pl(kCap / 2, g.N0, g.N1, g.N2);
+        P->PL_p = choose_pl(kCap, g.N0, g.N1, g.N2);
+    }
+    P->static_y = g.N1 > 1 && is_static(g.N1);
+    if (P->static_y) {
+        P->TY = ks_lines(g.N1);
+    } else {
+        int ty = 1;
+        while (ty * 2 <= 32 && ty * 2 * g.N1 <= kCap) ty *= 2;
+        P->TY = ty;
+    }
+    const int lines = g.N1 * g.N2h;
+    P->static_x = is_static(g.N0) && (lines + ks_lines(g.N0) - 1) / ks_lines(g.N0) >= 148;
+    if (P->static_x) {
+        P->NL = ks_lines(g.N0);
+    } else {
+        P->NL = std::max(1, kCap / g.N0);
+        if (P->NL > lines) P->NL = lines;
+        while (P->NL > 1 && (lines + P->NL - 1) / P->NL < 2 * 148) P->NL /= 2;
+    }
+}
+
 kw_status create(const kw_problem *pr, kw_plan *P) {
     if (!pr) return fail(KW_ERR_INVALID, "problem is NULL");
     if (pr->abi_version != KW_ABI_VERSION) return fail(KW_ERR_INVALID, "abi_version %u, library expects %d", pr->abi_version, KW_ABI_VERSION);
@@ -891,27 +1026,14 @@ kw_status create(const kw_problem *pr, kw_plan *P) {
     P->op.nabla2_exp = (float)(q.alpha_power - 1.0);
     P->op.scale = (float)(1.0 / (double)g.N);
 
-    // tiles
-    P->PL_u = choose_pl(kCap, g.N0, g.N1, g.N2);
-    P->PL_z = P->PL_u;
-    P->PL_r = choose_pl(kCap / 2, g.N0, g.N1, g.N2);
-    P->PL_p = choose_pl(kCap, g.N0, g.N1, g.N2);
+    plan_tiles(P);
     if (g.N2 > kCap / 2) return fail(KW_ERR_UNSUPPORTED, "axis length %d above %d", g.N2, kCap / 2);
-    {
-        int ty = 1;
-        while (ty * 2 <= 32 && ty * 2 * g.N1 <= kCap) ty *= 2;
-        P->TY = ty;
-        P->NL = std::max(1, kCap / g.N0);
-        const int lines = g.N1 * g.N2h;
-        if (P->NL > lines) P->NL = lines;
-        while (P->NL > 1 && (lines + P->NL - 1) / P->NL < 2 * 148) P->NL /= 2;
-    }
-
     const size_t N = (size_t)g.N, Nh = (size_t)g.Nh;
     KW_TRY(palloc(P, &P->d_t, 1));
     KW_TRY(palloc(P, &P->p, N));
     for (int i = 0; i < P->D; ++i) {
         KW_TRY(palloc(P, &P->rho[i], N));
+        KW_TRY(palloc(P, &P->rho_b[i], N));
         KW_TRY(palloc(P, &P->u[i], N));
     }
     const int nspec = 4;
@@ -1378,16 +1500,7 @@ kw_status kw_gradient_noalloc(int32_t dim, const uint64_t shape[3], const double
     P.op.kappa_a = (float)(c_ref * dt / 2.0);
     P.op.use_kspace = use_kspace ? 1 : 0;
     P.op.scale = (float)(1.0 / (double)g.N);
-    P.PL_z = choose_pl(kCap, g.N0, g.N1, g.N2);
-    {
-        int ty = 1;
-        while (ty * 2 <= 32 && ty * 2 * g.N1 <= kCap) ty *= 2;
-        P.TY = ty;
-        P.NL = std::max(1, kCap / g.N0);
-        const int lines = g.N1 * g.N2h;
-        if (P.NL > lines) P.NL = lines;
-        while (P.NL > 1 && (lines + P.NL - 1) / P.NL < 2 * 148) P.NL /= 2;
-    }
+    plan_tiles(&P);
     float2 *spec = (float2 *)(base + o_spec);
     // the spectrum is fully written by the forward z-transform, so nothing
     // left in the scratch by an earlier call is read

@@ -132,9 +132,25 @@ def make_case(name):
         data = np.stack([tone(0.3 * dx / 1500, 1e6, 2, 60) * (1 + 0.01 * i) for i in range(int(mask.sum()))])
         med = {"sound_speed": 1500.0, "density": 1000.0, "alpha_coeff": 0.75, "alpha_power": 1.5}
         return 3, shape, dx, 60, 0.3 * dx / 1500, med, {}, {"mask": mask, "time_reversal_boundary_data": data}, {"PMLSize": 4}
+    if name == "3d_static_mixed_radix":
+        # 96 x 160 x 64 takes the compile-time kernels (radix 16/2/3, 16/2/5, 16/4)
+        shape = (96, 160, 64)
+        c, rho = blob_medium(shape, rng)
+        dt = 0.3 * dx / c.max()
+        pm = np.zeros(shape); pm[8, 60:100, 20:44] = 1
+        med = {"sound_speed": c, "density": rho, "alpha_coeff": 0.75, "alpha_power": 1.5, "BonA": 6.0}
+        src = {"p_mask": pm, "p": 1e6 * tone(dt, 1e6, 3, 60)}
+        mask = np.zeros(shape); mask[:, :, 32] = 1
+        return 3, shape, dx, 60, dt, med, src, {"mask": mask, "record": ["p", "p_max", "p_rms"]}, {"PMLSize": 8}
+    if name == "3d_static_128":
+        shape = (128, 128, 128)
+        c, rho = blob_medium(shape, rng)
+        mask = np.zeros(shape); mask[64, :, :] = 1
+        return 3, shape, dx, 30, 0.3 * dx / c.max(), {"sound_speed": c, "density": rho}, \
+            {"p0": disc_p0(shape, 6)}, {"mask": mask, "record": ["p", "u_max", "p_final"]}, {"PMLSize": 10}
     raise KeyError(name)
 
 
 CASES = ["2d_homog_p0", "2d_hetero_abs_nl", "2d_stokes_dirichlet", "2d_nocorr_multi", "2d_u_additive",
          "2d_u_dirichlet", "2d_odd_sizes", "2d_pml_outside", "3d_hetero_abs_nl_plane", "3d_multi_signal_additive",
-         "3d_p0_u", "2d_time_reversal", "3d_time_reversal_abs"]
+         "3d_p0_u", "2d_time_reversal", "3d_time_reversal_abs", "3d_static_mixed_radix", "3d_static_128"]
