@@ -365,7 +365,8 @@ struct StageU {
     AxisFFT axz;
     int PL;
     Spec4 spec;
-    float *u[3];
+    float *u[3];              // velocity before this step's update
+    float *u_out[3];          // updated velocity (double-buffered)
     Med rho_sg_inv[3];
     const float *pml_sg[3];   // per internal axis
     float dt;
@@ -386,7 +387,8 @@ __global__ void __launch_bounds__(kThreads, 2) k_stage_u(StageU a) {
     const int N2 = N2S ? N2S : g.N2;
     const int x0 = blockIdx.x * TX, y = blockIdx.y;
     const int t = *a.d_t;
-    float *u = a.u[f];
+    const float *u = a.u[f];
+    float *uo_ = a.u_out[f];
     const int ax = a.comp_axis[f];
     const float *pmlv = a.pml_sg[ax];
 
@@ -424,7 +426,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_stage_u(StageU a) {
                 un.y = fmaf(dscale, F.y, un.y);
             }
         }
-        st2(u, gi, un, two, g.vec2);
+        st2(uo_, gi, un, two, g.vec2);
         sm[idx] = make_float2(un.x, two ? un.y : 0.f);
     }
     __syncthreads();
@@ -438,7 +440,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_stage_u(StageU a) {
             float *slot = reinterpret_cast<float *>(sm + z * PL + (xl >> 1)) + (xl & 1);
             const float nv = a.sparse.mode == 0 ? v : *slot + v;
             *slot = nv;
-            u[x0 + xl + (long long)g.N0 * (y + (long long)g.N1 * z)] = nv;
+            uo_[x0 + xl + (long long)g.N0 * (y + (long long)g.N1 * z)] = nv;
         }
         __syncthreads();
     }
@@ -466,26 +468,20 @@ struct StageR {
     float *rho[3];            // values before this step's update
     float *rho_out[3];        // updated values (double-buffered)
     float *p;
-    Med rho0, c0, BonA, alpha_np;
+    Med rho0, c0, BonA;
+    Med c2tau;                // c0^2 * absorb_tau (stokes equation of state)
     const float *pml[3];      // per internal axis
     int comp_axis[3];
     float dt;
     int nonlinear;
     int eos;                  // 0 lossless, 1 absorbing, 2 stokes
     int has_tau, has_eta;
-    float alpha_y;            // power-law exponent used for tau (stokes: 2)
-    float tau_sign;
     DenseSrc dense;
     SparseSrc sparse;
     TRSrc tr;
     int write_spec;
     const int *d_t;
 };
-
-__device__ __forceinline__ float tau_of(float anp, float c, float y, float sgn) {
-    // createAbsorptionVariables.m:45 (absorbing) / :84 (stokes, y = 2)
-    return -2.f * anp * powf(c, y - 1.f) * sgn;
-}
 
 __device__ __forceinline__ void apply_tr(float2 *sm, const TRSrc &tr, const Geom &g, int PL, int x0, int y, int t,
                                          float *rho0_, float *rho1_, float *rho2_, int D, const Med &c0, float *p) {
@@ -625,13 +621,6 @@ __global__ void __launch_bounds__(kThreads, 2) k_stage_r(StageR a) {
             const float2 c = med2(a.c0, gi, two, g.vec2);
             const float2 c2 = make_float2(c.x * c.x, c.y * c.y);
             pv = sr;
-            if (a.eos == 2) {
-                const float2 r0 = med2(a.rho0, gi, two, g.vec2);
-                const float2 an = med2(a.alpha_np, gi, two, g.vec2);
-                const float2 sd = acc_du[idx];
-                pv.x += tau_of(an.x, c.x, 2.f, a.tau_sign) * r0.x * sd.x;
-                pv.y += tau_of(an.y, c.y, 2.f, a.tau_sign) * r0.y * sd.y;
-            }
             if (a.nonlinear) {
                 const float2 r0 = med2(a.rho0, gi, two, g.vec2);
                 const float2 bn = med2(a.BonA, gi, two, g.vec2);
@@ -640,6 +629,13 @@ __global__ void __launch_bounds__(kThreads, 2) k_stage_r(StageR a) {
             }
             pv.x *= c2.x;
             pv.y *= c2.y;
+            if (a.eos == 2) {
+                const float2 r0 = med2(a.rho0, gi, two, g.vec2);
+                const float2 ct = med2(a.c2tau, gi, two, g.vec2);
+                const float2 sd = acc_du[idx];
+                pv.x += ct.x * r0.x * sd.x;
+                pv.y += ct.y * r0.y * sd.y;
+            }
             st2(a.p, gi, pv, two, g.vec2);
             if (absorbing && a.has_tau) {
                 const float2 r0 = med2(a.rho0, gi, two, g.vec2);
@@ -694,9 +690,9 @@ struct StageP {
     Spec4 spec;
     float *p;
     float *rho[3];
-    Med c0, alpha_np;
+    Med c0;
+    Med c2tau, c2eta;         // c0^2 * absorb_tau, c0^2 * absorb_eta
     int has_tau, has_eta;
-    float alpha_y, tau_sign, eta_sign, tan_term;
     TRSrc tr;
     int write_spec;
     const int *d_t;
@@ -728,18 +724,12 @@ __global__ void __launch_bounds__(kThreads, 2) k_stage_p(StageP a) {
             if (xa >= g.N0) continue;
             const bool two = xa + 1 < g.N0;
             const long long gi = xa + (long long)g.N0 * (y + (long long)g.N1 * z);
-            const float2 c = med2(a.c0, gi, two, g.vec2);
-            const float2 an = med2(a.alpha_np, gi, two, g.vec2);
             const float2 v = tile[idx];
+            const float2 w = term == 0 ? med2(a.c2tau, gi, two, g.vec2) : med2(a.c2eta, gi, two, g.vec2);
+            const float sg = term == 0 ? 1.f : -1.f;
             float2 ac = acc[idx];
-            if (term == 0) {
-                ac.x += tau_of(an.x, c.x, a.alpha_y, a.tau_sign) * v.x;
-                ac.y += tau_of(an.y, c.y, a.alpha_y, a.tau_sign) * v.y;
-            } else {
-                // eta = 2 alpha c^y tan(pi y / 2)   (createAbsorptionVariables.m:55)
-                ac.x -= 2.f * an.x * powf(c.x, a.alpha_y) * a.tan_term * a.eta_sign * v.x;
-                ac.y -= 2.f * an.y * powf(c.y, a.alpha_y) * a.tan_term * a.eta_sign * v.y;
-            }
+            ac.x = fmaf(sg * w.x, v.x, ac.x);
+            ac.y = fmaf(sg * w.y, v.y, ac.y);
             acc[idx] = ac;
         }
     }
@@ -751,11 +741,10 @@ __global__ void __launch_bounds__(kThreads, 2) k_stage_p(StageP a) {
         if (xa < g.N0) {
             const bool two = xa + 1 < g.N0;
             const long long gi = xa + (long long)g.N0 * (y + (long long)g.N1 * z);
-            const float2 c = med2(a.c0, gi, two, g.vec2);
             const float2 pp = ld2(a.p, gi, two, g.vec2);
             const float2 ac = acc[idx];
-            pv.x = fmaf(c.x * c.x, ac.x, pp.x);
-            pv.y = fmaf(c.y * c.y, ac.y, pp.y);
+            pv.x = pp.x + ac.x;
+            pv.y = pp.y + ac.y;
             st2(a.p, gi, pv, two, g.vec2);
             if (!two) pv.y = 0.f;
         }

@@ -367,29 +367,78 @@ __device__ __forceinline__ void smem_to_hold(const float2 *sm, Hold &hold) {
 }
 
 // ---------------------------------------------------------------------------
+// Asynchronous staging of read-only physics inputs: every thread copies the
+// values of the cells it will update into a thread-private slice of shared
+// memory (index (b*R + t)*kThreads + tid) before the inverse transform, so
+// the loads are in flight while the transform computes.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void cp_async8(void *smem, const void *gmem) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
+template <int N2> struct ZStage {
+    using ZT = ZTile<N2>;
+    using SH = typename ZT::SH;
+    static constexpr int PL = ZT::PL, TX = ZT::TX;
+    static constexpr int TILE = N2 * PL;                    // float2 of the transform tile
+    static constexpr int SLICE = SH::MAXB * SH::R * kThreads;   // float2 of one staged field
+    static __device__ __forceinline__ int sidx(int b, int t) { return (b * SH::R + t) * kThreads + threadIdx.x; }
+};
+
+// stage one real field (pairs of cells) of this thread's hand-off elements
+template <int N2>
+__device__ __forceinline__ void stage_field(float2 *slice, const float *field, const Geom &g, int x0, int y) {
+    using Z = ZStage<N2>;
+    using SH = typename Z::SH;
+#pragma unroll
+    for (int b = 0; b < SH::MAXB; ++b)
+#pragma unroll
+        for (int t = 0; t < SH::R; ++t) {
+            int l, z;
+            if (!hand_pos<N2, Z::PL, true>(b, t, l, z)) continue;
+            const int xa = x0 + 2 * l;
+            if (xa >= g.N0) continue;
+            cp_async8(slice + Z::sidx(b, t), field + xa + (long long)g.N0 * (y + (long long)g.N1 * z));
+        }
+}
+
+// ---------------------------------------------------------------------------
 // Stage U (momentum, velocity sources, forward z-transform of u); see k_stage_u.
-// grid = (ceil(N0/TX), N1, D)
+// u is double-buffered (read a.u, write a.u_out).  grid = (ceil(N0/TX), N1, D);
+// dynamic shared memory: tile + 2 staged fields.
 // ---------------------------------------------------------------------------
 template <int N2>
 __global__ void __launch_bounds__(kThreads, 2) ks_stage_u(StageU a, const float2 *__restrict__ tw) {
-    using ZT = ZTile<N2>;
-    using SH = typename ZT::SH;
-    constexpr int PL = ZT::PL, TX = ZT::TX;
+    using Z = ZStage<N2>;
+    using SH = typename Z::SH;
+    constexpr int PL = Z::PL, TX = Z::TX;
     static_assert(RPlan<N2, false>::M >= 2, "z-stages need two stages");
-    __shared__ float2 sm[N2 * PL];
+    extern __shared__ float2 dsm[];
+    float2 *sm = dsm;
+    float2 *s_u = dsm + Z::TILE;
+    float2 *s_r = s_u + Z::SLICE;
     const Geom &g = a.g;
     const int f = blockIdx.z;
     const int x0 = blockIdx.x * TX, y = blockIdx.y;
     const int t = *a.d_t;
-    float *u = a.u[f];
+    float *uout = a.u_out[f];
     const int ax = a.comp_axis[f];
     const float *pmlv = a.pml_sg[ax];
     const float2 *H = a.spec.p[f];
+    const Med rsi = a.rho_sg_inv[f];
+
+    if (!a.init) stage_field<N2>(s_u, a.u[f], g, x0, y);
+    if (rsi.arr) stage_field<N2>(s_r, rsi.arr, g, x0, y);
+    cp_async_commit();
 
     float2 hold[SH::MAXB][SH::R];
     auto ld = [&](int, int, int l, int i) -> float2 { return zpack_load<N2>(H, g, x0, y, l, i); };
     auto st = [&](int b, int tt, int, int, float2 v) { hold[b][tt] = v; };
     rs_fft<N2, PL, true, true>(sm, tw, ld, st);
+    cp_async_wait_all();
 
     float dscale = 0.f;
     const bool dense = dense_active(a.dense[f], t, dscale);
@@ -402,29 +451,28 @@ __global__ void __launch_bounds__(kThreads, 2) ks_stage_u(StageU a, const float2
             if (!hand_pos<N2, PL, true>(b, tt, l, z)) continue;
             const int xa = x0 + 2 * l;
             if (xa >= g.N0) { hold[b][tt] = make_float2(0.f, 0.f); continue; }
-            const bool two = xa + 1 < g.N0;
             const long long gi = xa + (long long)g.N0 * (y + (long long)g.N1 * z);
             const float2 gr = hold[b][tt];
-            const float2 ri = med2(a.rho_sg_inv[f], gi, two, g.vec2);
+            const float2 ri = rsi.arr ? s_r[Z::sidx(b, tt)] : make_float2(rsi.val, rsi.val);
             float2 un;
             if (a.init) {
                 un = make_float2(0.5f * a.dt * ri.x * gr.x, 0.5f * a.dt * ri.y * gr.y);
             } else {
                 float2 pm;
-                if (ax == 0) pm = make_float2(__ldg(pmlv + xa), two ? __ldg(pmlv + xa + 1) : 1.f);
+                if (ax == 0) pm = make_float2(__ldg(pmlv + xa), __ldg(pmlv + xa + 1));
                 else if (ax == 1) pm = make_float2(pml_y, pml_y);
                 else { const float q = __ldg(pmlv + z); pm = make_float2(q, q); }
-                const float2 uo = ld2(u, gi, two, g.vec2);
+                const float2 uo = s_u[Z::sidx(b, tt)];
                 un.x = pm.x * (pm.x * uo.x - a.dt * ri.x * gr.x);
                 un.y = pm.y * (pm.y * uo.y - a.dt * ri.y * gr.y);
                 if (dense) {
-                    const float2 F = ld2(a.dense[f].F, gi, two, g.vec2);
+                    const float2 F = __ldg(reinterpret_cast<const float2 *>(a.dense[f].F + gi));
                     un.x = fmaf(dscale, F.x, un.x);
                     un.y = fmaf(dscale, F.y, un.y);
                 }
             }
-            st2(u, gi, un, two, g.vec2);
-            hold[b][tt] = make_float2(un.x, two ? un.y : 0.f);
+            *reinterpret_cast<float2 *>(uout + gi) = un;
+            hold[b][tt] = un;
         }
     if (a.init || !a.write_spec) return;
     if (a.sparse.off && a.sparse.sig[f] && t <= a.sparse.T[f]) {
@@ -441,7 +489,7 @@ __global__ void __launch_bounds__(kThreads, 2) ks_stage_u(StageU a, const float2
                 float *slot = reinterpret_cast<float *>(sm + z * PL + (xl >> 1)) + (xl & 1);
                 const float nv = a.sparse.mode == 0 ? v : *slot + v;
                 *slot = nv;
-                u[x0 + xl + (long long)g.N0 * (y + (long long)g.N1 * z)] = nv;
+                uout[x0 + xl + (long long)g.N0 * (y + (long long)g.N1 * z)] = nv;
             }
             __syncthreads();
             smem_to_hold<N2>(sm, hold);
@@ -452,20 +500,26 @@ __global__ void __launch_bounds__(kThreads, 2) ks_stage_u(StageU a, const float2
 
 // ---------------------------------------------------------------------------
 // Stage R (mass conservation, pressure sources, equation of state); see
-// k_stage_r.  rho is double-buffered: old values are read from a.rho, new
-// values written to a.rho_out, so the nonlinear coefficient
-// 2 * sum(rho_old) + rho0 can be re-read per component instead of held.
-// grid = (ceil(N0/TX), N1, 1)
+// k_stage_r.  rho is double-buffered (read a.rho, write a.rho_out).  The old
+// rho of every component is staged into shared memory at the start; the
+// nonlinear coefficient 2 sum(rho_old) + rho0 is formed from the staged values
+// during component 0 and kept in component 0's slice.
+// grid = (ceil(N0/TX), N1, 1); dynamic shared memory: tile + D staged fields.
 // ---------------------------------------------------------------------------
 template <int N2>
-__global__ void __launch_bounds__(kThreads, 2) ks_stage_r(StageR a, const float2 *__restrict__ tw) {
-    using ZT = ZTile<N2>;
-    using SH = typename ZT::SH;
-    constexpr int PL = ZT::PL, TX = ZT::TX;
-    __shared__ float2 sm[N2 * PL];
+__global__ void __launch_bounds__(kThreads, 1) ks_stage_r(StageR a, const float2 *__restrict__ tw) {
+    using Z = ZStage<N2>;
+    using SH = typename Z::SH;
+    constexpr int PL = Z::PL, TX = Z::TX;
+    extern __shared__ float2 dsm[];
+    float2 *sm = dsm;
+    float2 *s_r = dsm + Z::TILE;     // D slices
     const Geom &g = a.g;
     const int x0 = blockIdx.x * TX, y = blockIdx.y;
     const int t = *a.d_t;
+    const int D = a.D;
+    for (int i = 0; i < D; ++i) stage_field<N2>(s_r + i * Z::SLICE, a.rho[i], g, x0, y);
+    cp_async_commit();
     float dscale = 0.f;
     const bool dense = dense_active(a.dense, t, dscale);
 
@@ -477,18 +531,19 @@ __global__ void __launch_bounds__(kThreads, 2) ks_stage_r(StageR a, const float2
             acc_r[b][tt] = make_float2(0.f, 0.f);
             acc_d[b][tt] = make_float2(0.f, 0.f);
         }
-    for (int i = 0; i < a.D; ++i) {
+#pragma unroll 1
+    for (int i = 0; i < D; ++i) {
         float2 hold[SH::MAXB][SH::R];
         const float2 *H = a.spec.p[i];
         auto ld = [&](int, int, int l, int z) -> float2 { return zpack_load<N2>(H, g, x0, y, l, z); };
         auto st = [&](int b, int tt, int, int, float2 v) { hold[b][tt] = v; };
-        __syncthreads();
         rs_fft<N2, PL, true, true>(sm, tw, ld, st);
+        if (i == 0) cp_async_wait_all();
         const int ax = a.comp_axis[i];
         const float *pmlv = a.pml[ax];
         const float pml_y = ax == 1 ? __ldg(pmlv + y) : 1.f;
-        const float *rin = a.rho[i];
         float *rout = a.rho_out[i];
+        float2 *s_i = s_r + i * Z::SLICE;
 #pragma unroll
         for (int b = 0; b < SH::MAXB; ++b)
 #pragma unroll
@@ -497,34 +552,41 @@ __global__ void __launch_bounds__(kThreads, 2) ks_stage_r(StageR a, const float2
                 if (!hand_pos<N2, PL, true>(b, tt, l, z)) continue;
                 const int xa = x0 + 2 * l;
                 if (xa >= g.N0) continue;
-                const bool two = xa + 1 < g.N0;
                 const long long gi = xa + (long long)g.N0 * (y + (long long)g.N1 * z);
+                const int si = Z::sidx(b, tt);
                 const float2 du = hold[b][tt];
-                float2 coef = med2(a.rho0, gi, two, g.vec2);
+                const float2 ro = s_i[si];
+                float2 coef;
                 if (a.nonlinear) {
-                    float2 so = make_float2(0.f, 0.f);
-                    for (int q = 0; q < a.D; ++q) {
-                        const float2 r = ld2(a.rho[q], gi, two, g.vec2);
-                        so.x += r.x;
-                        so.y += r.y;
+                    if (i == 0) {
+                        float2 so = ro;
+                        for (int q = 1; q < D; ++q) {
+                            const float2 r = s_r[q * Z::SLICE + si];
+                            so.x += r.x;
+                            so.y += r.y;
+                        }
+                        const float2 r0 = med2(a.rho0, gi, true, true);
+                        coef = make_float2(fmaf(2.f, so.x, r0.x), fmaf(2.f, so.y, r0.y));
+                        s_r[si] = coef;   // component 0's old value is no longer needed
+                    } else {
+                        coef = s_r[si];
                     }
-                    coef.x += 2.f * so.x;
-                    coef.y += 2.f * so.y;
+                } else {
+                    coef = med2(a.rho0, gi, true, true);
                 }
                 float2 pm;
-                if (ax == 0) pm = make_float2(__ldg(pmlv + xa), two ? __ldg(pmlv + xa + 1) : 1.f);
+                if (ax == 0) pm = make_float2(__ldg(pmlv + xa), __ldg(pmlv + xa + 1));
                 else if (ax == 1) pm = make_float2(pml_y, pml_y);
                 else { const float q = __ldg(pmlv + z); pm = make_float2(q, q); }
-                const float2 ro = ld2(rin, gi, two, g.vec2);
                 float2 rn;
                 rn.x = pm.x * (pm.x * ro.x - a.dt * coef.x * du.x);
                 rn.y = pm.y * (pm.y * ro.y - a.dt * coef.y * du.y);
                 if (dense) {
-                    const float2 F = ld2(a.dense.F, gi, two, g.vec2);
+                    const float2 F = __ldg(reinterpret_cast<const float2 *>(a.dense.F + gi));
                     rn.x = fmaf(dscale, F.x, rn.x);
                     rn.y = fmaf(dscale, F.y, rn.y);
                 }
-                st2(rout, gi, rn, two, g.vec2);
+                *reinterpret_cast<float2 *>(rout + gi) = rn;
                 acc_r[b][tt].x += rn.x;
                 acc_r[b][tt].y += rn.y;
                 acc_d[b][tt].x += du.x;
@@ -545,7 +607,7 @@ __global__ void __launch_bounds__(kThreads, 2) ks_stage_r(StageR a, const float2
                 const float v = __ldg(a.sparse.sig[0] + a.sparse.row[e] + (long long)a.sparse.nsig * (t - 1));
                 const long long gi = x0 + xl + (long long)g.N0 * (y + (long long)g.N1 * z);
                 float s = 0.f;
-                for (int i = 0; i < a.D; ++i) {
+                for (int i = 0; i < D; ++i) {
                     const float nv = a.sparse.mode == 0 ? v : a.rho_out[i][gi] + v;
                     a.rho_out[i][gi] = nv;
                     s += nv;
@@ -556,7 +618,8 @@ __global__ void __launch_bounds__(kThreads, 2) ks_stage_r(StageR a, const float2
             smem_to_hold<N2>(sm, acc_r);
         }
     }
-    // equation of state
+    // equation of state (c0^2 applied to the non-spectral terms here; the
+    // absorbing terms are finished in Stage P)
     const bool absorbing = a.eos == 1;
 #pragma unroll
     for (int b = 0; b < SH::MAXB; ++b)
@@ -568,73 +631,83 @@ __global__ void __launch_bounds__(kThreads, 2) ks_stage_r(StageR a, const float2
             float2 pv = make_float2(0.f, 0.f);
             float2 rd = make_float2(0.f, 0.f);
             if (xa < g.N0) {
-                const bool two = xa + 1 < g.N0;
                 const long long gi = xa + (long long)g.N0 * (y + (long long)g.N1 * z);
                 const float2 sr = acc_r[b][tt];
-                const float2 c = med2(a.c0, gi, two, g.vec2);
+                const float2 c = med2(a.c0, gi, true, true);
                 pv = sr;
-                if (a.eos == 2) {
-                    const float2 r0 = med2(a.rho0, gi, two, g.vec2);
-                    const float2 an = med2(a.alpha_np, gi, two, g.vec2);
-                    const float2 sd = acc_d[b][tt];
-                    pv.x += tau_of(an.x, c.x, 2.f, a.tau_sign) * r0.x * sd.x;
-                    pv.y += tau_of(an.y, c.y, 2.f, a.tau_sign) * r0.y * sd.y;
-                }
                 if (a.nonlinear) {
-                    const float2 r0 = med2(a.rho0, gi, two, g.vec2);
-                    const float2 bn = med2(a.BonA, gi, two, g.vec2);
+                    const float2 r0 = med2(a.rho0, gi, true, true);
+                    const float2 bn = med2(a.BonA, gi, true, true);
                     pv.x += bn.x * sr.x * sr.x / (2.f * r0.x);
                     pv.y += bn.y * sr.y * sr.y / (2.f * r0.y);
                 }
                 pv.x *= c.x * c.x;
                 pv.y *= c.y * c.y;
-                st2(a.p, gi, pv, two, g.vec2);
-                if (absorbing && a.has_tau) {
-                    const float2 r0 = med2(a.rho0, gi, two, g.vec2);
+                if (a.eos == 2 || (absorbing && a.has_tau)) {
+                    const float2 r0 = med2(a.rho0, gi, true, true);
                     const float2 sd = acc_d[b][tt];
                     rd = make_float2(r0.x * sd.x, r0.y * sd.y);
                 }
-                if (!two) { pv.y = 0.f; rd.y = 0.f; acc_r[b][tt].y = 0.f; }
+                if (a.eos == 2) {
+                    const float2 ct = med2(a.c2tau, gi, true, true);
+                    pv.x = fmaf(ct.x, rd.x, pv.x);
+                    pv.y = fmaf(ct.y, rd.y, pv.y);
+                }
+                *reinterpret_cast<float2 *>(a.p + gi) = pv;
             } else {
                 acc_r[b][tt] = make_float2(0.f, 0.f);
             }
-            acc_d[b][tt] = absorbing ? rd : pv;   // reuse as the next forward input
+            acc_d[b][tt] = absorbing ? rd : pv;   // next forward input
         }
     if (!absorbing) {
         if (a.tr.off) {
             __syncthreads();
             hold_to_smem<N2>(sm, acc_d);
             __syncthreads();
-            apply_tr(sm, a.tr, g, PL, x0, y, t, a.rho_out[0], a.rho_out[1], a.rho_out[2], a.D, a.c0, a.p);
+            apply_tr(sm, a.tr, g, PL, x0, y, t, a.rho_out[0], a.rho_out[1], a.rho_out[2], D, a.c0, a.p);
             __syncthreads();
             smem_to_hold<N2>(sm, acc_d);
         }
         if (a.write_spec) zforward_store<N2>(sm, tw, acc_d, a.spec.p[0], g, x0, y);
         return;
     }
+    // absorbing: forward transforms of rho0 * sum(du) (tau term) and sum(rho) (eta term)
     int out = 0;
-    if (a.has_tau) zforward_store<N2>(sm, tw, acc_d, a.spec.p[out++], g, x0, y);
-    if (a.has_eta) zforward_store<N2>(sm, tw, acc_r, a.spec.p[out++], g, x0, y);
+#pragma unroll 1
+    for (int term = 0; term < 2; ++term) {
+        if ((term == 0 && !a.has_tau) || (term == 1 && !a.has_eta)) continue;
+        float2 src[SH::MAXB][SH::R];
+#pragma unroll
+        for (int b = 0; b < SH::MAXB; ++b)
+#pragma unroll
+            for (int tt = 0; tt < SH::R; ++tt) src[b][tt] = term == 0 ? acc_d[b][tt] : acc_r[b][tt];
+        zforward_store<N2>(sm, tw, src, a.spec.p[out++], g, x0, y);
+    }
 }
 
 // ---------------------------------------------------------------------------
-// Stage P: p = p_partial + c0^2 (tau A1 - eta A2), time reversal, forward z of p.
+// Stage P: p = p_partial + c0^2 tau A1 - c0^2 eta A2, time reversal, forward z of p.
 // ---------------------------------------------------------------------------
 template <int N2>
 __global__ void __launch_bounds__(kThreads, 2) ks_stage_p(StageP a, const float2 *__restrict__ tw) {
-    using ZT = ZTile<N2>;
-    using SH = typename ZT::SH;
-    constexpr int PL = ZT::PL, TX = ZT::TX;
-    __shared__ float2 sm[N2 * PL];
+    using Z = ZStage<N2>;
+    using SH = typename Z::SH;
+    constexpr int PL = Z::PL, TX = Z::TX;
+    extern __shared__ float2 dsm[];
+    float2 *sm = dsm;
+    float2 *s_p = dsm + Z::TILE;
     const Geom &g = a.g;
     const int x0 = blockIdx.x * TX, y = blockIdx.y;
     const int t = *a.d_t;
+    stage_field<N2>(s_p, a.p, g, x0, y);
+    cp_async_commit();
     float2 acc[SH::MAXB][SH::R];
 #pragma unroll
     for (int b = 0; b < SH::MAXB; ++b)
 #pragma unroll
         for (int tt = 0; tt < SH::R; ++tt) acc[b][tt] = make_float2(0.f, 0.f);
     int in = 0;
+#pragma unroll 1
     for (int term = 0; term < 2; ++term) {
         if (term == 0 && !a.has_tau) continue;
         if (term == 1 && !a.has_eta) continue;
@@ -642,8 +715,9 @@ __global__ void __launch_bounds__(kThreads, 2) ks_stage_p(StageP a, const float2
         const float2 *H = a.spec.p[in++];
         auto ld = [&](int, int, int l, int z) -> float2 { return zpack_load<N2>(H, g, x0, y, l, z); };
         auto st = [&](int b, int tt, int, int, float2 v) { hold[b][tt] = v; };
-        __syncthreads();
         rs_fft<N2, PL, true, true>(sm, tw, ld, st);
+        const Med w = term == 0 ? a.c2tau : a.c2eta;
+        const float sg = term == 0 ? 1.f : -1.f;
 #pragma unroll
         for (int b = 0; b < SH::MAXB; ++b)
 #pragma unroll
@@ -652,20 +726,13 @@ __global__ void __launch_bounds__(kThreads, 2) ks_stage_p(StageP a, const float2
                 if (!hand_pos<N2, PL, true>(b, tt, l, z)) continue;
                 const int xa = x0 + 2 * l;
                 if (xa >= g.N0) continue;
-                const bool two = xa + 1 < g.N0;
                 const long long gi = xa + (long long)g.N0 * (y + (long long)g.N1 * z);
-                const float2 c = med2(a.c0, gi, two, g.vec2);
-                const float2 an = med2(a.alpha_np, gi, two, g.vec2);
-                const float2 v = hold[b][tt];
-                if (term == 0) {
-                    acc[b][tt].x += tau_of(an.x, c.x, a.alpha_y, a.tau_sign) * v.x;
-                    acc[b][tt].y += tau_of(an.y, c.y, a.alpha_y, a.tau_sign) * v.y;
-                } else {
-                    acc[b][tt].x -= 2.f * an.x * powf(c.x, a.alpha_y) * a.tan_term * a.eta_sign * v.x;
-                    acc[b][tt].y -= 2.f * an.y * powf(c.y, a.alpha_y) * a.tan_term * a.eta_sign * v.y;
-                }
+                const float2 wv = med2(w, gi, true, true);
+                acc[b][tt].x = fmaf(sg * wv.x, hold[b][tt].x, acc[b][tt].x);
+                acc[b][tt].y = fmaf(sg * wv.y, hold[b][tt].y, acc[b][tt].y);
             }
     }
+    cp_async_wait_all();
 #pragma unroll
     for (int b = 0; b < SH::MAXB; ++b)
 #pragma unroll
@@ -675,14 +742,11 @@ __global__ void __launch_bounds__(kThreads, 2) ks_stage_p(StageP a, const float2
             const int xa = x0 + 2 * l;
             float2 pv = make_float2(0.f, 0.f);
             if (xa < g.N0) {
-                const bool two = xa + 1 < g.N0;
                 const long long gi = xa + (long long)g.N0 * (y + (long long)g.N1 * z);
-                const float2 c = med2(a.c0, gi, two, g.vec2);
-                const float2 pp = ld2(a.p, gi, two, g.vec2);
-                pv.x = fmaf(c.x * c.x, acc[b][tt].x, pp.x);
-                pv.y = fmaf(c.y * c.y, acc[b][tt].y, pp.y);
-                st2(a.p, gi, pv, two, g.vec2);
-                if (!two) pv.y = 0.f;
+                const float2 pp = s_p[Z::sidx(b, tt)];
+                pv.x = pp.x + acc[b][tt].x;
+                pv.y = pp.y + acc[b][tt].y;
+                *reinterpret_cast<float2 *>(a.p + gi) = pv;
             }
             acc[b][tt] = pv;
         }

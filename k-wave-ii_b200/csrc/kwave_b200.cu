@@ -164,15 +164,17 @@ struct kw_plan {
     // fields
     float *p = nullptr, *rho[3] = {nullptr, nullptr, nullptr}, *u[3] = {nullptr, nullptr, nullptr};
     float *rho_b[3] = {nullptr, nullptr, nullptr};   // second rho buffer (Stage R writes it, then they swap)
+    float *u_b[3] = {nullptr, nullptr, nullptr};     // second velocity buffer (Stage U writes it, then they swap)
     float2 *spec[4] = {nullptr, nullptr, nullptr, nullptr};
     float *p0_dev = nullptr;
     int *d_t = nullptr;
 
     // medium
     float *c0_arr = nullptr, *rho0_arr = nullptr, *rsi_arr[3] = {nullptr, nullptr, nullptr};
-    float *bona_arr = nullptr, *anp_arr = nullptr;
-    Med c0{}, rho0{}, rsi[3]{}, bona{}, anp{};
-    float alpha_y = 0, tau_sign = 1, eta_sign = 1, tan_term = 0;
+    float *bona_arr = nullptr;
+    Med c0{}, rho0{}, rsi[3]{}, bona{};
+    float *c2tau_arr = nullptr, *c2eta_arr = nullptr;
+    Med c2tau{}, c2eta{};           // c0^2 * absorb_tau, c0^2 * absorb_eta
 
     SourceDev psrc, usrc;
 
@@ -484,7 +486,10 @@ template <int N> struct ULaunch {
     static kw_status run(kw_plan *P, StageU a) {
         dim3 grid((P->g.N0 + 2 * a.PL - 1) / (2 * a.PL), P->g.N1, P->D);
         if constexpr (N > 0) {
-            ks_stage_u<N><<<grid, kThreads, 0, P->stream>>>(a, P->tw[2]);
+            using Z = ZStage<(N > 0 ? N : 64)>;
+            const size_t sh = (size_t)(Z::TILE + 2 * Z::SLICE) * sizeof(float2);
+            KW_TRY(set_smem((const void *)ks_stage_u<N>, sh));
+            ks_stage_u<N><<<grid, kThreads, sh, P->stream>>>(a, P->tw[2]);
         } else {
             size_t sh = (size_t)a.PL * P->g.N2 * sizeof(float2);
             KW_TRY(set_smem((const void *)k_stage_u<0, 0>, sh));
@@ -497,7 +502,10 @@ template <int N> struct RLaunch {
     static kw_status run(kw_plan *P, StageR a) {
         dim3 grid((P->g.N0 + 2 * a.PL - 1) / (2 * a.PL), P->g.N1, 1);
         if constexpr (N > 0) {
-            ks_stage_r<N><<<grid, kThreads, 0, P->stream>>>(a, P->tw[2]);
+            using Z = ZStage<(N > 0 ? N : 64)>;
+            const size_t sh = (size_t)(Z::TILE + P->D * Z::SLICE) * sizeof(float2);
+            KW_TRY(set_smem((const void *)ks_stage_r<N>, sh));
+            ks_stage_r<N><<<grid, kThreads, sh, P->stream>>>(a, P->tw[2]);
         } else {
             size_t sh = (size_t)4 * a.PL * P->g.N2 * sizeof(float2);
             KW_TRY(set_smem((const void *)k_stage_r<0, 0>, sh));
@@ -510,7 +518,10 @@ template <int N> struct PLaunch {
     static kw_status run(kw_plan *P, StageP a) {
         dim3 grid((P->g.N0 + 2 * a.PL - 1) / (2 * a.PL), P->g.N1, 1);
         if constexpr (N > 0) {
-            ks_stage_p<N><<<grid, kThreads, 0, P->stream>>>(a, P->tw[2]);
+            using Z = ZStage<(N > 0 ? N : 64)>;
+            const size_t sh = (size_t)(Z::TILE + Z::SLICE) * sizeof(float2);
+            KW_TRY(set_smem((const void *)ks_stage_p<N>, sh));
+            ks_stage_p<N><<<grid, kThreads, sh, P->stream>>>(a, P->tw[2]);
         } else {
             size_t sh = (size_t)2 * a.PL * P->g.N2 * sizeof(float2);
             KW_TRY(set_smem((const void *)k_stage_p<0, 0>, sh));
@@ -528,6 +539,7 @@ kw_status stage_u(kw_plan *P, int init, int t) {
     for (int i = 0; i < 3; ++i) {
         a.spec.p[i] = P->spec[i];
         a.u[i] = P->u[i];
+        a.u_out[i] = P->u_b[i];
         a.rho_sg_inv[i] = P->rsi[i];
         a.pml_sg[i] = P->pml_sg[i];
         a.comp_axis[i] = P->comp_axis[i];
@@ -541,7 +553,9 @@ kw_status stage_u(kw_plan *P, int init, int t) {
     a.d_t = P->d_t;
     (void)t;
     Scope s(P, KW_KCLASS_ZSTAGE_U);
-    return dispatch<ULaunch>(P->static_z ? P->g.N2 : 0, P, a);
+    KW_TRY(dispatch<ULaunch>(P->static_z ? P->g.N2 : 0, P, a));
+    for (int i = 0; i < 3; ++i) std::swap(P->u[i], P->u_b[i]);   // the new velocity becomes current
+    return KW_OK;
 }
 
 kw_status stage_r(kw_plan *P, int write_spec) {
@@ -561,14 +575,12 @@ kw_status stage_r(kw_plan *P, int write_spec) {
     a.rho0 = P->rho0;
     a.c0 = P->c0;
     a.BonA = P->bona;
-    a.alpha_np = P->anp;
+    a.c2tau = P->c2tau;
     a.dt = (float)P->prob.dt;
     a.nonlinear = P->prob.nonlinear_flag ? 1 : 0;
     a.eos = P->prob.absorbing_flag;
     a.has_tau = P->has_tau;
     a.has_eta = P->has_eta;
-    a.alpha_y = P->alpha_y;
-    a.tau_sign = P->tau_sign;
     a.dense = dense_of(P->psrc, 0);
     a.sparse = sparse_of(P->psrc);
     a.tr = P->absorbing ? TRSrc{} : tr_of(P);
@@ -592,13 +604,10 @@ kw_status stage_p(kw_plan *P, int write_spec) {
     }
     a.p = P->p;
     a.c0 = P->c0;
-    a.alpha_np = P->anp;
+    a.c2tau = P->c2tau;
+    a.c2eta = P->c2eta;
     a.has_tau = P->has_tau;
     a.has_eta = P->has_eta;
-    a.alpha_y = P->alpha_y;
-    a.tau_sign = P->tau_sign;
-    a.eta_sign = P->eta_sign;
-    a.tan_term = P->tan_term;
     a.tr = tr_of(P);
     a.write_spec = write_spec;
     a.d_t = P->d_t;
@@ -869,7 +878,7 @@ void plan_tiles(kw_plan *P) {
     const Geom &g = P->g;
     // compile-time kernels where the axis length has one and the grid still
     // fills one wave of blocks; their tile widths are fixed by ks_lines
-    P->static_z = is_static(g.N2) && (long long)((g.N0 + 2 * ks_lines(g.N2) - 1) / (2 * ks_lines(g.N2))) * g.N1 >= 148;
+    P->static_z = g.vec2 && is_static(g.N2) && (long long)((g.N0 + 2 * ks_lines(g.N2) - 1) / (2 * ks_lines(g.N2))) * g.N1 >= 148;
     if (P->static_z) {
         P->PL_u = P->PL_z = P->PL_p = P->PL_r = ks_lines(g.N2);
     } else {
@@ -1035,6 +1044,7 @@ kw_status create(const kw_problem *pr, kw_plan *P) {
         KW_TRY(palloc(P, &P->rho[i], N));
         KW_TRY(palloc(P, &P->rho_b[i], N));
         KW_TRY(palloc(P, &P->u[i], N));
+        KW_TRY(palloc(P, &P->u_b[i], N));
     }
     const int nspec = 4;
     for (int i = 0; i < nspec; ++i) KW_TRY(palloc(P, &P->spec[i], Nh));
@@ -1078,23 +1088,44 @@ kw_status create(const kw_problem *pr, kw_plan *P) {
         }
     }
     if (q.absorbing_flag != KW_LOSSLESS) {
-        const double y = q.absorbing_flag == KW_STOKES ? 2.0 : q.alpha_power;
-        P->alpha_y = (float)y;
-        if (q.alpha_coeff) {
-            std::vector<float> a(N);
-            for (size_t i = 0; i < N; ++i) a[i] = (float)db2neper(q.alpha_coeff[i], y);
-            KW_TRY(pupload(P, &P->anp_arr, a.data(), N));
-            P->anp.arr = P->anp_arr;
-        } else {
-            P->anp.val = (float)db2neper(q.alpha_coeff_scalar, y);
-        }
+        // absorb_tau / absorb_eta of createAbsorptionVariables.m:29-101 in
+        // FP64, multiplied by c0^2 so the equation of state needs no powers
+        const bool stokes = q.absorbing_flag == KW_STOKES;
+        const double y = stokes ? 2.0 : q.alpha_power;
         const double s0 = q.alpha_sign[0], s1 = q.alpha_sign[1];
-        P->tau_sign = (float)(s0 > 0 ? 1 : (s0 < 0 ? -1 : 0));
-        P->eta_sign = (float)(s1 > 0 ? 1 : (s1 < 0 ? -1 : 0));
+        const double sg0 = s0 > 0 ? 1 : (s0 < 0 ? -1 : 0), sg1 = s1 > 0 ? 1 : (s1 < 0 ? -1 : 0);
+        const double tanv = stokes ? 0.0 : std::tan(M_PI * q.alpha_power / 2.0);
         if (q.absorbing_flag == KW_ABSORBING) {
             P->has_tau = q.alpha_mode != KW_ALPHA_NO_ABSORPTION;
             P->has_eta = q.alpha_mode != KW_ALPHA_NO_DISPERSION;
-            P->tan_term = (float)std::tan(M_PI * q.alpha_power / 2.0);
+        }
+        auto tau_eta = [&](double c, double acoef, double &c2tau, double &c2eta) {
+            const double anp = db2neper(acoef, y);
+            const double tau = stokes ? -2.0 * anp * c : -2.0 * anp * std::pow(c, y - 1.0);
+            const double eta = stokes ? 0.0 : 2.0 * anp * std::pow(c, y) * tanv;
+            c2tau = c * c * tau * sg0;
+            c2eta = c * c * eta * sg1;
+        };
+        if (q.c0 || q.alpha_coeff) {
+            std::vector<float> ta(N), ea(N);
+            for (size_t i = 0; i < N; ++i) {
+                double ct, ce;
+                tau_eta(q.c0 ? (double)q.c0[i] : q.c0_scalar, q.alpha_coeff ? (double)q.alpha_coeff[i] : q.alpha_coeff_scalar,
+                        ct, ce);
+                ta[i] = (float)ct;
+                ea[i] = (float)ce;
+            }
+            KW_TRY(pupload(P, &P->c2tau_arr, ta.data(), N));
+            P->c2tau.arr = P->c2tau_arr;
+            if (!stokes) {
+                KW_TRY(pupload(P, &P->c2eta_arr, ea.data(), N));
+                P->c2eta.arr = P->c2eta_arr;
+            }
+        } else {
+            double ct, ce;
+            tau_eta(q.c0_scalar, q.alpha_coeff_scalar, ct, ce);
+            P->c2tau.val = (float)ct;
+            P->c2eta.val = (float)ce;
         }
     }
     if (P->p0) KW_TRY(pupload(P, &P->p0_dev, q.p0_source_input, N));
