@@ -467,6 +467,7 @@ struct StageR {
     Spec4 spec;
     float *rho[3];            // values before this step's update
     float *rho_out[3];        // updated values (double-buffered)
+    float *srho;              // sum of rho over components: read (old), rewritten (new)
     float *p;
     Med rho0, c0, BonA;
     Med c2tau;                // c0^2 * absorb_tau (stokes equation of state)
@@ -484,7 +485,8 @@ struct StageR {
 };
 
 __device__ __forceinline__ void apply_tr(float2 *sm, const TRSrc &tr, const Geom &g, int PL, int x0, int y, int t,
-                                         float *rho0_, float *rho1_, float *rho2_, int D, const Med &c0, float *p) {
+                                         float *rho0_, float *rho1_, float *rho2_, int D, const Med &c0, float *p,
+                                         float *srho) {
     // Dirichlet overwrite of p on the mask with the flipped data for step t+1
     // (kspaceFirstOrder3D.m:772-788; 2D :715-729) and the matching rho.
     if (!tr.off) return;
@@ -637,6 +639,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_stage_r(StageR a) {
                 pv.y += ct.y * r0.y * sd.y;
             }
             st2(a.p, gi, pv, two, g.vec2);
+            if (a.srho) st2(a.srho, gi, sr, two, g.vec2);
             if (absorbing && a.has_tau) {
                 const float2 r0 = med2(a.rho0, gi, two, g.vec2);
                 const float2 sd = acc_du[idx];
@@ -648,7 +651,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_stage_r(StageR a) {
     }
     __syncthreads();
     if (!absorbing) {
-        apply_tr(tile, a.tr, g, PL, x0, y, t, a.rho_out[0], a.rho_out[1], a.rho_out[2], a.D, a.c0, a.p);
+        apply_tr(tile, a.tr, g, PL, x0, y, t, a.rho_out[0], a.rho_out[1], a.rho_out[2], a.D, a.c0, a.p, a.srho);
         __syncthreads();
         if (a.write_spec) {
             tile_fft_il<N2S, PLS, false>(tile, a.axz, PL);
@@ -690,6 +693,7 @@ struct StageP {
     Spec4 spec;
     float *p;
     float *rho[3];
+    float *srho;
     Med c0;
     Med c2tau, c2eta;         // c0^2 * absorb_tau, c0^2 * absorb_eta
     int has_tau, has_eta;
@@ -751,7 +755,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_stage_p(StageP a) {
         tile[idx] = pv;
     }
     __syncthreads();
-    apply_tr(tile, a.tr, g, PL, x0, y, t, a.rho[0], a.rho[1], a.rho[2], a.D, a.c0, a.p);
+    apply_tr(tile, a.tr, g, PL, x0, y, t, a.rho[0], a.rho[1], a.rho[2], a.D, a.c0, a.p, a.srho);
     __syncthreads();
     if (a.write_spec) {
         tile_fft_il<N2S, PLS, false>(tile, a.axz, PL);
@@ -881,19 +885,21 @@ __global__ void k_rms_finish(float *sq, int M, float inv_n) {
 }
 
 // rho_i = p0 / (D c0^2) on every cell (kspaceFirstOrder3D.m:1027-1030)
-__global__ void k_init_rho(const float *__restrict__ p0, Med c0, float *r0, float *r1, float *r2, long long N, int D) {
+__global__ void k_init_rho(const float *__restrict__ p0, Med c0, float *r0, float *r1, float *r2, float *srho,
+                           long long N, int D) {
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < N; i += (long long)gridDim.x * blockDim.x) {
         const float c = c0.arr ? c0.arr[i] : c0.val;
         const float v = p0[i] / ((float)D * c * c);
         r0[i] = v;
         r1[i] = v;
         if (D == 3) r2[i] = v;
+        srho[i] = (float)D * v;
     }
 }
 
 // time-reversal start: p(mask) = data(:, flipped column 1), rho(mask) = p/(D c0^2)
 __global__ void k_tr_start(const long long *idx, int M, const float *data, int Nt, Med c0, float *p, float *r0,
-                           float *r1, float *r2, int D) {
+                           float *r1, float *r2, float *srho, int D) {
     const int m = blockIdx.x * blockDim.x + threadIdx.x;
     if (m >= M) return;
     const long long gi = idx[m];
@@ -904,6 +910,7 @@ __global__ void k_tr_start(const long long *idx, int M, const float *data, int N
     r0[gi] = r;
     r1[gi] = r;
     if (D == 3) r2[gi] = r;
+    srho[gi] = (float)D * r;
 }
 
 // final time-reversal assignment p(mask) = data(:, flipped column Nt) (:1211-1213)

@@ -507,18 +507,20 @@ __global__ void __launch_bounds__(kThreads, 2) ks_stage_u(StageU a, const float2
 // grid = (ceil(N0/TX), N1, 1); dynamic shared memory: tile + D staged fields.
 // ---------------------------------------------------------------------------
 template <int N2>
-__global__ void __launch_bounds__(kThreads, 1) ks_stage_r(StageR a, const float2 *__restrict__ tw) {
+__global__ void __launch_bounds__(kThreads, 2) ks_stage_r(StageR a, const float2 *__restrict__ tw) {
     using Z = ZStage<N2>;
     using SH = typename Z::SH;
     constexpr int PL = Z::PL, TX = Z::TX;
     extern __shared__ float2 dsm[];
     float2 *sm = dsm;
-    float2 *s_r = dsm + Z::TILE;     // D slices
+    float2 *s_c = dsm + Z::TILE;        // staged sum(rho_old) (nonlinear)
+    float2 *s_a = s_c + Z::SLICE;       // staged rho_old of the current component
     const Geom &g = a.g;
     const int x0 = blockIdx.x * TX, y = blockIdx.y;
     const int t = *a.d_t;
     const int D = a.D;
-    for (int i = 0; i < D; ++i) stage_field<N2>(s_r + i * Z::SLICE, a.rho[i], g, x0, y);
+    if (a.nonlinear) stage_field<N2>(s_c, a.srho, g, x0, y);
+    stage_field<N2>(s_a, a.rho[0], g, x0, y);
     cp_async_commit();
     float dscale = 0.f;
     const bool dense = dense_active(a.dense, t, dscale);
@@ -538,12 +540,11 @@ __global__ void __launch_bounds__(kThreads, 1) ks_stage_r(StageR a, const float2
         auto ld = [&](int, int, int l, int z) -> float2 { return zpack_load<N2>(H, g, x0, y, l, z); };
         auto st = [&](int b, int tt, int, int, float2 v) { hold[b][tt] = v; };
         rs_fft<N2, PL, true, true>(sm, tw, ld, st);
-        if (i == 0) cp_async_wait_all();
+        cp_async_wait_all();
         const int ax = a.comp_axis[i];
         const float *pmlv = a.pml[ax];
         const float pml_y = ax == 1 ? __ldg(pmlv + y) : 1.f;
         float *rout = a.rho_out[i];
-        float2 *s_i = s_r + i * Z::SLICE;
 #pragma unroll
         for (int b = 0; b < SH::MAXB; ++b)
 #pragma unroll
@@ -555,24 +556,12 @@ __global__ void __launch_bounds__(kThreads, 1) ks_stage_r(StageR a, const float2
                 const long long gi = xa + (long long)g.N0 * (y + (long long)g.N1 * z);
                 const int si = Z::sidx(b, tt);
                 const float2 du = hold[b][tt];
-                const float2 ro = s_i[si];
-                float2 coef;
+                const float2 ro = s_a[si];
+                float2 coef = med2(a.rho0, gi, true, true);
                 if (a.nonlinear) {
-                    if (i == 0) {
-                        float2 so = ro;
-                        for (int q = 1; q < D; ++q) {
-                            const float2 r = s_r[q * Z::SLICE + si];
-                            so.x += r.x;
-                            so.y += r.y;
-                        }
-                        const float2 r0 = med2(a.rho0, gi, true, true);
-                        coef = make_float2(fmaf(2.f, so.x, r0.x), fmaf(2.f, so.y, r0.y));
-                        s_r[si] = coef;   // component 0's old value is no longer needed
-                    } else {
-                        coef = s_r[si];
-                    }
-                } else {
-                    coef = med2(a.rho0, gi, true, true);
+                    const float2 so = s_c[si];
+                    coef.x = fmaf(2.f, so.x, coef.x);
+                    coef.y = fmaf(2.f, so.y, coef.y);
                 }
                 float2 pm;
                 if (ax == 0) pm = make_float2(__ldg(pmlv + xa), __ldg(pmlv + xa + 1));
@@ -592,6 +581,12 @@ __global__ void __launch_bounds__(kThreads, 1) ks_stage_r(StageR a, const float2
                 acc_d[b][tt].x += du.x;
                 acc_d[b][tt].y += du.y;
             }
+        // every thread reads only its own slots, so the next component can be
+        // staged into the same slice right away
+        if (i + 1 < D) {
+            stage_field<N2>(s_a, a.rho[i + 1], g, x0, y);
+            cp_async_commit();
+        }
     }
     // sparse pressure sources act on every rho component (:930-962)
     if (a.sparse.off && t <= a.sparse.T[0]) {
@@ -659,12 +654,25 @@ __global__ void __launch_bounds__(kThreads, 1) ks_stage_r(StageR a, const float2
             }
             acc_d[b][tt] = absorbing ? rd : pv;   // next forward input
         }
+    if (a.nonlinear && a.srho) {
+        // sum of the new rho for the next step's nonlinear coefficient
+#pragma unroll
+        for (int b = 0; b < SH::MAXB; ++b)
+#pragma unroll
+            for (int tt = 0; tt < SH::R; ++tt) {
+                int l, z;
+                if (!hand_pos<N2, PL, true>(b, tt, l, z)) continue;
+                const int xa = x0 + 2 * l;
+                if (xa >= g.N0) continue;
+                *reinterpret_cast<float2 *>(a.srho + xa + (long long)g.N0 * (y + (long long)g.N1 * z)) = acc_r[b][tt];
+            }
+    }
     if (!absorbing) {
         if (a.tr.off) {
             __syncthreads();
             hold_to_smem<N2>(sm, acc_d);
             __syncthreads();
-            apply_tr(sm, a.tr, g, PL, x0, y, t, a.rho_out[0], a.rho_out[1], a.rho_out[2], D, a.c0, a.p);
+            apply_tr(sm, a.tr, g, PL, x0, y, t, a.rho_out[0], a.rho_out[1], a.rho_out[2], D, a.c0, a.p, a.srho);
             __syncthreads();
             smem_to_hold<N2>(sm, acc_d);
         }
@@ -754,7 +762,7 @@ __global__ void __launch_bounds__(kThreads, 2) ks_stage_p(StageP a, const float2
         __syncthreads();
         hold_to_smem<N2>(sm, acc);
         __syncthreads();
-        apply_tr(sm, a.tr, g, PL, x0, y, t, a.rho[0], a.rho[1], a.rho[2], a.D, a.c0, a.p);
+        apply_tr(sm, a.tr, g, PL, x0, y, t, a.rho[0], a.rho[1], a.rho[2], a.D, a.c0, a.p, a.srho);
         __syncthreads();
         smem_to_hold<N2>(sm, acc);
     }

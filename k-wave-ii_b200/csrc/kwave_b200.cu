@@ -165,6 +165,7 @@ struct kw_plan {
     float *p = nullptr, *rho[3] = {nullptr, nullptr, nullptr}, *u[3] = {nullptr, nullptr, nullptr};
     float *rho_b[3] = {nullptr, nullptr, nullptr};   // second rho buffer (Stage R writes it, then they swap)
     float *u_b[3] = {nullptr, nullptr, nullptr};     // second velocity buffer (Stage U writes it, then they swap)
+    float *srho = nullptr;                           // sum of rho over components
     float2 *spec[4] = {nullptr, nullptr, nullptr, nullptr};
     float *p0_dev = nullptr;
     int *d_t = nullptr;
@@ -503,7 +504,7 @@ template <int N> struct RLaunch {
         dim3 grid((P->g.N0 + 2 * a.PL - 1) / (2 * a.PL), P->g.N1, 1);
         if constexpr (N > 0) {
             using Z = ZStage<(N > 0 ? N : 64)>;
-            const size_t sh = (size_t)(Z::TILE + P->D * Z::SLICE) * sizeof(float2);
+            const size_t sh = (size_t)(Z::TILE + 2 * Z::SLICE) * sizeof(float2);
             KW_TRY(set_smem((const void *)ks_stage_r<N>, sh));
             ks_stage_r<N><<<grid, kThreads, sh, P->stream>>>(a, P->tw[2]);
         } else {
@@ -572,6 +573,7 @@ kw_status stage_r(kw_plan *P, int write_spec) {
         a.comp_axis[i] = P->comp_axis[i];
     }
     a.p = P->p;
+    a.srho = P->srho;
     a.rho0 = P->rho0;
     a.c0 = P->c0;
     a.BonA = P->bona;
@@ -603,6 +605,7 @@ kw_status stage_p(kw_plan *P, int write_spec) {
         a.rho[i] = P->rho[i];
     }
     a.p = P->p;
+    a.srho = P->srho;
     a.c0 = P->c0;
     a.c2tau = P->c2tau;
     a.c2eta = P->c2eta;
@@ -670,6 +673,7 @@ kw_status sensors(kw_plan *P, int t) {
 kw_status zero_state(kw_plan *P) {
     const size_t N = (size_t)P->g.N, Nh = (size_t)P->g.Nh;
     KW_CUDA(cudaMemsetAsync(P->p, 0, N * sizeof(float), P->stream));
+    KW_CUDA(cudaMemsetAsync(P->srho, 0, N * sizeof(float), P->stream));
     for (int i = 0; i < P->D; ++i) {
         KW_CUDA(cudaMemsetAsync(P->rho[i], 0, N * sizeof(float), P->stream));
         KW_CUDA(cudaMemsetAsync(P->u[i], 0, N * sizeof(float), P->stream));
@@ -687,7 +691,7 @@ kw_status start(kw_plan *P) {
     if (P->time_rev) {
         // kspaceFirstOrder3D.m:772-788 at t = 1
         k_tr_start<<<(P->M + 255) / 256, 256, 0, P->stream>>>(P->sidx, P->M, P->tr_data, P->Nt, P->c0, P->p,
-                                                              P->rho[0], P->rho[1], P->rho[2], P->D);
+                                                              P->rho[0], P->rho[1], P->rho[2], P->srho, P->D);
         KW_TRY(launched(P));
         KW_TRY(zr2c(P, P->p, P->spec[0]));
         KW_TRY(grad_group(P));
@@ -704,7 +708,7 @@ kw_status run_step(kw_plan *P) {
         // p0 initial condition (kspaceFirstOrder3D.m:1023-1040): the first
         // step's update is overwritten, so the state is set directly.
         KW_CUDA(cudaMemcpyAsync(P->p, P->p0_dev, (size_t)P->g.N * sizeof(float), cudaMemcpyDeviceToDevice, P->stream));
-        k_init_rho<<<1024, 256, 0, P->stream>>>(P->p0_dev, P->c0, P->rho[0], P->rho[1], P->rho[2], P->g.N, P->D);
+        k_init_rho<<<1024, 256, 0, P->stream>>>(P->p0_dev, P->c0, P->rho[0], P->rho[1], P->rho[2], P->srho, P->g.N, P->D);
         KW_TRY(launched(P));
         KW_TRY(zr2c(P, P->p, P->spec[0]));
         KW_TRY(grad_group(P));
@@ -1046,6 +1050,7 @@ kw_status create(const kw_problem *pr, kw_plan *P) {
         KW_TRY(palloc(P, &P->u[i], N));
         KW_TRY(palloc(P, &P->u_b[i], N));
     }
+    KW_TRY(palloc(P, &P->srho, N));
     const int nspec = 4;
     for (int i = 0; i < nspec; ++i) KW_TRY(palloc(P, &P->spec[i], Nh));
 
