@@ -854,3 +854,14 @@ def rel_l2(a, b):
     b = np.asarray(b, dtype=np.float64)
     den = np.linalg.norm(b.ravel())
     return float(np.linalg.norm((a - b).ravel()) / (den if den > 0 else 1.0))
+
+
+def spectral_derivative(f, kgrid, axis, shift=0):
+    """real(ifft(i k exp(shift * i k d / 2) fft(f))) along one axis: the
+    staggered derivative operators of kspaceFirstOrder3D.m:629-650
+    (shift = +1: ddx_k_shift_pos, -1: ddx_k_shift_neg, 0: unstaggered)."""
+    kv = kgrid.k_vecs()[axis]
+    d = kgrid.spacing[axis]
+    op = ifftshift(1j * kv * np.exp(shift * 1j * kv * d / 2))
+    op = _axis(op, axis, f.ndim)
+    return np.real(np.fft.ifft(op * np.fft.fft(f, axis=axis), axis=axis))

@@ -46,3 +46,46 @@ def test_parity(name):
         assert gpu.shape == ref.shape
         e = _rel(gpu, ref)
         assert e <= TOL, "%s rel-L2 %.3e" % (name, e)
+
+
+GOLDEN = __import__("os").path.join(__import__("os").path.dirname(__file__), "golden")
+
+
+@pytest.mark.gpu
+def test_golden_cfg1_small():
+    """Config 1 recipe at 64^2 (Cartesian circle sensor, nearest) against the fixture."""
+    import kwave_b200 as kw
+    g = np.load(GOLDEN + "/cfg1_small.npz")
+    N, dx = int(g["N"]), float(g["dx"])
+    kg = kw.kWaveGrid(N, dx, N, dx)
+    kg.setTime(int(g["Nt"]), float(g["dt"]))
+    out = kw.kspaceFirstOrder2D(kg, {"sound_speed": float(g["c"]), "density": 1000.0}, {"p0": g["p0"]},
+                                {"mask": g["sensor_mask"]}, PMLSize=10, CartInterp="nearest")
+    assert _rel(out, g["p"]) <= TOL
+
+
+@pytest.mark.gpu
+def test_golden_absorbing_3d():
+    import kwave_b200 as kw
+    g = np.load(GOLDEN + "/absorbing_3d.npz")
+    shape = tuple(int(v) for v in g["shape"])
+    dx = float(g["dx"])
+    kg = kw.kWaveGrid(shape[0], dx, shape[1], dx, shape[2], dx)
+    kg.setTime(int(g["Nt"]), float(g["dt"]))
+    med = {"sound_speed": g["c"], "density": g["rho"], "alpha_coeff": 0.75, "alpha_power": 1.5, "BonA": 6.0}
+    out = kw.kspaceFirstOrder3D(kg, med, {"p_mask": g["p_mask"], "p": g["sig"]},
+                                {"mask": g["sensor_mask"], "record": ["p", "p_max", "p_final"]}, PMLSize=4)
+    for k in ("p", "p_max", "p_final"):
+        assert _rel(out[k], g["out_" + k]) <= TOL, k
+
+
+@pytest.mark.gpu
+def test_golden_time_reversal_2d():
+    import kwave_b200 as kw
+    g = np.load(GOLDEN + "/time_reversal_2d.npz")
+    N, dx = int(g["N"]), float(g["dx"])
+    kg = kw.kWaveGrid(N, dx, N, dx)
+    kg.setTime(int(g["Nt"]), float(g["dt"]))
+    p = kw.kspaceFirstOrder2D(kg, {"sound_speed": float(g["c"]), "density": 1000.0}, {},
+                              {"mask": g["sensor_mask"], "time_reversal_boundary_data": g["data"]}, PMLSize=8)
+    assert _rel(p, g["p_final"]) <= TOL

@@ -1,0 +1,156 @@
+"""Host-side setup of the drop-in (CPU only, no device calls).
+
+The product's restatements of the reference helpers are checked against the
+oracle's independent ones, and the setup that precedes the C ABI
+(private/kspaceFirstOrder_inputChecking.m, scaleSourceTerms.m, the staggered
+density of kspaceFirstOrder3D.m:585-607) is checked for the values it hands
+over and for the errors the reference raises.
+"""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+import kwave_b200 as kw
+from kwave_b200 import _abi
+from kwave_b200.solver import KWaveInputError, _prepare
+from oracle import kspace as ks
+
+
+def _arr(ptr, n, dtype=np.float32):
+    ctype = C.c_float if dtype == np.float32 else C.c_uint64
+    return np.ctypeslib.as_array(C.cast(ptr, C.POINTER(ctype)), shape=(n,)).copy()
+
+
+def _grids(shape, dx):
+    a = []
+    for s in shape:
+        a += [s, dx]
+    return kw.kWaveGrid(*a), ks.KWaveGrid(*a)
+
+
+@pytest.mark.parametrize("n,d", [(64, 1e-3), (45, 2e-4)])
+def test_kgrid_matches_oracle(n, d):
+    g, o = _grids((n, n + 3, n - 1), d)
+    for a in range(3):
+        assert np.array_equal(g.k_vec(a), o.k_vecs()[a])
+        assert np.allclose(g.grid_vec(a), o.vec(a), rtol=0, atol=1e-15)
+    g.makeTime(np.array([1480.0, 1620.0]))
+    o.makeTime(np.array([1480.0, 1620.0]))
+    assert (g.Nt, g.dt) == (o.Nt, o.dt)
+
+
+def test_shape_helpers_match_oracle():
+    assert np.array_equal(kw.makeDisc(64, 48, 20, 30, 6), ks.make_disc(64, 48, 20, 30, 6))
+    assert np.array_equal(kw.makeDisc(63, 47, 0, 0, 9), ks.make_disc(63, 47, 0, 0, 9))
+    assert np.array_equal(kw.makeBall(20, 22, 24, 9, 10, 12, 5), ks.make_ball(20, 22, 24, 9, 10, 12, 5))
+    assert np.allclose(kw.makeCartCircle(4e-3, 33, (1e-3, -2e-3)), ks.make_cart_circle(4e-3, 33, (1e-3, -2e-3)),
+                       rtol=0, atol=1e-15)
+    g, o = _grids((40, 40), 2e-4)
+    pts = ks.make_cart_circle(3e-3, 50)
+    m1, o1, r1 = kw.cart2grid(g, pts)
+    m2, o2, r2 = ks.cart2grid(o, pts)
+    assert np.array_equal(m1, m2) and np.array_equal(o1, o2) and np.array_equal(r1, r2)
+
+
+@pytest.mark.parametrize("shape", [(64, 64), (45, 36), (20, 22, 17)])
+def test_smooth_matches_oracle(shape):
+    rng = np.random.default_rng(3)
+    f = rng.random(shape)
+    assert np.allclose(kw.smooth(f, True), ks.smooth(f, True), rtol=1e-12, atol=1e-12)
+    assert np.allclose(kw.getWin(shape, "Blackman", Rotation=True, Symmetric=[s % 2 == 1 for s in shape]),
+                       ks.get_win(list(shape), "Blackman", rotation=True, symmetric=[s % 2 == 1 for s in shape]))
+
+
+def test_problem_contents_heterogeneous_absorbing_source():
+    shape = (24, 20, 16)
+    g, o = _grids(shape, 1e-4)
+    g.setTime(30, 2e-8)
+    rng = np.random.default_rng(5)
+    c = 1500 + 100 * rng.random(shape)
+    rho = 1000 + 50 * rng.random(shape)
+    pm = np.zeros(shape)
+    pm[3, 4:8, 5:9] = 1
+    sig = np.sin(np.arange(12.0))
+    sensor = np.zeros(shape)
+    sensor[10, :, 3] = 1
+    P = _prepare(3, g, {"sound_speed": c, "density": rho, "alpha_coeff": 0.5, "alpha_power": 1.3, "BonA": 4.0},
+                 {"p_mask": pm, "p": sig}, {"mask": sensor, "record": ["p", "p_rms"]}, {"PMLSize": 3})
+    pr = P.problem
+    N = int(np.prod(shape))
+    assert (pr.dim, pr.Nx, pr.Ny, pr.Nz, pr.Nt) == (3, 24, 20, 16, 30)
+    assert pr.c_ref == pytest.approx(c.max())
+    assert pr.absorbing_flag == _abi.KW_ABSORBING and pr.nonlinear_flag == 1
+    assert np.allclose(_arr(pr.c0, N), c.ravel(order="F").astype(np.float32))
+    # staggered density: midpoint average along each axis, last plane kept (kspaceFirstOrder3D.m:590-601)
+    sgx = _arr(pr.rho0_sgx, N).reshape(shape, order="F")
+    assert np.allclose(sgx[:-1], (0.5 * (rho[:-1] + rho[1:])).astype(np.float32))
+    assert np.allclose(sgx[-1], rho[-1].astype(np.float32))
+    # source: find(mask) order, one signal scaled by 2 dt / (N c0(first point) dx) (scaleSourceTerms.m)
+    pos = np.flatnonzero(pm.ravel(order="F"))
+    assert np.array_equal(_arr(pr.p_source.index, pos.size, np.uint64), pos + 1)
+    scale = 2 * 2e-8 / (3 * c.ravel(order="F")[pos[0]] * 1e-4)
+    assert np.allclose(_arr(pr.p_source.input, 12), (sig * scale).astype(np.float32), rtol=1e-6)
+    assert pr.p_source.mode == _abi.SOURCE_MODES["additive"]
+    idx = np.flatnonzero(sensor.ravel(order="F"))
+    assert np.array_equal(_arr(pr.sensor_mask_index, idx.size, np.uint64), idx + 1)
+    assert pr.record == (1 << _abi.REC_BITS["p"]) | (1 << _abi.REC_BITS["p_rms"])
+
+
+def test_pml_outside_expands_grid():
+    g, _ = _grids((30, 26), 1e-4)
+    g.setTime(10, 2e-8)
+    mask = np.zeros((30, 26))
+    mask[5, :] = 1
+    P = _prepare(2, g, {"sound_speed": 1500.0, "density": 1000.0}, {"p0": np.ones((30, 26))},
+                 {"mask": mask, "record": ["p_final"]}, {"PMLSize": [4, 6], "PMLInside": False})
+    assert (P.problem.Nx, P.problem.Ny) == (38, 38)
+    assert list(P.problem.inside_lo)[:2] == [5, 7] and list(P.problem.inside_hi)[:2] == [34, 32]
+
+
+@pytest.mark.parametrize("medium,source,sensor,opts,msg", [
+    ({}, {}, None, {}, "sound_speed"),
+    ({"sound_speed": 1500.0, "alpha_coeff": 0.5, "alpha_power": 3.2}, {}, None, {}, "between 0 and 3"),
+    ({"sound_speed": 1500.0, "alpha_coeff": 0.5, "alpha_power": 1.0}, {}, None, {}, "alpha_power = 1"),
+    ({"sound_speed": 1500.0, "BonA": 5.0}, {"p0": np.ones((16, 16))}, None, {}, "density must be explicitly"),
+    ({"sound_speed": 1500.0, "density": 1.0}, {"p0": np.ones((16, 16)), "p": np.ones(4), "p_mask": np.ones((16, 16))},
+     None, {}, "can't be defined in the same"),
+    ({"sound_speed": 1500.0}, {"p0": np.ones((16, 16))}, {"mask": np.ones((16, 16)), "record": ["q"]}, {},
+     "not a valid input"),
+    ({"sound_speed": 1500.0}, {"p0": np.ones((16, 16))}, {"mask": np.ones((16, 16))}, {"PMLSize": 9},
+     "PML must be smaller"),
+    ({"sound_speed": 1500.0}, {"p0": np.ones((16, 16))}, {"mask": np.ones((16, 16)), "record_start_index": 99}, {},
+     "record_start_index"),
+    ({"sound_speed": 1500.0}, {"p0": np.ones((16, 16))}, {"mask": 2 * np.ones((16, 16))}, {}, "binary grid"),
+    ({"sound_speed": 1500.0}, {"p0": np.ones((16, 16))}, None, {"Smooth": [True, 1]}, "Boolean"),
+    ({"sound_speed": 1500.0}, {"p0": np.ones((16, 16))}, None, {"NoSuchOption": 1}, "Unknown optional input"),
+])
+def test_setup_errors_mirror_reference(medium, source, sensor, opts, msg):
+    g = kw.kWaveGrid(16, 1e-4, 16, 1e-4)
+    g.setTime(10, 2e-8)
+    with pytest.raises(KWaveInputError, match=msg):
+        _prepare(2, g, medium, source, sensor, opts)
+
+
+def test_time_varying_source_needs_explicit_time():
+    g = kw.kWaveGrid(16, 1e-4, 16, 1e-4)
+    pm = np.zeros((16, 16))
+    pm[4, 4] = 1
+    with pytest.raises(KWaveInputError, match="defined explicitly"):
+        _prepare(2, g, {"sound_speed": 1500.0}, {"p": np.ones(5), "p_mask": pm}, None, {})
+
+
+def test_labelled_source_rows():
+    g = kw.kWaveGrid(16, 1e-4, 16, 1e-4)
+    g.setTime(10, 2e-8)
+    pm = np.zeros((16, 16))
+    pm[2, 3] = 2
+    pm[5, 3] = 1
+    pm[7, 9] = 2
+    P = _prepare(2, g, {"sound_speed": 1500.0}, {"p": np.ones((2, 5)), "p_mask": pm, "p_mode": "dirichlet"}, None,
+                 {"PMLSize": 4})
+    src = P.problem.p_source
+    assert src.num_signals == 2 and src.num_points == 3
+    assert list(_arr(src.signal_index, 3, np.uint64)) == [2, 1, 2]
+    with pytest.raises(KWaveInputError, match="labelled"):
+        _prepare(2, g, {"sound_speed": 1500.0}, {"p": np.ones((3, 5)), "p_mask": pm}, None, {"PMLSize": 4})
