@@ -181,13 +181,13 @@ __host__ __device__ constexpr int ks_lines(int n) {
 // y-pass (C2C along axis 1, in place).  grid = (ceil(N0/TY), N2h, nfields)
 // ---------------------------------------------------------------------------
 template <bool INV, int N1>
-__global__ void __launch_bounds__(kThreads, 3) ks_ypass(Spec4 bufs, Geom g, const float2 *__restrict__ tw) {
+__global__ void __launch_bounds__(kThreads, 3) ks_ypass(Spec4 bufs, Geom g, const float2 *__restrict__ tw, int kz0) {
     constexpr int TY = ks_lines(N1);
     static_assert(RPlan<N1, false>::M >= 2, "in-place pass needs two stages");
     __shared__ float2 sm[N1 * TY];
     float2 *buf = bufs.p[blockIdx.z];
     const int x0 = blockIdx.x * TY;
-    const long long base = (long long)blockIdx.y * N1 * g.N0 + x0;
+    const long long base = (long long)(blockIdx.y + kz0) * N1 * g.N0 + x0;
     const int N0 = g.N0;
     auto ld = [&](int, int, int l, int i) -> float2 {
         return x0 + l < N0 ? buf[base + (long long)i * N0 + l] : make_float2(0.f, 0.f);
@@ -204,14 +204,15 @@ __global__ void __launch_bounds__(kThreads, 3) ks_ypass(Spec4 bufs, Geom g, cons
 // ---------------------------------------------------------------------------
 template <int N0>
 __global__ void __launch_bounds__(kThreads, 3) ks_xpass(Spec4 bufs, Geom g, const float2 *__restrict__ tw,
-                                                         OpParams P, OpSet ops, int fanout) {
+                                                         OpParams P, OpSet ops, int fanout, int kz0, int nkz) {
     constexpr int NL = ks_lines(N0);
     static_assert(RPlan<N0, false>::M >= 2, "in-place pass needs two stages");
     __shared__ float2 sm[NL * Padded<N0>::LS];
     __shared__ float kyz2[NL];
     __shared__ int liy[NL], liz[NL];
-    const int lines_total = g.N1 * g.N2h;
-    const int line0 = blockIdx.x * NL;
+    // lines (y, kz) of kz planes kz0 .. kz0+nkz-1
+    const int lines_total = (kz0 + nkz) * g.N1;
+    const int line0 = kz0 * g.N1 + blockIdx.x * NL;
     const int f = fanout ? 0 : blockIdx.z;
     for (int l = threadIdx.x; l < NL; l += kThreads) {
         const int line = min(line0 + l, lines_total - 1);

@@ -15,6 +15,8 @@
 #include <cstdio>
 #include <cstring>
 #include <string>
+#include <cstdlib>
+#include <map>
 #include <mutex>
 #include <vector>
 
@@ -182,6 +184,7 @@ struct kw_plan {
     // tiles
     int PL_u = 1, PL_r = 1, PL_p = 1, PL_z = 1, TY = 1, NL = 1;
     bool static_x = false, static_y = false, static_z = false;
+    int kz_chunks = 1;               // kz chunks of the y / x / y groups (L2 reuse)
 
     // sensors / outputs
     int M = 0;
@@ -205,6 +208,16 @@ struct kw_plan {
     std::vector<TimerRec> timers;
     double t_ms[KW_KCLASS_COUNT] = {0};
     uint64_t t_count[KW_KCLASS_COUNT] = {0};
+
+    // CUDA graphs of steady-state steps, keyed by the step's structure
+    struct GraphEntry {
+        cudaGraphExec_t exec = nullptr;
+        uint64_t launches = 0;
+        int seen = 0;
+    };
+    std::map<uint32_t, GraphEntry> graphs;
+    bool use_graphs = true;
+    float *rho_first = nullptr, *u_first = nullptr;   // buffer identity for the key
 
     std::vector<void *> allocs;
     size_t bytes = 0;
@@ -310,11 +323,11 @@ kw_status dispatch(int n, A... args) {
 
 // ---- transform passes -----------------------------------------------------
 template <int N> struct YLaunch {
-    static kw_status run(kw_plan *P, bool inv, Spec4 bufs, int nf) {
-        dim3 grid((P->g.N0 + P->TY - 1) / P->TY, P->g.N2h, nf);
+    static kw_status run(kw_plan *P, bool inv, Spec4 bufs, int nf, int kz0, int nkz) {
+        dim3 grid((P->g.N0 + P->TY - 1) / P->TY, N > 0 ? nkz : P->g.N2h, nf);
         if constexpr (N > 0) {
-            if (inv) ks_ypass<true, N><<<grid, kThreads, 0, P->stream>>>(bufs, P->g, P->tw[1]);
-            else ks_ypass<false, N><<<grid, kThreads, 0, P->stream>>>(bufs, P->g, P->tw[1]);
+            if (inv) ks_ypass<true, N><<<grid, kThreads, 0, P->stream>>>(bufs, P->g, P->tw[1], kz0);
+            else ks_ypass<false, N><<<grid, kThreads, 0, P->stream>>>(bufs, P->g, P->tw[1], kz0);
         } else {
             size_t sh = (size_t)P->TY * P->g.N1 * sizeof(float2);
             if (inv) {
@@ -329,18 +342,21 @@ template <int N> struct YLaunch {
     }
 };
 
-kw_status ypass(kw_plan *P, bool inv, Spec4 bufs, int nf) {
+// kz planes [kz0, kz0 + nkz) only (static kernels); the runtime kernels
+// always take every plane and must be called with the full range
+kw_status ypass(kw_plan *P, bool inv, Spec4 bufs, int nf, int kz0 = 0, int nkz = -1) {
     if (P->g.N1 == 1 || nf == 0) return KW_OK;
     Scope s(P, KW_KCLASS_YPASS);
-    return dispatch<YLaunch>(P->static_y ? P->g.N1 : 0, P, inv, bufs, nf);
+    if (nkz < 0) { kz0 = 0; nkz = P->g.N2h; }
+    return dispatch<YLaunch>(P->static_y ? P->g.N1 : 0, P, inv, bufs, nf, kz0, nkz);
 }
 
 template <int N> struct XLaunch {
-    static kw_status run(kw_plan *P, Spec4 bufs, OpSet ops, int fanout, int nf) {
-        const int lines = P->g.N1 * P->g.N2h;
+    static kw_status run(kw_plan *P, Spec4 bufs, OpSet ops, int fanout, int nf, int kz0, int nkz) {
+        const int lines = P->g.N1 * (N > 0 ? nkz : P->g.N2h);
         dim3 grid((lines + P->NL - 1) / P->NL, 1, fanout ? 1 : nf);
         if constexpr (N > 0) {
-            ks_xpass<N><<<grid, kThreads, 0, P->stream>>>(bufs, P->g, P->tw[0], P->op, ops, fanout);
+            ks_xpass<N><<<grid, kThreads, 0, P->stream>>>(bufs, P->g, P->tw[0], P->op, ops, fanout, kz0, nkz);
         } else {
             size_t sh = (size_t)(fanout ? 2 : 1) * P->NL * P->g.N0 * sizeof(float2);
             KW_TRY(set_smem((const void *)k_xpass<0, 0>, sh));
@@ -350,9 +366,27 @@ template <int N> struct XLaunch {
     }
 };
 
-kw_status xpass(kw_plan *P, Spec4 bufs, OpSet ops, int fanout, int nf) {
+kw_status xpass(kw_plan *P, Spec4 bufs, OpSet ops, int fanout, int nf, int kz0 = 0, int nkz = -1) {
     Scope s(P, KW_KCLASS_XPASS);
-    return dispatch<XLaunch>(P->static_x ? P->g.N0 : 0, P, bufs, ops, fanout, nf);
+    if (nkz < 0) { kz0 = 0; nkz = P->g.N2h; }
+    return dispatch<XLaunch>(P->static_x ? P->g.N0 : 0, P, bufs, ops, fanout, nf, kz0, nkz);
+}
+
+// y / x / y passes of one spectral group, chunked over kz planes so that a
+// chunk's half spectrum written by one pass is still in L2 when the next pass
+// reads it.  fanout: buffer 0 is transformed once and ops 0..n-1 write
+// buffers 0..n-1; otherwise the n buffers each get their own operator.
+kw_status yxy_group(kw_plan *P, Spec4 bufs, int n, OpSet ops, bool fanout) {
+    const int nch = (P->static_x && (P->static_y || P->g.N1 == 1)) ? P->kz_chunks : 1;
+    const int N2h = P->g.N2h;
+    for (int c = 0; c < nch; ++c) {
+        const int kz0 = (int)((long long)N2h * c / nch), kz1 = (int)((long long)N2h * (c + 1) / nch);
+        const int nkz = nch > 1 ? kz1 - kz0 : -1;
+        KW_TRY(ypass(P, false, bufs, fanout ? 1 : n, kz0, nkz));
+        KW_TRY(xpass(P, bufs, ops, fanout ? 1 : 0, fanout ? 1 : n, kz0, nkz));
+        KW_TRY(ypass(P, true, bufs, n, kz0, nkz));
+    }
+    return KW_OK;
 }
 
 template <int N> struct ZR2CLaunch {
@@ -403,14 +437,10 @@ Spec4 specs(kw_plan *P, int a, int b = -1, int c = -1) {
 // z-half spectrum of p on entry; spec[0..D-1] hold dd_pos_i kappa p_k after
 // the inverse x and y passes on exit.
 kw_status grad_group(kw_plan *P) {
-    KW_TRY(ypass(P, false, specs(P, 0), 1));
     OpSet ops{};
     ops.n = P->D;
     for (int i = 0; i < P->D; ++i) { ops.kind[i] = OP_GRAD_POS; ops.axis[i] = P->comp_axis[i]; }
-    Spec4 all = specs(P, 0, 1, 2);
-    KW_TRY(xpass(P, all, ops, 1, 1));
-    KW_TRY(ypass(P, true, all, P->D));
-    return KW_OK;
+    return yxy_group(P, specs(P, 0, 1, 2), P->D, ops, true);
 }
 
 // real(ifftn(source_kappa .* fftn(field))) into out, via spec[3]
@@ -421,12 +451,10 @@ kw_status source_filter(kw_plan *P, const float *field, float *out) {
     }
     Spec4 b{};
     b.p[0] = P->spec[3];
-    KW_TRY(ypass(P, false, b, 1));
     OpSet ops{};
     ops.n = 1;
     ops.kind[0] = OP_SRC_KAPPA;
-    KW_TRY(xpass(P, b, ops, 1, 1));
-    KW_TRY(ypass(P, true, b, 1));
+    KW_TRY(yxy_group(P, b, 1, ops, false));
     Scope s(P, KW_KCLASS_SOURCE);
     KW_TRY(zc2r(P, P->spec[3], out));
     return KW_OK;
@@ -716,18 +744,13 @@ kw_status run_step(kw_plan *P) {
     } else {
         for (int c = 0; c < P->D; ++c) KW_TRY(general_source(P, P->usrc, c, t));
         KW_TRY(stage_u(P, 0, t));
-        // divergence: real(ifftn(dd_neg_i kappa fftn(u_i))).  One field at a
-        // time through its y / x / y passes, so the half spectrum a pass
-        // writes is still in L2 when the next pass reads it.
-        for (int i = 0; i < P->D; ++i) {
-            Spec4 one = specs(P, i);
+        // divergence: real(ifftn(dd_neg_i kappa fftn(u_i))), every component in
+        // one launch per pass
+        {
             OpSet ops{};
-            ops.n = 1;
-            ops.kind[0] = OP_GRAD_NEG;
-            ops.axis[0] = P->comp_axis[i];
-            KW_TRY(ypass(P, false, one, 1));
-            KW_TRY(xpass(P, one, ops, 0, 1));
-            KW_TRY(ypass(P, true, one, 1));
+            ops.n = P->D;
+            for (int i = 0; i < P->D; ++i) { ops.kind[i] = OP_GRAD_NEG; ops.axis[i] = P->comp_axis[i]; }
+            KW_TRY(yxy_group(P, specs(P, 0, 1, 2), P->D, ops, false));
         }
         KW_TRY(general_source(P, P->psrc, 0, t));
         if (!P->absorbing) {
@@ -735,17 +758,10 @@ kw_status run_step(kw_plan *P) {
         } else {
             KW_TRY(stage_r(P, 0));
             const int nabs = (P->has_tau ? 1 : 0) + (P->has_eta ? 1 : 0);
-            int k = 0;
-            for (int term = 0; term < 2; ++term) {
-                if ((term == 0 && !P->has_tau) || (term == 1 && !P->has_eta)) continue;
-                Spec4 one = specs(P, k++);
-                OpSet o2{};
-                o2.n = 1;
-                o2.kind[0] = term == 0 ? OP_NABLA1 : OP_NABLA2;
-                KW_TRY(ypass(P, false, one, 1));
-                KW_TRY(xpass(P, one, o2, 0, 1));
-                KW_TRY(ypass(P, true, one, 1));
-            }
+            OpSet o2{};
+            if (P->has_tau) o2.kind[o2.n++] = OP_NABLA1;
+            if (P->has_eta) o2.kind[o2.n++] = OP_NABLA2;
+            if (o2.n) KW_TRY(yxy_group(P, specs(P, 0, 1), o2.n, o2, false));
             KW_TRY(stage_p(P, need_grad ? 1 : 0));
         }
         if (need_grad) KW_TRY(grad_group(P));
@@ -901,6 +917,20 @@ void plan_tiles(kw_plan *P) {
     }
     const int lines = g.N1 * g.N2h;
     P->static_x = is_static(g.N0) && (lines + ks_lines(g.N0) - 1) / ks_lines(g.N0) >= 148;
+    {
+        // chunk the y / x / y groups so one chunk of a half spectrum (written
+        // and re-read in place) stays well inside the 126 MB L2
+        // measured on B200 at 256^3: smaller chunks only add launches and
+        // tail waves, so the default is one chunk (KW_KZ_CHUNK_MB > 0 sets a size)
+        double mb = 0.0;
+        if (const char *e = getenv("KW_KZ_CHUNK_MB")) mb = atof(e);
+        const double bytes = (double)g.Nh * sizeof(float2);
+        int nch = mb > 0 ? (int)std::ceil(bytes / (mb * 1e6)) : 1;
+        nch = std::max(1, std::min(nch, g.N2h));
+        // every chunk must still fill the GPU
+        while (nch > 1 && (long long)(g.N2h / nch) * g.N1 / std::max(1, ks_lines(g.N0)) < 148) --nch;
+        P->kz_chunks = nch;
+    }
     if (P->static_x) {
         P->NL = ks_lines(g.N0);
     } else {
@@ -1051,6 +1081,9 @@ kw_status create(const kw_problem *pr, kw_plan *P) {
         KW_TRY(palloc(P, &P->u_b[i], N));
     }
     KW_TRY(palloc(P, &P->srho, N));
+    P->rho_first = P->rho[0];
+    P->u_first = P->u[0];
+    if (const char *e = getenv("KW_GRAPHS")) P->use_graphs = atoi(e) != 0;
     const int nspec = 4;
     for (int i = 0; i < nspec; ++i) KW_TRY(palloc(P, &P->spec[i], Nh));
 
@@ -1233,9 +1266,59 @@ kw_status rms_out(kw_plan *P, float *dst, const float *sq) {
     return KW_OK;
 }
 
+// A steady-state step always launches the same kernels with the same
+// arguments, except for: which of the double buffers is current, whether a
+// general (filtered) source is active, whether sensors record, and whether
+// the next step's gradient is needed.  Each combination is captured once as a
+// CUDA graph (on its second occurrence; the first runs directly) and replayed.
+kw_status run_step_graphed(kw_plan *P) {
+    const int t = P->t;
+    if (!P->use_graphs || P->timing_mask || (t == 1 && P->p0)) return run_step(P);
+    uint32_t key = 0;
+    key |= (P->rho[0] == P->rho_first) ? 1u : 0u;
+    key |= (P->u[0] == P->u_first) ? 2u : 0u;
+    bool usrc = false;
+    for (int c = 0; c < P->D; ++c) usrc = usrc || (P->usrc.dense_general && P->usrc.sig[c] && t <= P->usrc.T[c]);
+    key |= usrc ? 4u : 0u;
+    key |= (P->psrc.dense_general && t <= P->psrc.T[0]) ? 8u : 0u;
+    key |= (!P->time_rev && t >= P->record_start) ? 16u : 0u;
+    key |= (t < P->index_end) ? 32u : 0u;
+    kw_plan::GraphEntry &e = P->graphs[key];
+    if (e.exec) {
+        KW_CUDA(cudaGraphLaunch(e.exec, P->stream));
+        for (int i = 0; i < 3; ++i) {
+            std::swap(P->u[i], P->u_b[i]);
+            std::swap(P->rho[i], P->rho_b[i]);
+        }
+        P->launches += e.launches;
+        P->t += 1;
+        return KW_OK;
+    }
+    if (e.seen == 0) {
+        e.seen = 1;
+        return run_step(P);
+    }
+    const uint64_t l0 = P->launches;
+    KW_CUDA(cudaStreamBeginCapture(P->stream, cudaStreamCaptureModeThreadLocal));
+    const kw_status st = run_step(P);
+    cudaGraph_t graph = nullptr;
+    const cudaError_t ce = cudaStreamEndCapture(P->stream, &graph);
+    if (st != KW_OK) {
+        if (graph) cudaGraphDestroy(graph);
+        return st;
+    }
+    if (ce != cudaSuccess) return fail(KW_ERR_CUDA, "step capture failed: %s", cudaGetErrorString(ce));
+    const cudaError_t ie = cudaGraphInstantiate(&e.exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (ie != cudaSuccess) return fail(KW_ERR_CUDA, "graph instantiation failed: %s", cudaGetErrorString(ie));
+    e.launches = P->launches - l0;
+    KW_CUDA(cudaGraphLaunch(e.exec, P->stream));   // the captured step has not run yet
+    return KW_OK;
+}
+
 kw_status run_steps(kw_plan *P, uint64_t n) {
     if (!P->started) KW_TRY(start(P));
-    for (uint64_t k = 0; k < n && P->t <= P->index_end; ++k) KW_TRY(run_step(P));
+    for (uint64_t k = 0; k < n && P->t <= P->index_end; ++k) KW_TRY(run_step_graphed(P));
     if (P->time_rev && P->t > P->index_end) {
         k_tr_final<<<(P->M + 255) / 256, 256, 0, P->stream>>>(P->sidx, P->M, P->tr_data, P->p);
         KW_TRY(launched(P));
@@ -1388,6 +1471,8 @@ kw_status kw_plan_destroy(kw_plan *P) {
     if (!P) return KW_OK;
     cudaSetDevice(P->device);
     if (P->stream) cudaStreamSynchronize(P->stream);
+    for (auto &kv : P->graphs)
+        if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
     for (auto &r : P->timers) { cudaEventDestroy(r.a); cudaEventDestroy(r.b); }
     for (void *a : P->allocs) cudaFree(a);
     if (P->stream) cudaStreamDestroy(P->stream);
@@ -1543,11 +1628,11 @@ kw_status kw_gradient_noalloc(int32_t dim, const uint64_t shape[3], const double
     KW_TRY(zr2c(&P, field, spec));
     Spec4 b{};
     b.p[0] = spec;
-    KW_TRY(ypass(&P, false, b, 1));
     OpSet ops{};
     ops.n = 1;
     ops.kind[0] = OP_GRAD_POS;
     ops.axis[0] = iaxis;
+    KW_TRY(ypass(&P, false, b, 1));
     KW_TRY(xpass(&P, b, ops, 1, 1));
     KW_TRY(ypass(&P, true, b, 1));
     KW_TRY(zc2r(&P, spec, out));
