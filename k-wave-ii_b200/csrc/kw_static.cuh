@@ -51,29 +51,30 @@ __device__ __forceinline__ void bmap(int g, int &l, int &j) {
     else { j = g % NB; l = g / NB; }
 }
 
-// Registers a thread owns after stage S of plan (N, INV): MAXB butterflies of R values.
-template <int N, int NL, bool INV, int S> struct StageShape {
+// Registers a thread owns after stage S of plan (N, INV) in a block of NT
+// threads: MAXB butterflies of R values.
+template <int N, int NL, bool INV, int S, int NT = kThreads> struct StageShape {
     static constexpr int R = RPlan<N, INV>::R(S);
     static constexpr int NB = N / R;
     static constexpr int TOT = NB * NL;
-    static constexpr int MAXB = (TOT + kThreads - 1) / kThreads;
+    static constexpr int MAXB = (TOT + NT - 1) / NT;
 };
 // the shape of the registers handed between an inverse's last stage and a
 // forward's first stage (identical by construction)
-template <int N, int NL> using HandShape = StageShape<N, NL, false, 0>;
+template <int N, int NL, int NT = kThreads> using HandShape = StageShape<N, NL, false, 0, NT>;
 
-template <int N, int NL, bool IL, bool INV, int S, class Ld, class St>
+template <int N, int NL, bool IL, bool INV, int S, int NT, class Ld, class St>
 __device__ __forceinline__ void rs_stage(float2 *sm, const float2 *__restrict__ tw, Ld &ld, St &st) {
     using P = RPlan<N, INV>;
-    using SH = StageShape<N, NL, INV, S>;
+    using SH = StageShape<N, NL, INV, S, NT>;
     constexpr int M = P::M, R = SH::R, NS = P::NS(S), NB = SH::NB;
     constexpr int TOT = SH::TOT, MAXB = SH::MAXB;
     constexpr int TWS = N / (NS * R);
     float2 v[MAXB][R];
 #pragma unroll
     for (int b = 0; b < MAXB; ++b) {
-        const int g = threadIdx.x + b * kThreads;
-        if (TOT % kThreads == 0 || g < TOT) {
+        const int g = threadIdx.x + b * NT;
+        if (TOT % NT == 0 || g < TOT) {
             int l, j;
             bmap<NB, NL, IL>(g, l, j);
 #pragma unroll
@@ -97,8 +98,8 @@ __device__ __forceinline__ void rs_stage(float2 *sm, const float2 *__restrict__ 
     if constexpr (S == M - 1) {
 #pragma unroll
         for (int b = 0; b < MAXB; ++b) {
-            const int g = threadIdx.x + b * kThreads;
-            if (TOT % kThreads == 0 || g < TOT) {
+            const int g = threadIdx.x + b * NT;
+            if (TOT % NT == 0 || g < TOT) {
                 int l, j;
                 bmap<NB, NL, IL>(g, l, j);
                 const int base = (j / NS) * NS * R + j % NS;
@@ -110,8 +111,8 @@ __device__ __forceinline__ void rs_stage(float2 *sm, const float2 *__restrict__ 
         __syncthreads();   // earlier readers of the tile are done
 #pragma unroll
         for (int b = 0; b < MAXB; ++b) {
-            const int g = threadIdx.x + b * kThreads;
-            if (TOT % kThreads == 0 || g < TOT) {
+            const int g = threadIdx.x + b * NT;
+            if (TOT % NT == 0 || g < TOT) {
                 int l, j;
                 bmap<NB, NL, IL>(g, l, j);
                 const int base = (j / NS) * NS * R + j % NS;
@@ -123,18 +124,18 @@ __device__ __forceinline__ void rs_stage(float2 *sm, const float2 *__restrict__ 
     }
 }
 
-template <int N, int NL, bool IL, bool INV, int S = 0, class Ld, class St>
+template <int N, int NL, bool IL, bool INV, int S = 0, int NT = kThreads, class Ld, class St>
 __device__ __forceinline__ void rs_fft(float2 *sm, const float2 *__restrict__ tw, Ld &ld, St &st) {
-    rs_stage<N, NL, IL, INV, S>(sm, tw, ld, st);
-    if constexpr (S + 1 < RPlan<N, INV>::M) rs_fft<N, NL, IL, INV, S + 1>(sm, tw, ld, st);
+    rs_stage<N, NL, IL, INV, S, NT>(sm, tw, ld, st);
+    if constexpr (S + 1 < RPlan<N, INV>::M) rs_fft<N, NL, IL, INV, S + 1, NT>(sm, tw, ld, st);
 }
 
 // (line, element) owned by hand-off register (b, t)
-template <int N, int NL, bool IL>
+template <int N, int NL, bool IL, int NT = kThreads>
 __device__ __forceinline__ bool hand_pos(int b, int t, int &l, int &i) {
-    using SH = HandShape<N, NL>;
-    const int g = threadIdx.x + b * kThreads;
-    if (!(SH::TOT % kThreads == 0 || g < SH::TOT)) return false;
+    using SH = HandShape<N, NL, NT>;
+    const int g = threadIdx.x + b * NT;
+    if (!(SH::TOT % NT == 0 || g < SH::TOT)) return false;
     int j;
     bmap<SH::NB, NL, IL>(g, l, j);
     i = j + t * SH::NB;

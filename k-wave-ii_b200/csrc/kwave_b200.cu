@@ -931,6 +931,7 @@ void plan_tiles(kw_plan *P) {
         while (nch > 1 && (long long)(g.N2h / nch) * g.N1 / std::max(1, ks_lines(g.N0)) < 148) --nch;
         P->kz_chunks = nch;
     }
+
     if (P->static_x) {
         P->NL = ks_lines(g.N0);
     } else {
