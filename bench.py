@@ -82,7 +82,31 @@ def workload(seed=0, N=256, Nt=1000, dx=0.2e-3, pml=10):
                 options={"PMLSize": pml}, src_len=len(sig))
 
 
+def workload2d(seed=0, N=256, Nt=500, dx=0.1e-3, pml=10, absorbing=True):
+    """2-D heterogeneous run: blob sound speed, disc p0, one sensor line."""
+    rng = np.random.default_rng(seed)
+    c = np.full((N, N), 1500.0)
+    ax = np.arange(N, dtype=np.float64)
+    for _ in range(6):
+        cx, cy = rng.uniform(pml, N - pml, 2)
+        sg = rng.uniform(4.0, 16.0)
+        c += rng.uniform(-100.0, 200.0) * np.exp(-((ax[:, None] - cx) ** 2 + (ax[None, :] - cy) ** 2) / (2 * sg * sg))
+    medium = {"sound_speed": c, "density": 1000.0 + 0.6 * (c - 1500.0)}
+    if absorbing:
+        medium.update(alpha_coeff=0.75, alpha_power=1.5)
+    yy, xx = np.meshgrid(ax, ax)
+    p0 = ((xx - N / 2) ** 2 + (yy - N / 2) ** 2 <= (N / 16) ** 2).astype(np.float64)
+    sensor_mask = np.zeros((N, N))
+    sensor_mask[pml + 2, :] = 1
+    return dict(shape=(N, N), dx=dx, Nt=Nt, dt=0.3 * dx / c.max(), medium=medium, source={"p0": p0},
+                sensor={"mask": sensor_mask, "record": ["p", "p_max"]}, options={"PMLSize": pml}, src_len=0)
+
+
 def make_grid(kw, w):
+    if len(w["shape"]) == 2:
+        g = kw.kWaveGrid(w["shape"][0], w["dx"], w["shape"][1], w["dx"])
+        g.setTime(w["Nt"], w["dt"])
+        return g
     g = kw.kWaveGrid(w["shape"][0], w["dx"], w["shape"][1], w["dx"], w["shape"][2], w["dx"])
     g.setTime(w["Nt"], w["dt"])
     return g
@@ -232,6 +256,105 @@ def run_reference(args, ws, rank):
     print(json.dumps(line), flush=True)
 
 
+# Request mix of the served stream: (kind, size, Nt, weight).  Sizes are the
+# small-to-medium runs a service sees next to the 256^3 headline run.
+SERVE_MIX = [("2d", 256, 500, 0.30), ("2d", 512, 800, 0.15), ("3d", 64, 300, 0.30), ("3d", 96, 400, 0.15),
+             ("3d", 128, 500, 0.10)]
+
+
+def _latency_stats(lat_ms):
+    v = np.sort(np.asarray(lat_ms, dtype=np.float64))
+    return {"p50_ms": float(np.percentile(v, 50)), "p99_ms": float(np.percentile(v, 99)), "mean_ms": float(v.mean())}
+
+
+def _rel_l2(a, b):
+    if isinstance(b, dict):
+        return max(_rel_l2(a[k], b[k]) for k in b)
+    a = np.asarray(a, dtype=np.float64).ravel()
+    b = np.asarray(b, dtype=np.float64).ravel()
+    d = np.linalg.norm(b)
+    return float(np.linalg.norm(a - b) / (d if d > 0 else 1.0))
+
+
+def served_section(kw, device, n_req=48, seed=7, load=0.9):
+    """Continuous batching against the plain path on the same request stream.
+
+    Two passes per path over the same n_req requests drawn from SERVE_MIX:
+    'saturated' submits everything at t = 0 (aggregate Gcell-steps/s =
+    cell-steps / makespan); 'poisson' submits at Poisson arrival times whose
+    rate is `load` x the plain path's capacity (p50 / p99 of submit->result
+    latency).  The plain path runs the requests one after another through
+    the drop-in call on a prepared problem (plan, loop, outputs to host);
+    the served path hands them to kwave_b200.Server.  Host setup (input
+    checking, smoothing) is done beforehand for both.  Every served result
+    is compared with the plain result of the same request.
+    """
+    rng = np.random.default_rng(seed)
+    kinds = [m[:3] for m in SERVE_MIX]
+    wts = np.array([m[3] for m in SERVE_MIX])
+    picks = rng.choice(len(kinds), size=n_req, p=wts / wts.sum())
+    preps, cells = {}, {}
+    for i, (kind, n, nt) in enumerate(kinds):
+        w = workload2d(seed=i, N=n, Nt=nt) if kind == "2d" else workload(seed=i, N=n, Nt=nt)
+        dim = 2 if kind == "2d" else 3
+        preps[i] = kw.Server.prepare(dim, make_grid(kw, w), w["medium"], w["source"], w["sensor"],
+                                     **dict(w["options"], DeviceNum=device))
+        cells[i] = float(np.prod(w["shape"])) * nt
+    work = float(sum(cells[k] for k in picks))
+
+    def plain(arrivals):
+        lat, outs = [], []
+        t0 = time.perf_counter()
+        for k, a in zip(picks, arrivals):
+            now = time.perf_counter() - t0
+            if a > now:
+                time.sleep(a - now)
+            with kw.Simulation.from_prepared(preps[k]) as sim:
+                outs.append(sim.run())
+            lat.append((time.perf_counter() - t0 - a) * 1e3)
+        return time.perf_counter() - t0, lat, outs
+
+    def served(arrivals):
+        with kw.Server(device=device) as srv:
+            t0 = time.perf_counter()
+            tickets = []
+            for k, a in zip(picks, arrivals):
+                now = time.perf_counter() - t0
+                if a > now:
+                    time.sleep(a - now)
+                tickets.append(srv.submit_prepared(preps[k]))
+            res = [srv.result(t, with_latency=True) for t in tickets]
+            span = time.perf_counter() - t0
+        return span, [r[1] for r in res], [r[0] for r in res]
+
+    # warm both paths (module load, first plans, graph capture paths)
+    for k in preps:
+        with kw.Simulation.from_prepared(preps[k]) as sim:
+            sim.run()
+    zeros = np.zeros(n_req)
+    p_span, _, p_outs = plain(zeros)
+    s_span, _, s_outs = served(zeros)
+    err = max(_rel_l2(a, b) for a, b in zip(s_outs, p_outs))
+    rate = load * n_req / p_span
+    arrivals = np.cumsum(rng.exponential(1.0 / rate, size=n_req))
+    arrivals -= arrivals[0]
+    pp_span, pp_lat, _ = plain(arrivals)
+    sp_span, sp_lat, sp_outs = served(arrivals)
+    err = max(err, max(_rel_l2(a, b) for a, b in zip(sp_outs, p_outs)))
+    mix = ["%s %s Nt=%d x%d" % (kind, "x".join([str(n)] * (2 if kind == "2d" else 3)), nt, int((picks == i).sum()))
+           for i, (kind, n, nt) in enumerate(kinds)]
+    return {
+        "requests": n_req, "mix": mix, "cell_steps": work,
+        "saturated": {"served_gcell_steps_per_s": work / s_span / 1e9, "plain_gcell_steps_per_s": work / p_span / 1e9,
+                      "served_makespan_s": s_span, "plain_makespan_s": p_span},
+        "poisson": {"rate_per_s": rate, "load_vs_plain_capacity": load,
+                    "served": _latency_stats(sp_lat), "plain": _latency_stats(pp_lat),
+                    "served_gcell_steps_per_s": work / sp_span / 1e9, "plain_gcell_steps_per_s": work / pp_span / 1e9},
+        "max_rel_l2_served_vs_plain": err, "tolerance": 1e-4,
+        "latency": "submit -> outputs on the host, wall clock",
+    }
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -243,6 +366,7 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--Nt", type=int, default=1000)
     ap.add_argument("--N", type=int, default=256)
+    ap.add_argument("--serve-requests", type=int, default=48, help="0 skips the served-stream section")
     args = ap.parse_args()
     ws, rank, local = dist_setup()
     if args.impl == "reference":
@@ -321,6 +445,10 @@ def main():
                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "steps": args.e2e_steps,
                "call": "kwave_b200.Simulation(...).run() == kspaceFirstOrder3D(kgrid, medium, source, sensor)"}
 
+    served = None
+    if args.serve_requests > 0:
+        served = served_section(kw, local, n_req=args.serve_requests, seed=7 + rank)
+
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu:
         try:
@@ -341,7 +469,7 @@ def main():
                            "l2": "no flush: inputs larger than L2 (device working set %.2f GB vs 126 MB L2)" % dev_gb,
                            "parallelism": "replicas x%d" % ws},
                 "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
-                "clocks": clocks, "kernel_classes": classes}
+                "clocks": clocks, "kernel_classes": classes, "served": served}
         print(json.dumps(line), flush=True)
     if ws > 1:
         import torch.distributed as dist

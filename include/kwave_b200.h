@@ -216,6 +216,41 @@ kw_status kw_run_timed(kw_plan *plan, uint32_t n, double *device_ms);
 kw_status kw_launch_count(const kw_plan *plan, uint64_t *launches);
 
 /*
+ * Serving: continuous batching of independent simulations on one GPU.  A
+ * persistent worker thread admits submitted problems in arrival order
+ * whenever the HBM budget and the slot limit allow, keeps every admitted
+ * simulation's fields and operators resident, and advances all of them in
+ * slices of steps on their own streams so their kernels overlap on the
+ * device; finished simulations release their memory and slot at once.  No
+ * reference counterpart (the reference runs one simulation per call).
+ */
+typedef struct kw_server kw_server;
+
+typedef struct kw_server_config {
+    int32_t  device;             /* CUDA device ordinal */
+    uint64_t hbm_budget_bytes;   /* admission budget; 0 = 80% of free memory */
+    int32_t  max_active;         /* simulations resident at once; 0 = 32 */
+    int32_t  steps_per_slice;    /* steps issued per simulation per round; 0 = 32 */
+} kw_server_config;
+
+typedef struct kw_server_stats {
+    uint64_t submitted, admitted, completed, failed;
+    uint64_t active, pending;
+    double   p50_ms, p99_ms, mean_ms;   /* submit -> result latency of completed requests */
+    double   cell_steps;                /* cell-steps of completed requests */
+    double   busy_seconds;              /* first admission -> last completion */
+} kw_server_stats;
+
+kw_status kw_server_create(const kw_server_config *config, kw_server **server);
+/* Copies every array of *problem; the caller may free them on return. */
+kw_status kw_server_submit(kw_server *server, const kw_problem *problem, uint64_t *ticket);
+/* Blocks until the request is done; copies its outputs (like kw_copy_outputs). */
+kw_status kw_server_wait(kw_server *server, uint64_t ticket, kw_outputs *out, double *latency_ms);
+kw_status kw_server_get_stats(kw_server *server, kw_server_stats *stats);
+/* Stops the worker after the admitted and pending requests finish. */
+kw_status kw_server_destroy(kw_server *server);
+
+/*
  * Allocation-free staggered spectral gradient.  No counterpart in the
  * reference: it exists for callers that must not have this library allocate
  * device memory -- a MEX function working on gpuArray data owned by MATLAB's

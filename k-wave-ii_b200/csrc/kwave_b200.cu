@@ -22,6 +22,11 @@
 
 #include "kw_kernels.cuh"
 #include "kw_static.cuh"
+#include <chrono>
+#include <condition_variable>
+#include <deque>
+#include <memory>
+#include <thread>
 #include "../../include/kwave_b200.h"
 
 using namespace kw;
@@ -97,26 +102,6 @@ std::vector<double> get_pml(int n, double d, double dt, double c, int size, doub
 
 // db2neper.m:52
 double db2neper(double a, double y) { return 100.0 * a * std::pow(1e-6 / (2 * M_PI), y) / (20.0 * std::log10(std::exp(1.0))); }
-
-template <typename T>
-kw_status dev_alloc(T **p, size_t count) {
-    *p = nullptr;
-    if (count == 0) return KW_OK;
-    cudaError_t e = cudaMalloc((void **)p, count * sizeof(T));
-    if (e != cudaSuccess) {
-        *p = nullptr;
-        return fail(e == cudaErrorMemoryAllocation ? KW_ERR_NOMEM : KW_ERR_CUDA, "cudaMalloc of %zu bytes failed: %s",
-                    count * sizeof(T), cudaGetErrorString(e));
-    }
-    return KW_OK;
-}
-
-template <typename T>
-kw_status upload(T **p, const T *host, size_t count) {
-    KW_TRY(dev_alloc(p, count));
-    if (count) KW_CUDA(cudaMemcpy(*p, host, count * sizeof(T), cudaMemcpyHostToDevice));
-    return KW_OK;
-}
 
 }  // namespace
 
@@ -227,9 +212,21 @@ struct kw_plan {
 
 namespace {
 
+// Plan memory is stream-ordered (cudaMallocAsync / cudaFreeAsync on the plan's
+// stream), so creating and destroying plans never synchronises other plans'
+// work on the device (the serving loop relies on this).
 template <typename T>
 kw_status palloc(kw_plan *P, T **p, size_t count) {
-    KW_TRY(dev_alloc(p, count));
+    *p = nullptr;
+    if (count == 0) return KW_OK;
+    {
+        cudaError_t e = cudaMallocAsync((void **)p, count * sizeof(T), P->stream);
+        if (e != cudaSuccess) {
+            *p = nullptr;
+            return fail(e == cudaErrorMemoryAllocation ? KW_ERR_NOMEM : KW_ERR_CUDA,
+                        "device allocation of %zu bytes failed: %s", count * sizeof(T), cudaGetErrorString(e));
+        }
+    }
     if (*p) {
         P->allocs.push_back((void *)*p);
         P->bytes += count * sizeof(T);
@@ -867,13 +864,12 @@ kw_status setup_source(kw_plan *P, SourceDev &S, const kw_source *src, int ncomp
             S.dense_fast = true;
             KW_TRY(palloc(P, &S.F, N));
             float *m = nullptr;
-            KW_TRY(dev_alloc(&m, N));
+            KW_CUDA(cudaMallocAsync((void **)&m, N * sizeof(float), P->stream));
             KW_CUDA(cudaMemsetAsync(m, 0, N * sizeof(float), P->stream));
             k_set_points<<<(S.npts + 255) / 256, 256, 0, P->stream>>>(S.pos, S.npts, 1.0f, m);
             KW_TRY(launched(P));
             kw_status st = source_filter(P, m, S.F);
-            cudaStreamSynchronize(P->stream);
-            cudaFree(m);
+            cudaFreeAsync(m, P->stream);
             KW_TRY(st);
         } else {
             S.dense_general = true;
@@ -1003,6 +999,13 @@ kw_status create(const kw_problem *pr, kw_plan *P) {
         if (q.device < 0 || q.device >= ndev) return fail(KW_ERR_INVALID, "device %d not present (%d devices)", q.device, ndev);
     }
     KW_CUDA(cudaSetDevice(P->device));
+    {
+        cudaMemPool_t pool;
+        if (cudaDeviceGetDefaultMemPool(&pool, P->device) == cudaSuccess) {
+            uint64_t keep = UINT64_MAX;
+            cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+        }
+    }
     KW_CUDA(cudaStreamCreateWithFlags(&P->stream, cudaStreamNonBlocking));
 
     // FFT plans and operator tables (FP64 -> FP32)
@@ -1475,8 +1478,11 @@ kw_status kw_plan_destroy(kw_plan *P) {
     for (auto &kv : P->graphs)
         if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
     for (auto &r : P->timers) { cudaEventDestroy(r.a); cudaEventDestroy(r.b); }
-    for (void *a : P->allocs) cudaFree(a);
-    if (P->stream) cudaStreamDestroy(P->stream);
+    for (void *a : P->allocs) cudaFreeAsync(a, P->stream);
+    if (P->stream) {
+        cudaStreamSynchronize(P->stream);
+        cudaStreamDestroy(P->stream);
+    }
     delete P;
     return KW_OK;
 }
@@ -1648,3 +1654,5 @@ kw_status kw_plan_device_bytes(const kw_plan *P, uint64_t *bytes) {
 }
 
 }  // extern "C"
+
+#include "kw_server.inc"

@@ -9,11 +9,11 @@ is no CPU fallback.
 """
 from .kgrid import kWaveGrid
 from .helpers import makeDisc, makeBall, makeCartCircle, cart2grid, smooth, getWin, reorderBinarySensorData
-from .solver import Simulation, kspaceFirstOrder2D, kspaceFirstOrder3D, KWaveInputError
+from .solver import Simulation, Server, kspaceFirstOrder2D, kspaceFirstOrder3D, KWaveInputError
 from ._abi import KWaveError, load_library, LIB_PATH
 
 __all__ = [
     "kWaveGrid", "makeDisc", "makeBall", "makeCartCircle", "cart2grid", "smooth", "getWin",
-    "reorderBinarySensorData", "Simulation", "kspaceFirstOrder2D", "kspaceFirstOrder3D",
+    "reorderBinarySensorData", "Simulation", "Server", "kspaceFirstOrder2D", "kspaceFirstOrder3D",
     "KWaveInputError", "KWaveError", "load_library", "LIB_PATH",
 ]

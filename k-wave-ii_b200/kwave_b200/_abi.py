@@ -115,6 +115,18 @@ class kw_outputs(C.Structure):
 
 
 # every symbol the header declares, with its signature
+class kw_server_config(C.Structure):
+    _fields_ = [("device", C.c_int32), ("hbm_budget_bytes", C.c_uint64), ("max_active", C.c_int32),
+                ("steps_per_slice", C.c_int32)]
+
+
+class kw_server_stats(C.Structure):
+    _fields_ = [("submitted", C.c_uint64), ("admitted", C.c_uint64), ("completed", C.c_uint64),
+                ("failed", C.c_uint64), ("active", C.c_uint64), ("pending", C.c_uint64),
+                ("p50_ms", C.c_double), ("p99_ms", C.c_double), ("mean_ms", C.c_double),
+                ("cell_steps", C.c_double), ("busy_seconds", C.c_double)]
+
+
 SYMBOLS = {
     "kw_last_error": (C.c_char_p, []),
     "kw_abi_version": (C.c_int, []),
@@ -134,6 +146,11 @@ SYMBOLS = {
     "kw_gradient_noalloc": (C.c_int, [C.c_int32, C.POINTER(C.c_uint64), C.POINTER(C.c_double), C.c_int32,
                                       C.c_int32, C.c_double, C.c_double, C.c_int32, C.c_void_p, C.c_void_p,
                                       C.c_void_p]),
+    "kw_server_create": (C.c_int, [C.POINTER(kw_server_config), C.POINTER(C.c_void_p)]),
+    "kw_server_submit": (C.c_int, [C.c_void_p, C.POINTER(kw_problem), C.POINTER(C.c_uint64)]),
+    "kw_server_wait": (C.c_int, [C.c_void_p, C.c_uint64, C.POINTER(kw_outputs), C.POINTER(C.c_double)]),
+    "kw_server_get_stats": (C.c_int, [C.c_void_p, C.POINTER(kw_server_stats)]),
+    "kw_server_destroy": (C.c_int, [C.c_void_p]),
 }
 
 _lib = None

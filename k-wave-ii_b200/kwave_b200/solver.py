@@ -554,13 +554,24 @@ class Simulation:
     """
 
     def __init__(self, dim, kgrid, medium, source, sensor, **options):
-        self._lib = _abi.load_library()
-        self.prep = _prepare(dim, kgrid, medium, source, sensor, options)
-        h = C.c_void_p()
-        _abi.check(self._lib.kw_plan_create(C.byref(self.prep.problem), C.byref(h)))
-        self.handle = h
+        self._bind(_prepare(dim, kgrid, medium, source, sensor, options))
         self.prep.keep = None    # the library copied everything it needs
-        self.h2d_bytes = self.prep.h2d_bytes
+
+    @classmethod
+    def from_prepared(cls, prep):
+        """A plan for a problem prepared by ``Server.prepare`` (which stays
+        usable for further plans or submissions)."""
+        self = cls.__new__(cls)
+        self._bind(prep)
+        return self
+
+    def _bind(self, prep):
+        self._lib = _abi.load_library()
+        self.prep = prep
+        h = C.c_void_p()
+        _abi.check(self._lib.kw_plan_create(C.byref(prep.problem), C.byref(h)))
+        self.handle = h
+        self.h2d_bytes = prep.h2d_bytes
         d = _abi.kw_output_desc()
         _abi.check(self._lib.kw_plan_outputs(self.handle, C.byref(d)))
         self.desc = d
@@ -620,99 +631,173 @@ class Simulation:
         return b.value
 
     # -- outputs ---------------------------------------------------------------
-    def _alloc_outputs(self):
-        P = self.prep
-        M, T = P.M, P.Nt - P.record_start + 1
-        ins = tuple(int(self.desc.inside_shape[a]) for a in range(P.dim))
-        host = {}
-        o = _abi.kw_outputs()
-        rec = P.record
-
-        def buf(key, shape, slot, idx=None):
-            a = np.zeros(int(np.prod(shape)), dtype=np.float32)
-            host[key] = (a, shape)
-            if idx is None:
-                setattr(o, slot, _abi.fptr(a))
-            else:
-                getattr(o, slot)[idx] = _abi.fptr(a)
-
-        if not P.time_rev:
-            if "p" in rec:
-                buf("p", (M, T), "p")
-            for k in ("p_max", "p_min", "p_rms"):
-                if k in rec:
-                    buf(k, (M,), k)
-            for k in ("p_max_all", "p_min_all"):
-                if k in rec:
-                    buf(k, ins, k)
-            comps = ["ux", "uy", "uz"][:P.dim]
-            for i, n in enumerate(comps):
-                if "u" in rec:
-                    buf(n, (M, T), "u", i)
-                for k in ("max", "min", "rms"):
-                    if "u_" + k in rec:
-                        buf(n + "_" + k, (M,), "u_" + k, i)
-                for k in ("max_all", "min_all"):
-                    if "u_" + k in rec:
-                        buf(n + "_" + k, ins, "u_" + k, i)
-                if "u_final" in rec:
-                    buf(n + "_final", ins, "u_final", i)
-        if "p_final" in rec or P.time_rev:
-            buf("p_final", ins, "p_final")
-        return o, host
-
     def copy_outputs(self):
-        o, host = self._alloc_outputs()
+        o, host = _alloc_outputs(self.prep)
         _abi.check(self._lib.kw_copy_outputs(self.handle, C.byref(o)))
-        return self._finish(host)
+        return _finish(self.prep, host)
 
     def run(self):
-        o, host = self._alloc_outputs()
+        o, host = _alloc_outputs(self.prep)
         _abi.check(self._lib.kw_run(self.handle, C.byref(o)))
-        return self._finish(host)
+        return _finish(self.prep, host)
 
-    def _finish(self, host):
-        P = self.prep
-        out = {}
-        for k, (a, shape) in host.items():
-            out[k] = a.reshape(shape, order="F")
-        # Cartesian nearest-neighbour reorder (reorderCartData.m)
-        if P.reorder_index is not None:
-            for k in list(out):
-                if k.endswith("_all") or k.endswith("_final"):
-                    continue
-                out[k] = reorderBinarySensorData(out[k], P.reorder_index)
-        if P.cuboid_list is not None:
-            out = self._cuboids(out)
-        if not P.use_sensor:
-            return None
-        if P.time_rev:
-            return out["p_final"]
-        if not P.record_given and P.cuboid_list is None:
-            return out["p"]
-        return out
 
-    def _cuboids(self, out):
-        """Per-cuboid outputs shaped [X, Y, (Z,) T] (reorderCuboidCorners.m)."""
-        P = self.prep
-        all_idx = _find_union(P.cuboid_rows)
-        pos = {v: i for i, v in enumerate(all_idx)}
-        res = []
-        for c, rows in enumerate(P.cuboid_rows):
-            sel = np.array([pos[v] for v in rows], dtype=np.int64)
-            lo = P.cuboid_list[:P.dim, c]
-            hi = P.cuboid_list[P.dim:, c]
-            size = tuple(int(h - l + 1) for l, h in zip(lo, hi))
-            d = {}
-            for k, v in out.items():
-                if k.endswith("_all") or k.endswith("_final"):
-                    d[k] = v
-                elif v.ndim == 2:
-                    d[k] = v[sel].reshape(size + (v.shape[1],), order="F")
-                else:
-                    d[k] = v[sel].reshape(size, order="F")
-            res.append(d)
-        return res
+class Server:
+    """Continuous batching of independent kspaceFirstOrder runs on one GPU.
+
+    No counterpart in the reference, which runs one simulation per call.
+    ``submit`` runs the same setup as kspaceFirstOrder2D/3D and hands the
+    problem to the library's serving loop, which admits it against an HBM
+    budget, keeps it resident next to the other admitted runs, advances
+    every resident run by a slice of time steps per round on its own stream
+    and retires it when its loop ends; ``result`` returns exactly what the
+    plain call returns for the same inputs.
+    """
+
+    def __init__(self, device=0, hbm_budget_bytes=0, max_active=0, steps_per_slice=0):
+        self._lib = _abi.load_library()
+        cfg = _abi.kw_server_config(device=device, hbm_budget_bytes=hbm_budget_bytes, max_active=max_active,
+                                    steps_per_slice=steps_per_slice)
+        h = C.c_void_p()
+        _abi.check(self._lib.kw_server_create(C.byref(cfg), C.byref(h)))
+        self.handle = h
+        self._preps = {}
+
+    @staticmethod
+    def prepare(dim, kgrid, medium, source, sensor, **options):
+        """Input checking and setup only (host side), for submitting later."""
+        return _prepare(dim, kgrid, medium, source, sensor, options)
+
+    def submit(self, dim, kgrid, medium, source, sensor, **options):
+        return self.submit_prepared(self.prepare(dim, kgrid, medium, source, sensor, **options))
+
+    def submit_prepared(self, prep):
+        t = C.c_uint64()
+        _abi.check(self._lib.kw_server_submit(self.handle, C.byref(prep.problem), C.byref(t)))
+        self._preps[t.value] = prep
+        return t.value
+
+    def result(self, ticket, with_latency=False):
+        prep = self._preps.pop(ticket)
+        o, host = _alloc_outputs(prep)
+        ms = C.c_double()
+        _abi.check(self._lib.kw_server_wait(self.handle, ticket, C.byref(o), C.byref(ms)))
+        out = _finish(prep, host)
+        return (out, ms.value) if with_latency else out
+
+    def stats(self):
+        st = _abi.kw_server_stats()
+        _abi.check(self._lib.kw_server_get_stats(self.handle, C.byref(st)))
+        return {k: getattr(st, k) for k, _ in st._fields_}
+
+    def close(self):
+        if getattr(self, "handle", None):
+            self._lib.kw_server_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+
+def _inside_shape(prep):
+    pr = prep.problem
+    return tuple(int(pr.inside_hi[a] - pr.inside_lo[a] + 1) for a in range(prep.dim))
+
+
+def _alloc_outputs(prep):
+    """Host buffers for every recorded output and the kw_outputs naming them."""
+    P = prep
+    M, T = P.M, P.Nt - P.record_start + 1
+    ins = _inside_shape(P)
+    host = {}
+    o = _abi.kw_outputs()
+    rec = P.record
+
+    def buf(key, shape, slot, idx=None):
+        a = np.zeros(int(np.prod(shape)), dtype=np.float32)
+        host[key] = (a, shape)
+        if idx is None:
+            setattr(o, slot, _abi.fptr(a))
+        else:
+            getattr(o, slot)[idx] = _abi.fptr(a)
+
+    if not P.time_rev:
+        if "p" in rec:
+            buf("p", (M, T), "p")
+        for k in ("p_max", "p_min", "p_rms"):
+            if k in rec:
+                buf(k, (M,), k)
+        for k in ("p_max_all", "p_min_all"):
+            if k in rec:
+                buf(k, ins, k)
+        comps = ["ux", "uy", "uz"][:P.dim]
+        for i, n in enumerate(comps):
+            if "u" in rec:
+                buf(n, (M, T), "u", i)
+            for k in ("max", "min", "rms"):
+                if "u_" + k in rec:
+                    buf(n + "_" + k, (M,), "u_" + k, i)
+            for k in ("max_all", "min_all"):
+                if "u_" + k in rec:
+                    buf(n + "_" + k, ins, "u_" + k, i)
+            if "u_final" in rec:
+                buf(n + "_final", ins, "u_final", i)
+    if "p_final" in rec or P.time_rev:
+        buf("p_final", ins, "p_final")
+    return o, host
+
+
+def _finish(P, host):
+    """Shape the raw outputs the way kspaceFirstOrder2D/3D returns them."""
+    out = {}
+    for k, (a, shape) in host.items():
+        out[k] = a.reshape(shape, order="F")
+    # Cartesian nearest-neighbour reorder (reorderCartData.m)
+    if P.reorder_index is not None:
+        for k in list(out):
+            if k.endswith("_all") or k.endswith("_final"):
+                continue
+            out[k] = reorderBinarySensorData(out[k], P.reorder_index)
+    if P.cuboid_list is not None:
+        out = _cuboids(P, out)
+    if not P.use_sensor:
+        return None
+    if P.time_rev:
+        return out["p_final"]
+    if not P.record_given and P.cuboid_list is None:
+        return out["p"]
+    return out
+
+
+def _cuboids(P, out):
+    """Per-cuboid outputs shaped [X, Y, (Z,) T] (reorderCuboidCorners.m)."""
+    all_idx = _find_union(P.cuboid_rows)
+    pos = {v: i for i, v in enumerate(all_idx)}
+    res = []
+    for c, rows in enumerate(P.cuboid_rows):
+        sel = np.array([pos[v] for v in rows], dtype=np.int64)
+        lo = P.cuboid_list[:P.dim, c]
+        hi = P.cuboid_list[P.dim:, c]
+        size = tuple(int(h - l + 1) for l, h in zip(lo, hi))
+        d = {}
+        for k, v in out.items():
+            if k.endswith("_all") or k.endswith("_final"):
+                d[k] = v
+            elif v.ndim == 2:
+                d[k] = v[sel].reshape(size + (v.shape[1],), order="F")
+            else:
+                d[k] = v[sel].reshape(size, order="F")
+        res.append(d)
+    return res
 
 
 def _find_union(parts):

@@ -1,0 +1,103 @@
+"""Serving form: results of a run served in a mix equal the run alone.
+
+The serving loop admits many independent runs, keeps them resident
+together and advances each in slices of time steps interleaved with the
+others.  Every run must come back with what the plain drop-in call returns
+for the same inputs: relative L2 error <= 1e-4 on every output (the bound
+the FP32 path meets against the FP64 oracle), and in fact bit-identical,
+since each run executes the same kernels on the same data in the same
+order whatever else is resident.
+"""
+import numpy as np
+import pytest
+
+from cases import CASES, make_case
+
+TOL = 1e-4
+
+
+def _grid(mod, shape, dx, Nt, dt):
+    args = []
+    for s in shape:
+        args += [s, dx]
+    g = mod.kWaveGrid(*args)
+    g.setTime(Nt, dt)
+    return g
+
+
+def _rel(a, b):
+    a = np.asarray(a, dtype=np.float64)
+    b = np.asarray(b, dtype=np.float64)
+    d = np.linalg.norm(b.ravel())
+    return float(np.linalg.norm((a - b).ravel()) / (d if d > 0 else 1.0))
+
+
+def _flat(out):
+    if out is None:
+        return {}
+    if isinstance(out, np.ndarray):
+        return {"": out}
+    if isinstance(out, list):
+        return {"%d.%s" % (i, k): v for i, d in enumerate(out) for k, v in d.items()}
+    return dict(out)
+
+
+def _alone(kw, name):
+    dim, shape, dx, Nt, dt, med, src, sen, opts = make_case(name)
+    run = kw.kspaceFirstOrder2D if dim == 2 else kw.kspaceFirstOrder3D
+    return run(_grid(kw, shape, dx, Nt, dt), med, src, sen, **opts)
+
+
+def _submit(kw, server, name):
+    dim, shape, dx, Nt, dt, med, src, sen, opts = make_case(name)
+    return server.submit(dim, _grid(kw, shape, dx, Nt, dt), med, src, sen, **opts)
+
+
+def _compare(name, served, alone):
+    a, b = _flat(served), _flat(alone)
+    assert set(a) == set(b), (name, sorted(a), sorted(b))
+    for k in b:
+        assert a[k].shape == b[k].shape, (name, k)
+        e = _rel(a[k], b[k])
+        assert e <= TOL, "%s %s: served vs alone rel-L2 %.3e" % (name, k, e)
+        assert np.array_equal(a[k], b[k]), "%s %s: served result not bit-identical (rel-L2 %.3e)" % (name, k, e)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("max_active,slice_steps,budget", [(4, 5, 0), (32, 32, 0), (32, 16, 1)])
+def test_mix_equals_alone(max_active, slice_steps, budget):
+    """Every case of the parity suite, submitted at once, against its plain run.
+    (4, 5): few slots, short slices -- runs queue and interleave finely;
+    (32, 32): everything resident at once; budget 1 byte: one run at a time."""
+    import kwave_b200 as kw
+    alone = {n: _alone(kw, n) for n in CASES}
+    with kw.Server(max_active=max_active, steps_per_slice=slice_steps, hbm_budget_bytes=budget) as srv:
+        tickets = [(n, _submit(kw, srv, n)) for n in CASES + CASES[::-1]]
+        for n, t in tickets:
+            _compare(n, srv.result(t), alone[n])
+        st = srv.stats()
+    assert st["completed"] == 2 * len(CASES) and st["failed"] == 0
+    assert st["active"] == 0 and st["pending"] == 0
+    assert 0 < st["p50_ms"] <= st["p99_ms"]
+
+
+@pytest.mark.gpu
+def test_failed_request_does_not_disturb_others():
+    """A request the library rejects at admission (a prime factor of 11 in
+    the grid size) fails alone; the runs around it finish unchanged."""
+    import kwave_b200 as kw
+    name = "2d_hetero_abs_nl"
+    ref = _alone(kw, name)
+    bad = kw.kWaveGrid(22, 1e-4, 22, 1e-4)
+    bad.setTime(10, 2e-8)
+    with kw.Server(max_active=2, steps_per_slice=3) as srv:
+        t0 = _submit(kw, srv, name)
+        tb = srv.submit(2, bad, {"sound_speed": 1500.0}, {"p0": np.ones((22, 22))}, {"mask": np.ones((22, 22))},
+                        PMLSize=2)
+        t1 = _submit(kw, srv, name)
+        with pytest.raises(kw.KWaveError, match="prime factor"):
+            srv.result(tb)
+        _compare(name, srv.result(t0), ref)
+        _compare(name, srv.result(t1), ref)
+        st = srv.stats()
+    assert st["completed"] == 2 and st["failed"] == 1
