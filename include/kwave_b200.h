@@ -38,7 +38,7 @@ typedef int kw_status;
 #define KW_ERR_UNSUPPORTED 4   /* valid reference input this build does not handle */
 #define KW_ERR_TIMEOUT     5   /* a bounded device wait gave up */
 
-#define KW_ABI_VERSION 1
+#define KW_ABI_VERSION 2
 
 /* sensor.record bit mask (inputChecking.m:340-400 list of record flags) */
 #define KW_REC_P               (1u << 0)
@@ -61,6 +61,10 @@ typedef int kw_status;
 #define KW_SOURCE_DIRICHLET              0
 #define KW_SOURCE_ADDITIVE_NO_CORRECTION 1
 #define KW_SOURCE_ADDITIVE               2
+
+/* array_order */
+#define KW_COLUMN_MAJOR 0
+#define KW_ROW_MAJOR    1
 
 /* absorbing_flag: saveToDisk.m (0 lossless, 1 power-law absorbing, 2 stokes) */
 #define KW_LOSSLESS  0
@@ -137,6 +141,19 @@ typedef struct kw_problem {
     uint64_t inside_lo[3], inside_hi[3];
 
     int32_t  device;             /* CUDA device ordinal of the plan ('DeviceNum') */
+
+    /* Memory order of the grid-sized arrays (c0, rho0, rho0_sg*, BonA,
+       alpha_coeff, p0_source_input): KW_COLUMN_MAJOR as MATLAB stores them,
+       or KW_ROW_MAJOR (C / numpy order, last axis fastest), which the library
+       transposes on the device.  Linear indices (source and sensor) are
+       column-major in both cases. */
+    int32_t  array_order;
+    /* Non-zero: form rho0_sg{x,y,z} on the device as the midpoint average of
+       rho0 with its +1 neighbour along each axis, rho0 itself on the last
+       plane (the linear interpolation at x + dx/2 of
+       kspaceFirstOrder3D.m:585-601, NaN edge replaced by rho0); the rho0_sg*
+       pointers must then be NULL and rho0 an array. */
+    int32_t  derive_rho0_sg;
 } kw_problem;
 
 /* Output sizes (createStorageVariables.m:58-88). */

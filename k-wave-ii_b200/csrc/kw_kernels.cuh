@@ -936,4 +936,70 @@ __global__ void k_set_points(const long long *pos, int npts, float v, float *fie
 
 __global__ void k_step_advance(int *d_t) { *d_t += 1; }
 
+// ---------------------------------------------------------------------------
+// set-up kernels (run once per plan)
+// ---------------------------------------------------------------------------
+
+// Row-major (C order) grid of shape (A, B, C) -> the column-major layout:
+// in[(x B + y) C + z] -> out[x + A (y + B z)].  32 x 32 tiles over (z, x)
+// per y; block (32, 8), grid (ceil(C/32), ceil(A/32), B).
+__global__ void k_rowmajor_to_col(const float *__restrict__ in, float *__restrict__ out, int A, int B, int C) {
+    __shared__ float t[32][33];
+    const int y = blockIdx.z;
+    const int z0 = blockIdx.x * 32, x0 = blockIdx.y * 32;
+    for (int i = threadIdx.y; i < 32; i += blockDim.y) {
+        const int x = x0 + i, z = z0 + threadIdx.x;
+        if (x < A && z < C) t[i][threadIdx.x] = in[((long long)x * B + y) * C + z];
+    }
+    __syncthreads();
+    for (int i = threadIdx.y; i < 32; i += blockDim.y) {
+        const int z = z0 + i, x = x0 + threadIdx.x;
+        if (x < A && z < C) out[x + (long long)A * (y + (long long)B * z)] = t[threadIdx.x][i];
+    }
+}
+
+// 1 / rho0_sg along internal axis `axis` (stride `s`, extent `n`): with
+// derive != 0 the staggered density is the midpoint average of rho0 and its
+// +1 neighbour (rho0 on the last plane) rounded to FP32, as the set-up
+// forms it; without, in holds rho0_sg already.  The reciprocal is taken in
+// FP64 and rounded once.
+__global__ void k_inv_rho_sg(const float *in, float *out, Geom g, int axis, int derive) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= g.N) return;
+    float r = in[i];
+    if (derive) {
+        const int x = (int)(i % g.N0);
+        const long long q = i / g.N0;
+        const int y = (int)(q % g.N1), z = (int)(q / g.N1);
+        const int c = axis == 0 ? x : (axis == 1 ? y : z);
+        const int n = axis == 0 ? g.N0 : (axis == 1 ? g.N1 : g.N2);
+        const long long s = axis == 0 ? 1 : (axis == 1 ? (long long)g.N0 : (long long)g.N0 * g.N1);
+        if (c + 1 < n) r = (float)(0.5 * ((double)in[i] + (double)in[i + s]));
+    }
+    out[i] = (float)(1.0 / (double)r);
+}
+
+// c0^2 absorb_tau and c0^2 absorb_eta (createAbsorptionVariables.m:29-101)
+// in FP64: tau = -2 a c^(y-1), eta = 2 a c^y tan(pi y / 2) for the power
+// law, tau = -2 a c, eta = 0 for stokes; a = alpha_coeff * np_per_db
+// (db2neper with the frequency power folded in).
+__global__ void k_absorb_coeffs(const float *__restrict__ c0, double c0s, const float *__restrict__ alpha, double alphas,
+                                long long N, double y, double np_per_db, int stokes, double tanv, double sg0, double sg1,
+                                float *__restrict__ c2tau, float *__restrict__ c2eta) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    const double c = c0 ? (double)c0[i] : c0s;
+    const double anp = (alpha ? (double)alpha[i] : alphas) * np_per_db;
+    const double tau = stokes ? -2.0 * anp * c : -2.0 * anp * pow(c, y - 1.0);
+    const double eta = stokes ? 0.0 : 2.0 * anp * pow(c, y) * tanv;
+    c2tau[i] = (float)(c * c * tau * sg0);
+    if (c2eta) c2eta[i] = (float)(c * c * eta * sg1);
+}
+
+// flags |= bit where a value is not strictly positive (or NaN)
+__global__ void k_check_positive(const float *__restrict__ a, long long N, int *flags, int bit) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < N && !(a[i] > 0.f)) atomicOr(flags, bit);
+}
+
 }  // namespace kw

@@ -244,6 +244,28 @@ kw_status pupload(kw_plan *P, T **p, const T *host, size_t count) {
     return KW_OK;
 }
 
+// Device buffers needed only while a plan is set up; released (stream
+// ordered) when the set-up returns, on success or failure.
+struct TempDev {
+    cudaStream_t stream;
+    std::vector<void *> ptrs;
+    template <typename T>
+    kw_status get(T **p, size_t count) {
+        *p = nullptr;
+        const cudaError_t e = cudaMallocAsync((void **)p, count * sizeof(T), stream);
+        if (e != cudaSuccess) {
+            *p = nullptr;
+            return fail(e == cudaErrorMemoryAllocation ? KW_ERR_NOMEM : KW_ERR_CUDA,
+                        "device allocation of %zu bytes failed: %s", count * sizeof(T), cudaGetErrorString(e));
+        }
+        ptrs.push_back((void *)*p);
+        return KW_OK;
+    }
+    ~TempDev() {
+        for (void *a : ptrs) cudaFreeAsync(a, stream);
+    }
+};
+
 // ---- timing ---------------------------------------------------------------
 kw_status timer_flush(kw_plan *P) {
     if (P->timers.empty()) return KW_OK;
@@ -754,7 +776,6 @@ kw_status run_step(kw_plan *P) {
             KW_TRY(stage_r(P, need_grad ? 1 : 0));
         } else {
             KW_TRY(stage_r(P, 0));
-            const int nabs = (P->has_tau ? 1 : 0) + (P->has_eta ? 1 : 0);
             OpSet o2{};
             if (P->has_tau) o2.kind[o2.n++] = OP_NABLA1;
             if (P->has_eta) o2.kind[o2.n++] = OP_NABLA2;
@@ -1091,39 +1112,73 @@ kw_status create(const kw_problem *pr, kw_plan *P) {
     const int nspec = 4;
     for (int i = 0; i < nspec; ++i) KW_TRY(palloc(P, &P->spec[i], Nh));
 
-    // medium
-    double cmin = 1e300;
+    // medium.  Grid arrays reach the device in column-major order (row-major
+    // input is staged and transposed there); the derived arrays (1/rho0_sg,
+    // c0^2 tau, c0^2 eta) are formed on the device in FP64, and the
+    // positivity checks run there too
+    const bool row_major = q.array_order == KW_ROW_MAJOR;
+    if (q.array_order != KW_COLUMN_MAJOR && !row_major)
+        return fail(KW_ERR_INVALID, "array_order must be %d (column-major) or %d (row-major)", KW_COLUMN_MAJOR, KW_ROW_MAJOR);
+    TempDev tmp{P->stream, {}};
+    float *stage_buf = nullptr;
+    int *flags = nullptr;
+    KW_TRY(tmp.get(&flags, 1));
+    KW_CUDA(cudaMemsetAsync(flags, 0, sizeof(int), P->stream));
+    const unsigned ew_blocks = (unsigned)((N + 255) / 256);
+    auto put_grid = [&](float *dst, const float *host) -> kw_status {
+        if (!row_major) {
+            KW_CUDA(cudaMemcpyAsync(dst, host, N * sizeof(float), cudaMemcpyHostToDevice, P->stream));
+            return KW_OK;
+        }
+        if (!stage_buf) KW_TRY(tmp.get(&stage_buf, N));
+        KW_CUDA(cudaMemcpyAsync(stage_buf, host, N * sizeof(float), cudaMemcpyHostToDevice, P->stream));
+        const int A = (int)shp[0], B = q.dim == 3 ? (int)shp[1] : 1, Cn = q.dim == 3 ? (int)shp[2] : (int)shp[1];
+        k_rowmajor_to_col<<<dim3((Cn + 31) / 32, (A + 31) / 32, B), dim3(32, 8), 0, P->stream>>>(stage_buf, dst, A, B, Cn);
+        return launched(P);
+    };
+    auto upload_grid = [&](float **dst, const float *host) -> kw_status {
+        KW_TRY(palloc(P, dst, N));
+        return put_grid(*dst, host);
+    };
     if (q.c0) {
-        KW_TRY(pupload(P, &P->c0_arr, q.c0, N));
+        KW_TRY(upload_grid(&P->c0_arr, q.c0));
         P->c0.arr = P->c0_arr;
-        for (size_t i = 0; i < N; ++i) cmin = std::min(cmin, (double)q.c0[i]);
+        k_check_positive<<<ew_blocks, 256, 0, P->stream>>>(P->c0_arr, (long long)N, flags, 1);
+        KW_TRY(launched(P));
     } else {
         P->c0.val = (float)q.c0_scalar;
-        cmin = q.c0_scalar;
+        if (!(q.c0_scalar > 0)) return fail(KW_ERR_INVALID, "medium.sound_speed must be positive");
     }
-    if (!(cmin > 0)) return fail(KW_ERR_INVALID, "medium.sound_speed must be positive");
     if (q.rho0) {
-        KW_TRY(pupload(P, &P->rho0_arr, q.rho0, N));
+        KW_TRY(upload_grid(&P->rho0_arr, q.rho0));
         P->rho0.arr = P->rho0_arr;
+        k_check_positive<<<ew_blocks, 256, 0, P->stream>>>(P->rho0_arr, (long long)N, flags, 2);
+        KW_TRY(launched(P));
     } else {
         P->rho0.val = (float)q.rho0_scalar;
         if (!(q.rho0_scalar > 0)) return fail(KW_ERR_INVALID, "medium.density must be positive");
     }
     const float *sg[3] = {q.rho0_sgx, q.rho0_sgy, q.rho0_sgz};
+    if (q.derive_rho0_sg && (!q.rho0 || sg[0] || sg[1] || sg[2]))
+        return fail(KW_ERR_INVALID, "derive_rho0_sg needs an rho0 array and NULL rho0_sg pointers");
     for (int c = 0; c < P->D; ++c) {
-        const float *src = sg[c] ? sg[c] : q.rho0;
-        if (src) {
-            std::vector<float> inv(N);
-            for (size_t i = 0; i < N; ++i) inv[i] = (float)(1.0 / (double)src[i]);
-            KW_TRY(pupload(P, &P->rsi_arr[c], inv.data(), N));
-            P->rsi[c].arr = P->rsi_arr[c];
+        if (sg[c]) {
+            KW_TRY(upload_grid(&P->rsi_arr[c], sg[c]));
+            k_inv_rho_sg<<<ew_blocks, 256, 0, P->stream>>>(P->rsi_arr[c], P->rsi_arr[c], g, P->comp_axis[c], 0);
+        } else if (q.rho0) {
+            KW_TRY(palloc(P, &P->rsi_arr[c], N));
+            k_inv_rho_sg<<<ew_blocks, 256, 0, P->stream>>>(P->rho0_arr, P->rsi_arr[c], g, P->comp_axis[c],
+                                                          q.derive_rho0_sg ? 1 : 0);
         } else {
             P->rsi[c].val = (float)(1.0 / q.rho0_scalar);
+            continue;
         }
+        KW_TRY(launched(P));
+        P->rsi[c].arr = P->rsi_arr[c];
     }
     if (q.nonlinear_flag) {
         if (q.BonA) {
-            KW_TRY(pupload(P, &P->bona_arr, q.BonA, N));
+            KW_TRY(upload_grid(&P->bona_arr, q.BonA));
             P->bona.arr = P->bona_arr;
         } else {
             P->bona.val = (float)q.BonA_scalar;
@@ -1141,36 +1196,38 @@ kw_status create(const kw_problem *pr, kw_plan *P) {
             P->has_tau = q.alpha_mode != KW_ALPHA_NO_ABSORPTION;
             P->has_eta = q.alpha_mode != KW_ALPHA_NO_DISPERSION;
         }
-        auto tau_eta = [&](double c, double acoef, double &c2tau, double &c2eta) {
-            const double anp = db2neper(acoef, y);
-            const double tau = stokes ? -2.0 * anp * c : -2.0 * anp * std::pow(c, y - 1.0);
-            const double eta = stokes ? 0.0 : 2.0 * anp * std::pow(c, y) * tanv;
-            c2tau = c * c * tau * sg0;
-            c2eta = c * c * eta * sg1;
-        };
         if (q.c0 || q.alpha_coeff) {
-            std::vector<float> ta(N), ea(N);
-            for (size_t i = 0; i < N; ++i) {
-                double ct, ce;
-                tau_eta(q.c0 ? (double)q.c0[i] : q.c0_scalar, q.alpha_coeff ? (double)q.alpha_coeff[i] : q.alpha_coeff_scalar,
-                        ct, ce);
-                ta[i] = (float)ct;
-                ea[i] = (float)ce;
+            float *a_dev = nullptr;
+            if (q.alpha_coeff) {
+                KW_TRY(tmp.get(&a_dev, N));
+                KW_TRY(put_grid(a_dev, q.alpha_coeff));
             }
-            KW_TRY(pupload(P, &P->c2tau_arr, ta.data(), N));
+            KW_TRY(palloc(P, &P->c2tau_arr, N));
             P->c2tau.arr = P->c2tau_arr;
             if (!stokes) {
-                KW_TRY(pupload(P, &P->c2eta_arr, ea.data(), N));
+                KW_TRY(palloc(P, &P->c2eta_arr, N));
                 P->c2eta.arr = P->c2eta_arr;
             }
+            k_absorb_coeffs<<<ew_blocks, 256, 0, P->stream>>>(P->c0_arr, q.c0_scalar, a_dev, q.alpha_coeff_scalar,
+                                                             (long long)N, y, db2neper(1.0, y), stokes ? 1 : 0, tanv,
+                                                             sg0, sg1, P->c2tau_arr, P->c2eta_arr);
+            KW_TRY(launched(P));
         } else {
-            double ct, ce;
-            tau_eta(q.c0_scalar, q.alpha_coeff_scalar, ct, ce);
-            P->c2tau.val = (float)ct;
-            P->c2eta.val = (float)ce;
+            const double anp = db2neper(q.alpha_coeff_scalar, y), c = q.c0_scalar;
+            const double tau = stokes ? -2.0 * anp * c : -2.0 * anp * std::pow(c, y - 1.0);
+            const double eta = stokes ? 0.0 : 2.0 * anp * std::pow(c, y) * tanv;
+            P->c2tau.val = (float)(c * c * tau * sg0);
+            P->c2eta.val = (float)(c * c * eta * sg1);
         }
     }
-    if (P->p0) KW_TRY(pupload(P, &P->p0_dev, q.p0_source_input, N));
+    if (P->p0) KW_TRY(upload_grid(&P->p0_dev, q.p0_source_input));
+    {
+        int hf = 0;
+        KW_CUDA(cudaMemcpyAsync(&hf, flags, sizeof(int), cudaMemcpyDeviceToHost, P->stream));
+        KW_CUDA(cudaStreamSynchronize(P->stream));
+        if (hf & 1) return fail(KW_ERR_INVALID, "medium.sound_speed must be positive");
+        if (hf & 2) return fail(KW_ERR_INVALID, "medium.density must be positive");
+    }
 
     // sources
     KW_TRY(setup_source(P, P->psrc, &q.p_source, 1, P->PL_r));

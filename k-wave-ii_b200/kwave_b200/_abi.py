@@ -14,7 +14,7 @@ import numpy as np
 LIB_NAME = "libkwave_b200.so"
 LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), LIB_NAME)
 
-KW_ABI_VERSION = 1
+KW_ABI_VERSION = 2
 
 KW_OK = 0
 KW_ERR_INVALID = 1
@@ -31,6 +31,7 @@ REC_BITS = {
 
 SOURCE_MODES = {"dirichlet": 0, "additive-no-correction": 1, "additive": 2}
 KW_LOSSLESS, KW_ABSORBING, KW_STOKES = 0, 1, 2
+KW_COLUMN_MAJOR, KW_ROW_MAJOR = 0, 1
 ALPHA_MODES = {None: 0, "no_absorption": 1, "no_dispersion": 2}
 
 KCLASS = {"zstage_u": 0, "zstage_r": 1, "zstage_p": 2, "ypass": 3, "xpass": 4, "sensor": 5, "source": 6}
@@ -92,6 +93,8 @@ class kw_problem(C.Structure):
         ("inside_lo", C.c_uint64 * 3),
         ("inside_hi", C.c_uint64 * 3),
         ("device", C.c_int32),
+        ("array_order", C.c_int32),
+        ("derive_rho0_sg", C.c_int32),
     ]
 
 

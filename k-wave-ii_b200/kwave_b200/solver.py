@@ -70,8 +70,29 @@ def _pick(values, dim):
 
 
 def _find(mask):
-    """MATLAB find(mask ~= 0): 0-based column-major indices."""
-    return np.flatnonzero(np.asarray(mask).ravel(order="F") != 0)
+    """MATLAB find(mask ~= 0): 0-based column-major indices, increasing.
+
+    Found in the array's own memory order and sorted, so no column-major
+    copy of the grid is made."""
+    m = np.asarray(mask)
+    if m.ndim < 2:
+        return np.flatnonzero(m)
+    nz = np.flatnonzero(m)
+    f = np.ravel_multi_index(np.unravel_index(nz, m.shape), m.shape, order="F")
+    f.sort()
+    return f
+
+
+def _at(a, fidx):
+    """Values of grid array a at 0-based column-major linear indices."""
+    a = np.asarray(a)
+    return a[np.unravel_index(fidx, a.shape, order="F")]
+
+
+def _grid32(a):
+    """A grid-sized array as FP32 in row-major (C) order, the layout the
+    library transposes on the device (KW_ROW_MAJOR)."""
+    return np.ascontiguousarray(a, dtype=np.float32)
 
 
 def _f32(a):
@@ -362,50 +383,44 @@ def _prepare(dim, kgrid, medium, source, sensor, options):
     sensor_idx = _find(mask) if mask is not None else np.zeros(0, dtype=np.int64)
 
     # ---- source scaling (scaleSourceTerms.m) ----
-    c0_flat = c0.ravel(order="F") if c0.size > 1 else None
+    hetero_c = c0.size > 1
     src_struct = []
     if psrc is not None:
         pos = _find(psrc["mask"])
-        labels = np.asarray(psrc["mask"]).ravel(order="F")[pos]
+        labels = _at(psrc["mask"], pos)
         sig = psrc["sig"].copy()
-        rows = _signal_rows(psrc["mask"], labels, sig.shape[0], pos.size, "source.p", "source.p_mask")
+        rows = _signal_rows(labels, sig.shape[0], pos.size, "source.p", "source.p_mask")
+        cpos = _at(c0, pos[:sig.shape[0]]) if hetero_c else None
         if scale_source_terms:
             if psrc["mode"] == "dirichlet":
                 for r in range(sig.shape[0]):
-                    cc = c0 if c0_flat is None else c0_flat[pos[r]]
+                    cc = c0 if cpos is None else cpos[r]
                     sig[r] = sig[r] / (dim * cc ** 2)
             else:
                 for r in range(sig.shape[0]):
-                    cc = c0 if c0_flat is None else c0_flat[pos[r]]
+                    cc = c0 if cpos is None else cpos[r]
                     sig[r] = sig[r] * (2.0 * dt / (dim * cc * kgrid.dx))
         src_struct.append(("p", psrc["mode"], pos, rows, [sig]))
     if usrc is not None:
         pos = _find(usrc["mask"])
-        labels = np.asarray(usrc["mask"]).ravel(order="F")[pos]
+        labels = _at(usrc["mask"], pos)
         sigs = [s.copy() if s is not None else None for s in usrc["sigs"]]
         nrows = max(s.shape[0] for s in sigs if s is not None) if any(s is not None for s in sigs) else 1
-        rows = _signal_rows(usrc["mask"], labels, nrows, pos.size, "source.ux (etc)", "source.u_mask")
+        rows = _signal_rows(labels, nrows, pos.size, "source.ux (etc)", "source.u_mask")
+        cpos = _at(c0, pos[:nrows]) if hetero_c else None
         if scale_source_terms and usrc["mode"] != "dirichlet":
             for i, s in enumerate(sigs):
                 if s is None:
                     continue
                 d = spacing[i]
                 for r in range(s.shape[0]):
-                    cc = c0 if c0_flat is None else c0_flat[pos[r]]
+                    cc = c0 if cpos is None else cpos[r]
                     s[r] = s[r] * (2.0 * cc * dt / d)
         src_struct.append(("u", usrc["mode"], pos, rows, sigs))
 
     # ---- staggered density (kspaceFirstOrder3D.m:585-607) ----
-    rho_sg = [None] * dim
-    if rho0.ndim == dim and rho0.size > 1 and use_sg:
-        for a in range(dim):
-            r = rho0.copy()
-            lo = [slice(None)] * dim
-            hi = [slice(None)] * dim
-            lo[a] = slice(0, shape[a] - 1)
-            hi[a] = slice(1, shape[a])
-            r[tuple(lo)] = 0.5 * (rho0[tuple(lo)] + rho0[tuple(hi)])
-            rho_sg[a] = r
+    # the midpoint averages are formed on the device from rho0
+    derive_rho_sg = rho0.ndim == dim and rho0.size > 1 and use_sg
 
     # ---- the C problem ----
     keep = []   # arrays referenced by raw pointers must outlive the call
@@ -414,6 +429,11 @@ def _prepare(dim, kgrid, medium, source, sensor, options):
         if a is None:
             return _abi.f32p()
         x = _f32(a)
+        keep.append(x)
+        return _abi.fptr(x)
+
+    def grid_arr(a):
+        x = _grid32(a)
         keep.append(x)
         return _abi.fptr(x)
 
@@ -434,19 +454,16 @@ def _prepare(dim, kgrid, medium, source, sensor, options):
     pr.dz = spacing[2] if dim == 3 else 0.0
     pr.dt = dt
     pr.c_ref = c_ref
+    pr.array_order = _abi.KW_ROW_MAJOR
     if c0.size > 1:
-        pr.c0 = arr(c0)
+        pr.c0 = grid_arr(c0)
     else:
         pr.c0_scalar = float(c0)
     if rho0.size > 1:
-        pr.rho0 = arr(rho0)
+        pr.rho0 = grid_arr(rho0)
     else:
         pr.rho0_scalar = float(rho0)
-    if rho_sg[0] is not None:
-        pr.rho0_sgx = arr(rho_sg[0])
-        pr.rho0_sgy = arr(rho_sg[1])
-        if dim == 3:
-            pr.rho0_sgz = arr(rho_sg[2])
+    pr.derive_rho0_sg = int(derive_rho_sg)
     pr.pml_x_size, pr.pml_y_size = pml_size[0], pml_size[1]
     pr.pml_z_size = pml_size[2] if dim == 3 else 0
     pr.pml_x_alpha, pr.pml_y_alpha = pml_alpha[0], pml_alpha[1]
@@ -456,13 +473,13 @@ def _prepare(dim, kgrid, medium, source, sensor, options):
     pr.nonlinear_flag = int(nonlinear)
     if nonlinear:
         if BonA.size > 1:
-            pr.BonA = arr(BonA)
+            pr.BonA = grid_arr(BonA)
         else:
             pr.BonA_scalar = float(BonA)
     pr.absorbing_flag = {"lossless": 0, "absorbing": 1, "stokes": 2}[eos]
     if alpha_coeff is not None:
         if alpha_coeff.size > 1:
-            pr.alpha_coeff = arr(alpha_coeff)
+            pr.alpha_coeff = grid_arr(alpha_coeff)
         else:
             pr.alpha_coeff_scalar = float(alpha_coeff)
     pr.alpha_power = alpha_power
@@ -485,7 +502,7 @@ def _prepare(dim, kgrid, medium, source, sensor, options):
             tgt.signal_index = row_p
             tgt.input = _abi.fptr(x)
     if source_p0:
-        pr.p0_source_input = arr(p0)
+        pr.p0_source_input = grid_arr(p0)
     pr.sensor_num = sensor_idx.size
     if sensor_idx.size:
         pr.sensor_mask_index = idx_arr(sensor_idx)
@@ -526,10 +543,11 @@ def _round(v):
     return math.copysign(math.floor(abs(v) + 0.5), v)
 
 
-def _signal_rows(mask, labels, nrows, npts, sname, mname):
-    """0-based signal row of each source point (inputChecking.m:853-887)."""
-    uniq = np.unique(mask)
-    if uniq.size <= 2 and uniq.sum() == 1:
+def _signal_rows(labels, nrows, npts, sname, mname):
+    """0-based signal row of each source point (inputChecking.m:853-887);
+    labels are the mask's non-zero values in find() order."""
+    uniq = np.unique(labels)
+    if uniq.size == 1 and uniq[0] == 1:
         if nrows > 1 and nrows != npts:
             raise KWaveInputError("The number of time series in %s must match the number of source elements in %s."
                                   % (sname, mname))

@@ -81,11 +81,12 @@ def test_problem_contents_heterogeneous_absorbing_source():
     assert (pr.dim, pr.Nx, pr.Ny, pr.Nz, pr.Nt) == (3, 24, 20, 16, 30)
     assert pr.c_ref == pytest.approx(c.max())
     assert pr.absorbing_flag == _abi.KW_ABSORBING and pr.nonlinear_flag == 1
-    assert np.allclose(_arr(pr.c0, N), c.ravel(order="F").astype(np.float32))
-    # staggered density: midpoint average along each axis, last plane kept (kspaceFirstOrder3D.m:590-601)
-    sgx = _arr(pr.rho0_sgx, N).reshape(shape, order="F")
-    assert np.allclose(sgx[:-1], (0.5 * (rho[:-1] + rho[1:])).astype(np.float32))
-    assert np.allclose(sgx[-1], rho[-1].astype(np.float32))
+    # grid arrays go over in row-major order; the library transposes them
+    assert pr.array_order == _abi.KW_ROW_MAJOR
+    assert np.array_equal(_arr(pr.c0, N), c.ravel().astype(np.float32))
+    assert np.array_equal(_arr(pr.rho0, N), rho.ravel().astype(np.float32))
+    # staggered densities (kspaceFirstOrder3D.m:590-601) are formed on the device
+    assert pr.derive_rho0_sg == 1 and not pr.rho0_sgx and not pr.rho0_sgy and not pr.rho0_sgz
     # source: find(mask) order, one signal scaled by 2 dt / (N c0(first point) dx) (scaleSourceTerms.m)
     pos = np.flatnonzero(pm.ravel(order="F"))
     assert np.array_equal(_arr(pr.p_source.index, pos.size, np.uint64), pos + 1)
@@ -154,3 +155,15 @@ def test_labelled_source_rows():
     assert list(_arr(src.signal_index, 3, np.uint64)) == [2, 1, 2]
     with pytest.raises(KWaveInputError, match="labelled"):
         _prepare(2, g, {"sound_speed": 1500.0}, {"p": np.ones((3, 5)), "p_mask": pm}, None, {"PMLSize": 4})
+
+
+@pytest.mark.parametrize("shape", [(17, 12), (9, 11, 7), (64,)])
+def test_find_is_matlab_find(shape):
+    """find(mask) in column-major order, for C- and Fortran-ordered masks."""
+    from kwave_b200.solver import _at, _find
+    rng = np.random.default_rng(11)
+    m = (rng.random(shape) < 0.3) * rng.integers(1, 4, shape)
+    ref = np.flatnonzero(m.ravel(order="F"))
+    for a in (m, np.asfortranarray(m)):
+        assert np.array_equal(_find(a), ref)
+        assert np.array_equal(_at(a, ref), m.ravel(order="F")[ref])
