@@ -325,7 +325,9 @@ def served_section(kw, device, n_req=48, seed=7, load=0.9):
                 tickets.append(srv.submit_prepared(preps[k]))
             res = [srv.result(t, with_latency=True) for t in tickets]
             span = time.perf_counter() - t0
-        return span, [r[1] for r in res], [r[0] for r in res]
+            st = srv.stats()
+        worker = {k: st[k] for k in ("setup_seconds", "issue_seconds", "retire_seconds", "wait_seconds")}
+        return span, [r[1] for r in res], [r[0] for r in res], worker
 
     # warm both paths (module load, first plans, graph capture paths)
     for k in preps:
@@ -333,20 +335,20 @@ def served_section(kw, device, n_req=48, seed=7, load=0.9):
             sim.run()
     zeros = np.zeros(n_req)
     p_span, _, p_outs = plain(zeros)
-    s_span, _, s_outs = served(zeros)
+    s_span, _, s_outs, s_worker = served(zeros)
     err = max(_rel_l2(a, b) for a, b in zip(s_outs, p_outs))
     rate = load * n_req / p_span
     arrivals = np.cumsum(rng.exponential(1.0 / rate, size=n_req))
     arrivals -= arrivals[0]
     pp_span, pp_lat, _ = plain(arrivals)
-    sp_span, sp_lat, sp_outs = served(arrivals)
+    sp_span, sp_lat, sp_outs, _ = served(arrivals)
     err = max(err, max(_rel_l2(a, b) for a, b in zip(sp_outs, p_outs)))
     mix = ["%s %s Nt=%d x%d" % (kind, "x".join([str(n)] * (2 if kind == "2d" else 3)), nt, int((picks == i).sum()))
            for i, (kind, n, nt) in enumerate(kinds)]
     return {
         "requests": n_req, "mix": mix, "cell_steps": work,
         "saturated": {"served_gcell_steps_per_s": work / s_span / 1e9, "plain_gcell_steps_per_s": work / p_span / 1e9,
-                      "served_makespan_s": s_span, "plain_makespan_s": p_span},
+                      "served_makespan_s": s_span, "plain_makespan_s": p_span, "served_worker_seconds": s_worker},
         "poisson": {"rate_per_s": rate, "load_vs_plain_capacity": load,
                     "served": _latency_stats(sp_lat), "plain": _latency_stats(pp_lat),
                     "served_gcell_steps_per_s": work / sp_span / 1e9, "plain_gcell_steps_per_s": work / pp_span / 1e9},

@@ -256,6 +256,9 @@ typedef struct kw_server_stats {
     double   p50_ms, p99_ms, mean_ms;   /* submit -> result latency of completed requests */
     double   cell_steps;                /* cell-steps of completed requests */
     double   busy_seconds;              /* first admission -> last completion */
+    /* worker thread time: plan set-up, issuing step slices, retiring
+       (outputs to host, release), waiting with every run in flight */
+    double   setup_seconds, issue_seconds, retire_seconds, wait_seconds;
 } kw_server_stats;
 
 kw_status kw_server_create(const kw_server_config *config, kw_server **server);

@@ -285,7 +285,7 @@ __device__ __forceinline__ void zstore_r2c(const float2 *s, float2 *__restrict__
     const int PL = PLS ? PLS : PLrt;
     const int tot = PL * (N2 / 2 + 1);
 #pragma unroll 4
-    for (int idx = threadIdx.x; idx < tot; idx += kThreads) {
+    for (int idx = threadIdx.x; idx < tot; idx += blockDim.x) {
         const int l = idx % PL, k = idx / PL;
         const float2 Zk = s[k * PL + l];
         const int nk = k == 0 ? 0 : N2 - k;
@@ -495,7 +495,7 @@ __device__ __forceinline__ void apply_tr(float2 *sm, const TRSrc &tr, const Geom
     const int TX = 2 * PL;
     const int tile = blockIdx.x + gridDim.x * blockIdx.y;
     const int e0 = tr.off[tile], e1 = tr.off[tile + 1];
-    for (int e = e0 + threadIdx.x; e < e1; e += kThreads) {
+    for (int e = e0 + threadIdx.x; e < e1; e += blockDim.x) {
         const int c = tr.cell[e];
         const int z = c / TX, xl = c - z * TX;
         const float v = __ldg(tr.data + tr.row[e] + (long long)tr.M * col);

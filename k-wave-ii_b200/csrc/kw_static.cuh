@@ -177,13 +177,21 @@ __device__ __forceinline__ float cos_series(float a2) {
 __host__ __device__ constexpr int ks_lines(int n) {
     return pow2_floor(kCap / n) < 64 ? pow2_floor(kCap / n) : 64;
 }
+// Narrower tiles (pl < ks_lines(n) lines, for grids too small to fill the
+// GPU with full tiles) keep the per-thread share of a full tile, so the block
+// shrinks with the tile: ks_threads(n, pl) threads.
+__host__ __device__ constexpr int ks_threads(int n, int pl) { return kThreads * pl / ks_lines(n); }
+// the narrow tile width used when full tiles give less than one wave of blocks
+__host__ __device__ constexpr int ks_narrow(int n) { return ks_lines(n) / 4; }
 
 // ---------------------------------------------------------------------------
-// y-pass (C2C along axis 1, in place).  grid = (ceil(N0/TY), N2h, nfields)
+// y-pass (C2C along axis 1, in place).  grid = (ceil(N0/TY), N2h, nfields),
+// ks_threads(N1, TY) threads
 // ---------------------------------------------------------------------------
-template <bool INV, int N1>
-__global__ void __launch_bounds__(kThreads, 3) ks_ypass(Spec4 bufs, Geom g, const float2 *__restrict__ tw, int kz0) {
-    constexpr int TY = ks_lines(N1);
+template <bool INV, int N1, int TY>
+__global__ void __launch_bounds__(ks_threads(N1, TY), 3 * kThreads / ks_threads(N1, TY))
+    ks_ypass(Spec4 bufs, Geom g, const float2 *__restrict__ tw, int kz0) {
+    constexpr int NT = ks_threads(N1, TY);
     static_assert(RPlan<N1, false>::M >= 2, "in-place pass needs two stages");
     __shared__ float2 sm[N1 * TY];
     float2 *buf = bufs.p[blockIdx.z];
@@ -196,17 +204,17 @@ __global__ void __launch_bounds__(kThreads, 3) ks_ypass(Spec4 bufs, Geom g, cons
     auto st = [&](int, int, int l, int i, float2 v) {
         if (x0 + l < N0) buf[base + (long long)i * N0 + l] = v;
     };
-    rs_fft<N1, TY, true, INV>(sm, tw, ld, st);
+    rs_fft<N1, TY, true, INV, 0, NT>(sm, tw, ld, st);
 }
 
 // ---------------------------------------------------------------------------
 // x-pass: forward C2C along axis 0, operator, inverse C2C, in place.
-// grid = (ceil(N1*N2h/NL), 1, fanout ? 1 : nfields)
+// grid = (ceil(N1*N2h/NL), 1, fanout ? 1 : nfields), ks_threads(N0, NL) threads
 // ---------------------------------------------------------------------------
-template <int N0>
-__global__ void __launch_bounds__(kThreads, 3) ks_xpass(Spec4 bufs, Geom g, const float2 *__restrict__ tw,
-                                                         OpParams P, OpSet ops, int fanout, int kz0, int nkz) {
-    constexpr int NL = ks_lines(N0);
+template <int N0, int NL>
+__global__ void __launch_bounds__(ks_threads(N0, NL), 3 * kThreads / ks_threads(N0, NL))
+    ks_xpass(Spec4 bufs, Geom g, const float2 *__restrict__ tw, OpParams P, OpSet ops, int fanout, int kz0, int nkz) {
+    constexpr int NT = ks_threads(N0, NL);
     static_assert(RPlan<N0, false>::M >= 2, "in-place pass needs two stages");
     __shared__ float2 sm[NL * Padded<N0>::LS];
     __shared__ float kyz2[NL];
@@ -215,7 +223,7 @@ __global__ void __launch_bounds__(kThreads, 3) ks_xpass(Spec4 bufs, Geom g, cons
     const int lines_total = (kz0 + nkz) * g.N1;
     const int line0 = kz0 * g.N1 + blockIdx.x * NL;
     const int f = fanout ? 0 : blockIdx.z;
-    for (int l = threadIdx.x; l < NL; l += kThreads) {
+    for (int l = threadIdx.x; l < NL; l += NT) {
         const int line = min(line0 + l, lines_total - 1);
         const int iy = line % g.N1, iz = line / g.N1;
         liy[l] = iy;
@@ -227,18 +235,18 @@ __global__ void __launch_bounds__(kThreads, 3) ks_xpass(Spec4 bufs, Geom g, cons
     auto ld = [&](int, int, int l, int i) -> float2 {
         return line0 + l < lines_total ? in[l * N0 + i] : make_float2(0.f, 0.f);
     };
-    using SH = StageShape<N0, NL, false, RPlan<N0, false>::M - 1>;   // forward last stage
+    using SH = StageShape<N0, NL, false, RPlan<N0, false>::M - 1, NT>;   // forward last stage
     float2 spec[SH::MAXB][SH::R];
     auto keep = [&](int b, int t, int, int, float2 v) { spec[b][t] = v; };
-    rs_fft<N0, NL, false, false>(sm, tw, ld, keep);
+    rs_fft<N0, NL, false, false, 0, NT>(sm, tw, ld, keep);
 
     // common factor of the operator (kappa, |k|^e or cos), times 1/N
     const int kind0 = ops.kind[f];
     const bool grad = kind0 == OP_GRAD_POS || kind0 == OP_GRAD_NEG;
 #pragma unroll
     for (int b = 0; b < SH::MAXB; ++b) {
-        const int gg = threadIdx.x + b * kThreads;
-        if (!(SH::TOT % kThreads == 0 || gg < SH::TOT)) continue;
+        const int gg = threadIdx.x + b * NT;
+        if (!(SH::TOT % NT == 0 || gg < SH::TOT)) continue;
         int l, j;
         bmap<SH::NB, NL, false>(gg, l, j);
         const float ky = kyz2[l];
@@ -276,7 +284,7 @@ __global__ void __launch_bounds__(kThreads, 3) ks_xpass(Spec4 bufs, Geom g, cons
         auto st2 = [&](int, int, int l, int i, float2 v) {
             if (line0 + l < lines_total) out[l * N0 + i] = v;
         };
-        rs_fft<N0, NL, false, true>(sm, tw, ld2, st2);
+        rs_fft<N0, NL, false, true, 0, NT>(sm, tw, ld2, st2);
     }
 }
 
@@ -284,11 +292,12 @@ __global__ void __launch_bounds__(kThreads, 3) ks_xpass(Spec4 bufs, Geom g, cons
 // z-tiles: TX = 2*PL consecutive x at one y, all z; hand-off register (b, t)
 // holds packed element (l, z) = (f(x0+2l), f(x0+2l+1)).
 // ---------------------------------------------------------------------------
-template <int N2>
+template <int N2, int PL_>
 struct ZTile {
-    static constexpr int PL = ks_lines(N2);
+    static constexpr int PL = PL_;
     static constexpr int TX = 2 * PL;
-    using SH = HandShape<N2, PL>;
+    static constexpr int NT = ks_threads(N2, PL);
+    using SH = HandShape<N2, PL, NT>;
 };
 
 // packed C2R input: element z of packed line l from the z-half spectrum
@@ -316,11 +325,11 @@ __device__ __forceinline__ float2 zpack_load(const float2 *__restrict__ H, const
 
 // forward transform of the hand-off registers, then unpack and store the
 // z-half spectrum (two real columns per packed line)
-template <int N2, class Hold>
+template <int N2, int PL, class Hold>
 __device__ __forceinline__ void zforward_store(float2 *sm, const float2 *__restrict__ tw, Hold &hold, float2 *H,
                                                const Geom &g, int x0, int y) {
-    constexpr int PL = ZTile<N2>::PL;
-    using SL = StageShape<N2, PL, false, RPlan<N2, false>::M - 1>;   // forward last stage
+    constexpr int NT = ZTile<N2, PL>::NT;
+    using SL = StageShape<N2, PL, false, RPlan<N2, false>::M - 1, NT>;   // forward last stage
     float2 outv[SL::MAXB][SL::R];
     int outi[SL::MAXB];
     auto ld = [&](int b, int t, int, int) -> float2 { return hold[b][t]; };
@@ -328,13 +337,13 @@ __device__ __forceinline__ void zforward_store(float2 *sm, const float2 *__restr
         outv[b][t] = v;
         if (t == 0) outi[b] = i * PL + l;   // element i + t*NS of line l sits at outi + t*NS*PL
     };
-    rs_fft<N2, PL, true, false>(sm, tw, ld, st);
+    rs_fft<N2, PL, true, false, 0, NT>(sm, tw, ld, st);
     __syncthreads();   // every thread has read its last-stage inputs from the tile
     constexpr int NSL = RPlan<N2, false>::NS(RPlan<N2, false>::M - 1);
 #pragma unroll
     for (int b = 0; b < SL::MAXB; ++b) {
-        const int gg = threadIdx.x + b * kThreads;
-        if (!(SL::TOT % kThreads == 0 || gg < SL::TOT)) continue;
+        const int gg = threadIdx.x + b * NT;
+        if (!(SL::TOT % NT == 0 || gg < SL::TOT)) continue;
 #pragma unroll
         for (int t = 0; t < SL::R; ++t) sm[outi[b] + t * NSL * PL] = outv[b][t];
     }
@@ -343,35 +352,35 @@ __device__ __forceinline__ void zforward_store(float2 *sm, const float2 *__restr
 }
 
 // write hand-off registers into the tile (packed layout z*PL + l)
-template <int N2, class Hold>
+template <int N2, int PL, class Hold>
 __device__ __forceinline__ void hold_to_smem(float2 *sm, Hold &hold) {
-    constexpr int PL = ZTile<N2>::PL;
-    using SH = typename ZTile<N2>::SH;
+    constexpr int NT = ZTile<N2, PL>::NT;
+    using SH = typename ZTile<N2, PL>::SH;
 #pragma unroll
     for (int b = 0; b < SH::MAXB; ++b)
 #pragma unroll
         for (int t = 0; t < SH::R; ++t) {
             int l, i;
-            if (hand_pos<N2, PL, true>(b, t, l, i)) sm[i * PL + l] = hold[b][t];
+            if (hand_pos<N2, PL, true, NT>(b, t, l, i)) sm[i * PL + l] = hold[b][t];
         }
 }
-template <int N2, class Hold>
+template <int N2, int PL, class Hold>
 __device__ __forceinline__ void smem_to_hold(const float2 *sm, Hold &hold) {
-    constexpr int PL = ZTile<N2>::PL;
-    using SH = typename ZTile<N2>::SH;
+    constexpr int NT = ZTile<N2, PL>::NT;
+    using SH = typename ZTile<N2, PL>::SH;
 #pragma unroll
     for (int b = 0; b < SH::MAXB; ++b)
 #pragma unroll
         for (int t = 0; t < SH::R; ++t) {
             int l, i;
-            if (hand_pos<N2, PL, true>(b, t, l, i)) hold[b][t] = sm[i * PL + l];
+            if (hand_pos<N2, PL, true, NT>(b, t, l, i)) hold[b][t] = sm[i * PL + l];
         }
 }
 
 // ---------------------------------------------------------------------------
 // Asynchronous staging of read-only physics inputs: every thread copies the
 // values of the cells it will update into a thread-private slice of shared
-// memory (index (b*R + t)*kThreads + tid) before the inverse transform, so
+// memory (index (b*R + t)*NT + tid) before the inverse transform, so
 // the loads are in flight while the transform computes.
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ void cp_async8(void *smem, const void *gmem) {
@@ -381,26 +390,26 @@ __device__ __forceinline__ void cp_async8(void *smem, const void *gmem) {
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
 
-template <int N2> struct ZStage {
-    using ZT = ZTile<N2>;
+template <int N2, int PL_> struct ZStage {
+    using ZT = ZTile<N2, PL_>;
     using SH = typename ZT::SH;
-    static constexpr int PL = ZT::PL, TX = ZT::TX;
-    static constexpr int TILE = N2 * PL;                    // float2 of the transform tile
-    static constexpr int SLICE = SH::MAXB * SH::R * kThreads;   // float2 of one staged field
-    static __device__ __forceinline__ int sidx(int b, int t) { return (b * SH::R + t) * kThreads + threadIdx.x; }
+    static constexpr int PL = ZT::PL, TX = ZT::TX, NT = ZT::NT;
+    static constexpr int TILE = N2 * PL;                  // float2 of the transform tile
+    static constexpr int SLICE = SH::MAXB * SH::R * NT;   // float2 of one staged field
+    static __device__ __forceinline__ int sidx(int b, int t) { return (b * SH::R + t) * NT + threadIdx.x; }
 };
 
 // stage one real field (pairs of cells) of this thread's hand-off elements
-template <int N2>
+template <int N2, int PL>
 __device__ __forceinline__ void stage_field(float2 *slice, const float *field, const Geom &g, int x0, int y) {
-    using Z = ZStage<N2>;
+    using Z = ZStage<N2, PL>;
     using SH = typename Z::SH;
 #pragma unroll
     for (int b = 0; b < SH::MAXB; ++b)
 #pragma unroll
         for (int t = 0; t < SH::R; ++t) {
             int l, z;
-            if (!hand_pos<N2, Z::PL, true>(b, t, l, z)) continue;
+            if (!hand_pos<N2, PL, true, Z::NT>(b, t, l, z)) continue;
             const int xa = x0 + 2 * l;
             if (xa >= g.N0) continue;
             cp_async8(slice + Z::sidx(b, t), field + xa + (long long)g.N0 * (y + (long long)g.N1 * z));
@@ -412,11 +421,12 @@ __device__ __forceinline__ void stage_field(float2 *slice, const float *field, c
 // u is double-buffered (read a.u, write a.u_out).  grid = (ceil(N0/TX), N1, D);
 // dynamic shared memory: tile + 2 staged fields.
 // ---------------------------------------------------------------------------
-template <int N2>
-__global__ void __launch_bounds__(kThreads, 2) ks_stage_u(StageU a, const float2 *__restrict__ tw) {
-    using Z = ZStage<N2>;
+template <int N2, int PL>
+__global__ void __launch_bounds__(ks_threads(N2, PL), 2 * kThreads / ks_threads(N2, PL))
+    ks_stage_u(StageU a, const float2 *__restrict__ tw) {
+    using Z = ZStage<N2, PL>;
     using SH = typename Z::SH;
-    constexpr int PL = Z::PL, TX = Z::TX;
+    constexpr int TX = Z::TX, NT = Z::NT;
     static_assert(RPlan<N2, false>::M >= 2, "z-stages need two stages");
     extern __shared__ float2 dsm[];
     float2 *sm = dsm;
@@ -432,14 +442,14 @@ __global__ void __launch_bounds__(kThreads, 2) ks_stage_u(StageU a, const float2
     const float2 *H = a.spec.p[f];
     const Med rsi = a.rho_sg_inv[f];
 
-    if (!a.init) stage_field<N2>(s_u, a.u[f], g, x0, y);
-    if (rsi.arr) stage_field<N2>(s_r, rsi.arr, g, x0, y);
+    if (!a.init) stage_field<N2, PL>(s_u, a.u[f], g, x0, y);
+    if (rsi.arr) stage_field<N2, PL>(s_r, rsi.arr, g, x0, y);
     cp_async_commit();
 
     float2 hold[SH::MAXB][SH::R];
     auto ld = [&](int, int, int l, int i) -> float2 { return zpack_load<N2>(H, g, x0, y, l, i); };
     auto st = [&](int b, int tt, int, int, float2 v) { hold[b][tt] = v; };
-    rs_fft<N2, PL, true, true>(sm, tw, ld, st);
+    rs_fft<N2, PL, true, true, 0, NT>(sm, tw, ld, st);
     cp_async_wait_all();
 
     float dscale = 0.f;
@@ -450,7 +460,7 @@ __global__ void __launch_bounds__(kThreads, 2) ks_stage_u(StageU a, const float2
 #pragma unroll
         for (int tt = 0; tt < SH::R; ++tt) {
             int l, z;
-            if (!hand_pos<N2, PL, true>(b, tt, l, z)) continue;
+            if (!hand_pos<N2, PL, true, NT>(b, tt, l, z)) continue;
             const int xa = x0 + 2 * l;
             if (xa >= g.N0) { hold[b][tt] = make_float2(0.f, 0.f); continue; }
             const long long gi = xa + (long long)g.N0 * (y + (long long)g.N1 * z);
@@ -482,9 +492,9 @@ __global__ void __launch_bounds__(kThreads, 2) ks_stage_u(StageU a, const float2
         const int e0 = a.sparse.off[tile], e1 = a.sparse.off[tile + 1];
         if (e1 > e0) {
             __syncthreads();
-            hold_to_smem<N2>(sm, hold);
+            hold_to_smem<N2, PL>(sm, hold);
             __syncthreads();
-            for (int e = e0 + threadIdx.x; e < e1; e += kThreads) {
+            for (int e = e0 + threadIdx.x; e < e1; e += NT) {
                 const int c = a.sparse.cell[e];
                 const int z = c / TX, xl = c - z * TX;
                 const float v = __ldg(a.sparse.sig[f] + a.sparse.row[e] + (long long)a.sparse.nsig * (t - 1));
@@ -494,10 +504,10 @@ __global__ void __launch_bounds__(kThreads, 2) ks_stage_u(StageU a, const float2
                 uout[x0 + xl + (long long)g.N0 * (y + (long long)g.N1 * z)] = nv;
             }
             __syncthreads();
-            smem_to_hold<N2>(sm, hold);
+            smem_to_hold<N2, PL>(sm, hold);
         }
     }
-    zforward_store<N2>(sm, tw, hold, a.spec.p[f], g, x0, y);
+    zforward_store<N2, PL>(sm, tw, hold, a.spec.p[f], g, x0, y);
 }
 
 // ---------------------------------------------------------------------------
@@ -508,11 +518,12 @@ __global__ void __launch_bounds__(kThreads, 2) ks_stage_u(StageU a, const float2
 // during component 0 and kept in component 0's slice.
 // grid = (ceil(N0/TX), N1, 1); dynamic shared memory: tile + D staged fields.
 // ---------------------------------------------------------------------------
-template <int N2>
-__global__ void __launch_bounds__(kThreads, 2) ks_stage_r(StageR a, const float2 *__restrict__ tw) {
-    using Z = ZStage<N2>;
+template <int N2, int PL>
+__global__ void __launch_bounds__(ks_threads(N2, PL), 2 * kThreads / ks_threads(N2, PL))
+    ks_stage_r(StageR a, const float2 *__restrict__ tw) {
+    using Z = ZStage<N2, PL>;
     using SH = typename Z::SH;
-    constexpr int PL = Z::PL, TX = Z::TX;
+    constexpr int TX = Z::TX, NT = Z::NT;
     extern __shared__ float2 dsm[];
     float2 *sm = dsm;
     float2 *s_c = dsm + Z::TILE;        // staged sum(rho_old) (nonlinear)
@@ -521,8 +532,8 @@ __global__ void __launch_bounds__(kThreads, 2) ks_stage_r(StageR a, const float2
     const int x0 = blockIdx.x * TX, y = blockIdx.y;
     const int t = *a.d_t;
     const int D = a.D;
-    if (a.nonlinear) stage_field<N2>(s_c, a.srho, g, x0, y);
-    stage_field<N2>(s_a, a.rho[0], g, x0, y);
+    if (a.nonlinear) stage_field<N2, PL>(s_c, a.srho, g, x0, y);
+    stage_field<N2, PL>(s_a, a.rho[0], g, x0, y);
     cp_async_commit();
     float dscale = 0.f;
     const bool dense = dense_active(a.dense, t, dscale);
@@ -541,7 +552,7 @@ __global__ void __launch_bounds__(kThreads, 2) ks_stage_r(StageR a, const float2
         const float2 *H = a.spec.p[i];
         auto ld = [&](int, int, int l, int z) -> float2 { return zpack_load<N2>(H, g, x0, y, l, z); };
         auto st = [&](int b, int tt, int, int, float2 v) { hold[b][tt] = v; };
-        rs_fft<N2, PL, true, true>(sm, tw, ld, st);
+        rs_fft<N2, PL, true, true, 0, NT>(sm, tw, ld, st);
         cp_async_wait_all();
         const int ax = a.comp_axis[i];
         const float *pmlv = a.pml[ax];
@@ -552,7 +563,7 @@ __global__ void __launch_bounds__(kThreads, 2) ks_stage_r(StageR a, const float2
 #pragma unroll
             for (int tt = 0; tt < SH::R; ++tt) {
                 int l, z;
-                if (!hand_pos<N2, PL, true>(b, tt, l, z)) continue;
+                if (!hand_pos<N2, PL, true, NT>(b, tt, l, z)) continue;
                 const int xa = x0 + 2 * l;
                 if (xa >= g.N0) continue;
                 const long long gi = xa + (long long)g.N0 * (y + (long long)g.N1 * z);
@@ -586,7 +597,7 @@ __global__ void __launch_bounds__(kThreads, 2) ks_stage_r(StageR a, const float2
         // every thread reads only its own slots, so the next component can be
         // staged into the same slice right away
         if (i + 1 < D) {
-            stage_field<N2>(s_a, a.rho[i + 1], g, x0, y);
+            stage_field<N2, PL>(s_a, a.rho[i + 1], g, x0, y);
             cp_async_commit();
         }
     }
@@ -596,9 +607,9 @@ __global__ void __launch_bounds__(kThreads, 2) ks_stage_r(StageR a, const float2
         const int e0 = a.sparse.off[tile], e1 = a.sparse.off[tile + 1];
         if (e1 > e0) {
             __syncthreads();
-            hold_to_smem<N2>(sm, acc_r);
+            hold_to_smem<N2, PL>(sm, acc_r);
             __syncthreads();
-            for (int e = e0 + threadIdx.x; e < e1; e += kThreads) {
+            for (int e = e0 + threadIdx.x; e < e1; e += NT) {
                 const int c = a.sparse.cell[e];
                 const int z = c / TX, xl = c - z * TX;
                 const float v = __ldg(a.sparse.sig[0] + a.sparse.row[e] + (long long)a.sparse.nsig * (t - 1));
@@ -612,7 +623,7 @@ __global__ void __launch_bounds__(kThreads, 2) ks_stage_r(StageR a, const float2
                 *(reinterpret_cast<float *>(sm + z * PL + (xl >> 1)) + (xl & 1)) = s;
             }
             __syncthreads();
-            smem_to_hold<N2>(sm, acc_r);
+            smem_to_hold<N2, PL>(sm, acc_r);
         }
     }
     // equation of state (c0^2 applied to the non-spectral terms here; the
@@ -623,7 +634,7 @@ __global__ void __launch_bounds__(kThreads, 2) ks_stage_r(StageR a, const float2
 #pragma unroll
         for (int tt = 0; tt < SH::R; ++tt) {
             int l, z;
-            if (!hand_pos<N2, PL, true>(b, tt, l, z)) continue;
+            if (!hand_pos<N2, PL, true, NT>(b, tt, l, z)) continue;
             const int xa = x0 + 2 * l;
             float2 pv = make_float2(0.f, 0.f);
             float2 rd = make_float2(0.f, 0.f);
@@ -663,7 +674,7 @@ __global__ void __launch_bounds__(kThreads, 2) ks_stage_r(StageR a, const float2
 #pragma unroll
             for (int tt = 0; tt < SH::R; ++tt) {
                 int l, z;
-                if (!hand_pos<N2, PL, true>(b, tt, l, z)) continue;
+                if (!hand_pos<N2, PL, true, NT>(b, tt, l, z)) continue;
                 const int xa = x0 + 2 * l;
                 if (xa >= g.N0) continue;
                 *reinterpret_cast<float2 *>(a.srho + xa + (long long)g.N0 * (y + (long long)g.N1 * z)) = acc_r[b][tt];
@@ -672,13 +683,13 @@ __global__ void __launch_bounds__(kThreads, 2) ks_stage_r(StageR a, const float2
     if (!absorbing) {
         if (a.tr.off) {
             __syncthreads();
-            hold_to_smem<N2>(sm, acc_d);
+            hold_to_smem<N2, PL>(sm, acc_d);
             __syncthreads();
             apply_tr(sm, a.tr, g, PL, x0, y, t, a.rho_out[0], a.rho_out[1], a.rho_out[2], D, a.c0, a.p, a.srho);
             __syncthreads();
-            smem_to_hold<N2>(sm, acc_d);
+            smem_to_hold<N2, PL>(sm, acc_d);
         }
-        if (a.write_spec) zforward_store<N2>(sm, tw, acc_d, a.spec.p[0], g, x0, y);
+        if (a.write_spec) zforward_store<N2, PL>(sm, tw, acc_d, a.spec.p[0], g, x0, y);
         return;
     }
     // absorbing: forward transforms of rho0 * sum(du) (tau term) and sum(rho) (eta term)
@@ -691,25 +702,26 @@ __global__ void __launch_bounds__(kThreads, 2) ks_stage_r(StageR a, const float2
         for (int b = 0; b < SH::MAXB; ++b)
 #pragma unroll
             for (int tt = 0; tt < SH::R; ++tt) src[b][tt] = term == 0 ? acc_d[b][tt] : acc_r[b][tt];
-        zforward_store<N2>(sm, tw, src, a.spec.p[out++], g, x0, y);
+        zforward_store<N2, PL>(sm, tw, src, a.spec.p[out++], g, x0, y);
     }
 }
 
 // ---------------------------------------------------------------------------
 // Stage P: p = p_partial + c0^2 tau A1 - c0^2 eta A2, time reversal, forward z of p.
 // ---------------------------------------------------------------------------
-template <int N2>
-__global__ void __launch_bounds__(kThreads, 2) ks_stage_p(StageP a, const float2 *__restrict__ tw) {
-    using Z = ZStage<N2>;
+template <int N2, int PL>
+__global__ void __launch_bounds__(ks_threads(N2, PL), 2 * kThreads / ks_threads(N2, PL))
+    ks_stage_p(StageP a, const float2 *__restrict__ tw) {
+    using Z = ZStage<N2, PL>;
     using SH = typename Z::SH;
-    constexpr int PL = Z::PL, TX = Z::TX;
+    constexpr int TX = Z::TX, NT = Z::NT;
     extern __shared__ float2 dsm[];
     float2 *sm = dsm;
     float2 *s_p = dsm + Z::TILE;
     const Geom &g = a.g;
     const int x0 = blockIdx.x * TX, y = blockIdx.y;
     const int t = *a.d_t;
-    stage_field<N2>(s_p, a.p, g, x0, y);
+    stage_field<N2, PL>(s_p, a.p, g, x0, y);
     cp_async_commit();
     float2 acc[SH::MAXB][SH::R];
 #pragma unroll
@@ -725,7 +737,7 @@ __global__ void __launch_bounds__(kThreads, 2) ks_stage_p(StageP a, const float2
         const float2 *H = a.spec.p[in++];
         auto ld = [&](int, int, int l, int z) -> float2 { return zpack_load<N2>(H, g, x0, y, l, z); };
         auto st = [&](int b, int tt, int, int, float2 v) { hold[b][tt] = v; };
-        rs_fft<N2, PL, true, true>(sm, tw, ld, st);
+        rs_fft<N2, PL, true, true, 0, NT>(sm, tw, ld, st);
         const Med w = term == 0 ? a.c2tau : a.c2eta;
         const float sg = term == 0 ? 1.f : -1.f;
 #pragma unroll
@@ -733,7 +745,7 @@ __global__ void __launch_bounds__(kThreads, 2) ks_stage_p(StageP a, const float2
 #pragma unroll
             for (int tt = 0; tt < SH::R; ++tt) {
                 int l, z;
-                if (!hand_pos<N2, PL, true>(b, tt, l, z)) continue;
+                if (!hand_pos<N2, PL, true, NT>(b, tt, l, z)) continue;
                 const int xa = x0 + 2 * l;
                 if (xa >= g.N0) continue;
                 const long long gi = xa + (long long)g.N0 * (y + (long long)g.N1 * z);
@@ -748,7 +760,7 @@ __global__ void __launch_bounds__(kThreads, 2) ks_stage_p(StageP a, const float2
 #pragma unroll
         for (int tt = 0; tt < SH::R; ++tt) {
             int l, z;
-            if (!hand_pos<N2, PL, true>(b, tt, l, z)) continue;
+            if (!hand_pos<N2, PL, true, NT>(b, tt, l, z)) continue;
             const int xa = x0 + 2 * l;
             float2 pv = make_float2(0.f, 0.f);
             if (xa < g.N0) {
@@ -762,24 +774,24 @@ __global__ void __launch_bounds__(kThreads, 2) ks_stage_p(StageP a, const float2
         }
     if (a.tr.off) {
         __syncthreads();
-        hold_to_smem<N2>(sm, acc);
+        hold_to_smem<N2, PL>(sm, acc);
         __syncthreads();
         apply_tr(sm, a.tr, g, PL, x0, y, t, a.rho[0], a.rho[1], a.rho[2], a.D, a.c0, a.p, a.srho);
         __syncthreads();
-        smem_to_hold<N2>(sm, acc);
+        smem_to_hold<N2, PL>(sm, acc);
     }
-    if (a.write_spec) zforward_store<N2>(sm, tw, acc, a.spec.p[0], g, x0, y);
+    if (a.write_spec) zforward_store<N2, PL>(sm, tw, acc, a.spec.p[0], g, x0, y);
 }
 
 // ---------------------------------------------------------------------------
 // plain z-transforms
 // ---------------------------------------------------------------------------
-template <int N2>
-__global__ void __launch_bounds__(kThreads, 2) ks_zr2c(const float *__restrict__ R, float2 *H, Geom g,
-                                                        const float2 *__restrict__ tw) {
-    using ZT = ZTile<N2>;
+template <int N2, int PL>
+__global__ void __launch_bounds__(ks_threads(N2, PL), 2 * kThreads / ks_threads(N2, PL))
+    ks_zr2c(const float *__restrict__ R, float2 *H, Geom g, const float2 *__restrict__ tw) {
+    using ZT = ZTile<N2, PL>;
     using SH = typename ZT::SH;
-    constexpr int PL = ZT::PL, TX = ZT::TX;
+    constexpr int TX = ZT::TX, NT = ZT::NT;
     __shared__ float2 sm[N2 * PL];
     const int x0 = blockIdx.x * TX, y = blockIdx.y;
     float2 hold[SH::MAXB][SH::R];
@@ -789,20 +801,20 @@ __global__ void __launch_bounds__(kThreads, 2) ks_zr2c(const float *__restrict__
         for (int tt = 0; tt < SH::R; ++tt) {
             int l, z;
             hold[b][tt] = make_float2(0.f, 0.f);
-            if (!hand_pos<N2, PL, true>(b, tt, l, z)) continue;
+            if (!hand_pos<N2, PL, true, NT>(b, tt, l, z)) continue;
             const int xa = x0 + 2 * l;
             if (xa >= g.N0) continue;
             const long long gi = xa + (long long)g.N0 * (y + (long long)g.N1 * z);
             hold[b][tt] = ld2(R, gi, xa + 1 < g.N0, g.vec2);
         }
-    zforward_store<N2>(sm, tw, hold, H, g, x0, y);
+    zforward_store<N2, PL>(sm, tw, hold, H, g, x0, y);
 }
 
-template <int N2>
-__global__ void __launch_bounds__(kThreads, 2) ks_zc2r(const float2 *__restrict__ H, float *R, Geom g,
-                                                        const float2 *__restrict__ tw) {
-    using ZT = ZTile<N2>;
-    constexpr int PL = ZT::PL, TX = ZT::TX;
+template <int N2, int PL>
+__global__ void __launch_bounds__(ks_threads(N2, PL), 2 * kThreads / ks_threads(N2, PL))
+    ks_zc2r(const float2 *__restrict__ H, float *R, Geom g, const float2 *__restrict__ tw) {
+    using ZT = ZTile<N2, PL>;
+    constexpr int TX = ZT::TX, NT = ZT::NT;
     __shared__ float2 sm[N2 * PL];
     const int x0 = blockIdx.x * TX, y = blockIdx.y;
     auto ld = [&](int, int, int l, int z) -> float2 { return zpack_load<N2>(H, g, x0, y, l, z); };
@@ -812,7 +824,7 @@ __global__ void __launch_bounds__(kThreads, 2) ks_zc2r(const float2 *__restrict_
         const long long gi = xa + (long long)g.N0 * (y + (long long)g.N1 * z);
         st2(R, gi, v, xa + 1 < g.N0, g.vec2);
     };
-    rs_fft<N2, PL, true, true>(sm, tw, ld, st);
+    rs_fft<N2, PL, true, true, 0, NT>(sm, tw, ld, st);
 }
 
 }  // namespace kw

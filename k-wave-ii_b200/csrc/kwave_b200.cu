@@ -342,11 +342,17 @@ kw_status dispatch(int n, A... args) {
 
 // ---- transform passes -----------------------------------------------------
 template <int N> struct YLaunch {
+    template <int TY>
+    static void go(kw_plan *P, bool inv, Spec4 bufs, dim3 grid, int kz0) {
+        constexpr int NT = ks_threads(N, TY);
+        if (inv) ks_ypass<true, N, TY><<<grid, NT, 0, P->stream>>>(bufs, P->g, P->tw[1], kz0);
+        else ks_ypass<false, N, TY><<<grid, NT, 0, P->stream>>>(bufs, P->g, P->tw[1], kz0);
+    }
     static kw_status run(kw_plan *P, bool inv, Spec4 bufs, int nf, int kz0, int nkz) {
         dim3 grid((P->g.N0 + P->TY - 1) / P->TY, N > 0 ? nkz : P->g.N2h, nf);
         if constexpr (N > 0) {
-            if (inv) ks_ypass<true, N><<<grid, kThreads, 0, P->stream>>>(bufs, P->g, P->tw[1], kz0);
-            else ks_ypass<false, N><<<grid, kThreads, 0, P->stream>>>(bufs, P->g, P->tw[1], kz0);
+            if (P->TY == ks_lines(N)) go<ks_lines(N)>(P, inv, bufs, grid, kz0);
+            else go<ks_narrow(N)>(P, inv, bufs, grid, kz0);
         } else {
             size_t sh = (size_t)P->TY * P->g.N1 * sizeof(float2);
             if (inv) {
@@ -365,6 +371,7 @@ template <int N> struct YLaunch {
 // always take every plane and must be called with the full range
 kw_status ypass(kw_plan *P, bool inv, Spec4 bufs, int nf, int kz0 = 0, int nkz = -1) {
     if (P->g.N1 == 1 || nf == 0) return KW_OK;
+    if (P->static_y && !P->tw[1]) return fail(KW_ERR_INVALID, "internal: axis-1 twiddle table missing");
     Scope s(P, KW_KCLASS_YPASS);
     if (nkz < 0) { kz0 = 0; nkz = P->g.N2h; }
     return dispatch<YLaunch>(P->static_y ? P->g.N1 : 0, P, inv, bufs, nf, kz0, nkz);
@@ -375,7 +382,12 @@ template <int N> struct XLaunch {
         const int lines = P->g.N1 * (N > 0 ? nkz : P->g.N2h);
         dim3 grid((lines + P->NL - 1) / P->NL, 1, fanout ? 1 : nf);
         if constexpr (N > 0) {
-            ks_xpass<N><<<grid, kThreads, 0, P->stream>>>(bufs, P->g, P->tw[0], P->op, ops, fanout, kz0, nkz);
+            if (P->NL == ks_lines(N))
+                ks_xpass<N, ks_lines(N)><<<grid, ks_threads(N, ks_lines(N)), 0, P->stream>>>(bufs, P->g, P->tw[0], P->op,
+                                                                                          ops, fanout, kz0, nkz);
+            else
+                ks_xpass<N, ks_narrow(N)><<<grid, ks_threads(N, ks_narrow(N)), 0, P->stream>>>(bufs, P->g, P->tw[0], P->op,
+                                                                                            ops, fanout, kz0, nkz);
         } else {
             size_t sh = (size_t)(fanout ? 2 : 1) * P->NL * P->g.N0 * sizeof(float2);
             KW_TRY(set_smem((const void *)k_xpass<0, 0>, sh));
@@ -386,6 +398,7 @@ template <int N> struct XLaunch {
 };
 
 kw_status xpass(kw_plan *P, Spec4 bufs, OpSet ops, int fanout, int nf, int kz0 = 0, int nkz = -1) {
+    if (P->static_x && !P->tw[0]) return fail(KW_ERR_INVALID, "internal: axis-0 twiddle table missing");
     Scope s(P, KW_KCLASS_XPASS);
     if (nkz < 0) { kz0 = 0; nkz = P->g.N2h; }
     return dispatch<XLaunch>(P->static_x ? P->g.N0 : 0, P, bufs, ops, fanout, nf, kz0, nkz);
@@ -412,7 +425,8 @@ template <int N> struct ZR2CLaunch {
     static kw_status run(kw_plan *P, const float *R, float2 *H) {
         dim3 grid((P->g.N0 + 2 * P->PL_z - 1) / (2 * P->PL_z), P->g.N1, 1);
         if constexpr (N > 0) {
-            ks_zr2c<N><<<grid, kThreads, 0, P->stream>>>(R, H, P->g, P->tw[2]);
+            if (P->PL_z == ks_lines(N)) ks_zr2c<N, ks_lines(N)><<<grid, ks_threads(N, ks_lines(N)), 0, P->stream>>>(R, H, P->g, P->tw[2]);
+            else ks_zr2c<N, ks_narrow(N)><<<grid, ks_threads(N, ks_narrow(N)), 0, P->stream>>>(R, H, P->g, P->tw[2]);
         } else {
             size_t sh = (size_t)P->PL_z * P->g.N2 * sizeof(float2);
             KW_TRY(set_smem((const void *)k_zr2c<0, 0>, sh));
@@ -425,7 +439,8 @@ template <int N> struct ZC2RLaunch {
     static kw_status run(kw_plan *P, const float2 *H, float *R) {
         dim3 grid((P->g.N0 + 2 * P->PL_z - 1) / (2 * P->PL_z), P->g.N1, 1);
         if constexpr (N > 0) {
-            ks_zc2r<N><<<grid, kThreads, 0, P->stream>>>(H, R, P->g, P->tw[2]);
+            if (P->PL_z == ks_lines(N)) ks_zc2r<N, ks_lines(N)><<<grid, ks_threads(N, ks_lines(N)), 0, P->stream>>>(H, R, P->g, P->tw[2]);
+            else ks_zc2r<N, ks_narrow(N)><<<grid, ks_threads(N, ks_narrow(N)), 0, P->stream>>>(H, R, P->g, P->tw[2]);
         } else {
             size_t sh = (size_t)P->PL_z * P->g.N2 * sizeof(float2);
             KW_TRY(set_smem((const void *)k_zc2r<0, 0>, sh));
@@ -436,10 +451,12 @@ template <int N> struct ZC2RLaunch {
 };
 
 kw_status zr2c(kw_plan *P, const float *R, float2 *H) {
+    if (P->static_z && !P->tw[2]) return fail(KW_ERR_INVALID, "internal: axis-2 twiddle table missing");
     return dispatch<ZR2CLaunch>(P->static_z ? P->g.N2 : 0, P, R, H);
 }
 
 kw_status zc2r(kw_plan *P, const float2 *H, float *R) {
+    if (P->static_z && !P->tw[2]) return fail(KW_ERR_INVALID, "internal: axis-2 twiddle table missing");
     return dispatch<ZC2RLaunch>(P->static_z ? P->g.N2 : 0, P, H, R);
 }
 
@@ -531,13 +548,19 @@ TRSrc tr_of(kw_plan *P) {
 }
 
 template <int N> struct ULaunch {
+    template <int PL>
+    static kw_status go(kw_plan *P, const StageU &a, dim3 grid) {
+        using Z = ZStage<N, PL>;
+        const size_t sh = (size_t)(Z::TILE + 2 * Z::SLICE) * sizeof(float2);
+        KW_TRY(set_smem((const void *)ks_stage_u<N, PL>, sh));
+        ks_stage_u<N, PL><<<grid, Z::NT, sh, P->stream>>>(a, P->tw[2]);
+        return KW_OK;
+    }
     static kw_status run(kw_plan *P, StageU a) {
         dim3 grid((P->g.N0 + 2 * a.PL - 1) / (2 * a.PL), P->g.N1, P->D);
         if constexpr (N > 0) {
-            using Z = ZStage<(N > 0 ? N : 64)>;
-            const size_t sh = (size_t)(Z::TILE + 2 * Z::SLICE) * sizeof(float2);
-            KW_TRY(set_smem((const void *)ks_stage_u<N>, sh));
-            ks_stage_u<N><<<grid, kThreads, sh, P->stream>>>(a, P->tw[2]);
+            if (a.PL == ks_lines(N)) KW_TRY(go<ks_lines(N)>(P, a, grid));
+            else KW_TRY(go<ks_narrow(N)>(P, a, grid));
         } else {
             size_t sh = (size_t)a.PL * P->g.N2 * sizeof(float2);
             KW_TRY(set_smem((const void *)k_stage_u<0, 0>, sh));
@@ -547,13 +570,19 @@ template <int N> struct ULaunch {
     }
 };
 template <int N> struct RLaunch {
+    template <int PL>
+    static kw_status go(kw_plan *P, const StageR &a, dim3 grid) {
+        using Z = ZStage<N, PL>;
+        const size_t sh = (size_t)(Z::TILE + 2 * Z::SLICE) * sizeof(float2);
+        KW_TRY(set_smem((const void *)ks_stage_r<N, PL>, sh));
+        ks_stage_r<N, PL><<<grid, Z::NT, sh, P->stream>>>(a, P->tw[2]);
+        return KW_OK;
+    }
     static kw_status run(kw_plan *P, StageR a) {
         dim3 grid((P->g.N0 + 2 * a.PL - 1) / (2 * a.PL), P->g.N1, 1);
         if constexpr (N > 0) {
-            using Z = ZStage<(N > 0 ? N : 64)>;
-            const size_t sh = (size_t)(Z::TILE + 2 * Z::SLICE) * sizeof(float2);
-            KW_TRY(set_smem((const void *)ks_stage_r<N>, sh));
-            ks_stage_r<N><<<grid, kThreads, sh, P->stream>>>(a, P->tw[2]);
+            if (a.PL == ks_lines(N)) KW_TRY(go<ks_lines(N)>(P, a, grid));
+            else KW_TRY(go<ks_narrow(N)>(P, a, grid));
         } else {
             size_t sh = (size_t)4 * a.PL * P->g.N2 * sizeof(float2);
             KW_TRY(set_smem((const void *)k_stage_r<0, 0>, sh));
@@ -563,13 +592,19 @@ template <int N> struct RLaunch {
     }
 };
 template <int N> struct PLaunch {
+    template <int PL>
+    static kw_status go(kw_plan *P, const StageP &a, dim3 grid) {
+        using Z = ZStage<N, PL>;
+        const size_t sh = (size_t)(Z::TILE + Z::SLICE) * sizeof(float2);
+        KW_TRY(set_smem((const void *)ks_stage_p<N, PL>, sh));
+        ks_stage_p<N, PL><<<grid, Z::NT, sh, P->stream>>>(a, P->tw[2]);
+        return KW_OK;
+    }
     static kw_status run(kw_plan *P, StageP a) {
         dim3 grid((P->g.N0 + 2 * a.PL - 1) / (2 * a.PL), P->g.N1, 1);
         if constexpr (N > 0) {
-            using Z = ZStage<(N > 0 ? N : 64)>;
-            const size_t sh = (size_t)(Z::TILE + Z::SLICE) * sizeof(float2);
-            KW_TRY(set_smem((const void *)ks_stage_p<N>, sh));
-            ks_stage_p<N><<<grid, kThreads, sh, P->stream>>>(a, P->tw[2]);
+            if (a.PL == ks_lines(N)) KW_TRY(go<ks_lines(N)>(P, a, grid));
+            else KW_TRY(go<ks_narrow(N)>(P, a, grid));
         } else {
             size_t sh = (size_t)2 * a.PL * P->g.N2 * sizeof(float2);
             KW_TRY(set_smem((const void *)k_stage_p<0, 0>, sh));
@@ -913,11 +948,15 @@ int choose_pl(int cap, int N0, int N1, int N2) {
 
 void plan_tiles(kw_plan *P) {
     const Geom &g = P->g;
-    // compile-time kernels where the axis length has one and the grid still
-    // fills one wave of blocks; their tile widths are fixed by ks_lines
-    P->static_z = g.vec2 && is_static(g.N2) && (long long)((g.N0 + 2 * ks_lines(g.N2) - 1) / (2 * ks_lines(g.N2))) * g.N1 >= 148;
+    // compile-time kernels where the axis length has one; their tiles are
+    // ks_lines(n) lines wide, or ks_narrow(n) when full tiles would give less
+    // than one block per SM (small grids)
+    constexpr long long kWave = 148;
+    P->static_z = g.vec2 && is_static(g.N2);
     if (P->static_z) {
-        P->PL_u = P->PL_z = P->PL_p = P->PL_r = ks_lines(g.N2);
+        int pl = ks_lines(g.N2);
+        if ((long long)((g.N0 + 2 * pl - 1) / (2 * pl)) * g.N1 < kWave) pl = ks_narrow(g.N2);
+        P->PL_u = P->PL_z = P->PL_p = P->PL_r = pl;
     } else {
         P->PL_u = choose_pl(kCap, g.N0, g.N1, g.N2);
         P->PL_z = P->PL_u;
@@ -927,13 +966,22 @@ void plan_tiles(kw_plan *P) {
     P->static_y = g.N1 > 1 && is_static(g.N1);
     if (P->static_y) {
         P->TY = ks_lines(g.N1);
+        if ((long long)((g.N0 + P->TY - 1) / P->TY) * g.N2h < kWave) P->TY = ks_narrow(g.N1);
     } else {
         int ty = 1;
         while (ty * 2 <= 32 && ty * 2 * g.N1 <= kCap) ty *= 2;
         P->TY = ty;
     }
     const int lines = g.N1 * g.N2h;
-    P->static_x = is_static(g.N0) && (lines + ks_lines(g.N0) - 1) / ks_lines(g.N0) >= 148;
+    P->static_x = is_static(g.N0);
+    if (P->static_x) {
+        P->NL = ks_lines(g.N0);
+        if ((lines + P->NL - 1) / P->NL < kWave) P->NL = ks_narrow(g.N0);
+    } else {
+        P->NL = std::max(1, kCap / g.N0);
+        if (P->NL > lines) P->NL = lines;
+        while (P->NL > 1 && (lines + P->NL - 1) / P->NL < 2 * kWave) P->NL /= 2;
+    }
     {
         // chunk the y / x / y groups so one chunk of a half spectrum (written
         // and re-read in place) stays well inside the 126 MB L2
@@ -945,16 +993,8 @@ void plan_tiles(kw_plan *P) {
         int nch = mb > 0 ? (int)std::ceil(bytes / (mb * 1e6)) : 1;
         nch = std::max(1, std::min(nch, g.N2h));
         // every chunk must still fill the GPU
-        while (nch > 1 && (long long)(g.N2h / nch) * g.N1 / std::max(1, ks_lines(g.N0)) < 148) --nch;
+        while (nch > 1 && (long long)(g.N2h / nch) * g.N1 / std::max(1, P->NL) < kWave) --nch;
         P->kz_chunks = nch;
-    }
-
-    if (P->static_x) {
-        P->NL = ks_lines(g.N0);
-    } else {
-        P->NL = std::max(1, kCap / g.N0);
-        if (P->NL > lines) P->NL = lines;
-        while (P->NL > 1 && (lines + P->NL - 1) / P->NL < 2 * 148) P->NL /= 2;
     }
 }
 
@@ -1663,7 +1703,10 @@ kw_status kw_gradient_noalloc(int32_t dim, const uint64_t shape[3], const double
         }
         KW_CUDA(cudaMemcpyAsync(base + o_tw[a], tw.data(), tw.size() * sizeof(float2), cudaMemcpyHostToDevice, P.stream));
         KW_CUDA(cudaMemcpyAsync(base + o_k2[a], k2.data(), k2.size() * sizeof(float), cudaMemcpyHostToDevice, P.stream));
-        f.tw = (const float2 *)(base + o_tw[a]);
+        // both kernel families read the twiddles: the runtime-radix ones
+        // through fft[a], the compile-time ones through tw[a]
+        P.tw[a] = (float2 *)(base + o_tw[a]);
+        f.tw = P.tw[a];
         P.op.k2[a] = (const float *)(base + o_k2[a]);
         P.op.dd_pos[a] = P.op.dd_neg[a] = (const float2 *)(base + o_dd);
     }

@@ -127,7 +127,9 @@ class kw_server_stats(C.Structure):
     _fields_ = [("submitted", C.c_uint64), ("admitted", C.c_uint64), ("completed", C.c_uint64),
                 ("failed", C.c_uint64), ("active", C.c_uint64), ("pending", C.c_uint64),
                 ("p50_ms", C.c_double), ("p99_ms", C.c_double), ("mean_ms", C.c_double),
-                ("cell_steps", C.c_double), ("busy_seconds", C.c_double)]
+                ("cell_steps", C.c_double), ("busy_seconds", C.c_double),
+                ("setup_seconds", C.c_double), ("issue_seconds", C.c_double), ("retire_seconds", C.c_double),
+                ("wait_seconds", C.c_double)]
 
 
 SYMBOLS = {

@@ -48,7 +48,7 @@ def _noalloc(lib, f_dev, out_dev, shape, dx, axis, c, dt):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("shape", [(64, 48), (24, 20, 30)])
+@pytest.mark.parametrize("shape", [(64, 48), (24, 20, 30), (64, 64), (32, 64, 64)])
 def test_noalloc_gradient_matches_allocating_path(shape):
     torch = pytest.importorskip("torch")
     import kwave_b200 as kw
