@@ -271,6 +271,30 @@ kw_status kw_server_get_stats(kw_server *server, kw_server_stats *stats);
 kw_status kw_server_destroy(kw_server *server);
 
 /*
+ * Gradient of a sensor misfit with respect to the sound speed and the density
+ * (the adjoint form).  No counterpart in the reference, which offers time
+ * reversal only: this is the exact discrete adjoint of the plan's own time
+ * loop for lossless linear media with additive pressure sources and a binary
+ * sensor mask (kspaceFirstOrder3D.m:792-1040 run backwards).
+ *
+ * residual[m + M * (t - record_start_index)] = dJ/dp_m(t), in the layout of
+ * the p output (M = sensor_num rows, Nt - record_start_index + 1 columns);
+ * for J = 1/2 sum (p - d)^2 it is p - d.  grad_c and grad_rho (either may be
+ * NULL) receive dJ/dc0 and dJ/drho0 at every grid cell, column-major.  c_ref,
+ * dt, the PML and the (already scaled) source signals are held fixed; the
+ * density gradient includes the chain through rho0_sg{x,y,z} when they are
+ * formed from rho0 (derive_rho0_sg, or a scalar density).
+ *
+ * Memory: sqrt(Nt) checkpointing -- the state (u_i, rho_i, p) is kept after
+ * every checkpoint_interval-th step (0: round(sqrt(Nt))) and each segment is
+ * re-run once, so about (Nt / K + K) (2 D + 1) N floats of device memory are
+ * used for the call.  The plan's recorded outputs are left as they were; the
+ * plan is reset on return.  Other media or sources: KW_ERR_UNSUPPORTED.
+ */
+kw_status kw_adjoint_gradient(kw_plan *plan, const float *residual, uint32_t checkpoint_interval, double *grad_c,
+                              double *grad_rho);
+
+/*
  * Allocation-free staggered spectral gradient.  No counterpart in the
  * reference: it exists for callers that must not have this library allocate
  * device memory -- a MEX function working on gpuArray data owned by MATLAB's

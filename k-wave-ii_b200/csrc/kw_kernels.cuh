@@ -996,6 +996,128 @@ __global__ void k_absorb_coeffs(const float *__restrict__ c0, double c0s, const 
     if (c2eta) c2eta[i] = (float)(c * c * eta * sg1);
 }
 
+// ---------------------------------------------------------------------------
+// adjoint kernels (gradient entry point).  One thread per cell, grid-stride;
+// the discrete adjoint of the lossless linear step, component by component:
+//   w_i     = rho_sg_i^-1 pml_sg_i lambda_u_i                  (k_adj_w)
+//   mu      = S^T r(t) + dt sum_i D_i w_i
+//   lambda_rho_i = c0^2 mu + pml_i^2 lambda_rho_i, v_i = rho0 pml_i lambda_rho_i,
+//   dJ/dc0 += 2 c0 mu sum_i rho_i(t)                           (k_adj_mid)
+//   dJ/drho0 += sum_i lambda_rho_i (-dt pml_i D_i u_i(t))      (k_adj_grho)
+//   lambda_u_i = pml_sg_i^2 lambda_u_i + dt G_i v_i            (k_adj_u)
+//   dJ/drho_sg_i^-1 += lambda_u_i (-dt pml_sg_i G_i p(t-1))    (k_adj_gR)
+// Gradients accumulate in FP64.
+// ---------------------------------------------------------------------------
+struct AdjArgs {
+    Geom g;
+    int D;
+    float dt;
+    int axis[3];                 // internal axis of each component
+    const float *pml[3];         // mass PML profile along that axis
+    const float *pml_sg[3];      // momentum PML profile along that axis
+    Med rsi[3];                  // 1 / rho_sg_i
+    Med c0, rho0;
+    float *lu[3], *lr[3];        // adjoint velocity / density
+    float *A[3];                 // work fields
+    const float *B[3];           // spectral results
+    const float *mu;             // scattered residual S^T r(t)
+    const float *rho_t[3];       // forward rho after step t
+    double *g_c, *g_r0, *g_R[3];
+};
+
+__device__ __forceinline__ int adj_coord(const Geom &g, long long i, int axis) {
+    if (axis == 0) return (int)(i % g.N0);
+    const long long q = i / g.N0;
+    return axis == 1 ? (int)(q % g.N1) : (int)(q / g.N1);
+}
+__device__ __forceinline__ float med1(const Med &m, long long i) { return m.arr ? __ldg(m.arr + i) : m.val; }
+
+__global__ void k_adj_w(AdjArgs a) {
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < a.g.N; i += (long long)gridDim.x * blockDim.x)
+        for (int c = 0; c < a.D; ++c) {
+            const float pu = __ldg(a.pml_sg[c] + adj_coord(a.g, i, a.axis[c]));
+            a.A[c][i] = med1(a.rsi[c], i) * pu * a.lu[c][i];
+        }
+}
+
+__global__ void k_adj_mid(AdjArgs a) {
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < a.g.N; i += (long long)gridDim.x * blockDim.x) {
+        float mu = a.mu[i];
+        for (int c = 0; c < a.D; ++c) mu = fmaf(a.dt, a.B[c][i], mu);
+        const float cc = med1(a.c0, i), r0 = med1(a.rho0, i);
+        float srho = 0.f;
+        for (int c = 0; c < a.D; ++c) {
+            const float pr = __ldg(a.pml[c] + adj_coord(a.g, i, a.axis[c]));
+            const float lr = fmaf(cc * cc, mu, pr * pr * a.lr[c][i]);
+            a.lr[c][i] = lr;
+            a.A[c][i] = r0 * pr * lr;
+            srho += a.rho_t[c][i];
+        }
+        a.g_c[i] += 2.0 * (double)cc * (double)mu * (double)srho;
+    }
+}
+
+__global__ void k_adj_grho(AdjArgs a) {
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < a.g.N; i += (long long)gridDim.x * blockDim.x) {
+        double s = 0.0;
+        for (int c = 0; c < a.D; ++c) {
+            const float pr = __ldg(a.pml[c] + adj_coord(a.g, i, a.axis[c]));
+            s += (double)a.lr[c][i] * (double)(-a.dt * pr * a.B[c][i]);
+        }
+        a.g_r0[i] += s;
+    }
+}
+
+__global__ void k_adj_u(AdjArgs a) {
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < a.g.N; i += (long long)gridDim.x * blockDim.x)
+        for (int c = 0; c < a.D; ++c) {
+            const float pu = __ldg(a.pml_sg[c] + adj_coord(a.g, i, a.axis[c]));
+            a.lu[c][i] = fmaf(pu * pu, a.lu[c][i], a.dt * a.B[c][i]);
+        }
+}
+
+__global__ void k_adj_gR(AdjArgs a) {
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < a.g.N; i += (long long)gridDim.x * blockDim.x)
+        for (int c = 0; c < a.D; ++c) {
+            const float pu = __ldg(a.pml_sg[c] + adj_coord(a.g, i, a.axis[c]));
+            a.g_R[c][i] += (double)a.lu[c][i] * (double)(-a.dt * pu * a.B[c][i]);
+        }
+}
+
+// mu[sidx[m]] = r[m] (sensor cells are distinct)
+__global__ void k_adj_scatter(float *mu, const long long *sidx, int M, const float *r) {
+    const int m = blockIdx.x * blockDim.x + threadIdx.x;
+    if (m < M) mu[sidx[m]] = r[m];
+}
+
+// dJ/drho0 = direct term + the chain through rho_sg_i^-1 = 1 / rho_sg_i:
+// h_i = dJ/drho_sg_i = -rho_sg_i^-2 dJ/drho_sg_i^-1; with derive != 0 the
+// staggered density is the midpoint average of rho0 at x and x + e_i (rho0
+// itself on the last plane), otherwise rho_sg_i = rho0.
+__global__ void k_adj_rho_chain(AdjArgs a, int derive, double *out) {
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < a.g.N; i += (long long)gridDim.x * blockDim.x) {
+        double s = a.g_r0[i];
+        for (int c = 0; c < a.D; ++c) {
+            const int ax = a.axis[c];
+            const int n = ax == 0 ? a.g.N0 : (ax == 1 ? a.g.N1 : a.g.N2);
+            const long long st = ax == 0 ? 1 : (ax == 1 ? (long long)a.g.N0 : (long long)a.g.N0 * a.g.N1);
+            const int k = adj_coord(a.g, i, ax);
+            const double r = med1(a.rsi[c], i);
+            const double h = -r * r * a.g_R[c][i];
+            if (!derive || k == n - 1) {
+                s += h;
+            } else {
+                s += 0.5 * h;
+            }
+            if (derive && k >= 1) {
+                const double rm = med1(a.rsi[c], i - st);
+                s += 0.5 * (-rm * rm * a.g_R[c][i - st]);
+            }
+        }
+        out[i] = s;
+    }
+}
+
 // flags |= bit where a value is not strictly positive (or NaN)
 __global__ void k_check_positive(const float *__restrict__ a, long long N, int *flags, int bit) {
     const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;

@@ -187,6 +187,7 @@ struct kw_plan {
 
     int t = 1;                     // next step to run (1-based)
     bool started = false;
+    bool no_record = false;        // steps re-run by the gradient do not record
 
     // timing
     uint32_t timing_mask = 0;
@@ -701,7 +702,7 @@ kw_status stage_p(kw_plan *P, int write_spec) {
 }
 
 kw_status sensors(kw_plan *P, int t) {
-    if (P->time_rev || t < P->record_start) return KW_OK;
+    if (P->no_record || P->time_rev || t < P->record_start) return KW_OK;
     if (P->M > 0) {
         SensorArgs a{};
         a.M = P->M;
@@ -1382,7 +1383,7 @@ kw_status run_step_graphed(kw_plan *P) {
     for (int c = 0; c < P->D; ++c) usrc = usrc || (P->usrc.dense_general && P->usrc.sig[c] && t <= P->usrc.T[c]);
     key |= usrc ? 4u : 0u;
     key |= (P->psrc.dense_general && t <= P->psrc.T[0]) ? 8u : 0u;
-    key |= (!P->time_rev && t >= P->record_start) ? 16u : 0u;
+    key |= (!P->no_record && !P->time_rev && t >= P->record_start) ? 16u : 0u;
     key |= (t < P->index_end) ? 32u : 0u;
     kw_plan::GraphEntry &e = P->graphs[key];
     if (e.exec) {
@@ -1756,3 +1757,4 @@ kw_status kw_plan_device_bytes(const kw_plan *P, uint64_t *bytes) {
 }  // extern "C"
 
 #include "kw_server.inc"
+#include "kw_adjoint.inc"

@@ -648,6 +648,37 @@ class Simulation:
         _abi.check(self._lib.kw_plan_device_bytes(self.handle, C.byref(b)))
         return b.value
 
+    # -- adjoint -----------------------------------------------------------------
+    def adjoint_gradient(self, residual, checkpoint_interval=0, density=True):
+        """Gradient of a sensor misfit J with respect to the sound speed and
+        the density at every grid cell (the library's discrete adjoint of this
+        plan's loop; lossless linear media, additive pressure sources).
+
+        ``residual`` is dJ/dp with the shape and row order of the recorded
+        ``p`` output (for J = 1/2 sum (p - d)^2, ``p - d``).  Returns
+        ``(dJ/dc0, dJ/drho0)`` shaped like the grid (``dJ/drho0`` is None when
+        ``density`` is False).  c_ref, dt, the PML and the scaled source
+        signal are held fixed."""
+        P = self.prep
+        T = P.Nt - P.record_start + 1
+        r = np.asarray(residual, dtype=np.float64)
+        if r.shape != (P.M, T):
+            raise ValueError("residual must be %d x %d (sensor points x recorded steps)" % (P.M, T))
+        if P.reorder_index is not None:
+            # rows came back in Cartesian order: put them back in find(mask) order
+            raw = np.empty_like(r)
+            raw[np.argsort(np.asarray(P.reorder_index), kind="stable")] = r
+            r = raw
+        r = np.asfortranarray(r, dtype=np.float32)
+        shape = P.shape
+        gc = np.zeros(int(np.prod(shape)), dtype=np.float64)
+        gr = np.zeros_like(gc) if density else None
+        _abi.check(self._lib.kw_adjoint_gradient(self.handle, r.ctypes.data_as(C.c_void_p), int(checkpoint_interval),
+                                                 gc.ctypes.data_as(C.c_void_p),
+                                                 gr.ctypes.data_as(C.c_void_p) if density else None))
+        gc = gc.reshape(shape, order="F")
+        return gc, (gr.reshape(shape, order="F") if density else None)
+
     # -- outputs ---------------------------------------------------------------
     def copy_outputs(self):
         o, host = _alloc_outputs(self.prep)

@@ -154,3 +154,21 @@ def make_case(name):
 CASES = ["2d_homog_p0", "2d_hetero_abs_nl", "2d_stokes_dirichlet", "2d_nocorr_multi", "2d_u_additive",
          "2d_u_dirichlet", "2d_odd_sizes", "2d_pml_outside", "3d_hetero_abs_nl_plane", "3d_multi_signal_additive",
          "3d_p0_u", "2d_time_reversal", "3d_time_reversal_abs", "3d_static_mixed_radix", "3d_static_128"]
+
+
+def adjoint_problem(shape, Nt, seed=0, dx=1e-4):
+    """Heterogeneous lossless medium, one additive point source, a sensor
+    plane: (shape, dx, Nt, dt, c, rho, p_mask, signal, sensor_mask)."""
+    rng = np.random.default_rng(seed)
+    dim = len(shape)
+    c = 1500 + 100 * rng.random(shape)
+    rho = 1000 + 80 * rng.random(shape)
+    dt = 0.3 * dx / c.max()
+    pm = np.zeros(shape)
+    pm[(shape[0] // 3,) + tuple(s // 2 for s in shape[1:])] = 1
+    sig = 1e3 * np.sin(2 * np.pi * 2e6 * np.arange(Nt) * dt) * np.hanning(Nt)
+    sm = np.zeros(shape)
+    sl = [slice(None)] * dim
+    sl[0] = 2 * shape[0] // 3
+    sm[tuple(sl)] = 1
+    return shape, dx, Nt, dt, c, rho, pm, sig, sm

@@ -1,0 +1,72 @@
+"""Adjoint form: kw_adjoint_gradient against the FP64 discrete adjoint.
+
+The oracle's adjoint (oracle/adjoint.py) is pinned by central finite
+differences on the CPU (tests/test_oracle_adjoint.py).  Here the library's
+gradient of J = 1/2 sum (p(sensor) - d)^2 with respect to the sound speed and
+the density, computed from the FP32 loop with FP64 accumulation and sqrt(Nt)
+checkpointing, must match it: relative L2 error <= 1e-3 over the grid (the
+loop runs in FP32; the residual is the same array for both).  Every
+checkpoint interval must give the same gradient.
+"""
+import numpy as np
+import pytest
+
+from cases import adjoint_problem
+
+TOL = 1e-3
+
+
+def _rel(a, b):
+    return float(np.linalg.norm((np.asarray(a) - b).ravel()) / np.linalg.norm(np.ravel(b)))
+
+
+def _grid(mod, shape, dx, Nt, dt):
+    args = []
+    for s in shape:
+        args += [s, dx]
+    g = (mod.kWaveGrid if hasattr(mod, "kWaveGrid") else mod.KWaveGrid)(*args)
+    g.setTime(Nt, dt)
+    return g
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("shape,Nt", [((32, 28), 60), ((64, 64), 120), ((12, 14, 10), 25), ((32, 64, 48), 40)])
+def test_gradient_matches_oracle_adjoint(shape, Nt):
+    import kwave_b200 as kw
+    from oracle import adjoint as adj
+    from oracle import kspace as ks
+    shape, dx, Nt, dt, c, rho, pm, sig, sm = adjoint_problem(shape, Nt)
+    dim = len(shape)
+    medium = {"sound_speed": c, "density": rho, "sound_speed_ref": 1700.0}
+    sim = kw.Simulation(dim, _grid(kw, shape, dx, Nt, dt), medium, {"p_mask": pm, "p": sig[None, :]},
+                        {"mask": sm}, PMLSize=4, Smooth=False)
+    y = sim.run()
+    ops = adj.setup(_grid(ks, shape, dx, Nt, dt), c, rho, pm, sig, sm, pml_size=4, c_ref=1700.0)
+    y64 = adj.forward(ops)
+    assert ks.rel_l2(y, y64) < 1e-4
+    rng = np.random.default_rng(3)
+    d = 0.9 * y64 + 0.01 * np.abs(y64).max() * rng.standard_normal(y64.shape)
+    r = y.astype(np.float64) - d
+    gc, gr = sim.adjoint_gradient(r)
+    rc, rr = adj.gradient(ops, r)
+    ec, er = _rel(gc, rc), _rel(gr, rr)
+    assert ec <= TOL and er <= TOL, "rel-L2 dJ/dc %.2e dJ/drho %.2e" % (ec, er)
+    # checkpoint interval changes memory, not the result
+    for K in (1, 7, Nt):
+        gc2, gr2 = sim.adjoint_gradient(r, checkpoint_interval=K)
+        assert np.array_equal(gc2, gc) and np.array_equal(gr2, gr), K
+    # the plan still runs and its outputs are unchanged
+    assert np.array_equal(sim.run(), y)
+    sim.close()
+
+
+@pytest.mark.gpu
+def test_gradient_rejects_unsupported_media():
+    import kwave_b200 as kw
+    shape, dx, Nt, dt, c, rho, pm, sig, sm = adjoint_problem((32, 28), 20)
+    medium = {"sound_speed": c, "density": rho, "alpha_coeff": 0.5, "alpha_power": 1.5}
+    with kw.Simulation(2, _grid(kw, shape, dx, Nt, dt), medium, {"p_mask": pm, "p": sig[None, :]},
+                       {"mask": sm}, PMLSize=4) as sim:
+        y = sim.run()
+        with pytest.raises(kw.KWaveError, match="lossless"):
+            sim.adjoint_gradient(np.zeros_like(y))
