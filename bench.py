@@ -357,6 +357,103 @@ def served_section(kw, device, n_req=48, seed=7, load=0.9):
     }
 
 
+def ricker(dt, Nt, f0=1e6):
+    """Ricker wavelet (1 - 2 (pi f0 tau)^2) exp(-(pi f0 tau)^2), tau = t - 1.5 / f0."""
+    tau = np.arange(Nt) * dt - 1.5 / f0
+    a = (np.pi * f0 * tau) ** 2
+    return (1.0 - 2.0 * a) * np.exp(-a)
+
+
+def adjoint_workload(N=512, Nt=3000, n_elem=256, radius=230, n_shots=16, dx=0.1e-3, seed=4, c_ref=1800.0):
+    """Sound-speed inversion set-up: a ring array of n_elem elements (radius in
+    cells) around a blob medium; n_shots elements fire in turn a 1 MHz Ricker
+    wavelet (additive point source) and every element records p."""
+    rng = np.random.default_rng(seed)
+    ax = np.arange(N, dtype=np.float64) - N / 2
+    c_true = np.full((N, N), 1500.0)
+    for _ in range(6):
+        r0 = rng.uniform(0, 0.6 * radius)
+        ang = rng.uniform(0, 2 * np.pi)
+        cx, cy = r0 * np.cos(ang), r0 * np.sin(ang)
+        sg = rng.uniform(10.0, 30.0)
+        c_true += rng.uniform(-80.0, 150.0) * np.exp(-((ax[:, None] - cx) ** 2 + (ax[None, :] - cy) ** 2) / (2 * sg * sg))
+    dt = 0.3 * dx / c_ref
+    return dict(N=N, Nt=Nt, dx=dx, dt=dt, c_true=c_true, c_start=np.full((N, N), 1500.0), rho=np.full((N, N), 1000.0),
+                n_elem=n_elem, radius=radius, n_shots=n_shots, c_ref=c_ref, src=1e5 * ricker(dt, Nt))
+
+
+def _adjoint_problem(kw, w, c, shot, mask_cells):
+    g = kw.kWaveGrid(w["N"], w["dx"], w["N"], w["dx"])
+    g.setTime(w["Nt"], w["dt"])
+    shape = (w["N"], w["N"])
+    pm = np.zeros(shape)
+    pm[np.unravel_index(mask_cells[shot * (len(mask_cells) // w["n_shots"])], shape, order="F")] = 1
+    ring = np.zeros(shape)
+    ring[np.unravel_index(mask_cells, shape, order="F")] = 1
+    med = {"sound_speed": c, "density": w["rho"], "sound_speed_ref": w["c_ref"]}
+    return kw.Server.prepare(2, g, med, {"p_mask": pm, "p": w["src"][None, :]}, {"mask": ring}, PMLSize=20, Smooth=False)
+
+
+def adjoint_section(kw, device, Nt=3000, n_shots=16, fd_cells=32, seed=4):
+    """Gradient of J = 1/2 sum over shots of |p(ring) - d|^2 at the homogeneous
+    starting model (16 shots, Nt steps, sqrt(Nt) checkpointing), timed per
+    shot, and central finite differences of J for shot 0 at fd_cells random
+    cells inside the ring (FP32 forward runs, h = 1 % of c)."""
+    w = adjoint_workload(Nt=Nt, n_shots=n_shots, seed=seed)
+    g = kw.kWaveGrid(w["N"], w["dx"], w["N"], w["dx"])
+    ring_mask, _, _ = kw.cart2grid(g, kw.makeCartCircle(w["radius"] * w["dx"], w["n_elem"]))
+    cells = np.flatnonzero(ring_mask.ravel(order="F"))
+    data = []
+    for s in range(n_shots):
+        with kw.Simulation.from_prepared(_adjoint_problem(kw, w, w["c_true"], s, cells)) as sim:
+            data.append(sim.run())
+    grad = np.zeros((w["N"], w["N"]))
+    J = 0.0
+    shot_s = []
+    for s in range(n_shots):
+        t0 = time.perf_counter()
+        with kw.Simulation.from_prepared(_adjoint_problem(kw, w, w["c_start"], s, cells)) as sim:
+            y = sim.run()
+            r = y.astype(np.float64) - data[s]
+            gc, _ = sim.adjoint_gradient(r)
+        shot_s.append(time.perf_counter() - t0)
+        grad += gc
+        J += 0.5 * float(np.sum(r * r))
+        if s == 0:
+            g0 = gc.copy()
+    # finite differences for shot 0
+    rng = np.random.default_rng(seed + 1)
+    fd, ad = [], []
+    h = 15.0
+    inside = np.argwhere((np.arange(w["N"])[:, None] - w["N"] / 2) ** 2 + (np.arange(w["N"])[None, :] - w["N"] / 2) ** 2
+                         < (0.8 * w["radius"]) ** 2)
+    for k in rng.choice(len(inside), size=fd_cells, replace=False):
+        x, yy = inside[k]
+        vals = []
+        for sgn in (1, -1):
+            c = w["c_start"].copy()
+            c[x, yy] += sgn * h
+            with kw.Simulation.from_prepared(_adjoint_problem(kw, w, c, 0, cells)) as sim:
+                rr = sim.run().astype(np.float64) - data[0]
+            vals.append(0.5 * float(np.sum(rr * rr)))
+        fd.append((vals[0] - vals[1]) / (2 * h))
+        ad.append(float(g0[x, yy]))
+    fd, ad = np.array(fd), np.array(ad)
+    big = np.abs(fd) > 0.05 * np.abs(fd).max()
+    return {
+        "workload": "2D %dx%d ring array of %d elements (radius %d cells), %d shots, 1 MHz Ricker, Nt=%d, "
+                    "homogeneous 1500 m/s start, blob true medium" % (w["N"], w["N"], w["n_elem"], w["radius"],
+                                                                       n_shots, Nt),
+        "checkpoint_interval": int(round(np.sqrt(Nt))), "misfit": J,
+        "seconds_per_shot": float(np.median(shot_s)), "seconds_all_shots": float(np.sum(shot_s)),
+        "seconds_per_shot_note": "forward run + gradient (forward with checkpoints, per-segment re-run, adjoint)",
+        "fd_check": {"cells": fd_cells, "h_m_per_s": h,
+                     "cosine": float(np.dot(fd, ad) / (np.linalg.norm(fd) * np.linalg.norm(ad))),
+                     "max_rel_err_where_fd_above_5pct": float(np.max(np.abs(ad[big] - fd[big]) / np.abs(fd[big]))),
+                     "median_rel_err_where_fd_above_5pct": float(np.median(np.abs(ad[big] - fd[big]) / np.abs(fd[big])))},
+    }
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -369,6 +466,8 @@ def main():
     ap.add_argument("--Nt", type=int, default=1000)
     ap.add_argument("--N", type=int, default=256)
     ap.add_argument("--serve-requests", type=int, default=48, help="0 skips the served-stream section")
+    ap.add_argument("--adjoint-shots", type=int, default=16, help="0 skips the adjoint section")
+    ap.add_argument("--adjoint-fd", type=int, default=32, help="finite-difference cells of the adjoint check")
     args = ap.parse_args()
     ws, rank, local = dist_setup()
     if args.impl == "reference":
@@ -451,6 +550,10 @@ def main():
     if args.serve_requests > 0:
         served = served_section(kw, local, n_req=args.serve_requests, seed=7 + rank)
 
+    adjoint = None
+    if args.adjoint_shots > 0:
+        adjoint = adjoint_section(kw, local, n_shots=args.adjoint_shots, fd_cells=args.adjoint_fd, seed=4 + rank)
+
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu:
         try:
@@ -471,7 +574,7 @@ def main():
                            "l2": "no flush: inputs larger than L2 (device working set %.2f GB vs 126 MB L2)" % dev_gb,
                            "parallelism": "replicas x%d" % ws},
                 "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
-                "clocks": clocks, "kernel_classes": classes, "served": served}
+                "clocks": clocks, "kernel_classes": classes, "served": served, "adjoint": adjoint}
         print(json.dumps(line), flush=True)
     if ws > 1:
         import torch.distributed as dist
