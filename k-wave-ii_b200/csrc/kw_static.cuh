@@ -387,14 +387,23 @@ __device__ __forceinline__ void cp_async8(void *smem, const void *gmem) {
     const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
     asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem) : "memory");
 }
+__device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
+}
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+// wait until at most N of this thread's most recent commit groups are pending
+template <int N>
+__device__ __forceinline__ void cp_async_wait_group() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
 
 template <int N2, int PL_> struct ZStage {
     using ZT = ZTile<N2, PL_>;
     using SH = typename ZT::SH;
     static constexpr int PL = ZT::PL, TX = ZT::TX, NT = ZT::NT;
-    static constexpr int TILE = N2 * PL;                  // float2 of the transform tile
+    // float2 of the transform tile; it also holds the raw half-spectrum rows of
+    // a prefetched input, (N2/2 + 1) rows of TX values
+    static constexpr int TILE = N2 * PL + 2 * PL;
     static constexpr int SLICE = SH::MAXB * SH::R * NT;   // float2 of one staged field
     static __device__ __forceinline__ int sidx(int b, int t) { return (b * SH::R + t) * NT + threadIdx.x; }
 };
@@ -414,6 +423,37 @@ __device__ __forceinline__ void stage_field(float2 *slice, const float *field, c
             if (xa >= g.N0) continue;
             cp_async8(slice + Z::sidx(b, t), field + xa + (long long)g.N0 * (y + (long long)g.N1 * z));
         }
+}
+
+// Prefetch of one z-tile's input half spectrum: rows kz = 0 .. N2/2 of the
+// TX columns x0 .. x0+TX-1 at this y, into raw[kz * TX + x - x0], with
+// 16-byte cp.async (two complex values; N0 is even on this path).  Issued
+// while the previous component is processed, so the next inverse transform
+// reads its inputs from shared memory.
+template <int N2, int PL>
+__device__ __forceinline__ void zraw_prefetch(float2 *raw, const float2 *__restrict__ H, const Geom &g, int x0, int y) {
+    constexpr int TX = 2 * PL, CH = TX / 2, ROWS = N2 / 2 + 1;
+    constexpr int NT = ks_threads(N2, PL);
+    for (int q = threadIdx.x; q < ROWS * CH; q += NT) {
+        const int k = q / CH, c = q - k * CH;
+        const int xa = x0 + 2 * c;
+        if (xa >= g.N0) continue;
+        cp_async16(raw + k * TX + 2 * c, H + ((long long)k * g.N1 + y) * g.N0 + xa);
+    }
+}
+// packed C2R input (as zpack_load) from prefetched raw rows
+template <int N2, int PL>
+__device__ __forceinline__ float2 zpack_raw(const float2 *raw, const Geom &g, int x0, int l, int z) {
+    constexpr int TX = 2 * PL, N2h = N2 / 2 + 1;
+    int k = z;
+    bool cj = false;
+    if (z >= N2h) { k = N2 - z; cj = true; }
+    if (x0 + 2 * l >= g.N0) return make_float2(0.f, 0.f);
+    const float4 q = *reinterpret_cast<const float4 *>(raw + k * TX + 2 * l);
+    float2 A = make_float2(q.x, q.y), B = make_float2(q.z, q.w);
+    if (cj) { A.y = -A.y; B.y = -B.y; }
+    if (k == 0 || 2 * k == N2) { A.y = 0.f; B.y = 0.f; }
+    return make_float2(A.x - B.y, A.y + B.x);
 }
 
 // ---------------------------------------------------------------------------
@@ -534,6 +574,7 @@ __global__ void __launch_bounds__(ks_threads(N2, PL), 2 * kThreads / ks_threads(
     const int D = a.D;
     if (a.nonlinear) stage_field<N2, PL>(s_c, a.srho, g, x0, y);
     stage_field<N2, PL>(s_a, a.rho[0], g, x0, y);
+    zraw_prefetch<N2, PL>(sm, a.spec.p[0], g, x0, y);
     cp_async_commit();
     float dscale = 0.f;
     const bool dense = dense_active(a.dense, t, dscale);
@@ -547,13 +588,22 @@ __global__ void __launch_bounds__(ks_threads(N2, PL), 2 * kThreads / ks_threads(
             acc_d[b][tt] = make_float2(0.f, 0.f);
         }
 #pragma unroll 1
+    // commit groups, oldest first: {srho, rho_0, rows_0}, then per component
+    // {rows_i+1} before its physics and {rho_i+1} after it
     for (int i = 0; i < D; ++i) {
         float2 hold[SH::MAXB][SH::R];
-        const float2 *H = a.spec.p[i];
-        auto ld = [&](int, int, int l, int z) -> float2 { return zpack_load<N2>(H, g, x0, y, l, z); };
+        if (i == 0) cp_async_wait_all();
+        else cp_async_wait_group<1>();   // rows_i landed; rho_i may be in flight
+        __syncthreads();                 // the prefetched rows of every thread are in the tile
+        auto ld = [&](int, int, int l, int z) -> float2 { return zpack_raw<N2, PL>(sm, g, x0, l, z); };
         auto st = [&](int b, int tt, int, int, float2 v) { hold[b][tt] = v; };
         rs_fft<N2, PL, true, true, 0, NT>(sm, tw, ld, st);
-        cp_async_wait_all();
+        cp_async_wait_all();             // staged rho_i (this thread's own slots)
+        if (i + 1 < D) {
+            __syncthreads();   // every thread has read the tile
+            zraw_prefetch<N2, PL>(sm, a.spec.p[i + 1], g, x0, y);
+            cp_async_commit();
+        }
         const int ax = a.comp_axis[i];
         const float *pmlv = a.pml[ax];
         const float pml_y = ax == 1 ? __ldg(pmlv + y) : 1.f;
@@ -717,28 +767,50 @@ __global__ void __launch_bounds__(ks_threads(N2, PL), 2 * kThreads / ks_threads(
     constexpr int TX = Z::TX, NT = Z::NT;
     extern __shared__ float2 dsm[];
     float2 *sm = dsm;
-    float2 *s_p = dsm + Z::TILE;
+    float2 *s_w[2] = {dsm + Z::TILE, dsm + Z::TILE + Z::SLICE};
     const Geom &g = a.g;
     const int x0 = blockIdx.x * TX, y = blockIdx.y;
     const int t = *a.d_t;
-    stage_field<N2, PL>(s_p, a.p, g, x0, y);
+    // the terms' spectra are spec[0 .. nterm-1]; term k's per-cell weight
+    // (c0^2 tau or c0^2 eta) is staged into slice k at the start, its rows
+    // are prefetched into the tile while term k-1 is applied, and p is staged
+    // into the slice that is free first
+    int terms[2], nterm = 0;
+    if (a.has_tau) terms[nterm++] = 0;
+    if (a.has_eta) terms[nterm++] = 1;
+    Med wk[2];
+    for (int k = 0; k < nterm; ++k) {
+        wk[k] = terms[k] == 0 ? a.c2tau : a.c2eta;
+        if (wk[k].arr) stage_field<N2, PL>(s_w[k], wk[k].arr, g, x0, y);
+    }
+    float2 *s_p = nterm == 2 ? s_w[0] : s_w[1];
+    if (nterm < 2) stage_field<N2, PL>(s_p, a.p, g, x0, y);
+    if (nterm > 0) zraw_prefetch<N2, PL>(sm, a.spec.p[0], g, x0, y);
     cp_async_commit();
     float2 acc[SH::MAXB][SH::R];
 #pragma unroll
     for (int b = 0; b < SH::MAXB; ++b)
 #pragma unroll
         for (int tt = 0; tt < SH::R; ++tt) acc[b][tt] = make_float2(0.f, 0.f);
-    int in = 0;
+    // commit groups, oldest first: {weights, p (one term), rows_0},
+    // {rows_1}, {p (two terms)}
 #pragma unroll 1
-    for (int term = 0; term < 2; ++term) {
-        if (term == 0 && !a.has_tau) continue;
-        if (term == 1 && !a.has_eta) continue;
+    for (int k = 0; k < nterm; ++k) {
+        const int term = terms[k];
         float2 hold[SH::MAXB][SH::R];
-        const float2 *H = a.spec.p[in++];
-        auto ld = [&](int, int, int l, int z) -> float2 { return zpack_load<N2>(H, g, x0, y, l, z); };
+        if (k == 0) cp_async_wait_all();
+        else cp_async_wait_group<1>();   // rows_1 landed; p may be in flight
+        __syncthreads();                 // the prefetched rows of every thread are in the tile
+        auto ld = [&](int, int, int l, int z) -> float2 { return zpack_raw<N2, PL>(sm, g, x0, l, z); };
         auto st = [&](int b, int tt, int, int, float2 v) { hold[b][tt] = v; };
         rs_fft<N2, PL, true, true, 0, NT>(sm, tw, ld, st);
-        const Med w = term == 0 ? a.c2tau : a.c2eta;
+        if (k + 1 < nterm) {
+            __syncthreads();   // every thread has read the tile
+            zraw_prefetch<N2, PL>(sm, a.spec.p[k + 1], g, x0, y);
+            cp_async_commit();
+        }
+        const Med w = wk[k];
+        const float2 *sw = s_w[k];
         const float sg = term == 0 ? 1.f : -1.f;
 #pragma unroll
         for (int b = 0; b < SH::MAXB; ++b)
@@ -748,11 +820,15 @@ __global__ void __launch_bounds__(ks_threads(N2, PL), 2 * kThreads / ks_threads(
                 if (!hand_pos<N2, PL, true, NT>(b, tt, l, z)) continue;
                 const int xa = x0 + 2 * l;
                 if (xa >= g.N0) continue;
-                const long long gi = xa + (long long)g.N0 * (y + (long long)g.N1 * z);
-                const float2 wv = med2(w, gi, true, true);
+                const float2 wv = w.arr ? sw[Z::sidx(b, tt)] : make_float2(w.val, w.val);
                 acc[b][tt].x = fmaf(sg * wv.x, hold[b][tt].x, acc[b][tt].x);
                 acc[b][tt].y = fmaf(sg * wv.y, hold[b][tt].y, acc[b][tt].y);
             }
+        if (k == 0 && nterm == 2) {
+            // slice 0's weights are consumed (this thread's own slots): p goes there
+            stage_field<N2, PL>(s_p, a.p, g, x0, y);
+            cp_async_commit();
+        }
     }
     cp_async_wait_all();
 #pragma unroll

@@ -596,7 +596,7 @@ template <int N> struct PLaunch {
     template <int PL>
     static kw_status go(kw_plan *P, const StageP &a, dim3 grid) {
         using Z = ZStage<N, PL>;
-        const size_t sh = (size_t)(Z::TILE + Z::SLICE) * sizeof(float2);
+        const size_t sh = (size_t)(Z::TILE + 2 * Z::SLICE) * sizeof(float2);
         KW_TRY(set_smem((const void *)ks_stage_p<N, PL>, sh));
         ks_stage_p<N, PL><<<grid, Z::NT, sh, P->stream>>>(a, P->tw[2]);
         return KW_OK;
