@@ -467,7 +467,7 @@ struct StageR {
     Spec4 spec;
     float *rho[3];            // values before this step's update
     float *rho_out[3];        // updated values (double-buffered)
-    float *srho;              // sum of rho over components: read (old), rewritten (new)
+    float *srho;              // nonlinear mass coefficient q = 2 sum(rho) + rho0: read (old), rewritten (new)
     float *p;
     Med rho0, c0, BonA;
     Med c2tau;                // c0^2 * absorb_tau (stokes equation of state)
@@ -486,7 +486,7 @@ struct StageR {
 
 __device__ __forceinline__ void apply_tr(float2 *sm, const TRSrc &tr, const Geom &g, int PL, int x0, int y, int t,
                                          float *rho0_, float *rho1_, float *rho2_, int D, const Med &c0, float *p,
-                                         float *srho) {
+                                         float *qnl, const Med &rho0m) {
     // Dirichlet overwrite of p on the mask with the flipped data for step t+1
     // (kspaceFirstOrder3D.m:772-788; 2D :715-729) and the matching rho.
     if (!tr.off) return;
@@ -508,6 +508,7 @@ __device__ __forceinline__ void apply_tr(float2 *sm, const TRSrc &tr, const Geom
         rho0_[gi] = r;
         rho1_[gi] = r;
         if (D == 3) rho2_[gi] = r;
+        if (qnl) qnl[gi] = fmaf(2.f * (float)D, r, rho0m.arr ? __ldg(rho0m.arr + gi) : rho0m.val);
     }
 }
 
@@ -639,7 +640,10 @@ __global__ void __launch_bounds__(kThreads, 2) k_stage_r(StageR a) {
                 pv.y += ct.y * r0.y * sd.y;
             }
             st2(a.p, gi, pv, two, g.vec2);
-            if (a.srho) st2(a.srho, gi, sr, two, g.vec2);
+            if (a.srho && a.nonlinear) {
+                const float2 r0 = med2(a.rho0, gi, two, g.vec2);
+                st2(a.srho, gi, make_float2(fmaf(2.f, sr.x, r0.x), fmaf(2.f, sr.y, r0.y)), two, g.vec2);
+            }
             if (absorbing && a.has_tau) {
                 const float2 r0 = med2(a.rho0, gi, two, g.vec2);
                 const float2 sd = acc_du[idx];
@@ -651,7 +655,8 @@ __global__ void __launch_bounds__(kThreads, 2) k_stage_r(StageR a) {
     }
     __syncthreads();
     if (!absorbing) {
-        apply_tr(tile, a.tr, g, PL, x0, y, t, a.rho_out[0], a.rho_out[1], a.rho_out[2], a.D, a.c0, a.p, a.srho);
+        apply_tr(tile, a.tr, g, PL, x0, y, t, a.rho_out[0], a.rho_out[1], a.rho_out[2], a.D, a.c0, a.p,
+                 a.nonlinear ? a.srho : nullptr, a.rho0);
         __syncthreads();
         if (a.write_spec) {
             tile_fft_il<N2S, PLS, false>(tile, a.axz, PL);
@@ -693,8 +698,8 @@ struct StageP {
     Spec4 spec;
     float *p;
     float *rho[3];
-    float *srho;
-    Med c0;
+    float *srho;              // nonlinear mass coefficient q (time-reversal overwrite)
+    Med c0, rho0;
     Med c2tau, c2eta;         // c0^2 * absorb_tau, c0^2 * absorb_eta
     int has_tau, has_eta;
     TRSrc tr;
@@ -755,7 +760,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_stage_p(StageP a) {
         tile[idx] = pv;
     }
     __syncthreads();
-    apply_tr(tile, a.tr, g, PL, x0, y, t, a.rho[0], a.rho[1], a.rho[2], a.D, a.c0, a.p, a.srho);
+    apply_tr(tile, a.tr, g, PL, x0, y, t, a.rho[0], a.rho[1], a.rho[2], a.D, a.c0, a.p, a.srho, a.rho0);
     __syncthreads();
     if (a.write_spec) {
         tile_fft_il<N2S, PLS, false>(tile, a.axz, PL);
@@ -884,8 +889,9 @@ __global__ void k_rms_finish(float *sq, int M, float inv_n) {
     if (m < M) sq[m] = sqrtf(sq[m] * inv_n);
 }
 
-// rho_i = p0 / (D c0^2) on every cell (kspaceFirstOrder3D.m:1027-1030)
-__global__ void k_init_rho(const float *__restrict__ p0, Med c0, float *r0, float *r1, float *r2, float *srho,
+// rho_i = p0 / (D c0^2) on every cell (kspaceFirstOrder3D.m:1027-1030);
+// q = 2 sum(rho) + rho0 for the nonlinear mass update
+__global__ void k_init_rho(const float *__restrict__ p0, Med c0, Med rho0, float *r0, float *r1, float *r2, float *srho,
                            long long N, int D) {
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < N; i += (long long)gridDim.x * blockDim.x) {
         const float c = c0.arr ? c0.arr[i] : c0.val;
@@ -893,13 +899,13 @@ __global__ void k_init_rho(const float *__restrict__ p0, Med c0, float *r0, floa
         r0[i] = v;
         r1[i] = v;
         if (D == 3) r2[i] = v;
-        srho[i] = (float)D * v;
+        srho[i] = fmaf(2.f * (float)D, v, rho0.arr ? rho0.arr[i] : rho0.val);
     }
 }
 
 // time-reversal start: p(mask) = data(:, flipped column 1), rho(mask) = p/(D c0^2)
-__global__ void k_tr_start(const long long *idx, int M, const float *data, int Nt, Med c0, float *p, float *r0,
-                           float *r1, float *r2, float *srho, int D) {
+__global__ void k_tr_start(const long long *idx, int M, const float *data, int Nt, Med c0, Med rho0, float *p,
+                           float *r0, float *r1, float *r2, float *srho, int D) {
     const int m = blockIdx.x * blockDim.x + threadIdx.x;
     if (m >= M) return;
     const long long gi = idx[m];
@@ -910,7 +916,7 @@ __global__ void k_tr_start(const long long *idx, int M, const float *data, int N
     r0[gi] = r;
     r1[gi] = r;
     if (D == 3) r2[gi] = r;
-    srho[gi] = (float)D * r;
+    srho[gi] = fmaf(2.f * (float)D, r, rho0.arr ? rho0.arr[gi] : rho0.val);
 }
 
 // final time-reversal assignment p(mask) = data(:, flipped column Nt) (:1211-1213)
@@ -935,6 +941,12 @@ __global__ void k_set_points(const long long *pos, int npts, float v, float *fie
 }
 
 __global__ void k_step_advance(int *d_t) { *d_t += 1; }
+
+// dst[i] = m (array or scalar)
+__global__ void k_fill_med(float *dst, Med m, long long N) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < N; i += (long long)gridDim.x * blockDim.x)
+        dst[i] = m.arr ? m.arr[i] : m.val;
+}
 
 // ---------------------------------------------------------------------------
 // set-up kernels (run once per plan)

@@ -566,18 +566,32 @@ __global__ void __launch_bounds__(ks_threads(N2, PL), 2 * kThreads / ks_threads(
     constexpr int TX = Z::TX, NT = Z::NT;
     extern __shared__ float2 dsm[];
     float2 *sm = dsm;
-    float2 *s_c = dsm + Z::TILE;        // staged sum(rho_old) (nonlinear)
+    float2 *s_c = dsm + Z::TILE;        // staged mass coefficient (q or rho0)
     float2 *s_a = s_c + Z::SLICE;       // staged rho_old of the current component
     const Geom &g = a.g;
     const int x0 = blockIdx.x * TX, y = blockIdx.y;
     const int t = *a.d_t;
     const int D = a.D;
+    const bool r0arr = a.rho0.arr != nullptr;
+    // mass coefficient: q = 2 sum(rho_old) + rho0, carried between steps
+    // (nonlinear), or rho0 (linear)
     if (a.nonlinear) stage_field<N2, PL>(s_c, a.srho, g, x0, y);
+    else if (r0arr) stage_field<N2, PL>(s_c, a.rho0.arr, g, x0, y);
     stage_field<N2, PL>(s_a, a.rho[0], g, x0, y);
     zraw_prefetch<N2, PL>(sm, a.spec.p[0], g, x0, y);
     cp_async_commit();
     float dscale = 0.f;
     const bool dense = dense_active(a.dense, t, dscale);
+    int e0 = 0, e1 = 0;
+    if (a.sparse.off && t <= a.sparse.T[0]) {
+        const int tile = blockIdx.x + gridDim.x * blockIdx.y;
+        e0 = a.sparse.off[tile];
+        e1 = a.sparse.off[tile + 1];
+    }
+    // nonlinear: rho0 for the equation of state is staged into the free
+    // transform tile after the last inverse transform (unless a sparse source
+    // needs the tile first)
+    const bool r0_tile = Z::SLICE <= Z::TILE && a.nonlinear && r0arr && e1 <= e0;
 
     float2 acc_r[SH::MAXB][SH::R], acc_d[SH::MAXB][SH::R];
 #pragma unroll
@@ -603,6 +617,10 @@ __global__ void __launch_bounds__(ks_threads(N2, PL), 2 * kThreads / ks_threads(
             __syncthreads();   // every thread has read the tile
             zraw_prefetch<N2, PL>(sm, a.spec.p[i + 1], g, x0, y);
             cp_async_commit();
+        } else if (r0_tile) {
+            __syncthreads();   // every thread has read the tile
+            stage_field<N2, PL>(sm, a.rho0.arr, g, x0, y);
+            cp_async_commit();
         }
         const int ax = a.comp_axis[i];
         const float *pmlv = a.pml[ax];
@@ -620,12 +638,7 @@ __global__ void __launch_bounds__(ks_threads(N2, PL), 2 * kThreads / ks_threads(
                 const int si = Z::sidx(b, tt);
                 const float2 du = hold[b][tt];
                 const float2 ro = s_a[si];
-                float2 coef = med2(a.rho0, gi, true, true);
-                if (a.nonlinear) {
-                    const float2 so = s_c[si];
-                    coef.x = fmaf(2.f, so.x, coef.x);
-                    coef.y = fmaf(2.f, so.y, coef.y);
-                }
+                const float2 coef = (a.nonlinear || r0arr) ? s_c[si] : make_float2(a.rho0.val, a.rho0.val);
                 float2 pm;
                 if (ax == 0) pm = make_float2(__ldg(pmlv + xa), __ldg(pmlv + xa + 1));
                 else if (ax == 1) pm = make_float2(pml_y, pml_y);
@@ -652,9 +665,7 @@ __global__ void __launch_bounds__(ks_threads(N2, PL), 2 * kThreads / ks_threads(
         }
     }
     // sparse pressure sources act on every rho component (:930-962)
-    if (a.sparse.off && t <= a.sparse.T[0]) {
-        const int tile = blockIdx.x + gridDim.x * blockIdx.y;
-        const int e0 = a.sparse.off[tile], e1 = a.sparse.off[tile + 1];
+    {
         if (e1 > e0) {
             __syncthreads();
             hold_to_smem<N2, PL>(sm, acc_r);
@@ -679,6 +690,12 @@ __global__ void __launch_bounds__(ks_threads(N2, PL), 2 * kThreads / ks_threads(
     // equation of state (c0^2 applied to the non-spectral terms here; the
     // absorbing terms are finished in Stage P)
     const bool absorbing = a.eos == 1;
+    if (r0_tile) cp_async_wait_all();
+    auto r0_at = [&](int si, long long gi) -> float2 {
+        if (r0_tile) return sm[si];
+        if (!a.nonlinear && r0arr) return s_c[si];
+        return med2(a.rho0, gi, true, true);
+    };
 #pragma unroll
     for (int b = 0; b < SH::MAXB; ++b)
 #pragma unroll
@@ -690,11 +707,14 @@ __global__ void __launch_bounds__(ks_threads(N2, PL), 2 * kThreads / ks_threads(
             float2 rd = make_float2(0.f, 0.f);
             if (xa < g.N0) {
                 const long long gi = xa + (long long)g.N0 * (y + (long long)g.N1 * z);
+                const int si = Z::sidx(b, tt);
                 const float2 sr = acc_r[b][tt];
                 const float2 c = med2(a.c0, gi, true, true);
                 pv = sr;
                 if (a.nonlinear) {
-                    const float2 r0 = med2(a.rho0, gi, true, true);
+                    const float2 r0 = r0_at(si, gi);
+                    // next step's mass coefficient q = 2 sum(rho) + rho0
+                    *reinterpret_cast<float2 *>(a.srho + gi) = make_float2(fmaf(2.f, sr.x, r0.x), fmaf(2.f, sr.y, r0.y));
                     const float2 bn = med2(a.BonA, gi, true, true);
                     pv.x += bn.x * sr.x * sr.x / (2.f * r0.x);
                     pv.y += bn.y * sr.y * sr.y / (2.f * r0.y);
@@ -702,7 +722,7 @@ __global__ void __launch_bounds__(ks_threads(N2, PL), 2 * kThreads / ks_threads(
                 pv.x *= c.x * c.x;
                 pv.y *= c.y * c.y;
                 if (a.eos == 2 || (absorbing && a.has_tau)) {
-                    const float2 r0 = med2(a.rho0, gi, true, true);
+                    const float2 r0 = r0_at(si, gi);
                     const float2 sd = acc_d[b][tt];
                     rd = make_float2(r0.x * sd.x, r0.y * sd.y);
                 }
@@ -717,25 +737,13 @@ __global__ void __launch_bounds__(ks_threads(N2, PL), 2 * kThreads / ks_threads(
             }
             acc_d[b][tt] = absorbing ? rd : pv;   // next forward input
         }
-    if (a.nonlinear && a.srho) {
-        // sum of the new rho for the next step's nonlinear coefficient
-#pragma unroll
-        for (int b = 0; b < SH::MAXB; ++b)
-#pragma unroll
-            for (int tt = 0; tt < SH::R; ++tt) {
-                int l, z;
-                if (!hand_pos<N2, PL, true, NT>(b, tt, l, z)) continue;
-                const int xa = x0 + 2 * l;
-                if (xa >= g.N0) continue;
-                *reinterpret_cast<float2 *>(a.srho + xa + (long long)g.N0 * (y + (long long)g.N1 * z)) = acc_r[b][tt];
-            }
-    }
     if (!absorbing) {
         if (a.tr.off) {
             __syncthreads();
             hold_to_smem<N2, PL>(sm, acc_d);
             __syncthreads();
-            apply_tr(sm, a.tr, g, PL, x0, y, t, a.rho_out[0], a.rho_out[1], a.rho_out[2], D, a.c0, a.p, a.srho);
+            apply_tr(sm, a.tr, g, PL, x0, y, t, a.rho_out[0], a.rho_out[1], a.rho_out[2], D, a.c0, a.p,
+                     a.nonlinear ? a.srho : nullptr, a.rho0);
             __syncthreads();
             smem_to_hold<N2, PL>(sm, acc_d);
         }
@@ -852,7 +860,7 @@ __global__ void __launch_bounds__(ks_threads(N2, PL), 2 * kThreads / ks_threads(
         __syncthreads();
         hold_to_smem<N2, PL>(sm, acc);
         __syncthreads();
-        apply_tr(sm, a.tr, g, PL, x0, y, t, a.rho[0], a.rho[1], a.rho[2], a.D, a.c0, a.p, a.srho);
+        apply_tr(sm, a.tr, g, PL, x0, y, t, a.rho[0], a.rho[1], a.rho[2], a.D, a.c0, a.p, a.srho, a.rho0);
         __syncthreads();
         smem_to_hold<N2, PL>(sm, acc);
     }

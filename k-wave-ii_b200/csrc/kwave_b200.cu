@@ -152,7 +152,7 @@ struct kw_plan {
     float *p = nullptr, *rho[3] = {nullptr, nullptr, nullptr}, *u[3] = {nullptr, nullptr, nullptr};
     float *rho_b[3] = {nullptr, nullptr, nullptr};   // second rho buffer (Stage R writes it, then they swap)
     float *u_b[3] = {nullptr, nullptr, nullptr};     // second velocity buffer (Stage U writes it, then they swap)
-    float *srho = nullptr;                           // sum of rho over components
+    float *srho = nullptr;                           // nonlinear mass coefficient q = 2 sum(rho) + rho0
     float2 *spec[4] = {nullptr, nullptr, nullptr, nullptr};
     float *p0_dev = nullptr;
     int *d_t = nullptr;
@@ -690,6 +690,7 @@ kw_status stage_p(kw_plan *P, int write_spec) {
     a.p = P->p;
     a.srho = P->srho;
     a.c0 = P->c0;
+    a.rho0 = P->rho0;
     a.c2tau = P->c2tau;
     a.c2eta = P->c2eta;
     a.has_tau = P->has_tau;
@@ -756,7 +757,9 @@ kw_status sensors(kw_plan *P, int t) {
 kw_status zero_state(kw_plan *P) {
     const size_t N = (size_t)P->g.N, Nh = (size_t)P->g.Nh;
     KW_CUDA(cudaMemsetAsync(P->p, 0, N * sizeof(float), P->stream));
-    KW_CUDA(cudaMemsetAsync(P->srho, 0, N * sizeof(float), P->stream));
+    // nonlinear mass coefficient q = 2 sum(rho) + rho0 of the zero state
+    k_fill_med<<<(unsigned)std::min<size_t>((N + 255) / 256, 148 * 16), 256, 0, P->stream>>>(P->srho, P->rho0, (long long)N);
+    KW_TRY(launched(P));
     for (int i = 0; i < P->D; ++i) {
         KW_CUDA(cudaMemsetAsync(P->rho[i], 0, N * sizeof(float), P->stream));
         KW_CUDA(cudaMemsetAsync(P->u[i], 0, N * sizeof(float), P->stream));
@@ -773,7 +776,7 @@ kw_status zero_state(kw_plan *P) {
 kw_status start(kw_plan *P) {
     if (P->time_rev) {
         // kspaceFirstOrder3D.m:772-788 at t = 1
-        k_tr_start<<<(P->M + 255) / 256, 256, 0, P->stream>>>(P->sidx, P->M, P->tr_data, P->Nt, P->c0, P->p,
+        k_tr_start<<<(P->M + 255) / 256, 256, 0, P->stream>>>(P->sidx, P->M, P->tr_data, P->Nt, P->c0, P->rho0, P->p,
                                                               P->rho[0], P->rho[1], P->rho[2], P->srho, P->D);
         KW_TRY(launched(P));
         KW_TRY(zr2c(P, P->p, P->spec[0]));
@@ -791,7 +794,8 @@ kw_status run_step(kw_plan *P) {
         // p0 initial condition (kspaceFirstOrder3D.m:1023-1040): the first
         // step's update is overwritten, so the state is set directly.
         KW_CUDA(cudaMemcpyAsync(P->p, P->p0_dev, (size_t)P->g.N * sizeof(float), cudaMemcpyDeviceToDevice, P->stream));
-        k_init_rho<<<1024, 256, 0, P->stream>>>(P->p0_dev, P->c0, P->rho[0], P->rho[1], P->rho[2], P->srho, P->g.N, P->D);
+        k_init_rho<<<1024, 256, 0, P->stream>>>(P->p0_dev, P->c0, P->rho0, P->rho[0], P->rho[1], P->rho[2], P->srho,
+                                                P->g.N, P->D);
         KW_TRY(launched(P));
         KW_TRY(zr2c(P, P->p, P->spec[0]));
         KW_TRY(grad_group(P));
