@@ -64,11 +64,16 @@ __device__ __forceinline__ void st2(float *p, long long gi, float2 v, bool two, 
 }
 
 // ---- spectral operators ----------------------------------------------------
-enum OpKind { OP_GRAD_POS = 0, OP_GRAD_NEG = 1, OP_NABLA1 = 2, OP_NABLA2 = 3, OP_SRC_KAPPA = 4, OP_IDENT = 5 };
+// OP_SHIFT_NEG: exp(-i k d / 2) along one axis, no kappa -- the shift of a
+// staggered velocity component onto the regular grid
+enum OpKind {
+    OP_GRAD_POS = 0, OP_GRAD_NEG = 1, OP_NABLA1 = 2, OP_NABLA2 = 3, OP_SRC_KAPPA = 4, OP_IDENT = 5, OP_SHIFT_NEG = 6
+};
 
 struct OpParams {
     const float2 *dd_pos[3];   // i k exp(+i k d/2) per axis, FFT order, Hermitian part
     const float2 *dd_neg[3];   // i k exp(-i k d/2)
+    const float2 *sh_neg[3];   // exp(-i k d/2) (1 without staggering), Hermitian part
     const float *k2[3];        // k_i^2 per axis, FFT order
     float kappa_a;             // c_ref * dt / 2
     int use_kspace;
@@ -102,6 +107,10 @@ __device__ __forceinline__ float2 eval_op(const OpParams &P, int kind, int axis,
             const int i = axis == 0 ? ix : (axis == 1 ? iy : iz);
             const float2 d = __ldg((kind == OP_GRAD_POS ? P.dd_pos[axis] : P.dd_neg[axis]) + i);
             return cscale(d, kap * P.scale);
+        }
+        case OP_SHIFT_NEG: {
+            const int i = axis == 0 ? ix : (axis == 1 ? iy : iz);
+            return cscale(__ldg(P.sh_neg[axis] + i), P.scale);
         }
         case OP_NABLA1: return make_float2(pow_k(km, P.nabla1_exp) * P.scale, 0.f);
         case OP_NABLA2: return make_float2(pow_k(km, P.nabla2_exp) * P.scale, 0.f);
@@ -941,6 +950,14 @@ __global__ void k_set_points(const long long *pos, int npts, float v, float *fie
 }
 
 __global__ void k_step_advance(int *d_t) { *d_t += 1; }
+
+// series[m + M (t - record_start)] = src[idx[m]], t from the device step counter
+__global__ void k_gather_series(const float *__restrict__ src, const long long *__restrict__ idx, int M, float *series,
+                                const int *d_t, int record_start) {
+    const int m = blockIdx.x * blockDim.x + threadIdx.x;
+    if (m >= M) return;
+    series[m + (long long)M * (*d_t - record_start)] = src[idx[m]];
+}
 
 // dst[i] = m (array or scalar)
 __global__ void k_fill_med(float *dst, Med m, long long N) {

@@ -273,8 +273,9 @@ __global__ void __launch_bounds__(ks_threads(N0, NL), 3 * kThreads / ks_threads(
     for (int o = 0; o < nout; ++o) {
         const int oi = fanout ? o : f;
         const int axis = ops.axis[oi];
-        const float2 *dd = ops.kind[oi] == OP_GRAD_POS ? P.dd_pos[axis] : P.dd_neg[axis];
-        const bool mul_dd = ops.kind[oi] == OP_GRAD_POS || ops.kind[oi] == OP_GRAD_NEG;
+        const int ko = ops.kind[oi];
+        const float2 *dd = ko == OP_GRAD_POS ? P.dd_pos[axis] : (ko == OP_GRAD_NEG ? P.dd_neg[axis] : P.sh_neg[axis]);
+        const bool mul_dd = ko == OP_GRAD_POS || ko == OP_GRAD_NEG || ko == OP_SHIFT_NEG;
         float2 *out = bufs.p[oi] + (long long)line0 * N0;
         auto ld2 = [&](int b, int t, int l, int i) -> float2 {
             if (!mul_dd) return spec[b][t];

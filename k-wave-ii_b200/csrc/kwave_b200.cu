@@ -144,6 +144,7 @@ struct kw_plan {
     AxisFFT fft[3]{};
     float2 *tw[3] = {nullptr, nullptr, nullptr};
     float2 *dd_pos[3] = {nullptr, nullptr, nullptr}, *dd_neg[3] = {nullptr, nullptr, nullptr};
+    float2 *sh_neg[3] = {nullptr, nullptr, nullptr};
     float *k2[3] = {nullptr, nullptr, nullptr};
     float *pml[3] = {nullptr, nullptr, nullptr}, *pml_sg[3] = {nullptr, nullptr, nullptr};
     OpParams op{};
@@ -182,6 +183,8 @@ struct kw_plan {
     float *o_sq[4] = {nullptr, nullptr, nullptr, nullptr};
     float *o_amax[4] = {nullptr, nullptr, nullptr, nullptr}, *o_amin[4] = {nullptr, nullptr, nullptr, nullptr};
     float *o_tmp = nullptr;        // crop / rms staging
+    float *o_uns[3] = {nullptr, nullptr, nullptr};   // u_non_staggered series
+    float *ush = nullptr;          // one unstaggered velocity component
     int in_lo[3] = {0, 0, 0}, in_n[3] = {1, 1, 1};
     long long in_count = 1;
 
@@ -726,6 +729,30 @@ kw_status sensors(kw_plan *P, int t) {
             k_sensor<<<(P->M + 255) / 256, 256, 0, P->stream>>>(a);
             KW_TRY(launched(P));
         }
+        if (P->o_uns[0]) {
+            // velocity on the regular grid: real(ifft(shift_neg_i fft(u_i)))
+            // along the component's own axis (extractSensorData.m:41-57),
+            // applied as a spectral operator that depends on k_i only
+            for (int i = 0; i < P->D; ++i) {
+                const float *src = P->u[i];
+                if (P->prob.use_sg) {
+                    KW_TRY(zr2c(P, P->u[i], P->spec[3]));
+                    Spec4 b{};
+                    b.p[0] = P->spec[3];
+                    OpSet ops{};
+                    ops.n = 1;
+                    ops.kind[0] = OP_SHIFT_NEG;
+                    ops.axis[0] = P->comp_axis[i];
+                    KW_TRY(yxy_group(P, b, 1, ops, false));
+                    KW_TRY(zc2r(P, P->spec[3], P->ush));
+                    src = P->ush;
+                }
+                Scope s(P, KW_KCLASS_SENSOR);
+                k_gather_series<<<(P->M + 255) / 256, 256, 0, P->stream>>>(src, P->sidx, P->M, P->o_uns[i], P->d_t,
+                                                                          P->record_start);
+                KW_TRY(launched(P));
+            }
+        }
     }
     bool any_all = false;
     for (int f = 0; f < 4; ++f) any_all = any_all || P->o_amax[f] || P->o_amin[f];
@@ -1091,7 +1118,7 @@ kw_status create(const kw_problem *pr, kw_plan *P) {
         KW_TRY(pupload(P, &P->tw[a], tw.data(), tw.size()));
         f.tw = P->tw[a];
 
-        std::vector<float2> dp(n), dn(n);
+        std::vector<float2> dp(n), dn(n), sn(n, make_float2(1.f, 0.f));
         std::vector<float> k2(n);
         std::vector<float> pml(n, 1.f), pmlsg(n, 1.f);
         if (phys_of_int[a] >= 0) {
@@ -1117,6 +1144,13 @@ kw_status create(const kw_problem *pr, kw_plan *P) {
                 const std::complex<double> hn = 0.5 * (cn[i] + std::conj(cn[j]));
                 dp[i] = make_float2((float)hp.real(), (float)hp.imag());
                 dn[i] = make_float2((float)hn.real(), (float)hn.imag());
+                if (q.use_sg) {
+                    // record.x_shift_neg (createStorageVariables.m:89-114)
+                    const std::complex<double> si = std::exp(std::complex<double>(0.0, -k[i] * P->d[a] / 2));
+                    const std::complex<double> sj = std::exp(std::complex<double>(0.0, -k[j] * P->d[a] / 2));
+                    const std::complex<double> hs = 0.5 * (si + std::conj(sj));
+                    sn[i] = make_float2((float)hs.real(), (float)hs.imag());
+                }
             }
             const std::vector<double> pr1 = get_pml(n, P->d[a], q.dt, q.c_ref, (int)pmls[pa], pmla[pa], false);
             const std::vector<double> pr2 = get_pml(n, P->d[a], q.dt, q.c_ref, (int)pmls[pa], pmla[pa], q.use_sg != 0);
@@ -1126,11 +1160,13 @@ kw_status create(const kw_problem *pr, kw_plan *P) {
         }
         KW_TRY(pupload(P, &P->dd_pos[a], dp.data(), dp.size()));
         KW_TRY(pupload(P, &P->dd_neg[a], dn.data(), dn.size()));
+        KW_TRY(pupload(P, &P->sh_neg[a], sn.data(), sn.size()));
         KW_TRY(pupload(P, &P->k2[a], k2.data(), k2.size()));
         KW_TRY(pupload(P, &P->pml[a], pml.data(), pml.size()));
         KW_TRY(pupload(P, &P->pml_sg[a], pmlsg.data(), pmlsg.size()));
         P->op.dd_pos[a] = P->dd_pos[a];
         P->op.dd_neg[a] = P->dd_neg[a];
+        P->op.sh_neg[a] = P->sh_neg[a];
         P->op.k2[a] = P->k2[a];
     }
     P->op.kappa_a = (float)(q.c_ref * q.dt / 2.0);
@@ -1330,7 +1366,10 @@ kw_status create(const kw_problem *pr, kw_plan *P) {
             if (P->rec & KW_REC_U_RMS) KW_TRY(palloc(P, &P->o_sq[1 + i], P->M));
         }
     }
-    if (P->rec & KW_REC_U_NON_STAGGERED) return fail(KW_ERR_UNSUPPORTED, "sensor.record 'u_non_staggered' is not built yet");
+    if ((P->rec & KW_REC_U_NON_STAGGERED) && !tr && P->M > 0) {
+        for (int i = 0; i < P->D; ++i) KW_TRY(palloc(P, &P->o_uns[i], ser));
+        KW_TRY(palloc(P, &P->ush, N));
+    }
     if (!tr) {
         if (P->rec & KW_REC_P_MAX_ALL) KW_TRY(palloc(P, &P->o_amax[0], P->in_count));
         if (P->rec & KW_REC_P_MIN_ALL) KW_TRY(palloc(P, &P->o_amin[0], P->in_count));
@@ -1563,6 +1602,7 @@ kw_status kw_copy_outputs(kw_plan *P, kw_outputs *o) {
         KW_TRY(copy_dev(P, o->u_max_all[i], P->o_amax[1 + i], P->in_count));
         KW_TRY(copy_dev(P, o->u_min_all[i], P->o_amin[1 + i], P->in_count));
         if (P->rec & KW_REC_U_FINAL) KW_TRY(crop_out(P, o->u_final[i], P->u[i]));
+        KW_TRY(copy_dev(P, o->u_non_staggered[i], P->o_uns[i], ser));
     }
     KW_CUDA(cudaStreamSynchronize(P->stream));
     return KW_OK;

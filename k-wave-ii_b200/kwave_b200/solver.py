@@ -224,10 +224,12 @@ def _prepare(dim, kgrid, medium, source, sensor, options):
         record = {"p"}
     if time_rev:
         record = set()
-    for r in ("I", "I_avg", "u_non_staggered"):
-        if r in record:
-            raise KWaveInputError("sensor.record '%s' is not supported by this solver yet." % r)
-    needs_mask = bool(record & {"p", "p_max", "p_min", "p_rms", "u", "u_max", "u_min", "u_rms"})
+    P.record_user = set(record)
+    if record & {"I", "I_avg"}:
+        # intensity is formed after the loop from p and the unstaggered
+        # velocity (createStorageVariables.m:89-148, 309; saveIntensity.m)
+        record |= {"p", "u_non_staggered"}
+    needs_mask = bool(record & {"p", "p_max", "p_min", "p_rms", "u", "u_max", "u_min", "u_rms", "u_non_staggered"})
     blank = use_sensor and not needs_mask and not time_rev
     rsi = _field(sensor, "record_start_index", 1) if use_sensor else 1
     record_start = int(_round(rsi))
@@ -509,7 +511,8 @@ def _prepare(dim, kgrid, medium, source, sensor, options):
     pr.record_start_index = record_start
     bits = 0
     for r in record:
-        bits |= 1 << _abi.REC_BITS[r]
+        if r in _abi.REC_BITS:
+            bits |= 1 << _abi.REC_BITS[r]
     pr.record = bits
     if time_rev:
         trd = np.atleast_2d(np.asarray(_field(sensor, "time_reversal_boundary_data"), dtype=np.float64))
@@ -800,6 +803,8 @@ def _alloc_outputs(prep):
                     buf(n + "_" + k, ins, "u_" + k, i)
             if "u_final" in rec:
                 buf(n + "_final", ins, "u_final", i)
+            if "u_non_staggered" in rec:
+                buf(n + "_non_staggered", (M, T), "u_non_staggered", i)
     if "p_final" in rec or P.time_rev:
         buf("p_final", ins, "p_final")
     return o, host
@@ -810,6 +815,22 @@ def _finish(P, host):
     out = {}
     for k, (a, shape) in host.items():
         out[k] = a.reshape(shape, order="F")
+    user = getattr(P, "record_user", P.record)
+    if not P.time_rev and user & {"I", "I_avg"}:
+        # kspaceFirstOrder_saveIntensity.m: u_non_staggered shifted forward by
+        # dt/2 in time (fourierShift.m), times p; I_avg is its time average
+        for i in range(P.dim):
+            n = ("ux", "uy", "uz")[i]
+            inten = out["p"].astype(np.float64) * _fourier_shift(out[n + "_non_staggered"], 0.5)
+            if "I" in user:
+                out["I" + n[1:]] = inten.astype(np.float32)
+            if "I_avg" in user:
+                out["I" + n[1:] + "_avg"] = inten.mean(axis=-1).astype(np.float32)
+        if "u_non_staggered" not in user:
+            for i in range(P.dim):
+                del out[("ux", "uy", "uz")[i] + "_non_staggered"]
+        if "p" not in user:
+            del out["p"]
     # Cartesian nearest-neighbour reorder (reorderCartData.m)
     if P.reorder_index is not None:
         for k in list(out):
@@ -847,6 +868,20 @@ def _cuboids(P, out):
                 d[k] = v[sel].reshape(size, order="F")
         res.append(d)
     return res
+
+
+def _fourier_shift(data, shift):
+    """fourierShift.m along the last axis: real(ifft(ifftshift(exp(i k shift)) fft(data)))
+    with k = 2 pi (-N/2 .. N/2-1) / N (odd N: -(N-1)/2 .. (N-1)/2) and k at
+    index floor(N/2) set to zero."""
+    data = np.asarray(data, dtype=np.float64)
+    N = data.shape[-1]
+    if N % 2 == 0:
+        k = 2 * np.pi * np.arange(-N // 2, N // 2) / N
+    else:
+        k = 2 * np.pi * np.arange(-(N - 1) // 2, (N - 1) // 2 + 1) / N
+    k[N // 2] = 0.0
+    return np.real(np.fft.ifft(np.fft.ifftshift(np.exp(1j * k * shift)) * np.fft.fft(data, axis=-1), axis=-1))
 
 
 def _find_union(parts):

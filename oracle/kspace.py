@@ -338,6 +338,21 @@ def reorder_binary_sensor_data(data, reorder_index):
     return data[order]
 
 
+def fourier_shift(data, shift):
+    """Shift data along its last axis by `shift` samples with the Fourier
+    interpolant (fourierShift.m): real(ifft(ifftshift(exp(i k shift)) fft(data)))
+    with k = 2 pi (-N/2 .. N/2-1) / N (odd N: -(N-1)/2 .. (N-1)/2), k at
+    index floor(N/2) (0-based) set to zero."""
+    data = np.asarray(data, dtype=np.float64)
+    N = data.shape[-1]
+    if N % 2 == 0:
+        k = 2 * np.pi * np.arange(-N // 2, N // 2) / N
+    else:
+        k = 2 * np.pi * np.arange(-(N - 1) // 2, (N - 1) // 2 + 1) / N
+    k[N // 2] = 0.0
+    return np.real(np.fft.ifft(np.fft.ifftshift(np.exp(1j * k * shift)) * np.fft.fft(data, axis=-1), axis=-1))
+
+
 def tone_burst_hann(sample_freq, signal_freq, num_cycles):
     """A sine tone burst of ``num_cycles`` cycles sampled at ``sample_freq``,
     windowed by getWin(N, 'Hanning') (toneBurst.m:102-180 time axis)."""
@@ -444,6 +459,11 @@ def kspace_first_order(kgrid, medium, source, sensor, **opts):
         record = {"p"}
     if time_rev:
         record = set()
+    rec_user = set(record)
+    if record & {"I", "I_avg"}:
+        # intensity needs the pressure and the unstaggered velocity series
+        # (createStorageVariables.m:89-148, 309)
+        record |= {"p", "u_non_staggered"}
     needs_mask = bool(record & {"p", "p_max", "p_min", "p_rms", "u", "u_non_staggered",
                                 "u_max", "u_min", "u_rms", "I", "I_avg"})
     blank_sensor = use_sensor and not needs_mask and not time_rev
@@ -832,6 +852,22 @@ def kspace_first_order(kgrid, medium, source, sensor, **opts):
     if "u_final" in record:
         for i in range(dim):
             out[u_comps[i] + "_final"] = u[i][ins].copy()
+
+    # intensity (kspaceFirstOrder_saveIntensity.m): u_non_staggered shifted
+    # forward in time by dt/2, times p; I_avg is its time average
+    if use_sensor and not time_rev and rec_user & {"I", "I_avg"}:
+        for i in range(dim):
+            n = u_comps[i]
+            inten = out["p"] * fourier_shift(out[n + "_non_staggered"], 0.5)
+            if "I" in rec_user:
+                out["I" + n[1:]] = inten
+            if "I_avg" in rec_user:
+                out["I" + n[1:] + "_avg"] = inten.mean(axis=-1)
+        if "u_non_staggered" not in rec_user:
+            for i in range(dim):
+                del out[u_comps[i] + "_non_staggered"]
+        if "p" not in rec_user:
+            del out["p"]
 
     # Cartesian nearest-neighbour reorder (reorderCartData.m)
     if reorder_index is not None and not time_rev:

@@ -148,12 +148,29 @@ def make_case(name):
         mask = np.zeros(shape); mask[64, :, :] = 1
         return 3, shape, dx, 30, 0.3 * dx / c.max(), {"sound_speed": c, "density": rho}, \
             {"p0": disc_p0(shape, 6)}, {"mask": mask, "record": ["p", "u_max", "p_final"]}, {"PMLSize": 10}
+    if name == "2d_intensity":
+        shape = (72, 60)
+        c, rho = blob_medium(shape, rng)
+        dt = 0.3 * dx / c.max()
+        pm = np.zeros(shape); pm[12, 20:40] = 1
+        mask = (rng.random(shape) < 0.02).astype(float)
+        return 2, shape, dx, 160, dt, {"sound_speed": c, "density": rho}, {"p_mask": pm, "p": 1e5 * tone(dt, 1.5e6, 3, 160)}, \
+            {"mask": mask, "record": ["p", "u_non_staggered", "I", "I_avg"]}, {"PMLSize": 10}
+    if name == "3d_intensity_static":
+        # 64^3: every pass on the compile-time (narrow-tile) kernels; p not requested
+        shape = (64, 64, 64)
+        c, rho = blob_medium(shape, rng)
+        mask = np.zeros(shape); mask[40, :, 32] = 1; mask[:, 20, 10] = 1
+        return 3, shape, dx, 50, 0.3 * dx / c.max(), {"sound_speed": c, "density": rho, "alpha_coeff": 0.5,
+                                                      "alpha_power": 1.5}, \
+            {"p0": disc_p0(shape, 5)}, {"mask": mask, "record": ["u_non_staggered", "I_avg", "p_max"]}, {"PMLSize": 8}
     raise KeyError(name)
 
 
 CASES = ["2d_homog_p0", "2d_hetero_abs_nl", "2d_stokes_dirichlet", "2d_nocorr_multi", "2d_u_additive",
          "2d_u_dirichlet", "2d_odd_sizes", "2d_pml_outside", "3d_hetero_abs_nl_plane", "3d_multi_signal_additive",
-         "3d_p0_u", "2d_time_reversal", "3d_time_reversal_abs", "3d_static_mixed_radix", "3d_static_128"]
+         "3d_p0_u", "2d_time_reversal", "3d_time_reversal_abs", "3d_static_mixed_radix", "3d_static_128",
+         "2d_intensity", "3d_intensity_static"]
 
 
 def adjoint_problem(shape, Nt, seed=0, dx=1e-4):
