@@ -168,3 +168,27 @@ def test_cart2grid_nearest_and_reorder():
     data = reorder_index[:, None] * np.ones((1, 3))
     back = ks.reorder_binary_sensor_data(data, reorder_index)
     assert np.array_equal(back[:, 0], np.arange(1, 13))
+
+
+def test_plane_wave_intensity():
+    """For a plane wave travelling along x, u = p / (rho c): the intensity
+    the oracle forms from p and the unstaggered, dt/2-shifted velocity
+    (kspaceFirstOrder_saveIntensity.m) is p^2 / (rho c) at every time step,
+    its time average is <p^2> / (rho c), and the transverse intensity is 0."""
+    N0, N1, dx, c, rho = 160, 16, 1e-4, 1500.0, 1000.0
+    kg = ks.KWaveGrid(N0, dx, N1, dx)
+    dt = 0.3 * dx / c
+    kg.setTime(500, dt)
+    pm = np.zeros((N0, N1))
+    pm[30, :] = 1
+    t = np.arange(500) * dt
+    sig = np.sin(2 * np.pi * 1e6 * t) * np.exp(-((t - 3e-6) / 1e-6) ** 2)
+    sm = np.zeros((N0, N1))
+    sm[100, :] = 1
+    out = ks.kspace_first_order(kg, {"sound_speed": c, "density": rho}, {"p_mask": pm, "p": sig[None, :]},
+                                {"mask": sm, "record": ["p", "I", "I_avg"]}, PMLSize=[20, 0])
+    p = out["p"]
+    assert ks.rel_l2(out["Ix"], p ** 2 / (rho * c)) < 1e-4
+    assert np.allclose(out["Ix_avg"], (p ** 2).mean(axis=1) / (rho * c), rtol=1e-5)
+    assert np.abs(out["Iy"]).max() <= 1e-6 * np.abs(out["Ix"]).max()
+    assert "ux_non_staggered" not in out
