@@ -154,6 +154,15 @@ typedef struct kw_problem {
        kspaceFirstOrder3D.m:585-601, NaN edge replaced by rho0); the rho0_sg*
        pointers must then be NULL and rho0 an array. */
     int32_t  derive_rho0_sg;
+
+    /* Interpolated sensor points (Cartesian sensor masks with 'CartInterp'
+       'linear', createStorageVariables.m:376-400): 0 or 1 = one grid cell
+       per point (sensor_mask_index as above); K > 1 = each of the sensor_num
+       points is sum_k sensor_weights[m + M k] * field(sensor_mask_index[m + M k])
+       (extractSensorData.m:301-352), both arrays column-major M x K, indices
+       1-based in any order.  Time reversal and the gradient need K <= 1. */
+    uint32_t sensor_vertices;
+    const float *sensor_weights;
 } kw_problem;
 
 /* Output sizes (createStorageVariables.m:58-88). */

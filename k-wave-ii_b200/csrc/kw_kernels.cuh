@@ -821,7 +821,9 @@ __global__ void __launch_bounds__(kThreads, 2) k_zc2r(const float2 *__restrict__
 // ---------------------------------------------------------------------------
 struct SensorArgs {
     int M;
+    int K;                     // grid cells per point (> 1: weighted, column-major M x K)
     const long long *idx;      // 0-based linear indices
+    const float *w;            // weights (K > 1)
     const float *field[4];     // p, u0, u1, u2
     float *series[4];          // [M x num_rec] or NULL
     float *vmax[4], *vmin[4], *vsq[4];
@@ -830,16 +832,24 @@ struct SensorArgs {
     const int *d_t;
 };
 
+// one sensor point: field at its cell, or sum_k w[m + M k] field[idx[m + M k]]
+__device__ __forceinline__ float sensor_value(const float *field, const long long *idx, const float *w, int M, int K,
+                                              int m) {
+    if (K <= 1) return field[idx[m]];
+    float v = 0.f;
+    for (int k = 0; k < K; ++k) v = fmaf(w[m + (long long)M * k], field[idx[m + (long long)M * k]], v);
+    return v;
+}
+
 __global__ void k_sensor(SensorArgs a) {
     const int m = blockIdx.x * blockDim.x + threadIdx.x;
     if (m >= a.M) return;
     const int t = *a.d_t;
     const int fi = t - a.record_start;   // 0-based column
     if (fi < 0) return;
-    const long long gi = a.idx[m];
     for (int f = 0; f < a.nfield; ++f) {
         if (!a.field[f]) continue;
-        const float v = a.field[f][gi];
+        const float v = sensor_value(a.field[f], a.idx, a.w, a.M, a.K, m);
         if (a.series[f]) a.series[f][m + (long long)a.M * fi] = v;
         if (a.vmax[f]) a.vmax[f][m] = fi == 0 ? v : fmaxf(a.vmax[f][m], v);
         if (a.vmin[f]) a.vmin[f][m] = fi == 0 ? v : fminf(a.vmin[f][m], v);
@@ -952,11 +962,12 @@ __global__ void k_set_points(const long long *pos, int npts, float v, float *fie
 __global__ void k_step_advance(int *d_t) { *d_t += 1; }
 
 // series[m + M (t - record_start)] = src[idx[m]], t from the device step counter
-__global__ void k_gather_series(const float *__restrict__ src, const long long *__restrict__ idx, int M, float *series,
-                                const int *d_t, int record_start) {
+__global__ void k_gather_series(const float *__restrict__ src, const long long *__restrict__ idx,
+                                const float *__restrict__ w, int M, int K, float *series, const int *d_t,
+                                int record_start) {
     const int m = blockIdx.x * blockDim.x + threadIdx.x;
     if (m >= M) return;
-    series[m + (long long)M * (*d_t - record_start)] = src[idx[m]];
+    series[m + (long long)M * (*d_t - record_start)] = sensor_value(src, idx, w, M, K, m);
 }
 
 // dst[i] = m (array or scalar)

@@ -174,7 +174,9 @@ struct kw_plan {
 
     // sensors / outputs
     int M = 0;
-    long long *sidx = nullptr;
+    int K = 1;                     // grid cells per sensor point (interpolated points: K > 1)
+    long long *sidx = nullptr;     // [M x K] column-major
+    float *sw = nullptr;           // [M x K] weights (K > 1)
     float *tr_data = nullptr;
     int *tr_off = nullptr, *tr_cell = nullptr, *tr_row = nullptr;
     uint32_t rec = 0;
@@ -710,7 +712,9 @@ kw_status sensors(kw_plan *P, int t) {
     if (P->M > 0) {
         SensorArgs a{};
         a.M = P->M;
+        a.K = P->K;
         a.idx = P->sidx;
+        a.w = P->sw;
         a.nfield = 1 + P->D;
         a.field[0] = P->p;
         for (int i = 0; i < P->D; ++i) a.field[1 + i] = P->u[i];
@@ -748,8 +752,8 @@ kw_status sensors(kw_plan *P, int t) {
                     src = P->ush;
                 }
                 Scope s(P, KW_KCLASS_SENSOR);
-                k_gather_series<<<(P->M + 255) / 256, 256, 0, P->stream>>>(src, P->sidx, P->M, P->o_uns[i], P->d_t,
-                                                                          P->record_start);
+                k_gather_series<<<(P->M + 255) / 256, 256, 0, P->stream>>>(src, P->sidx, P->sw, P->M, P->K, P->o_uns[i],
+                                                                          P->d_t, P->record_start);
                 KW_TRY(launched(P));
             }
         }
@@ -1317,16 +1321,23 @@ kw_status create(const kw_problem *pr, kw_plan *P) {
     // sensors
     P->rec = q.record;
     P->M = (int)q.sensor_num;
+    P->K = q.sensor_vertices > 1 ? (int)q.sensor_vertices : 1;
+    if (P->K > 8) return fail(KW_ERR_INVALID, "sensor_vertices must be at most 8");
+    if (P->K > 1 && P->time_rev) return fail(KW_ERR_INVALID, "interpolated sensor points cannot drive time reversal");
     if (P->M > 0) {
         if (!q.sensor_mask_index) return fail(KW_ERR_INVALID, "sensor_mask_index is NULL");
-        std::vector<long long> idx(P->M);
-        for (int m = 0; m < P->M; ++m) {
+        if (P->K > 1 && !q.sensor_weights) return fail(KW_ERR_INVALID, "sensor_weights is NULL");
+        const size_t MK = (size_t)P->M * P->K;
+        std::vector<long long> idx(MK);
+        for (size_t m = 0; m < MK; ++m) {
             const uint64_t v = q.sensor_mask_index[m];
             if (v < 1 || v > (uint64_t)g.N) return fail(KW_ERR_INVALID, "sensor index %llu outside the grid", (unsigned long long)v);
-            if (m > 0 && v <= q.sensor_mask_index[m - 1]) return fail(KW_ERR_INVALID, "sensor indices must be increasing (find(mask) order)");
+            if (P->K == 1 && m > 0 && v <= q.sensor_mask_index[m - 1])
+                return fail(KW_ERR_INVALID, "sensor indices must be increasing (find(mask) order)");
             idx[m] = (long long)v - 1;
         }
         KW_TRY(pupload(P, &P->sidx, idx.data(), idx.size()));
+        if (P->K > 1) KW_TRY(pupload(P, &P->sw, q.sensor_weights, MK));
         if (P->time_rev) {
             KW_TRY(pupload(P, &P->tr_data, q.time_reversal_input, (size_t)P->M * P->Nt));
             std::vector<int> rows(P->M);

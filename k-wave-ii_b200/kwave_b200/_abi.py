@@ -95,6 +95,8 @@ class kw_problem(C.Structure):
         ("device", C.c_int32),
         ("array_order", C.c_int32),
         ("derive_rho0_sg", C.c_int32),
+        ("sensor_vertices", C.c_uint32),
+        ("sensor_weights", f32p),
     ]
 
 

@@ -154,3 +154,45 @@ def cart2grid(kgrid, cart_data):
 def reorderBinarySensorData(data, reorder_index):
     """Rows sorted by reorder_index (reorderBinarySensorData.m)."""
     return np.asarray(data)[np.argsort(np.asarray(reorder_index), kind="stable")]
+
+
+def cartLinearWeights(shape, spacing, cart_data):
+    """Barycentric interpolation of Cartesian points on a grid of the given
+    shape and spacing (grid origin at the centre, as kWaveGrid): returns the
+    containing simplex as 0-based column-major grid indices (M x (D+1)) and
+    the weights (M x (D+1)).
+
+    The reference triangulates every grid point with delaunayTriangulation and
+    locates the points in it (gridDataFast2D.m / gridDataFast3D.m).  On a
+    regular grid the Delaunay triangulation is not unique (each cell's
+    corners are co-circular), so this uses one documented choice, the Kuhn
+    triangulation: inside the cell with lower corner b and fractional offsets
+    f, the simplex walks the axes in decreasing order of f (ties: lower axis
+    first) and the weights are (1 - f_(1), f_(1) - f_(2), ..., f_(D))."""
+    cart = np.atleast_2d(np.asarray(cart_data, dtype=np.float64))
+    dim = len(shape)
+    M = cart.shape[1]
+    frac = np.empty((dim, M))
+    base = np.empty((dim, M), dtype=np.int64)
+    for a in range(dim):
+        n = int(shape[a])
+        fi = cart[a] / spacing[a] + n // 2
+        if np.any(fi < -1e-9) or np.any(fi > n - 1 + 1e-9):
+            raise ValueError("Cartesian points must lie within the k-space grid defined by kgrid.")
+        fi = np.clip(fi, 0, n - 1)
+        b = np.minimum(np.floor(fi).astype(np.int64), n - 2)
+        base[a] = b
+        frac[a] = fi - b
+    order = np.argsort(-frac, axis=0, kind="stable")
+    fs = np.take_along_axis(frac, order, axis=0)
+    tri = np.empty((M, dim + 1), dtype=np.int64)
+    bc = np.empty((M, dim + 1))
+    v = base.copy()
+    cols = np.arange(M)
+    tri[:, 0] = np.ravel_multi_index(tuple(v), tuple(shape), order="F")
+    bc[:, 0] = 1.0 - fs[0]
+    for k in range(dim):
+        v[order[k], cols] += 1
+        tri[:, k + 1] = np.ravel_multi_index(tuple(v), tuple(shape), order="F")
+        bc[:, k + 1] = fs[k] - (fs[k + 1] if k + 1 < dim else 0.0)
+    return tri, bc

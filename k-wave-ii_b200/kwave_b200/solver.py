@@ -23,7 +23,7 @@ import math
 import numpy as np
 
 from . import _abi
-from .helpers import cart2grid, reorderBinarySensorData, smooth
+from .helpers import cart2grid, cartLinearWeights, reorderBinarySensorData, smooth
 from .kgrid import kWaveGrid
 
 RECORD_FLAGS = ("p", "p_max", "p_min", "p_rms", "p_max_all", "p_min_all", "p_final",
@@ -259,12 +259,14 @@ def _prepare(dim, kgrid, medium, source, sensor, options):
                 sl = tuple(slice(int(m[a, c]) - 1, int(m[a + dim, c])) for a in range(dim))
                 mask[sl] = 1
         elif m.ndim == 2 and m.shape[0] == dim:
-            if cart_interp == "linear":
-                raise KWaveInputError("Cartesian sensor masks with 'CartInterp' = 'linear' (Delaunay barycentric "
-                                      "interpolation) are not supported yet; use 'CartInterp', 'nearest'.")
-            mask, order_index, reorder_index = cart2grid(kgrid, m)
-            P.reorder_index = None if time_rev else reorder_index
-            P.order_index = order_index
+            if cart_interp == "linear" and not time_rev:
+                # recorded by barycentric interpolation on the grid
+                # (createStorageVariables.m:376-400, extractSensorData.m:301-352)
+                P.cart_points = m
+            else:
+                mask, order_index, reorder_index = cart2grid(kgrid, m)
+                P.reorder_index = None if time_rev else reorder_index
+                P.order_index = order_index
         else:
             raise KWaveInputError("Cartesian sensor.mask for a %dD simulation must be given as a %d by N array." % (dim, dim))
 
@@ -383,6 +385,13 @@ def _prepare(dim, kgrid, medium, source, sensor, options):
             idx_parts.append(_find(tm))
         P.cuboid_rows = idx_parts
     sensor_idx = _find(mask) if mask is not None else np.zeros(0, dtype=np.int64)
+    sensor_w = None
+    if getattr(P, "cart_points", None) is not None:
+        try:
+            tri, sensor_w = cartLinearWeights(shape, spacing, P.cart_points)
+        except ValueError as e:
+            raise KWaveInputError(str(e))
+        sensor_idx = tri
 
     # ---- source scaling (scaleSourceTerms.m) ----
     hetero_c = c0.size > 1
@@ -505,9 +514,16 @@ def _prepare(dim, kgrid, medium, source, sensor, options):
             tgt.input = _abi.fptr(x)
     if source_p0:
         pr.p0_source_input = grid_arr(p0)
-    pr.sensor_num = sensor_idx.size
-    if sensor_idx.size:
-        pr.sensor_mask_index = idx_arr(sensor_idx)
+    if sensor_w is not None:
+        # M points x (D+1) vertices, column-major
+        pr.sensor_num = sensor_idx.shape[0]
+        pr.sensor_vertices = sensor_idx.shape[1]
+        pr.sensor_mask_index = idx_arr(np.asfortranarray(sensor_idx).ravel(order="F"))
+        pr.sensor_weights = arr(np.asfortranarray(sensor_w))
+    else:
+        pr.sensor_num = sensor_idx.size
+        if sensor_idx.size:
+            pr.sensor_mask_index = idx_arr(sensor_idx)
     pr.record_start_index = record_start
     bits = 0
     for r in record:
@@ -534,7 +550,7 @@ def _prepare(dim, kgrid, medium, source, sensor, options):
     P.record_given = record_given
     P.time_rev = time_rev
     P.use_sensor = use_sensor
-    P.M = sensor_idx.size
+    P.M = int(pr.sensor_num)
     P.Nt = Nt
     P.record_start = record_start
     P.inside = inside

@@ -332,6 +332,46 @@ def cart2grid(kgrid, cart):
     return mask, order_index, reorder_index
 
 
+def cart_linear(kgrid, cart):
+    """Containing simplex (0-based column-major grid indices, M x (D+1)) and
+    barycentric weights of Cartesian points in a Delaunay triangulation of
+    the grid points, as gridDataFast2D.m / gridDataFast3D.m obtain with
+    delaunayTriangulation + pointLocation.  A regular grid is a degenerate
+    Delaunay case (each cell's corners are co-circular), so the triangulation
+    is not unique and MATLAB's choice of cell diagonals is not documented.
+    This restatement uses the Kuhn triangulation: in the cell with lower
+    corner b and fractional offsets f, the simplex walks the axes in
+    decreasing order of f (ties: lower axis first), with weights
+    (1 - f_(1), f_(1) - f_(2), ..., f_(D))."""
+    dim = kgrid.dim
+    cart = np.atleast_2d(np.asarray(cart, dtype=np.float64))
+    M = cart.shape[1]
+    f = np.empty((dim, M))
+    base = np.empty((dim, M), dtype=np.int64)
+    for a in range(dim):
+        n = kgrid.shape[a]
+        fi = cart[a] / kgrid.spacing[a] + n // 2
+        if np.any(fi < -1e-9) or np.any(fi > n - 1 + 1e-9):
+            raise ValueError("Cartesian points must lie within the k-space grid defined by kgrid.")
+        fi = np.clip(fi, 0, n - 1)
+        b = np.minimum(np.floor(fi).astype(np.int64), n - 2)
+        base[a] = b
+        f[a] = fi - b
+    order = np.argsort(-f, axis=0, kind="stable")
+    fs = np.take_along_axis(f, order, axis=0)
+    tri = np.empty((M, dim + 1), dtype=np.int64)
+    bc = np.empty((M, dim + 1))
+    v = base.copy()
+    cols = np.arange(M)
+    tri[:, 0] = np.ravel_multi_index(tuple(v), kgrid.shape, order="F")
+    bc[:, 0] = 1.0 - fs[0]
+    for k in range(dim):
+        v[order[k], cols] += 1
+        tri[:, k + 1] = np.ravel_multi_index(tuple(v), kgrid.shape, order="F")
+        bc[:, k + 1] = fs[k] - (fs[k + 1] if k + 1 < dim else 0.0)
+    return tri, bc
+
+
 def reorder_binary_sensor_data(data, reorder_index):
     """reorderBinarySensorData.m: sort rows by reorder_index."""
     order = np.argsort(reorder_index, kind="stable")
@@ -470,14 +510,17 @@ def kspace_first_order(kgrid, medium, source, sensor, **opts):
     record_start = int(_mround(_get(sensor, "record_start_index", 1))) if use_sensor else 1
     reorder_index = None
     mask = None
+    cart_points = None
     if use_sensor and not blank_sensor:
         m = np.asarray(_get(sensor, "mask"), dtype=np.float64)
         if m.shape == kgrid.shape:
             mask = m
         elif m.ndim == 2 and m.shape[0] == dim:
-            if cart_interp != "nearest":
-                raise NotImplementedError("Cartesian 'linear' interpolation is not restated")
-            mask, order_index, reorder_index = cart2grid(kgrid, m)
+            if cart_interp == "linear" and not time_rev:
+                # recorded by barycentric interpolation (createStorageVariables.m:376-400)
+                cart_points = m
+            else:
+                mask, order_index, reorder_index = cart2grid(kgrid, m)
         else:
             raise ValueError("sensor.mask shape not understood")
 
@@ -551,6 +594,15 @@ def kspace_first_order(kgrid, medium, source, sensor, **opts):
 
     def gather(field, idx):
         return field.ravel(order="F")[idx]
+
+    sensor_interp = cart_linear(kgrid, cart_points) if cart_points is not None else None
+
+    def gather_s(field):
+        """the recorded value at every sensor point (extractSensorData.m:63-100, 301-352)"""
+        if sensor_interp is None:
+            return gather(field, sensor_idx)
+        tri, bc = sensor_interp
+        return (field.ravel(order="F")[tri] * bc).sum(axis=1)
 
     def scatter_set(field, idx, vals):
         f = field.ravel(order="F").copy()
@@ -682,7 +734,7 @@ def kspace_first_order(kgrid, medium, source, sensor, **opts):
     # ---- storage (createStorageVariables.m) ----
     num_rec = Nt - record_start + 1
     out = {}
-    M = sensor_idx.size if sensor_idx is not None else 0
+    M = sensor_idx.size if sensor_idx is not None else (cart_points.shape[1] if cart_points is not None else 0)
     if "p" in record:
         out["p"] = np.zeros((M, num_rec))
     if "p_rms" in record:
@@ -805,8 +857,8 @@ def kspace_first_order(kgrid, medium, source, sensor, **opts):
         # sensors (extractSensorData.m)
         if use_sensor and not time_rev and t >= record_start:
             fi = t - record_start + 1
-            if sensor_idx is not None:
-                ps = gather(p, sensor_idx)
+            if sensor_idx is not None or sensor_interp is not None:
+                ps = gather_s(p)
                 if "p" in record:
                     out["p"][:, fi - 1] = ps
                 if "p_max" in record:
@@ -816,7 +868,7 @@ def kspace_first_order(kgrid, medium, source, sensor, **opts):
                 if "p_rms" in record:
                     out["p_rms"] = np.sqrt((out["p_rms"] ** 2 * (fi - 1) + ps ** 2) / fi)
                 for i in range(dim):
-                    us = gather(u[i], sensor_idx)
+                    us = gather_s(u[i])
                     n = u_comps[i]
                     if "u" in record:
                         out[n][:, fi - 1] = us
@@ -828,7 +880,7 @@ def kspace_first_order(kgrid, medium, source, sensor, **opts):
                         out[n + "_rms"] = np.sqrt((out[n + "_rms"] ** 2 * (fi - 1) + us ** 2) / fi)
                     if "u_non_staggered" in record:
                         ush = np.real(np.fft.ifft(_axis(shift_neg[i], i, dim) * np.fft.fft(u[i], axis=i), axis=i))
-                        out[n + "_non_staggered"][:, fi - 1] = gather(ush, sensor_idx)
+                        out[n + "_non_staggered"][:, fi - 1] = gather_s(ush)
             ins = tuple(inside)
             if "p_max_all" in record:
                 out["p_max_all"] = p[ins].copy() if fi == 1 else np.maximum(out["p_max_all"], p[ins])

@@ -164,13 +164,29 @@ def make_case(name):
         return 3, shape, dx, 50, 0.3 * dx / c.max(), {"sound_speed": c, "density": rho, "alpha_coeff": 0.5,
                                                       "alpha_power": 1.5}, \
             {"p0": disc_p0(shape, 5)}, {"mask": mask, "record": ["u_non_staggered", "I_avg", "p_max"]}, {"PMLSize": 8}
+    if name == "2d_cart_linear":
+        # Cartesian circle recorded with the default CartInterp 'linear'
+        shape = (64, 64)
+        c, rho = blob_medium(shape, rng)
+        r = 22 * dx
+        ang = np.linspace(0, 2 * np.pi, 40, endpoint=False) + 0.1
+        pts = np.stack([r * np.cos(ang), r * np.sin(ang)])
+        return 2, shape, dx, 150, 0.3 * dx / c.max(), {"sound_speed": c, "density": rho}, \
+            {"p0": disc_p0(shape, 4)}, {"mask": pts, "record": ["p", "p_max", "u", "u_non_staggered"]}, {"PMLSize": 10}
+    if name == "3d_cart_linear":
+        shape = (32, 28, 30)
+        c, rho = blob_medium(shape, rng)
+        pts = (rng.random((3, 25)) - 0.5) * np.array([[20], [18], [20]]) * dx
+        med = {"sound_speed": c, "density": rho, "alpha_coeff": 0.5, "alpha_power": 1.5}
+        return 3, shape, dx, 60, 0.3 * dx / c.max(), med, {"p0": disc_p0(shape, 4)}, \
+            {"mask": pts, "record": ["p", "p_rms", "I_avg"]}, {"PMLSize": 5}
     raise KeyError(name)
 
 
 CASES = ["2d_homog_p0", "2d_hetero_abs_nl", "2d_stokes_dirichlet", "2d_nocorr_multi", "2d_u_additive",
          "2d_u_dirichlet", "2d_odd_sizes", "2d_pml_outside", "3d_hetero_abs_nl_plane", "3d_multi_signal_additive",
          "3d_p0_u", "2d_time_reversal", "3d_time_reversal_abs", "3d_static_mixed_radix", "3d_static_128",
-         "2d_intensity", "3d_intensity_static"]
+         "2d_intensity", "3d_intensity_static", "2d_cart_linear", "3d_cart_linear"]
 
 
 def adjoint_problem(shape, Nt, seed=0, dx=1e-4):

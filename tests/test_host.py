@@ -167,3 +167,30 @@ def test_find_is_matlab_find(shape):
     for a in (m, np.asfortranarray(m)):
         assert np.array_equal(_find(a), ref)
         assert np.array_equal(_at(a, ref), m.ravel(order="F")[ref])
+
+
+@pytest.mark.parametrize("shape", [(40, 36), (20, 22, 18), (41, 17)])
+def test_cart_linear_weights(shape):
+    """Barycentric weights of Cartesian points (CartInterp 'linear'): they are
+    non-negative, sum to 1, reproduce every affine field exactly (true for
+    any triangulation, so also for MATLAB's), and match the oracle's."""
+    from kwave_b200.helpers import cartLinearWeights
+    g, o = _grids(shape, 1e-4)
+    rng = np.random.default_rng(4)
+    dim = len(shape)
+    half = np.array([(s // 2 - 1) * 1e-4 for s in shape])
+    pts = (rng.random((dim, 50)) * 2 - 1) * half[:, None]
+    pts[:, 0] = 0.0                                    # a grid node
+    tri, bc = cartLinearWeights(shape, [1e-4] * dim, pts)
+    assert bc.min() >= -1e-12 and np.allclose(bc.sum(axis=1), 1.0)
+    coef = rng.standard_normal(dim + 1)
+    grid = np.meshgrid(*[g.grid_vec(a) for a in range(dim)], indexing="ij")
+    field = coef[0] + sum(coef[a + 1] * grid[a] for a in range(dim))
+    interp = (field.ravel(order="F")[tri] * bc).sum(axis=1)
+    exact = coef[0] + sum(coef[a + 1] * pts[a] for a in range(dim))
+    assert np.allclose(interp, exact, rtol=0, atol=1e-12 * np.abs(coef).sum())
+    assert np.isclose(bc[0].max(), 1.0)
+    t2, b2 = ks.cart_linear(o, pts)
+    assert np.array_equal(tri, t2) and np.allclose(bc, b2, rtol=0, atol=1e-15)
+    with pytest.raises(ValueError, match="within the k-space grid"):
+        cartLinearWeights(shape, [1e-4] * dim, pts + 1.0)
