@@ -233,6 +233,12 @@ def _prepare(dim, kgrid, medium, source, sensor, options):
     blank = use_sensor and not needs_mask and not time_rev
     rsi = _field(sensor, "record_start_index", 1) if use_sensor else 1
     record_start = int(_round(rsi))
+    P.frequency_response = None
+    if use_sensor and not time_rev and _has(sensor, "frequency_response"):
+        fr = np.asarray(_field(sensor, "frequency_response"), dtype=np.float64).ravel()
+        if fr.size != 2:
+            raise KWaveInputError("sensor.frequency_response must be a 2 element numerical array.")
+        P.frequency_response = (float(fr[0]), float(fr[1]))
     P.cuboid_list = None
     P.reorder_index = None
     mask = None
@@ -551,6 +557,7 @@ def _prepare(dim, kgrid, medium, source, sensor, options):
     P.time_rev = time_rev
     P.use_sensor = use_sensor
     P.M = int(pr.sensor_num)
+    P.dt = dt
     P.Nt = Nt
     P.record_start = record_start
     P.inside = inside
@@ -853,6 +860,9 @@ def _finish(P, host):
             if k.endswith("_all") or k.endswith("_final"):
                 continue
             out[k] = reorderBinarySensorData(out[k], P.reorder_index)
+    # sensor frequency response (kspaceFirstOrder3D.m:1345-1348)
+    if P.frequency_response is not None and "p" in out:
+        out["p"] = _gaussian_filter(out["p"], 1.0 / P.dt, *P.frequency_response).astype(np.float32)
     if P.cuboid_list is not None:
         out = _cuboids(P, out)
     if not P.use_sensor:
@@ -884,6 +894,22 @@ def _cuboids(P, out):
                 d[k] = v[sel].reshape(size, order="F")
         res.append(d)
     return res
+
+
+def _gaussian_filter(signal, fs, freq, bandwidth):
+    """gaussianFilter.m: every row filtered in frequency by
+    max(G(f - freq), G(f + freq)), G a unit-height Gaussian of FWHM
+    bandwidth % of freq."""
+    signal = np.asarray(signal, dtype=np.float64)
+    N = signal.shape[-1]
+    if N % 2 == 0:
+        f = np.arange(-N // 2, N // 2) * fs / N
+    else:
+        f = np.arange(-(N - 1) // 2, (N - 1) // 2 + 1) * fs / N
+    var = (bandwidth / 100.0 * freq / (2 * math.sqrt(2 * math.log(2)))) ** 2
+    g = np.maximum(np.exp(-(f - freq) ** 2 / (2 * var)), np.exp(-(f + freq) ** 2 / (2 * var)))
+    spec = np.fft.fftshift(np.fft.fft(signal, axis=-1), axes=-1)
+    return np.real(np.fft.ifft(np.fft.ifftshift(g * spec, axes=-1), axis=-1))
 
 
 def _fourier_shift(data, shift):

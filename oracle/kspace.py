@@ -393,6 +393,22 @@ def fourier_shift(data, shift):
     return np.real(np.fft.ifft(np.fft.ifftshift(np.exp(1j * k * shift)) * np.fft.fft(data, axis=-1), axis=-1))
 
 
+def gaussian_filter(signal, fs, freq, bandwidth):
+    """gaussianFilter.m: each row of signal filtered in frequency by
+    max(G(f - freq), G(f + freq)), G a unit-height Gaussian whose FWHM is
+    bandwidth % of freq."""
+    signal = np.asarray(signal, dtype=np.float64)
+    N = signal.shape[-1]
+    if N % 2 == 0:
+        f = np.arange(-N // 2, N // 2) * fs / N
+    else:
+        f = np.arange(-(N - 1) // 2, (N - 1) // 2 + 1) * fs / N
+    var = (bandwidth / 100.0 * freq / (2 * np.sqrt(2 * np.log(2)))) ** 2
+    g = np.maximum(np.exp(-(f - freq) ** 2 / (2 * var)), np.exp(-(f + freq) ** 2 / (2 * var)))
+    spec = np.fft.fftshift(np.fft.fft(signal, axis=-1), axes=-1)
+    return np.real(np.fft.ifft(np.fft.ifftshift(g * spec, axes=-1), axis=-1))
+
+
 def tone_burst_hann(sample_freq, signal_freq, num_cycles):
     """A sine tone burst of ``num_cycles`` cycles sampled at ``sample_freq``,
     windowed by getWin(N, 'Hanning') (toneBurst.m:102-180 time axis)."""
@@ -927,6 +943,11 @@ def kspace_first_order(kgrid, medium, source, sensor, **opts):
             if key.endswith("_all") or key.endswith("_final"):
                 continue
             out[key] = reorder_binary_sensor_data(out[key], reorder_index)
+
+    # sensor frequency response (kspaceFirstOrder3D.m:1345-1348)
+    if use_sensor and not time_rev and _has(sensor, "frequency_response") and "p" in out:
+        fr = np.asarray(_get(sensor, "frequency_response"), dtype=np.float64).ravel()
+        out["p"] = gaussian_filter(out["p"], 1.0 / dt, fr[0], fr[1])
 
     if not use_sensor:
         return None

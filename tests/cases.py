@@ -179,7 +179,7 @@ def make_case(name):
         pts = (rng.random((3, 25)) - 0.5) * np.array([[20], [18], [20]]) * dx
         med = {"sound_speed": c, "density": rho, "alpha_coeff": 0.5, "alpha_power": 1.5}
         return 3, shape, dx, 60, 0.3 * dx / c.max(), med, {"p0": disc_p0(shape, 4)}, \
-            {"mask": pts, "record": ["p", "p_rms", "I_avg"]}, {"PMLSize": 5}
+            {"mask": pts, "record": ["p", "p_rms", "I_avg"], "frequency_response": [1.5e6, 60.0]}, {"PMLSize": 5}
     raise KeyError(name)
 
 

@@ -192,3 +192,16 @@ def test_plane_wave_intensity():
     assert np.allclose(out["Ix_avg"], (p ** 2).mean(axis=1) / (rho * c), rtol=1e-5)
     assert np.abs(out["Iy"]).max() <= 1e-6 * np.abs(out["Ix"]).max()
     assert "ux_non_staggered" not in out
+
+
+def test_gaussian_filter_passes_centre_frequency():
+    """gaussianFilter.m keeps a tone at the centre frequency and attenuates
+    one at twice the half-power bandwidth away by the Gaussian's value."""
+    fs, f0, bw, N = 50e6, 2e6, 50.0, 1000
+    t = np.arange(N) / fs
+    sig = np.sin(2 * np.pi * f0 * t)[None, :]
+    assert ks.rel_l2(ks.gaussian_filter(sig, fs, f0, bw), sig) < 1e-3
+    off = f0 + bw / 100 * f0            # two half-widths away: gain exp(-4 ln 2) = 1/16
+    sig2 = np.sin(2 * np.pi * off * t)[None, :]
+    gain = np.abs(np.fft.rfft(ks.gaussian_filter(sig2, fs, f0, bw)[0])).max() / np.abs(np.fft.rfft(sig2[0])).max()
+    assert abs(gain - 1 / 16) < 5e-3
