@@ -33,11 +33,16 @@ struct AxisFFT {
     const float2 *tw;      // device table, n entries
 };
 
+// (a.x b.x - a.y b.y, a.x b.y + a.y b.x) as a packed multiply and a packed
+// fused multiply-add (each component rounds as fmaf(a.x, b.*, a.y * (+-b.*)))
 __device__ __forceinline__ float2 cmul(float2 a, float2 b) {
-    return make_float2(fmaf(a.x, b.x, -a.y * b.y), fmaf(a.x, b.y, a.y * b.x));
+    const float2 t = __fmul2_rn(make_float2(a.y, a.y), make_float2(-b.y, b.x));
+    return __ffma2_rn(make_float2(a.x, a.x), b, t);
 }
-__device__ __forceinline__ float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
-__device__ __forceinline__ float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+// complex add / subtract as one packed FP32 instruction (sm_100 FADD2 /
+// FFMA2); a - b = b * (-1) + a rounds exactly like a scalar subtraction
+__device__ __forceinline__ float2 cadd(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 csub(float2 a, float2 b) { return __ffma2_rn(b, make_float2(-1.f, -1.f), a); }
 __device__ __forceinline__ float2 cscale(float2 a, float s) { return make_float2(a.x * s, a.y * s); }
 __device__ __forceinline__ float2 cconj(float2 a) { return make_float2(a.x, -a.y); }
 // multiply by -i (forward) or +i (inverse)
