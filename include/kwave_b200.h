@@ -280,6 +280,17 @@ kw_status kw_server_get_stats(kw_server *server, kw_server_stats *stats);
 kw_status kw_server_destroy(kw_server *server);
 
 /*
+ * Tile widths of the compile-time transform kernels (lines per block of the
+ * z-stages, the y-pass and the x-pass; 0 for a class that runs the runtime
+ * kernels).  Plan creation picks them by rule and then by timing (the
+ * autotuner; environment variable KW_AUTOTUNE=0 turns it off).  kw_set_tiles
+ * accepts, per class, the full width or the narrow one (a quarter) and
+ * rejects anything else; results do not depend on the choice.
+ */
+kw_status kw_plan_tiles(const kw_plan *plan, int32_t tiles[3]);
+kw_status kw_set_tiles(kw_plan *plan, const int32_t tiles[3]);
+
+/*
  * Gradient of a sensor misfit with respect to the sound speed and the density
  * (the adjoint form).  No counterpart in the reference, which offers time
  * reversal only: this is the exact discrete adjoint of the plan's own time

@@ -16,6 +16,7 @@
 #include <cstring>
 #include <string>
 #include <cstdlib>
+#include <array>
 #include <map>
 #include <mutex>
 #include <vector>
@@ -1034,6 +1035,99 @@ void plan_tiles(kw_plan *P) {
     }
 }
 
+// ---- tile autotuner ------------------------------------------------------
+// The compile-time kernels of each pass class (z-stages, y-pass, x-pass)
+// exist with a full tile (ks_lines(n) lines) and a narrow one (ks_narrow(n)).
+// plan_tiles picks by a rule (narrow when full tiles give fewer blocks than
+// SMs); the autotuner then times a few steps with each class flipped and
+// keeps what is faster, once per grid shape and tile-relevant structure per
+// process.  Tile widths change how lines are grouped into blocks, never the
+// arithmetic of a line, so results are identical whichever is chosen.
+struct TileChoice {
+    int PL, TY, NL;
+};
+std::mutex g_tune_mu;
+std::map<std::array<int, 5>, TileChoice> g_tune;
+
+TileChoice tiles_of(const kw_plan *P) { return TileChoice{P->PL_z, P->TY, P->NL}; }
+void set_tiles(kw_plan *P, const TileChoice &c) {
+    P->PL_u = P->PL_z = P->PL_p = P->PL_r = c.PL;
+    P->TY = c.TY;
+    P->NL = c.NL;
+}
+
+// device milliseconds per step of the current tiles (steps run directly,
+// not recording; the state is reset by the caller)
+kw_status time_steps(kw_plan *P, int n, float *ms) {
+    KW_TRY(zero_state(P));
+    P->started = true;
+    KW_TRY(run_step(P));   // warm-up (and the t = 1 special cases)
+    cudaEvent_t a, b;
+    KW_CUDA(cudaEventCreate(&a));
+    KW_CUDA(cudaEventCreate(&b));
+    KW_CUDA(cudaEventRecord(a, P->stream));
+    kw_status st = KW_OK;
+    for (int k = 0; k < n && st == KW_OK; ++k) st = run_step(P);
+    cudaEventRecord(b, P->stream);
+    cudaEventSynchronize(b);
+    float t = 0.f;
+    cudaEventElapsedTime(&t, a, b);
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    KW_TRY(st);
+    *ms = t / (float)n;
+    return KW_OK;
+}
+
+kw_status autotune_tiles(kw_plan *P) {
+    if (const char *e = getenv("KW_AUTOTUNE"))
+        if (atoi(e) == 0) return KW_OK;
+    const Geom &g = P->g;
+    // z tiles fix the per-tile lists of sparse sources and time reversal, so
+    // those plans keep the rule's z tiles
+    const bool tune_z = P->static_z && !P->time_rev && !(P->psrc.present && !P->psrc.dense_fast && !P->psrc.dense_general) &&
+                        !(P->usrc.present && !P->usrc.dense_fast && !P->usrc.dense_general);
+    const bool tune_y = P->static_y;
+    const bool tune_x = P->static_x;
+    if (!tune_z && !tune_y && !tune_x) return KW_OK;
+    if (P->Nt < 4 || P->time_rev) return KW_OK;
+    const std::array<int, 5> key = {g.N0, g.N1, g.N2, P->absorbing ? 1 : 0, tune_z ? 1 : 0};
+    {
+        std::lock_guard<std::mutex> lock(g_tune_mu);
+        auto it = g_tune.find(key);
+        if (it != g_tune.end()) {
+            set_tiles(P, it->second);
+            return KW_OK;
+        }
+    }
+    const bool keep_no_record = P->no_record;
+    P->no_record = true;
+    TileChoice best = tiles_of(P);
+    float best_ms = 0.f;
+    kw_status st = time_steps(P, 2, &best_ms);
+    auto flip = [](int v, int full, int narrow) { return v == full ? narrow : full; };
+    for (int cls = 0; cls < 3 && st == KW_OK; ++cls) {
+        TileChoice c = best;
+        if (cls == 0 && tune_z) c.PL = flip(c.PL, ks_lines(g.N2), ks_narrow(g.N2));
+        else if (cls == 1 && tune_y) c.TY = flip(c.TY, ks_lines(g.N1), ks_narrow(g.N1));
+        else if (cls == 2 && tune_x) c.NL = flip(c.NL, ks_lines(g.N0), ks_narrow(g.N0));
+        else continue;
+        set_tiles(P, c);
+        float ms = 0.f;
+        st = time_steps(P, 2, &ms);
+        if (st == KW_OK && ms < 0.97f * best_ms) {
+            best = c;
+            best_ms = ms;
+        }
+    }
+    set_tiles(P, best);
+    P->no_record = keep_no_record;
+    KW_TRY(st);
+    std::lock_guard<std::mutex> lock(g_tune_mu);
+    g_tune[key] = best;
+    return KW_OK;
+}
+
 kw_status create(const kw_problem *pr, kw_plan *P) {
     if (!pr) return fail(KW_ERR_INVALID, "problem is NULL");
     if (pr->abi_version != KW_ABI_VERSION) return fail(KW_ERR_INVALID, "abi_version %u, library expects %d", pr->abi_version, KW_ABI_VERSION);
@@ -1391,6 +1485,7 @@ kw_status create(const kw_problem *pr, kw_plan *P) {
     }
     KW_TRY(palloc(P, &P->o_tmp, std::max<size_t>(std::max<size_t>(P->in_count, P->M), 1)));
     KW_CUDA(cudaStreamSynchronize(P->stream));
+    KW_TRY(autotune_tiles(P));
     KW_TRY(zero_state(P));
     return KW_OK;
 }
@@ -1800,6 +1895,39 @@ kw_status kw_gradient_noalloc(int32_t dim, const uint64_t shape[3], const double
     KW_TRY(ypass(&P, true, b, 1));
     KW_TRY(zc2r(&P, spec, out));
     KW_CUDA(cudaStreamSynchronize(P.stream));
+    return KW_OK;
+}
+
+kw_status kw_plan_tiles(const kw_plan *P, int32_t tiles[3]) {
+    if (!P || !tiles) return fail(KW_ERR_INVALID, "NULL argument");
+    tiles[0] = P->static_z ? P->PL_z : 0;
+    tiles[1] = P->static_y ? P->TY : 0;
+    tiles[2] = P->static_x ? P->NL : 0;
+    return KW_OK;
+}
+
+kw_status kw_set_tiles(kw_plan *P, const int32_t tiles[3]) {
+    if (!P || !tiles) return fail(KW_ERR_INVALID, "NULL argument");
+    const Geom &g = P->g;
+    auto ok = [](int v, int n) { return v == ks_lines(n) || v == ks_narrow(n); };
+    if (P->static_z && !ok(tiles[0], g.N2)) return fail(KW_ERR_INVALID, "z tile width must be %d or %d", ks_lines(g.N2), ks_narrow(g.N2));
+    if (P->static_y && !ok(tiles[1], g.N1)) return fail(KW_ERR_INVALID, "y tile width must be %d or %d", ks_lines(g.N1), ks_narrow(g.N1));
+    if (P->static_x && !ok(tiles[2], g.N0)) return fail(KW_ERR_INVALID, "x tile width must be %d or %d", ks_lines(g.N0), ks_narrow(g.N0));
+    const bool z_fixed = P->time_rev || (P->psrc.present && !P->psrc.dense_fast && !P->psrc.dense_general) ||
+                         (P->usrc.present && !P->usrc.dense_fast && !P->usrc.dense_general);
+    if (P->static_z && z_fixed && tiles[0] != P->PL_z)
+        return fail(KW_ERR_INVALID, "the z tiles of this plan are fixed by its sparse source or time-reversal lists");
+    KW_TRY(use_device(P));
+    KW_CUDA(cudaStreamSynchronize(P->stream));
+    TileChoice c = tiles_of(P);
+    if (P->static_z) c.PL = tiles[0];
+    if (P->static_y) c.TY = tiles[1];
+    if (P->static_x) c.NL = tiles[2];
+    set_tiles(P, c);
+    // graphs captured with the old tiles are stale
+    for (auto &kv : P->graphs)
+        if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
+    P->graphs.clear();
     return KW_OK;
 }
 

@@ -153,6 +153,8 @@ SYMBOLS = {
     "kw_gradient_noalloc": (C.c_int, [C.c_int32, C.POINTER(C.c_uint64), C.POINTER(C.c_double), C.c_int32,
                                       C.c_int32, C.c_double, C.c_double, C.c_int32, C.c_void_p, C.c_void_p,
                                       C.c_void_p]),
+    "kw_plan_tiles": (C.c_int, [C.c_void_p, C.POINTER(C.c_int32)]),
+    "kw_set_tiles": (C.c_int, [C.c_void_p, C.POINTER(C.c_int32)]),
     "kw_adjoint_gradient": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p]),
     "kw_server_create": (C.c_int, [C.POINTER(kw_server_config), C.POINTER(C.c_void_p)]),
     "kw_server_submit": (C.c_int, [C.c_void_p, C.POINTER(kw_problem), C.POINTER(C.c_uint64)]),

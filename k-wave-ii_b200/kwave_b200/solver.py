@@ -669,6 +669,16 @@ class Simulation:
         _abi.check(self._lib.kw_launch_count(self.handle, C.byref(n)))
         return n.value
 
+    def tiles(self):
+        """(z, y, x) lines per block of the compile-time transform kernels (0: runtime kernels)."""
+        t = (C.c_int32 * 3)()
+        _abi.check(self._lib.kw_plan_tiles(self.handle, t))
+        return tuple(t)
+
+    def set_tiles(self, tiles):
+        t = (C.c_int32 * 3)(*tiles)
+        _abi.check(self._lib.kw_set_tiles(self.handle, t))
+
     def device_bytes(self):
         b = C.c_uint64()
         _abi.check(self._lib.kw_plan_device_bytes(self.handle, C.byref(b)))

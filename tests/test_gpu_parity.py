@@ -139,3 +139,32 @@ def test_column_major_abi_matches_row_major(name):
     out = out if isinstance(out, dict) else {"p": out}
     for k in ref:
         assert _rel(out[k], ref[k]) <= 1e-5, (k, _rel(out[k], ref[k]))
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", ["3d_intensity_static", "3d_static_mixed_radix", "2d_homog_p0"])
+def test_tile_widths_do_not_change_results(name):
+    """Every choice of full or narrow tiles the autotuner may make gives
+    bit-identical outputs (tile widths group lines into blocks; the
+    arithmetic of a line does not depend on them)."""
+    import itertools
+    import kwave_b200 as kw
+    dim, shape, dx, Nt, dt, med, src, sen, opts = make_case(name)
+    sim = kw.Simulation(dim, _grid(kw, shape, dx, Nt, dt), med, src, sen, **opts)
+    chosen = sim.tiles()
+    ref = sim.run()
+    ref = ref if isinstance(ref, dict) else {"p": ref}
+    options = []
+    for t, n in zip(chosen, (shape[-1], shape[1] if dim == 3 else 1, shape[0])):
+        if t == 0:
+            options.append([0])
+        else:
+            full = min(64, 1 << int(np.floor(np.log2(4096 // n))))
+            options.append([full, full // 4])
+    for tiles in itertools.product(*options):
+        sim.set_tiles(tiles)
+        out = sim.run()
+        out = out if isinstance(out, dict) else {"p": out}
+        for k in ref:
+            assert np.array_equal(out[k], ref[k]), (name, tiles, k)
+    sim.close()
