@@ -449,7 +449,12 @@ def kspace_first_order(kgrid, medium, source, sensor, **opts):
     Smooth, UsekSpace, UseSG, CartInterp.  Returns what the MATLAB function
     returns: the ``p`` matrix (M x Nt) when ``sensor.record`` is absent, the
     ``p_final`` array in time-reversal mode, otherwise a dict of outputs.
+
+    ``StepCallback`` (not a reference option) is called as f(t, p) with the
+    pressure field after every time step t, for tests that need the field
+    history.
     """
+    step_callback = opts.pop("StepCallback", None)
     dim = kgrid.dim
     if dim not in (2, 3):
         raise ValueError("only 2D and 3D are restated")
@@ -869,6 +874,8 @@ def kspace_first_order(kgrid, medium, source, sensor, **opts):
                 u[i] = np.broadcast_to(u[i], shape).copy()
 
         p_k = fftn(p)
+        if step_callback is not None:
+            step_callback(t, p)
 
         # sensors (extractSensorData.m)
         if use_sensor and not time_rev and t >= record_start:
