@@ -19,6 +19,7 @@ from __future__ import annotations
 
 import ctypes as C
 import math
+import os
 
 import numpy as np
 
@@ -69,6 +70,39 @@ def _pick(values, dim):
     return [v[0], v[int(math.ceil((len(v) + 1) / 2)) - 1], v[-1]]
 
 
+# Full-grid host passes (masks, FP32 conversion, reductions) run over slabs
+# of the first axis in a few threads: NumPy releases the GIL inside them.
+_POOL = None
+_PAR_MIN = 1 << 20
+
+
+def _pool():
+    global _POOL
+    if _POOL is None:
+        import concurrent.futures
+        _POOL = concurrent.futures.ThreadPoolExecutor(max_workers=max(1, min(8, os.cpu_count() or 1)))
+    return _POOL
+
+
+def _slabs(a):
+    n0 = a.shape[0]
+    k = max(1, min(n0, 4 * _pool()._max_workers))
+    edges = np.linspace(0, n0, k + 1).astype(int)
+    return [slice(int(lo), int(hi)) for lo, hi in zip(edges[:-1], edges[1:]) if hi > lo]
+
+
+def _par(fn, a, combine):
+    """combine([fn(a[s]) for slabs s]) with the slabs in parallel (small arrays inline)."""
+    a = np.asarray(a)
+    if a.ndim == 0 or a.size < _PAR_MIN:
+        return combine([fn(a)])
+    return combine(list(_pool().map(lambda s: fn(a[s]), _slabs(a))))
+
+
+def _any(fn, a):
+    return _par(lambda x: bool(np.any(fn(x))), a, any)
+
+
 def _find(mask):
     """MATLAB find(mask ~= 0): 0-based column-major indices, increasing.
 
@@ -77,7 +111,11 @@ def _find(mask):
     m = np.asarray(mask)
     if m.ndim < 2:
         return np.flatnonzero(m)
-    nz = np.flatnonzero(m)
+    if m.size >= _PAR_MIN:
+        stride = m.size // m.shape[0]
+        nz = np.concatenate(list(_pool().map(lambda s: np.flatnonzero(m[s] != 0) + s.start * stride, _slabs(m))))
+    else:
+        nz = np.flatnonzero(m)
     f = np.ravel_multi_index(np.unravel_index(nz, m.shape), m.shape, order="F")
     f.sort()
     return f
@@ -92,7 +130,15 @@ def _at(a, fidx):
 def _grid32(a):
     """A grid-sized array as FP32 in row-major (C) order, the layout the
     library transposes on the device (KW_ROW_MAJOR)."""
-    return np.ascontiguousarray(a, dtype=np.float32)
+    a = np.asarray(a)
+    if a.ndim == 0 or a.size < _PAR_MIN or (a.dtype == np.float32 and a.flags.c_contiguous):
+        return np.ascontiguousarray(a, dtype=np.float32)
+    out = np.empty(a.shape, dtype=np.float32)
+
+    def conv(sl):
+        out[sl] = a[sl]
+    list(_pool().map(conv, _slabs(a)))
+    return out
 
 
 def _f32(a):
@@ -179,7 +225,7 @@ def _prepare(dim, kgrid, medium, source, sensor, options):
             if alpha_power == 1 and alpha_mode != "no_dispersion":
                 raise KWaveInputError("The power law dispersion term in the equation of state is not valid "
                                       "for medium.alpha_power = 1.")
-        if np.any(alpha_coeff < 0):
+        if _any(lambda x: x < 0, alpha_coeff):
             raise KWaveInputError("medium.alpha_coeff must be non-negative and real.")
         if _has(medium, "alpha_filter"):
             raise KWaveInputError("medium.alpha_filter is not supported by this solver.")
@@ -195,9 +241,9 @@ def _prepare(dim, kgrid, medium, source, sensor, options):
     BonA = np.asarray(_field(medium, "BonA"), dtype=np.float64) if nonlinear else None
     cref = _field(medium, "sound_speed_ref")
     if cref is None or (isinstance(cref, str) and cref == "max"):
-        c_ref = float(c0.max())
+        c_ref = float(_par(np.max, c0, max))
     elif isinstance(cref, str) and cref == "min":
-        c_ref = float(c0.min())
+        c_ref = float(_par(np.min, c0, min))
     elif isinstance(cref, str) and cref == "mean":
         c_ref = float(c0.mean())
     elif isinstance(cref, str):
@@ -247,9 +293,9 @@ def _prepare(dim, kgrid, medium, source, sensor, options):
             raise KWaveInputError("The field sensor.mask must be defined.")
         m = np.asarray(_field(sensor, "mask"), dtype=np.float64)
         if m.shape == kgrid.shape:
-            if np.any((m != 0) & (m != 1)):
+            if _any(lambda x: (x != 0) & (x != 1), m):
                 raise KWaveInputError("sensor.mask must be a binary grid (numeric values must be 0 or 1).")
-            if not np.any(m):
+            if not _any(lambda x: x, m):
                 raise KWaveInputError("sensor.mask must be a binary grid with at least one element set to 1.")
             mask = m
         elif m.ndim == 2 and m.shape[0] == 2 * dim:
@@ -278,7 +324,7 @@ def _prepare(dim, kgrid, medium, source, sensor, options):
 
     # ---- source (inputChecking.m:713-1220) ----
     p0 = _field(source, "p0")
-    source_p0 = p0 is not None and np.size(p0) > 0 and np.any(np.asarray(p0) != 0)
+    source_p0 = p0 is not None and np.size(p0) > 0 and _any(lambda x: x != 0, p0)
     if source_p0:
         p0 = np.asarray(p0, dtype=np.float64)
         if p0.shape != kgrid.shape:
@@ -290,7 +336,7 @@ def _prepare(dim, kgrid, medium, source, sensor, options):
         pm = np.asarray(_field(source, "p_mask"))
         if pm.shape != kgrid.shape:
             raise KWaveInputError("source.p_mask must be the same size as the computational grid.")
-        if not np.any(pm):
+        if not _any(lambda x: x, pm):
             raise KWaveInputError("source.p_mask must be a binary grid with at least one element set to 1.")
         if source_p0:
             raise KWaveInputError("source.p0 and source.p can't be defined in the same simulation.")
@@ -309,7 +355,7 @@ def _prepare(dim, kgrid, medium, source, sensor, options):
         um = np.asarray(_field(source, "u_mask"))
         if um.shape != kgrid.shape:
             raise KWaveInputError("source.u_mask must be the same size as the computational grid.")
-        if not np.any(um):
+        if not _any(lambda x: x, um):
             raise KWaveInputError("source.u_mask must be a binary grid with at least one element set to 1.")
         mode = _field(source, "u_mode", "additive")
         if mode not in _abi.SOURCE_MODES:
