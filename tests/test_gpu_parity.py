@@ -168,3 +168,32 @@ def test_tile_widths_do_not_change_results(name):
         for k in ref:
             assert np.array_equal(out[k], ref[k]), (name, tiles, k)
     sim.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("N", [256, 512])
+def test_full_size_homogeneous_is_exact(N):
+    """At the full sizes, where the FP64 oracle is too slow, a size-independent
+    check: in a homogeneous lossless medium with PMLAlpha = 0 the k-space
+    scheme is exact (kspaceFirstOrder3D.m:23-25), so p_final after Nt steps is
+    IFFT(FFT(p0) cos(c |k| (Nt - 1) dt)), evaluated here with an FP64 real FFT.
+    Tolerance: 1e-4 relative L2, as for every parity test."""
+    import scipy.fft as sfft
+    import kwave_b200 as kw
+    dx, c, Nt = 1e-4, 1500.0, 20
+    dt = 0.3 * dx / c
+    ax = np.arange(N) - N / 2
+    r2 = ax[:, None, None] ** 2 + ax[None, :, None] ** 2 + ax[None, None, :] ** 2
+    p0 = np.exp(-r2 / (2 * 6.0 ** 2))
+    kg = kw.kWaveGrid(N, dx, N, dx, N, dx)
+    kg.setTime(Nt, dt)
+    out = kw.kspaceFirstOrder3D(kg, {"sound_speed": c, "density": 1000.0}, {"p0": p0}, {"record": ["p_final"]},
+                                PMLAlpha=0.0, PMLSize=10, Smooth=False)
+    k = 2 * np.pi * sfft.fftfreq(N, dx)
+    kz = 2 * np.pi * sfft.rfftfreq(N, dx)
+    kmag = np.sqrt(k[:, None, None] ** 2 + k[None, :, None] ** 2 + kz[None, None, :] ** 2)
+    spec = sfft.rfftn(p0, workers=-1)
+    spec *= np.cos(c * kmag * (Nt - 1) * dt)
+    exact = sfft.irfftn(spec, s=p0.shape, workers=-1)
+    err = float(np.linalg.norm((out["p_final"] - exact).ravel()) / np.linalg.norm(exact.ravel()))
+    assert err <= TOL, "N=%d rel-L2 %.3e" % (N, err)
