@@ -34,6 +34,19 @@ struct Geom {
 
 struct Spec4 { float2 *p[4]; };
 
+// Element i of a small kernel-parameter array, read with constant indices
+// only.  A run-time index into a parameter array makes every thread copy the
+// whole parameter struct to local memory at kernel start; a chain of selects
+// reads the parameter bank directly.
+template <class T, int K>
+__device__ __forceinline__ T pick(const T (&a)[K], int i) {
+    T r = a[0];
+#pragma unroll
+    for (int k = 1; k < K; ++k)
+        if (i == k) r = a[k];
+    return r;
+}
+
 // Tile transform in the interleaved layout (element (l, i) at s[i*nl + l]):
 // compile-time plan when the axis length N is a template argument, the
 // runtime radix loop otherwise (N == 0).

@@ -194,7 +194,7 @@ __global__ void __launch_bounds__(ks_threads(N1, TY), 3 * kThreads / ks_threads(
     constexpr int NT = ks_threads(N1, TY);
     static_assert(RPlan<N1, false>::M >= 2, "in-place pass needs two stages");
     __shared__ float2 sm[N1 * TY];
-    float2 *buf = bufs.p[blockIdx.z];
+    float2 *buf = pick(bufs.p, blockIdx.z);
     const int x0 = blockIdx.x * TY;
     const long long base = (long long)(blockIdx.y + kz0) * N1 * g.N0 + x0;
     const int N0 = g.N0;
@@ -231,7 +231,7 @@ __global__ void __launch_bounds__(ks_threads(N0, NL), 3 * kThreads / ks_threads(
         kyz2[l] = __ldg(P.k2[1] + iy) + __ldg(P.k2[2] + iz);
     }
     __syncthreads();
-    const float2 *in = bufs.p[f] + (long long)line0 * N0;
+    const float2 *in = pick(bufs.p, f) + (long long)line0 * N0;
     auto ld = [&](int, int, int l, int i) -> float2 {
         return line0 + l < lines_total ? in[l * N0 + i] : make_float2(0.f, 0.f);
     };
@@ -241,7 +241,7 @@ __global__ void __launch_bounds__(ks_threads(N0, NL), 3 * kThreads / ks_threads(
     rs_fft<N0, NL, false, false, 0, NT>(sm, tw, ld, keep);
 
     // common factor of the operator (kappa, |k|^e or cos), times 1/N
-    const int kind0 = ops.kind[f];
+    const int kind0 = pick(ops.kind, f);
     const bool grad = kind0 == OP_GRAD_POS || kind0 == OP_GRAD_NEG;
 #pragma unroll
     for (int b = 0; b < SH::MAXB; ++b) {
@@ -272,11 +272,12 @@ __global__ void __launch_bounds__(ks_threads(N0, NL), 3 * kThreads / ks_threads(
     const int nout = fanout ? ops.n : 1;
     for (int o = 0; o < nout; ++o) {
         const int oi = fanout ? o : f;
-        const int axis = ops.axis[oi];
-        const int ko = ops.kind[oi];
-        const float2 *dd = ko == OP_GRAD_POS ? P.dd_pos[axis] : (ko == OP_GRAD_NEG ? P.dd_neg[axis] : P.sh_neg[axis]);
+        const int axis = pick(ops.axis, oi);
+        const int ko = pick(ops.kind, oi);
+        const float2 *dd = ko == OP_GRAD_POS ? pick(P.dd_pos, axis)
+                                             : (ko == OP_GRAD_NEG ? pick(P.dd_neg, axis) : pick(P.sh_neg, axis));
         const bool mul_dd = ko == OP_GRAD_POS || ko == OP_GRAD_NEG || ko == OP_SHIFT_NEG;
-        float2 *out = bufs.p[oi] + (long long)line0 * N0;
+        float2 *out = pick(bufs.p, oi) + (long long)line0 * N0;
         auto ld2 = [&](int b, int t, int l, int i) -> float2 {
             if (!mul_dd) return spec[b][t];
             const int idx = axis == 0 ? i : (axis == 1 ? liy[l] : liz[l]);
@@ -761,7 +762,7 @@ __global__ void __launch_bounds__(ks_threads(N2, PL), 2 * kThreads / ks_threads(
         for (int b = 0; b < SH::MAXB; ++b)
 #pragma unroll
             for (int tt = 0; tt < SH::R; ++tt) src[b][tt] = term == 0 ? acc_d[b][tt] : acc_r[b][tt];
-        zforward_store<N2, PL>(sm, tw, src, a.spec.p[out++], g, x0, y);
+        zforward_store<N2, PL>(sm, tw, src, pick(a.spec.p, out++), g, x0, y);
     }
 }
 
