@@ -260,7 +260,7 @@ __global__ void __launch_bounds__(ks_threads(N0, NL), 3 * kThreads / ks_threads(
                 fac = P.use_kspace ? sinc_series(P.kappa_a * P.kappa_a * k2) : 1.f;
             } else if (kind0 == OP_NABLA1 || kind0 == OP_NABLA2) {
                 const float e = kind0 == OP_NABLA1 ? P.nabla1_exp : P.nabla2_exp;
-                fac = k2 == 0.f ? (e > 0.f ? 0.f : (e == 0.f ? 1.f : 0.f)) : powf(k2, 0.5f * e);
+                fac = k2 == 0.f ? (e > 0.f ? 0.f : (e == 0.f ? 1.f : 0.f)) : pow_pos(k2, 0.5f * e);
             } else if (kind0 == OP_SRC_KAPPA) {
                 fac = P.use_kspace ? cos_series(P.kappa_a * P.kappa_a * k2) : 1.f;
             } else {
@@ -718,8 +718,8 @@ __global__ void __launch_bounds__(ks_threads(N2, PL), 2 * kThreads / ks_threads(
                     // next step's mass coefficient q = 2 sum(rho) + rho0
                     *reinterpret_cast<float2 *>(a.srho + gi) = make_float2(fmaf(2.f, sr.x, r0.x), fmaf(2.f, sr.y, r0.y));
                     const float2 bn = med2(a.BonA, gi, true, true);
-                    pv.x += bn.x * sr.x * sr.x / (2.f * r0.x);
-                    pv.y += bn.y * sr.y * sr.y / (2.f * r0.y);
+                    pv.x += bona_term(bn.x, sr.x, r0.x);
+                    pv.y += bona_term(bn.y, sr.y, r0.y);
                 }
                 pv.x *= c.x * c.x;
                 pv.y *= c.y * c.y;
