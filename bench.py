@@ -102,6 +102,70 @@ def workload2d(seed=0, N=256, Nt=500, dx=0.1e-3, pml=10, absorbing=True):
                 sensor={"mask": sensor_mask, "record": ["p", "p_max"]}, options={"PMLSize": pml}, src_len=0)
 
 
+# Layered medium of the large 512^3 simulation: sound speed per layer (the
+# recipe's 1480 / 1560 / 2800 / 1560 m/s), density tied to speed as in the
+# blob medium, alpha_power 1.1.  The recipe gives no absorption coefficient;
+# these per-layer values (dB/(MHz^y cm)) are this benchmark's choice.
+LAYER_C = (1480.0, 1560.0, 2800.0, 1560.0)
+LAYER_ALPHA = (0.5, 1.0, 4.0, 1.0)
+
+
+def rough_surface(n0, n1, rng, rms=3.0, corr=8.0):
+    """Random interface height (cells) over an n0 x n1 plane: white noise
+    low-passed by a Gaussian of `corr` cells, scaled to `rms` cells RMS."""
+    k0 = np.fft.fftfreq(n0)[:, None]
+    k1 = np.fft.fftfreq(n1)[None, :]
+    filt = np.exp(-2.0 * (np.pi * corr) ** 2 * (k0 ** 2 + k1 ** 2))
+    h = np.real(np.fft.ifft2(np.fft.fft2(rng.standard_normal((n0, n1))) * filt))
+    return h * (rms / h.std())
+
+
+def focused_burst(t, delay, f0, cycles, amp):
+    """amp sin(2 pi f0 tau) times a Hann window over `cycles` periods,
+    tau = t - delay, zero outside the window (one row per delay)."""
+    T = cycles / f0
+    tau = t[None, :] - delay[:, None]
+    inside = (tau >= 0) & (tau <= T)
+    return np.where(inside, amp * np.sin(2 * np.pi * f0 * tau) * (0.5 - 0.5 * np.cos(2 * np.pi * tau / T)), 0.0)
+
+
+def layered_workload(seed=0, N=512, Nt=2000, dx=0.1e-3, pml=20, f0=500e3, cycles=5, focus=300, src=128,
+                     amp=1e6):
+    """Large single 3-D simulation: four layers along x with rough interfaces
+    (3-cell RMS), alpha_power 1.1, B/A drawn from 5..9 per layer, a src x src
+    phased plane pressure source at x = pml (0-based) focused `focus` cells
+    deep by per-element delays, a Hann-windowed `cycles`-cycle burst at f0,
+    and full-volume p_max / p_rms (the mask is every cell)."""
+    rng = np.random.default_rng(seed)
+    shape = (N, N, N)
+    x = np.arange(N, dtype=np.float64)[:, None, None]
+    layer = np.zeros(shape, dtype=np.int8)
+    for k in (1, 2, 3):
+        depth = pml + (N - 2 * pml) * k / 4.0
+        layer += (x >= (depth + rough_surface(N, N, rng))[None, :, :]).astype(np.int8)
+    c = np.asarray(LAYER_C)[layer]
+    bona = rng.integers(5, 10, size=4).astype(np.float64)
+    medium = {"sound_speed": c, "density": 1000.0 + 0.6 * (c - 1500.0),
+              "alpha_coeff": np.asarray(LAYER_ALPHA)[layer], "alpha_power": 1.1, "BonA": bona[layer]}
+    del layer
+    dt = 0.3 * dx / c.max()
+    h = N // 2
+    lo, hi = h - src // 2, h - src // 2 + src
+    p_mask = np.zeros(shape, dtype=bool)
+    p_mask[pml, lo:hi, lo:hi] = True
+    # source points in find(p_mask) order (column-major: y fastest, then z)
+    zz, yy = np.meshgrid(np.arange(lo, hi), np.arange(lo, hi), indexing="ij")
+    dist = dx * np.sqrt(focus ** 2 + (yy.ravel() - h) ** 2 + (zz.ravel() - h) ** 2)
+    delay = (dist.max() - dist) / LAYER_C[0]
+    # the signal ends with the last element's burst (the source is active
+    # only while it has samples)
+    src_len = int(min(Nt, math.ceil((delay.max() + cycles / f0) / dt) + 1))
+    sig = focused_burst(np.arange(src_len) * dt, delay, f0, cycles, amp)
+    sensor = {"mask": np.ones(shape, dtype=bool), "record": ["p_max", "p_rms"]}
+    return dict(shape=shape, dx=dx, Nt=Nt, dt=dt, medium=medium, source={"p_mask": p_mask, "p": sig},
+                sensor=sensor, options={"PMLSize": pml}, src_len=src_len)
+
+
 def make_grid(kw, w):
     if len(w["shape"]) == 2:
         g = kw.kWaveGrid(w["shape"][0], w["dx"], w["shape"][1], w["dx"])
@@ -451,6 +515,42 @@ def tr_check(kw, N=256, n_elem=128, radius=110, Nt=1500, dx=0.1e-3, seed=5):
                               r, g_adj, inside)
 
 
+LARGE_BYTES_PER_CELL_STEP = 164.0   # 4 B x (6 + 7 state + 8 medium + 2 x 8 spectral + 4 full-volume accumulators)
+
+
+def large_section(kw, device, N=512, Nt=200, seed=11):
+    """The large layered simulation (512^3, full-volume p_max / p_rms) at a
+    reduced number of time steps: one warm-up and one timed simulation with
+    every input resident, per-class device times from a third run."""
+    t0 = time.perf_counter()
+    w = layered_workload(seed=seed, N=N, Nt=Nt)
+    cells = float(np.prod(w["shape"]))
+    with kw.Simulation(3, make_grid(kw, w), w["medium"], w["source"], w["sensor"], **dict(w["options"], DeviceNum=device)) as sim:
+        setup_s = time.perf_counter() - t0
+        dev_gb = sim.device_bytes() / 1e9
+        sim.run_timed(1)
+        ms = sim.run_timed(1)
+        classes = {}
+        sim.set_timing(["zstage_u", "zstage_r", "zstage_p", "ypass", "xpass", "sensor", "source"])
+        sim.run_device()
+        for c in ("zstage_u", "zstage_r", "zstage_p", "ypass", "xpass", "sensor", "source"):
+            classes[c] = round(sim.timing(c)[0] / Nt * 1e3, 1)
+        sim.set_timing([])
+    peak, peak_kind = measured_peak()
+    src_steps = min(w["src_len"], Nt)
+    alg = cells * (LARGE_BYTES_PER_CELL_STEP * Nt + BYTES_PER_CELL_SRC_STEP * src_steps)
+    achieved = alg / (ms / 1e3) / 1e9
+    return {"workload": "kspaceFirstOrder3D %d^3 layered 1480/1560/2800/1560 m/s (rough interfaces, 3-cell RMS), "
+                        "alpha_power 1.1, per-layer alpha_coeff %s dB/(MHz^y cm) and BonA 5..9, 128x128 phased plane "
+                        "p source focused 300 cells deep, 500 kHz 5-cycle burst, PML 20, full-volume p_max + p_rms"
+                        % (N, "/".join("%g" % a for a in LAYER_ALPHA)),
+            "Nt": Nt, "source_steps": src_steps, "value": cells * Nt / (ms / 1e3) / 1e9, "unit": UNIT,
+            "ms_per_time_step": ms / Nt, "device_gb": round(dev_gb, 2), "host_setup_s": round(setup_s, 1),
+            "roofline": {"achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                         "peak_source": peak_kind, "alg_bytes_per_cell_step": LARGE_BYTES_PER_CELL_STEP},
+            "us_per_time_step": classes}
+
+
 def adjoint_section(kw, device, Nt=3000, n_shots=16, fd_cells=32, seed=4, tr=True):
     """Gradient of J = 1/2 sum over shots of |p(ring) - d|^2 at the homogeneous
     starting model (16 shots, Nt steps, sqrt(Nt) checkpointing), timed per
@@ -532,6 +632,7 @@ def main():
     ap.add_argument("--serve-requests", type=int, default=48, help="0 skips the served-stream section")
     ap.add_argument("--adjoint-shots", type=int, default=16, help="0 skips the adjoint section")
     ap.add_argument("--adjoint-fd", type=int, default=32, help="finite-difference cells of the adjoint check")
+    ap.add_argument("--large-Nt", type=int, default=200, help="time steps of the 512^3 layered run (0 skips it)")
     args = ap.parse_args()
     ws, rank, local = dist_setup()
     if args.impl == "reference":
@@ -618,6 +719,10 @@ def main():
     if args.adjoint_shots > 0:
         adjoint = adjoint_section(kw, local, n_shots=args.adjoint_shots, fd_cells=args.adjoint_fd, seed=4 + rank)
 
+    large = None
+    if args.large_Nt > 0:
+        large = large_section(kw, local, Nt=args.large_Nt, seed=11 + rank)
+
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu:
         try:
@@ -638,7 +743,8 @@ def main():
                            "l2": "no flush: inputs larger than L2 (device working set %.2f GB vs 126 MB L2)" % dev_gb,
                            "parallelism": "replicas x%d" % ws},
                 "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
-                "clocks": clocks, "kernel_classes": classes, "served": served, "adjoint": adjoint}
+                "clocks": clocks, "kernel_classes": classes, "served": served, "adjoint": adjoint,
+                "large_512": large}
         print(json.dumps(line), flush=True)
     if ws > 1:
         import torch.distributed as dist

@@ -853,7 +853,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_zc2r(const float2 *__restrict__
 struct SensorArgs {
     int M;
     int K;                     // grid cells per point (> 1: weighted, column-major M x K)
-    const long long *idx;      // 0-based linear indices
+    const long long *idx;      // 0-based linear indices; NULL: every cell, in order
     const float *w;            // weights (K > 1)
     const float *field[4];     // p, u0, u1, u2
     float *series[4];          // [M x num_rec] or NULL
@@ -863,10 +863,11 @@ struct SensorArgs {
     const int *d_t;
 };
 
-// one sensor point: field at its cell, or sum_k w[m + M k] field[idx[m + M k]]
+// one sensor point: field at its cell, or sum_k w[m + M k] field[idx[m + M k]];
+// idx NULL: the mask holds every cell, so point m is cell m
 __device__ __forceinline__ float sensor_value(const float *field, const long long *idx, const float *w, int M, int K,
                                               int m) {
-    if (K <= 1) return field[idx[m]];
+    if (K <= 1) return field[idx ? idx[m] : m];
     float v = 0.f;
     for (int k = 0; k < K; ++k) v = fmaf(w[m + (long long)M * k], field[idx[m + (long long)M * k]], v);
     return v;
@@ -878,13 +879,51 @@ __global__ void k_sensor(SensorArgs a) {
     const int t = *a.d_t;
     const int fi = t - a.record_start;   // 0-based column
     if (fi < 0) return;
-    for (int f = 0; f < a.nfield; ++f) {
-        if (!a.field[f]) continue;
+    // unrolled: constant indices into the parameter arrays
+#pragma unroll
+    for (int f = 0; f < 4; ++f) {
+        if (f >= a.nfield || !a.field[f]) continue;
         const float v = sensor_value(a.field[f], a.idx, a.w, a.M, a.K, m);
         if (a.series[f]) a.series[f][m + (long long)a.M * fi] = v;
         if (a.vmax[f]) a.vmax[f][m] = fi == 0 ? v : fmaxf(a.vmax[f][m], v);
         if (a.vmin[f]) a.vmin[f][m] = fi == 0 ? v : fminf(a.vmin[f][m], v);
         if (a.vsq[f]) a.vsq[f][m] = fi == 0 ? v * v : fmaf(v, v, a.vsq[f][m]);
+    }
+}
+
+// The same for a mask that holds every cell (point m is cell m): four
+// consecutive points per thread with 16-byte loads and stores, so each thread
+// keeps four times the bytes in flight.  Needs M % 4 == 0 (every array then
+// starts each column on a 16-byte boundary).
+__global__ void k_sensor_all(SensorArgs a) {
+    const long long m = 4 * ((long long)blockIdx.x * blockDim.x + threadIdx.x);
+    if (m >= a.M) return;
+    const int t = *a.d_t;
+    const int fi = t - a.record_start;
+    if (fi < 0) return;
+#pragma unroll
+    for (int f = 0; f < 4; ++f) {
+        if (f >= a.nfield || !a.field[f]) continue;
+        const float4 v = *reinterpret_cast<const float4 *>(a.field[f] + m);
+        if (a.series[f]) *reinterpret_cast<float4 *>(a.series[f] + m + (long long)a.M * fi) = v;
+        if (a.vmax[f]) {
+            float4 *q = reinterpret_cast<float4 *>(a.vmax[f] + m);
+            if (fi == 0) *q = v;
+            else { const float4 o = *q; *q = make_float4(fmaxf(o.x, v.x), fmaxf(o.y, v.y), fmaxf(o.z, v.z), fmaxf(o.w, v.w)); }
+        }
+        if (a.vmin[f]) {
+            float4 *q = reinterpret_cast<float4 *>(a.vmin[f] + m);
+            if (fi == 0) *q = v;
+            else { const float4 o = *q; *q = make_float4(fminf(o.x, v.x), fminf(o.y, v.y), fminf(o.z, v.z), fminf(o.w, v.w)); }
+        }
+        if (a.vsq[f]) {
+            float4 *q = reinterpret_cast<float4 *>(a.vsq[f] + m);
+            if (fi == 0) *q = make_float4(v.x * v.x, v.y * v.y, v.z * v.z, v.w * v.w);
+            else {
+                const float4 o = *q;
+                *q = make_float4(fmaf(v.x, v.x, o.x), fmaf(v.y, v.y, o.y), fmaf(v.z, v.z, o.z), fmaf(v.w, v.w, o.w));
+            }
+        }
     }
 }
 
@@ -911,8 +950,9 @@ __global__ void k_region(RegionArgs a) {
         const int i1 = q % a.n[1];
         const int i2 = q / a.n[1];
         const long long gi = (i0 + a.lo[0]) + (long long)a.g.N0 * ((i1 + a.lo[1]) + (long long)a.g.N1 * (i2 + a.lo[2]));
-        for (int f = 0; f < a.nfield; ++f) {
-            if (!a.field[f]) continue;
+#pragma unroll
+        for (int f = 0; f < 4; ++f) {
+            if (f >= a.nfield || !a.field[f]) continue;
             const float v = a.field[f][gi];
             if (a.vmax[f]) a.vmax[f][r] = fi == 0 ? v : fmaxf(a.vmax[f][r], v);
             if (a.vmin[f]) a.vmin[f][r] = fi == 0 ? v : fminf(a.vmin[f][r], v);

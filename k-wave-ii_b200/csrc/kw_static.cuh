@@ -172,28 +172,36 @@ __device__ __forceinline__ float cos_series(float a2) {
     return r;
 }
 
-// Tile widths of the compile-time kernels: as many lines as fill one
-// 4096-element tile, so every thread owns one radix-R butterfly.
-__host__ __device__ constexpr int ks_lines(int n) {
+// Tile widths of the compile-time kernels.  x-pass: as many lines as fill
+// one 4096-element tile of 256 threads, so every thread owns one radix-R
+// butterfly (the lines are contiguous rows, so the width does not change how
+// HBM is accessed).
+__host__ __device__ constexpr int ks_xlines(int n) {
     return pow2_floor(kCap / n) < 64 ? pow2_floor(kCap / n) : 64;
 }
-// Narrower tiles (pl < ks_lines(n) lines, for grids too small to fill the
-// GPU with full tiles) keep the per-thread share of a full tile, so the block
-// shrinks with the tile: ks_threads(n, pl) threads.
-__host__ __device__ constexpr int ks_threads(int n, int pl) { return kThreads * pl / ks_lines(n); }
-// the narrow tile width used when full tiles give less than one wave of blocks
+// z-stages and y-pass, whose tile width is the length of every row segment
+// they move: the same, except that 512-point axes take 16 lines (8192
+// elements, 512 threads) so that rows of real fields are 64 bytes and rows of
+// spectra 128 bytes, not half that.
+__host__ __device__ constexpr int ks_lines(int n) { return n == 512 ? 16 : ks_xlines(n); }
+// Narrower tiles (pl lines, for grids too small to fill the GPU with full
+// tiles) keep the per-thread share of a full tile, so the block shrinks with
+// the tile: ks_threads(n, pl) threads.
+__host__ __device__ constexpr int ks_threads(int n, int pl) { return kThreads * pl / ks_xlines(n); }
+// the narrow tile widths used when full tiles give less than one wave of blocks
 __host__ __device__ constexpr int ks_narrow(int n) { return ks_lines(n) / 4; }
+__host__ __device__ constexpr int ks_xnarrow(int n) { return ks_xlines(n) / 4; }
 
 // ---------------------------------------------------------------------------
 // y-pass (C2C along axis 1, in place).  grid = (ceil(N0/TY), N2h, nfields),
-// ks_threads(N1, TY) threads
+// ks_threads(N1, TY) threads, N1 * TY float2 of dynamic shared memory
 // ---------------------------------------------------------------------------
 template <bool INV, int N1, int TY>
-__global__ void __launch_bounds__(ks_threads(N1, TY), 3 * kThreads / ks_threads(N1, TY))
+__global__ void __launch_bounds__(ks_threads(N1, TY), (4 * kThreads + ks_threads(N1, TY) - 1) / ks_threads(N1, TY))
     ks_ypass(Spec4 bufs, Geom g, const float2 *__restrict__ tw, int kz0) {
     constexpr int NT = ks_threads(N1, TY);
     static_assert(RPlan<N1, false>::M >= 2, "in-place pass needs two stages");
-    __shared__ float2 sm[N1 * TY];
+    extern __shared__ float2 sm[];   // N1 * TY
     float2 *buf = pick(bufs.p, blockIdx.z);
     const int x0 = blockIdx.x * TY;
     const long long base = (long long)(blockIdx.y + kz0) * N1 * g.N0 + x0;
@@ -870,7 +878,7 @@ __global__ void __launch_bounds__(ks_threads(N2, PL), 2 * kThreads / ks_threads(
 }
 
 // ---------------------------------------------------------------------------
-// plain z-transforms
+// plain z-transforms (N2 * PL float2 of dynamic shared memory)
 // ---------------------------------------------------------------------------
 template <int N2, int PL>
 __global__ void __launch_bounds__(ks_threads(N2, PL), 2 * kThreads / ks_threads(N2, PL))
@@ -878,7 +886,7 @@ __global__ void __launch_bounds__(ks_threads(N2, PL), 2 * kThreads / ks_threads(
     using ZT = ZTile<N2, PL>;
     using SH = typename ZT::SH;
     constexpr int TX = ZT::TX, NT = ZT::NT;
-    __shared__ float2 sm[N2 * PL];
+    extern __shared__ float2 sm[];   // N2 * PL
     const int x0 = blockIdx.x * TX, y = blockIdx.y;
     float2 hold[SH::MAXB][SH::R];
 #pragma unroll
@@ -901,7 +909,7 @@ __global__ void __launch_bounds__(ks_threads(N2, PL), 2 * kThreads / ks_threads(
     ks_zc2r(const float2 *__restrict__ H, float *R, Geom g, const float2 *__restrict__ tw) {
     using ZT = ZTile<N2, PL>;
     constexpr int TX = ZT::TX, NT = ZT::NT;
-    __shared__ float2 sm[N2 * PL];
+    extern __shared__ float2 sm[];   // N2 * PL
     const int x0 = blockIdx.x * TX, y = blockIdx.y;
     auto ld = [&](int, int, int l, int z) -> float2 { return zpack_load<N2>(H, g, x0, y, l, z); };
     auto st = [&](int, int, int l, int z, float2 v) {

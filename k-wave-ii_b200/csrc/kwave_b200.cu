@@ -177,6 +177,7 @@ struct kw_plan {
     int M = 0;
     int K = 1;                     // grid cells per sensor point (interpolated points: K > 1)
     long long *sidx = nullptr;     // [M x K] column-major
+    bool sidx_all = false;         // the mask holds every cell (sidx[m] == m): gathers read cell m directly
     float *sw = nullptr;           // [M x K] weights (K > 1)
     float *tr_data = nullptr;
     int *tr_off = nullptr, *tr_cell = nullptr, *tr_row = nullptr;
@@ -350,16 +351,23 @@ kw_status dispatch(int n, A... args) {
 // ---- transform passes -----------------------------------------------------
 template <int N> struct YLaunch {
     template <int TY>
-    static void go(kw_plan *P, bool inv, Spec4 bufs, dim3 grid, int kz0) {
+    static kw_status go(kw_plan *P, bool inv, Spec4 bufs, dim3 grid, int kz0) {
         constexpr int NT = ks_threads(N, TY);
-        if (inv) ks_ypass<true, N, TY><<<grid, NT, 0, P->stream>>>(bufs, P->g, P->tw[1], kz0);
-        else ks_ypass<false, N, TY><<<grid, NT, 0, P->stream>>>(bufs, P->g, P->tw[1], kz0);
+        constexpr size_t sh = (size_t)N * TY * sizeof(float2);
+        if (inv) {
+            KW_TRY(set_smem((const void *)ks_ypass<true, N, TY>, sh));
+            ks_ypass<true, N, TY><<<grid, NT, sh, P->stream>>>(bufs, P->g, P->tw[1], kz0);
+        } else {
+            KW_TRY(set_smem((const void *)ks_ypass<false, N, TY>, sh));
+            ks_ypass<false, N, TY><<<grid, NT, sh, P->stream>>>(bufs, P->g, P->tw[1], kz0);
+        }
+        return KW_OK;
     }
     static kw_status run(kw_plan *P, bool inv, Spec4 bufs, int nf, int kz0, int nkz) {
         dim3 grid((P->g.N0 + P->TY - 1) / P->TY, N > 0 ? nkz : P->g.N2h, nf);
         if constexpr (N > 0) {
-            if (P->TY == ks_lines(N)) go<ks_lines(N)>(P, inv, bufs, grid, kz0);
-            else go<ks_narrow(N)>(P, inv, bufs, grid, kz0);
+            if (P->TY == ks_lines(N)) KW_TRY(go<ks_lines(N)>(P, inv, bufs, grid, kz0));
+            else KW_TRY(go<ks_narrow(N)>(P, inv, bufs, grid, kz0));
         } else {
             size_t sh = (size_t)P->TY * P->g.N1 * sizeof(float2);
             if (inv) {
@@ -389,12 +397,12 @@ template <int N> struct XLaunch {
         const int lines = P->g.N1 * (N > 0 ? nkz : P->g.N2h);
         dim3 grid((lines + P->NL - 1) / P->NL, 1, fanout ? 1 : nf);
         if constexpr (N > 0) {
-            if (P->NL == ks_lines(N))
-                ks_xpass<N, ks_lines(N)><<<grid, ks_threads(N, ks_lines(N)), 0, P->stream>>>(bufs, P->g, P->tw[0], P->op,
-                                                                                          ops, fanout, kz0, nkz);
-            else
-                ks_xpass<N, ks_narrow(N)><<<grid, ks_threads(N, ks_narrow(N)), 0, P->stream>>>(bufs, P->g, P->tw[0], P->op,
+            if (P->NL == ks_xlines(N))
+                ks_xpass<N, ks_xlines(N)><<<grid, ks_threads(N, ks_xlines(N)), 0, P->stream>>>(bufs, P->g, P->tw[0], P->op,
                                                                                             ops, fanout, kz0, nkz);
+            else
+                ks_xpass<N, ks_xnarrow(N)><<<grid, ks_threads(N, ks_xnarrow(N)), 0, P->stream>>>(bufs, P->g, P->tw[0],
+                                                                                              P->op, ops, fanout, kz0, nkz);
         } else {
             size_t sh = (size_t)(fanout ? 2 : 1) * P->NL * P->g.N0 * sizeof(float2);
             KW_TRY(set_smem((const void *)k_xpass<0, 0>, sh));
@@ -429,11 +437,18 @@ kw_status yxy_group(kw_plan *P, Spec4 bufs, int n, OpSet ops, bool fanout) {
 }
 
 template <int N> struct ZR2CLaunch {
+    template <int PL>
+    static kw_status go(kw_plan *P, const float *R, float2 *H, dim3 grid) {
+        constexpr size_t sh = (size_t)N * PL * sizeof(float2);
+        KW_TRY(set_smem((const void *)ks_zr2c<N, PL>, sh));
+        ks_zr2c<N, PL><<<grid, ks_threads(N, PL), sh, P->stream>>>(R, H, P->g, P->tw[2]);
+        return KW_OK;
+    }
     static kw_status run(kw_plan *P, const float *R, float2 *H) {
         dim3 grid((P->g.N0 + 2 * P->PL_z - 1) / (2 * P->PL_z), P->g.N1, 1);
         if constexpr (N > 0) {
-            if (P->PL_z == ks_lines(N)) ks_zr2c<N, ks_lines(N)><<<grid, ks_threads(N, ks_lines(N)), 0, P->stream>>>(R, H, P->g, P->tw[2]);
-            else ks_zr2c<N, ks_narrow(N)><<<grid, ks_threads(N, ks_narrow(N)), 0, P->stream>>>(R, H, P->g, P->tw[2]);
+            if (P->PL_z == ks_lines(N)) KW_TRY(go<ks_lines(N)>(P, R, H, grid));
+            else KW_TRY(go<ks_narrow(N)>(P, R, H, grid));
         } else {
             size_t sh = (size_t)P->PL_z * P->g.N2 * sizeof(float2);
             KW_TRY(set_smem((const void *)k_zr2c<0, 0>, sh));
@@ -443,11 +458,18 @@ template <int N> struct ZR2CLaunch {
     }
 };
 template <int N> struct ZC2RLaunch {
+    template <int PL>
+    static kw_status go(kw_plan *P, const float2 *H, float *R, dim3 grid) {
+        constexpr size_t sh = (size_t)N * PL * sizeof(float2);
+        KW_TRY(set_smem((const void *)ks_zc2r<N, PL>, sh));
+        ks_zc2r<N, PL><<<grid, ks_threads(N, PL), sh, P->stream>>>(H, R, P->g, P->tw[2]);
+        return KW_OK;
+    }
     static kw_status run(kw_plan *P, const float2 *H, float *R) {
         dim3 grid((P->g.N0 + 2 * P->PL_z - 1) / (2 * P->PL_z), P->g.N1, 1);
         if constexpr (N > 0) {
-            if (P->PL_z == ks_lines(N)) ks_zc2r<N, ks_lines(N)><<<grid, ks_threads(N, ks_lines(N)), 0, P->stream>>>(H, R, P->g, P->tw[2]);
-            else ks_zc2r<N, ks_narrow(N)><<<grid, ks_threads(N, ks_narrow(N)), 0, P->stream>>>(H, R, P->g, P->tw[2]);
+            if (P->PL_z == ks_lines(N)) KW_TRY(go<ks_lines(N)>(P, H, R, grid));
+            else KW_TRY(go<ks_narrow(N)>(P, H, R, grid));
         } else {
             size_t sh = (size_t)P->PL_z * P->g.N2 * sizeof(float2);
             KW_TRY(set_smem((const void *)k_zc2r<0, 0>, sh));
@@ -714,24 +736,29 @@ kw_status sensors(kw_plan *P, int t) {
         SensorArgs a{};
         a.M = P->M;
         a.K = P->K;
-        a.idx = P->sidx;
+        a.idx = P->sidx_all ? nullptr : P->sidx;
         a.w = P->sw;
         a.nfield = 1 + P->D;
         a.field[0] = P->p;
         for (int i = 0; i < P->D; ++i) a.field[1 + i] = P->u[i];
+        bool any = false;
         for (int f = 0; f < 4; ++f) {
             a.series[f] = P->o_series[f];
             a.vmax[f] = P->o_max[f];
             a.vmin[f] = P->o_min[f];
             a.vsq[f] = P->o_sq[f];
+            // a field without outputs is not read
+            if (!(a.series[f] || a.vmax[f] || a.vmin[f] || a.vsq[f])) a.field[f] = nullptr;
+            any = any || a.field[f];
         }
-        bool any = false;
-        for (int f = 0; f < 4; ++f) any = any || a.series[f] || a.vmax[f] || a.vmin[f] || a.vsq[f];
         if (any) {
             Scope s(P, KW_KCLASS_SENSOR);
             a.record_start = P->record_start;
             a.d_t = P->d_t;
-            k_sensor<<<(P->M + 255) / 256, 256, 0, P->stream>>>(a);
+            if (P->sidx_all && P->M % 4 == 0)
+                k_sensor_all<<<(P->M / 4 + 255) / 256, 256, 0, P->stream>>>(a);
+            else
+                k_sensor<<<(P->M + 255) / 256, 256, 0, P->stream>>>(a);
             KW_TRY(launched(P));
         }
         if (P->o_uns[0]) {
@@ -753,7 +780,8 @@ kw_status sensors(kw_plan *P, int t) {
                     src = P->ush;
                 }
                 Scope s(P, KW_KCLASS_SENSOR);
-                k_gather_series<<<(P->M + 255) / 256, 256, 0, P->stream>>>(src, P->sidx, P->sw, P->M, P->K, P->o_uns[i],
+                k_gather_series<<<(P->M + 255) / 256, 256, 0, P->stream>>>(src, P->sidx_all ? nullptr : P->sidx,
+                                                                          P->sw, P->M, P->K, P->o_uns[i],
                                                                           P->d_t, P->record_start);
                 KW_TRY(launched(P));
             }
@@ -1012,8 +1040,8 @@ void plan_tiles(kw_plan *P) {
     const int lines = g.N1 * g.N2h;
     P->static_x = is_static(g.N0);
     if (P->static_x) {
-        P->NL = ks_lines(g.N0);
-        if ((lines + P->NL - 1) / P->NL < kWave) P->NL = ks_narrow(g.N0);
+        P->NL = ks_xlines(g.N0);
+        if ((lines + P->NL - 1) / P->NL < kWave) P->NL = ks_xnarrow(g.N0);
     } else {
         P->NL = std::max(1, kCap / g.N0);
         if (P->NL > lines) P->NL = lines;
@@ -1110,7 +1138,7 @@ kw_status autotune_tiles(kw_plan *P) {
         TileChoice c = best;
         if (cls == 0 && tune_z) c.PL = flip(c.PL, ks_lines(g.N2), ks_narrow(g.N2));
         else if (cls == 1 && tune_y) c.TY = flip(c.TY, ks_lines(g.N1), ks_narrow(g.N1));
-        else if (cls == 2 && tune_x) c.NL = flip(c.NL, ks_lines(g.N0), ks_narrow(g.N0));
+        else if (cls == 2 && tune_x) c.NL = flip(c.NL, ks_xlines(g.N0), ks_xnarrow(g.N0));
         else continue;
         set_tiles(P, c);
         float ms = 0.f;
@@ -1431,6 +1459,8 @@ kw_status create(const kw_problem *pr, kw_plan *P) {
             idx[m] = (long long)v - 1;
         }
         KW_TRY(pupload(P, &P->sidx, idx.data(), idx.size()));
+        // increasing indices in [0, N) number N only when they are 0 .. N-1
+        P->sidx_all = P->K == 1 && (long long)P->M == g.N;
         if (P->K > 1) KW_TRY(pupload(P, &P->sw, q.sensor_weights, MK));
         if (P->time_rev) {
             KW_TRY(pupload(P, &P->tr_data, q.time_reversal_input, (size_t)P->M * P->Nt));
@@ -1912,7 +1942,8 @@ kw_status kw_set_tiles(kw_plan *P, const int32_t tiles[3]) {
     auto ok = [](int v, int n) { return v == ks_lines(n) || v == ks_narrow(n); };
     if (P->static_z && !ok(tiles[0], g.N2)) return fail(KW_ERR_INVALID, "z tile width must be %d or %d", ks_lines(g.N2), ks_narrow(g.N2));
     if (P->static_y && !ok(tiles[1], g.N1)) return fail(KW_ERR_INVALID, "y tile width must be %d or %d", ks_lines(g.N1), ks_narrow(g.N1));
-    if (P->static_x && !ok(tiles[2], g.N0)) return fail(KW_ERR_INVALID, "x tile width must be %d or %d", ks_lines(g.N0), ks_narrow(g.N0));
+    if (P->static_x && tiles[2] != ks_xlines(g.N0) && tiles[2] != ks_xnarrow(g.N0))
+        return fail(KW_ERR_INVALID, "x tile width must be %d or %d", ks_xlines(g.N0), ks_xnarrow(g.N0));
     const bool z_fixed = P->time_rev || (P->psrc.present && !P->psrc.dense_fast && !P->psrc.dense_general) ||
                          (P->usrc.present && !P->usrc.dense_fast && !P->usrc.dense_general);
     if (P->static_z && z_fixed && tiles[0] != P->PL_z)

@@ -180,13 +180,20 @@ def make_case(name):
         med = {"sound_speed": c, "density": rho, "alpha_coeff": 0.5, "alpha_power": 1.5}
         return 3, shape, dx, 60, 0.3 * dx / c.max(), med, {"p0": disc_p0(shape, 4)}, \
             {"mask": pts, "record": ["p", "p_rms", "I_avg"], "frequency_response": [1.5e6, 60.0]}, {"PMLSize": 5}
+    if name == "3d_layered_full_volume":
+        # the large layered recipe at 64^3: rough interfaces, per-cell alpha_coeff
+        # and BonA, a focused phased plane source (one signal per point),
+        # p_max / p_rms over every cell
+        import bench
+        w = bench.layered_workload(seed=3, N=64, Nt=60, pml=6, f0=2e6, cycles=3, focus=20, src=16, amp=1e5)
+        return 3, w["shape"], w["dx"], w["Nt"], w["dt"], w["medium"], w["source"], w["sensor"], w["options"]
     raise KeyError(name)
 
 
 CASES = ["2d_homog_p0", "2d_hetero_abs_nl", "2d_stokes_dirichlet", "2d_nocorr_multi", "2d_u_additive",
          "2d_u_dirichlet", "2d_odd_sizes", "2d_pml_outside", "3d_hetero_abs_nl_plane", "3d_multi_signal_additive",
          "3d_p0_u", "2d_time_reversal", "3d_time_reversal_abs", "3d_static_mixed_radix", "3d_static_128",
-         "2d_intensity", "3d_intensity_static", "2d_cart_linear", "3d_cart_linear"]
+         "2d_intensity", "3d_intensity_static", "2d_cart_linear", "3d_cart_linear", "3d_layered_full_volume"]
 
 
 def adjoint_problem(shape, Nt, seed=0, dx=1e-4):
