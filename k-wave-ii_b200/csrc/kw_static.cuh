@@ -492,12 +492,25 @@ __global__ void __launch_bounds__(ks_threads(N2, PL), 2 * kThreads / ks_threads(
     const float2 *H = a.spec.p[f];
     const Med rsi = a.rho_sg_inv[f];
 
+    // the first transform stage's inputs are loaded before the per-cell
+    // staging is issued, so they are not queued behind it
+    using S0 = StageShape<N2, PL, true, 0, NT>;
+    float2 in0[S0::MAXB][S0::R];
+#pragma unroll
+    for (int b = 0; b < S0::MAXB; ++b) {
+        const int gg = threadIdx.x + b * NT;
+        if (!(S0::TOT % NT == 0 || gg < S0::TOT)) continue;
+        int l, j;
+        bmap<S0::NB, PL, true>(gg, l, j);
+#pragma unroll
+        for (int tt = 0; tt < S0::R; ++tt) in0[b][tt] = zpack_load<N2>(H, g, x0, y, l, j + tt * S0::NB);
+    }
     if (!a.init) stage_field<N2, PL>(s_u, a.u[f], g, x0, y);
     if (rsi.arr) stage_field<N2, PL>(s_r, rsi.arr, g, x0, y);
     cp_async_commit();
 
     float2 hold[SH::MAXB][SH::R];
-    auto ld = [&](int, int, int l, int i) -> float2 { return zpack_load<N2>(H, g, x0, y, l, i); };
+    auto ld = [&](int b, int tt, int, int) -> float2 { return in0[b][tt]; };
     auto st = [&](int b, int tt, int, int, float2 v) { hold[b][tt] = v; };
     rs_fft<N2, PL, true, true, 0, NT>(sm, tw, ld, st);
     cp_async_wait_all();
