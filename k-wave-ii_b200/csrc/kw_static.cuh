@@ -202,7 +202,9 @@ __global__ void __launch_bounds__(ks_threads(N1, TY), (4 * kThreads + ks_threads
     constexpr int NT = ks_threads(N1, TY);
     static_assert(RPlan<N1, false>::M >= 2, "in-place pass needs two stages");
     extern __shared__ float2 sm[];   // N1 * TY
-    float2 *buf = pick(bufs.p, blockIdx.z);
+    // fields in reverse order: blocks start on the field the previous pass
+    // (x-pass or z-stage, which walk them in order) wrote last, still in L2
+    float2 *buf = pick(bufs.p, gridDim.z - 1 - blockIdx.z);
     const int x0 = blockIdx.x * TY;
     const long long base = (long long)(blockIdx.y + kz0) * N1 * g.N0 + x0;
     const int N0 = g.N0;
