@@ -212,6 +212,10 @@ struct kw_plan {
     bool use_graphs = true;
     float *rho_first = nullptr, *u_first = nullptr;   // buffer identity for the key
 
+    // streamed series outputs of kw_run: copy stream and per-slot events
+    cudaStream_t copy_stream = nullptr;
+    cudaEvent_t ev_comp[2] = {nullptr, nullptr}, ev_copy[2] = {nullptr, nullptr};
+
     std::vector<void *> allocs;
     size_t bytes = 0;
     uint64_t launches = 0;
@@ -1612,6 +1616,102 @@ kw_status use_device(const kw_plan *P) {
     return KW_OK;
 }
 
+// ---- streamed series outputs ------------------------------------------------
+// kw_run copies the recorded time series to the caller's host buffers while
+// the loop runs: after every chunk of recorded steps a copy stream moves the
+// chunk's columns into one half of a pinned host ring, and the host thread
+// moves the previous chunk from the ring into the caller's buffers while the
+// GPU computes the next one.  Pinned rings are kept in a process-wide pool,
+// since pinning host memory costs about as much as the copy it saves.
+constexpr size_t kStreamChunkBytes = (size_t)16 << 20;     // per ring half
+constexpr size_t kStreamMinBytes = (size_t)64 << 20;       // smaller series are copied after the loop
+
+std::mutex g_pinned_mutex;
+std::vector<std::pair<void *, size_t>> g_pinned_free;
+
+kw_status pinned_get(size_t bytes, void **p, size_t *got) {
+    {
+        std::lock_guard<std::mutex> lock(g_pinned_mutex);
+        for (size_t k = 0; k < g_pinned_free.size(); ++k)
+            if (g_pinned_free[k].second >= bytes) {
+                *p = g_pinned_free[k].first;
+                *got = g_pinned_free[k].second;
+                g_pinned_free.erase(g_pinned_free.begin() + k);
+                return KW_OK;
+            }
+    }
+    void *q = nullptr;
+    cudaError_t e = cudaHostAlloc(&q, bytes, cudaHostAllocPortable);
+    if (e != cudaSuccess) return fail(KW_ERR_NOMEM, "pinned host allocation of %zu bytes failed: %s", bytes, cudaGetErrorString(e));
+    *p = q;
+    *got = bytes;
+    return KW_OK;
+}
+void pinned_put(void *p, size_t bytes) {
+    std::lock_guard<std::mutex> lock(g_pinned_mutex);
+    g_pinned_free.push_back({p, bytes});
+}
+
+struct SeriesOut {
+    float *dst;          // caller's buffer, M x num_rec, column-major
+    const float *src;    // device series
+};
+
+kw_status run_streamed(kw_plan *P, const std::vector<SeriesOut> &ser) {
+    const size_t M = (size_t)P->M, S = ser.size();
+    const int C = (int)std::max<size_t>(1, kStreamChunkBytes / (S * M * sizeof(float)));
+    const size_t half = S * M * (size_t)C;   // floats per ring half
+    if (!P->copy_stream) KW_CUDA(cudaStreamCreateWithFlags(&P->copy_stream, cudaStreamNonBlocking));
+    for (int k = 0; k < 2; ++k) {
+        if (!P->ev_comp[k]) KW_CUDA(cudaEventCreateWithFlags(&P->ev_comp[k], cudaEventDisableTiming));
+        if (!P->ev_copy[k]) KW_CUDA(cudaEventCreateWithFlags(&P->ev_copy[k], cudaEventDisableTiming));
+    }
+    void *ring_v = nullptr;
+    size_t ring_bytes = 0;
+    KW_TRY(pinned_get(2 * half * sizeof(float), &ring_v, &ring_bytes));
+    float *ring = (float *)ring_v;
+    // drain chunk [c0, c1) from ring half `slot` into the caller's buffers
+    auto drain = [&](int slot, int c0, int c1) -> kw_status {
+        KW_CUDA(cudaEventSynchronize(P->ev_copy[slot]));
+        const float *h = ring + (size_t)slot * half;
+        const size_t n = M * (size_t)(c1 - c0);
+        for (size_t s = 0; s < S; ++s) std::memcpy(ser[s].dst + M * (size_t)c0, h + s * M * C, n * sizeof(float));
+        return KW_OK;
+    };
+    kw_status st = KW_OK;
+    int prev_slot = -1, prev_c0 = 0, prev_c1 = 0, k = 0;
+    for (int c0 = 0; c0 < P->num_rec && st == KW_OK; c0 += C, ++k) {
+        const int c1 = std::min(P->num_rec, c0 + C);
+        const int slot = k & 1;
+        // column c is recorded at step record_start + c
+        const long long target = (long long)P->record_start + c1;   // next step after the chunk
+        if (target > P->t) st = run_steps(P, (uint64_t)(target - P->t));
+        if (st != KW_OK) break;
+        cudaError_t e = cudaEventRecord(P->ev_comp[slot], P->stream);
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(P->copy_stream, P->ev_comp[slot], 0);
+        float *h = ring + (size_t)slot * half;
+        for (size_t s = 0; s < S && e == cudaSuccess; ++s)
+            e = cudaMemcpyAsync(h + s * M * C, ser[s].src + M * (size_t)c0, M * (size_t)(c1 - c0) * sizeof(float),
+                                cudaMemcpyDeviceToHost, P->copy_stream);
+        if (e == cudaSuccess) e = cudaEventRecord(P->ev_copy[slot], P->copy_stream);
+        if (e != cudaSuccess) {
+            st = fail(KW_ERR_CUDA, "streamed output copy failed: %s", cudaGetErrorString(e));
+            break;
+        }
+        // the previous chunk's half is drained while the GPU runs this chunk
+        if (prev_slot >= 0) st = drain(prev_slot, prev_c0, prev_c1);
+        prev_slot = slot;
+        prev_c0 = c0;
+        prev_c1 = c1;
+    }
+    if (st == KW_OK && prev_slot >= 0) st = drain(prev_slot, prev_c0, prev_c1);
+    if (st == KW_OK && P->t <= P->index_end) st = run_steps(P, (uint64_t)P->index_end);
+    // no copy may still target the ring when it goes back to the pool
+    cudaStreamSynchronize(P->copy_stream);
+    pinned_put(ring_v, ring_bytes);
+    return st;
+}
+
 }  // namespace
 
 // --------------------------------------------------------------------------
@@ -1745,8 +1845,33 @@ kw_status kw_copy_outputs(kw_plan *P, kw_outputs *o) {
 }
 
 kw_status kw_run(kw_plan *P, kw_outputs *o) {
-    KW_TRY(kw_run_device(P));
-    return kw_copy_outputs(P, o);
+    if (!P || !o) return fail(KW_ERR_INVALID, "NULL argument");
+    KW_TRY(use_device(P));
+    // time series large enough to be worth streaming to the host during the loop
+    std::vector<SeriesOut> ser;
+    if (!P->time_rev && P->M > 0) {
+        if (o->p && P->o_series[0]) ser.push_back({o->p, P->o_series[0]});
+        for (int i = 0; i < P->D; ++i) {
+            if (o->u[i] && P->o_series[1 + i]) ser.push_back({o->u[i], P->o_series[1 + i]});
+            if (o->u_non_staggered[i] && P->o_uns[i]) ser.push_back({o->u_non_staggered[i], P->o_uns[i]});
+        }
+    }
+    const size_t ser_bytes = ser.size() * (size_t)P->M * P->num_rec * sizeof(float);
+    if (ser_bytes < kStreamMinBytes) {
+        KW_TRY(kw_run_device(P));
+        return kw_copy_outputs(P, o);
+    }
+    if (P->t != 1 || P->started) KW_TRY(zero_state(P));
+    KW_TRY(run_streamed(P, ser));
+    KW_CUDA(cudaStreamSynchronize(P->stream));
+    // the remaining (non-series) outputs after the loop
+    kw_outputs rest = *o;
+    rest.p = nullptr;
+    for (int i = 0; i < 3; ++i) {
+        rest.u[i] = nullptr;
+        rest.u_non_staggered[i] = nullptr;
+    }
+    return kw_copy_outputs(P, &rest);
 }
 
 kw_status kw_plan_destroy(kw_plan *P) {
@@ -1756,6 +1881,14 @@ kw_status kw_plan_destroy(kw_plan *P) {
     for (auto &kv : P->graphs)
         if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
     for (auto &r : P->timers) { cudaEventDestroy(r.a); cudaEventDestroy(r.b); }
+    if (P->copy_stream) {
+        cudaStreamSynchronize(P->copy_stream);
+        cudaStreamDestroy(P->copy_stream);
+    }
+    for (int k = 0; k < 2; ++k) {
+        if (P->ev_comp[k]) cudaEventDestroy(P->ev_comp[k]);
+        if (P->ev_copy[k]) cudaEventDestroy(P->ev_copy[k]);
+    }
     for (void *a : P->allocs) cudaFreeAsync(a, P->stream);
     if (P->stream) {
         cudaStreamSynchronize(P->stream);
