@@ -198,7 +198,10 @@ kw_status kw_plan_outputs(const kw_plan *plan, kw_output_desc *desc);
 
 /* Run the whole time loop and copy the recorded outputs to *out.
    Synchronous.  Equivalent of running the binary and reading its HDF5
-   outputs (kspaceFirstOrder3DC.m:546-780). */
+   outputs (kspaceFirstOrder3DC.m:546-780).  Recorded time series of 64 MB or
+   more are copied into *out chunk by chunk while the loop runs (through a
+   pinned host ring the library keeps for reuse); the results are the same as
+   kw_run_device followed by kw_copy_outputs. */
 kw_status kw_run(kw_plan *plan, kw_outputs *out);
 
 /* Split form of kw_run: kw_run_device leaves every output on the device;
