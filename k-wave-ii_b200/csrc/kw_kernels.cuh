@@ -1195,11 +1195,16 @@ __global__ void k_adj_gR(AdjArgs a) {
         }
 }
 
-// mu[sidx[m]] = r[m] (sensor cells are distinct)
-__global__ void k_adj_scatter(float *mu, const long long *sidx, int M, const float *r) {
+// mu[sidx[m]] = res[m + M col] (sensor cells are distinct) for the residual
+// column col = *d_col, nothing when col < 0 (steps before record_start).  The
+// column lives on the device, so a captured backward step replays unchanged.
+__global__ void k_adj_scatter(float *mu, const long long *sidx, int M, const float *res, const int *d_col) {
+    const int col = *d_col;
     const int m = blockIdx.x * blockDim.x + threadIdx.x;
-    if (m < M) mu[sidx[m]] = r[m];
+    if (col >= 0 && m < M) mu[sidx[m]] = res[m + (long long)M * col];
 }
+__global__ void k_adj_set_col(int *d_col, int col) { *d_col = col; }
+__global__ void k_adj_col_back(int *d_col) { *d_col -= 1; }
 
 // dJ/drho0 = direct term + the chain through rho_sg_i^-1 = 1 / rho_sg_i:
 // h_i = dJ/drho_sg_i = -rho_sg_i^-2 dJ/drho_sg_i^-1; with derive != 0 the
