@@ -800,7 +800,7 @@ __global__ void __launch_bounds__(ks_threads(N2, PL), 2 * kThreads / ks_threads(
     constexpr int TX = Z::TX, NT = Z::NT;
     extern __shared__ float2 dsm[];
     float2 *sm = dsm;
-    float2 *s_w[2] = {dsm + Z::TILE, dsm + Z::TILE + Z::SLICE};
+    float2 *const s_w0 = dsm + Z::TILE, *const s_w1 = dsm + Z::TILE + Z::SLICE;
     const Geom &g = a.g;
     const int x0 = blockIdx.x * TX, y = blockIdx.y;
     const int t = *a.d_t;
@@ -808,15 +808,13 @@ __global__ void __launch_bounds__(ks_threads(N2, PL), 2 * kThreads / ks_threads(
     // (c0^2 tau or c0^2 eta) is staged into slice k at the start, its rows
     // are prefetched into the tile while term k-1 is applied, and p is staged
     // into the slice that is free first
-    int terms[2], nterm = 0;
-    if (a.has_tau) terms[nterm++] = 0;
-    if (a.has_eta) terms[nterm++] = 1;
-    Med wk[2];
-    for (int k = 0; k < nterm; ++k) {
-        wk[k] = terms[k] == 0 ? a.c2tau : a.c2eta;
-        if (wk[k].arr) stage_field<N2, PL>(s_w[k], wk[k].arr, g, x0, y);
-    }
-    float2 *s_p = nterm == 2 ? s_w[0] : s_w[1];
+    // terms in order tau, eta; term k's weight is w0 / w1 in slice s_w0 /
+    // s_w1 (selects, not arrays, so nothing is indexed at run time)
+    const int nterm = (a.has_tau ? 1 : 0) + (a.has_eta ? 1 : 0);
+    const Med w0 = a.has_tau ? a.c2tau : a.c2eta, w1 = a.c2eta;
+    if (nterm > 0 && w0.arr) stage_field<N2, PL>(s_w0, w0.arr, g, x0, y);
+    if (nterm > 1 && w1.arr) stage_field<N2, PL>(s_w1, w1.arr, g, x0, y);
+    float2 *s_p = nterm == 2 ? s_w0 : s_w1;
     if (nterm < 2) stage_field<N2, PL>(s_p, a.p, g, x0, y);
     if (nterm > 0) zraw_prefetch<N2, PL>(sm, a.spec.p[0], g, x0, y);
     cp_async_commit();
@@ -829,7 +827,7 @@ __global__ void __launch_bounds__(ks_threads(N2, PL), 2 * kThreads / ks_threads(
     // {rows_1}, {p (two terms)}
 #pragma unroll 1
     for (int k = 0; k < nterm; ++k) {
-        const int term = terms[k];
+        const int term = (k == 0 && a.has_tau) ? 0 : 1;
         float2 hold[SH::MAXB][SH::R];
         if (k == 0) cp_async_wait_all();
         else cp_async_wait_group<1>();   // rows_1 landed; p may be in flight
@@ -842,8 +840,8 @@ __global__ void __launch_bounds__(ks_threads(N2, PL), 2 * kThreads / ks_threads(
             zraw_prefetch<N2, PL>(sm, a.spec.p[k + 1], g, x0, y);
             cp_async_commit();
         }
-        const Med w = wk[k];
-        const float2 *sw = s_w[k];
+        const Med w = k == 0 ? w0 : w1;
+        const float2 *sw = k == 0 ? s_w0 : s_w1;
         const float sg = term == 0 ? 1.f : -1.f;
 #pragma unroll
         for (int b = 0; b < SH::MAXB; ++b)
