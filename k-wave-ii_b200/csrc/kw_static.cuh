@@ -617,6 +617,7 @@ __global__ void __launch_bounds__(ks_threads(N2, PL), 2 * kThreads / ks_threads(
     // transform tile after the last inverse transform (unless a sparse source
     // needs the tile first)
     const bool r0_tile = Z::SLICE <= Z::TILE && a.nonlinear && r0arr && e1 <= e0;
+    const bool c0_staged = a.c0.arr != nullptr;
 
     float2 acc_r[SH::MAXB][SH::R], acc_d[SH::MAXB][SH::R];
 #pragma unroll
@@ -682,10 +683,14 @@ __global__ void __launch_bounds__(ks_threads(N2, PL), 2 * kThreads / ks_threads(
                 acc_d[b][tt].x += du.x;
                 acc_d[b][tt].y += du.y;
             }
-        // every thread reads only its own slots, so the next component can be
-        // staged into the same slice right away
+        // every thread reads only its own slots, so the next component (or,
+        // after the last one, c0 for the equation of state) can be staged
+        // into the same slice right away
         if (i + 1 < D) {
             stage_field<N2, PL>(s_a, a.rho[i + 1], g, x0, y);
+            cp_async_commit();
+        } else if (c0_staged) {
+            stage_field<N2, PL>(s_a, a.c0.arr, g, x0, y);
             cp_async_commit();
         }
     }
@@ -715,7 +720,7 @@ __global__ void __launch_bounds__(ks_threads(N2, PL), 2 * kThreads / ks_threads(
     // equation of state (c0^2 applied to the non-spectral terms here; the
     // absorbing terms are finished in Stage P)
     const bool absorbing = a.eos == 1;
-    if (r0_tile) cp_async_wait_all();
+    if (r0_tile || c0_staged) cp_async_wait_all();
     auto r0_at = [&](int si, long long gi) -> float2 {
         if (r0_tile) return sm[si];
         if (!a.nonlinear && r0arr) return s_c[si];
@@ -734,7 +739,7 @@ __global__ void __launch_bounds__(ks_threads(N2, PL), 2 * kThreads / ks_threads(
                 const long long gi = xa + (long long)g.N0 * (y + (long long)g.N1 * z);
                 const int si = Z::sidx(b, tt);
                 const float2 sr = acc_r[b][tt];
-                const float2 c = med2(a.c0, gi, true, true);
+                const float2 c = c0_staged ? s_a[si] : med2(a.c0, gi, true, true);
                 pv = sr;
                 if (a.nonlinear) {
                     const float2 r0 = r0_at(si, gi);
