@@ -618,6 +618,7 @@ __global__ void __launch_bounds__(ks_threads(N2, PL), 2 * kThreads / ks_threads(
     // needs the tile first)
     const bool r0_tile = Z::SLICE <= Z::TILE && a.nonlinear && r0arr && e1 <= e0;
     const bool c0_staged = a.c0.arr != nullptr;
+    const bool bona_staged = a.nonlinear && a.BonA.arr != nullptr;
 
     float2 acc_r[SH::MAXB][SH::R], acc_d[SH::MAXB][SH::R];
 #pragma unroll
@@ -689,8 +690,10 @@ __global__ void __launch_bounds__(ks_threads(N2, PL), 2 * kThreads / ks_threads(
         if (i + 1 < D) {
             stage_field<N2, PL>(s_a, a.rho[i + 1], g, x0, y);
             cp_async_commit();
-        } else if (c0_staged) {
-            stage_field<N2, PL>(s_a, a.c0.arr, g, x0, y);
+        } else {
+            if (c0_staged) stage_field<N2, PL>(s_a, a.c0.arr, g, x0, y);
+            // q is read by the mass updates only: its slice takes B/A
+            if (bona_staged) stage_field<N2, PL>(s_c, a.BonA.arr, g, x0, y);
             cp_async_commit();
         }
     }
@@ -720,7 +723,7 @@ __global__ void __launch_bounds__(ks_threads(N2, PL), 2 * kThreads / ks_threads(
     // equation of state (c0^2 applied to the non-spectral terms here; the
     // absorbing terms are finished in Stage P)
     const bool absorbing = a.eos == 1;
-    if (r0_tile || c0_staged) cp_async_wait_all();
+    if (r0_tile || c0_staged || bona_staged) cp_async_wait_all();
     auto r0_at = [&](int si, long long gi) -> float2 {
         if (r0_tile) return sm[si];
         if (!a.nonlinear && r0arr) return s_c[si];
@@ -745,7 +748,7 @@ __global__ void __launch_bounds__(ks_threads(N2, PL), 2 * kThreads / ks_threads(
                     const float2 r0 = r0_at(si, gi);
                     // next step's mass coefficient q = 2 sum(rho) + rho0
                     *reinterpret_cast<float2 *>(a.srho + gi) = make_float2(fmaf(2.f, sr.x, r0.x), fmaf(2.f, sr.y, r0.y));
-                    const float2 bn = med2(a.BonA, gi, true, true);
+                    const float2 bn = bona_staged ? s_c[si] : med2(a.BonA, gi, true, true);
                     pv.x += bona_term(bn.x, sr.x, r0.x);
                     pv.y += bona_term(bn.y, sr.y, r0.y);
                 }
