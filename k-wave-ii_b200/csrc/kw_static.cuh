@@ -783,7 +783,13 @@ __global__ void __launch_bounds__(ks_threads(N2, PL), 2 * kThreads / ks_threads(
         if (a.write_spec) zforward_store<N2, PL>(sm, tw, acc_d, a.spec.p[0], g, x0, y);
         return;
     }
-    // absorbing: forward transforms of rho0 * sum(du) (tau term) and sum(rho) (eta term)
+    // absorbing: forward transforms of rho0 * sum(du) (tau term) and sum(rho)
+    // (eta term).  sum(rho) waits in this thread's slots of the freed slice,
+    // so only one set of values is held in registers during each transform.
+#pragma unroll
+    for (int b = 0; b < SH::MAXB; ++b)
+#pragma unroll
+        for (int tt = 0; tt < SH::R; ++tt) s_a[Z::sidx(b, tt)] = acc_r[b][tt];
     int out = 0;
 #pragma unroll 1
     for (int term = 0; term < 2; ++term) {
@@ -792,7 +798,7 @@ __global__ void __launch_bounds__(ks_threads(N2, PL), 2 * kThreads / ks_threads(
 #pragma unroll
         for (int b = 0; b < SH::MAXB; ++b)
 #pragma unroll
-            for (int tt = 0; tt < SH::R; ++tt) src[b][tt] = term == 0 ? acc_d[b][tt] : acc_r[b][tt];
+            for (int tt = 0; tt < SH::R; ++tt) src[b][tt] = term == 0 ? acc_d[b][tt] : s_a[Z::sidx(b, tt)];
         zforward_store<N2, PL>(sm, tw, src, pick(a.spec.p, out++), g, x0, y);
     }
 }
