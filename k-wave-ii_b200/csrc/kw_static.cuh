@@ -63,8 +63,16 @@ template <int N, int NL, bool INV, int S, int NT = kThreads> struct StageShape {
 // forward's first stage (identical by construction)
 template <int N, int NL, int NT = kThreads> using HandShape = StageShape<N, NL, false, 0, NT>;
 
-template <int N, int NL, bool IL, bool INV, int S, int NT, class Ld, class St>
-__device__ __forceinline__ void rs_stage(float2 *sm, const float2 *__restrict__ tw, Ld &ld, St &st) {
+// Twiddle table access: a global table through the read-only path, or a
+// copy the block keeps in shared memory (SmemTable).
+struct SmemTable {
+    const float2 *p;
+};
+__device__ __forceinline__ float2 tw_at(const float2 *__restrict__ tw, int i) { return __ldg(tw + i); }
+__device__ __forceinline__ float2 tw_at(const SmemTable &tw, int i) { return tw.p[i]; }
+
+template <int N, int NL, bool IL, bool INV, int S, int NT, class TW, class Ld, class St>
+__device__ __forceinline__ void rs_stage(float2 *sm, const TW &tw, Ld &ld, St &st) {
     using P = RPlan<N, INV>;
     using SH = StageShape<N, NL, INV, S, NT>;
     constexpr int M = P::M, R = SH::R, NS = P::NS(S), NB = SH::NB;
@@ -87,7 +95,7 @@ __device__ __forceinline__ void rs_stage(float2 *sm, const float2 *__restrict__ 
                 const int k = j % NS;
 #pragma unroll
                 for (int t = 1; t < R; ++t) {
-                    float2 w = __ldg(tw + t * k * TWS);
+                    float2 w = tw_at(tw, t * k * TWS);
                     if (INV) w.y = -w.y;
                     v[b][t] = cmul(v[b][t], w);
                 }
@@ -124,8 +132,8 @@ __device__ __forceinline__ void rs_stage(float2 *sm, const float2 *__restrict__ 
     }
 }
 
-template <int N, int NL, bool IL, bool INV, int S = 0, int NT = kThreads, class Ld, class St>
-__device__ __forceinline__ void rs_fft(float2 *sm, const float2 *__restrict__ tw, Ld &ld, St &st) {
+template <int N, int NL, bool IL, bool INV, int S = 0, int NT = kThreads, class TW, class Ld, class St>
+__device__ __forceinline__ void rs_fft(float2 *sm, const TW &tw, Ld &ld, St &st) {
     rs_stage<N, NL, IL, INV, S, NT>(sm, tw, ld, st);
     if constexpr (S + 1 < RPlan<N, INV>::M) rs_fft<N, NL, IL, INV, S + 1, NT>(sm, tw, ld, st);
 }
@@ -229,10 +237,27 @@ __global__ void __launch_bounds__(ks_threads(N0, NL), 3 * kThreads / ks_threads(
     __shared__ float2 sm[NL * Padded<N0>::LS];
     __shared__ float kyz2[NL];
     __shared__ int liy[NL], liz[NL];
+    // per-x tables read on the transforms' dependency chains, kept in shared
+    // memory: twiddles, k_x^2 and the x-derivative table of an axis-0 output
+    __shared__ float2 s_tw[N0], s_ddx[N0];
+    __shared__ float s_kx2[N0];
     // lines (y, kz) of kz planes kz0 .. kz0+nkz-1
     const int lines_total = (kz0 + nkz) * g.N1;
     const int line0 = kz0 * g.N1 + blockIdx.x * NL;
     const int f = fanout ? 0 : blockIdx.z;
+    const float2 *ddx = nullptr;
+    for (int o = 0; o < (fanout ? ops.n : 1); ++o) {
+        const int oi = fanout ? o : f;
+        const int ko = pick(ops.kind, oi);
+        if (pick(ops.axis, oi) == 0 && (ko == OP_GRAD_POS || ko == OP_GRAD_NEG || ko == OP_SHIFT_NEG))
+            ddx = ko == OP_GRAD_POS ? P.dd_pos[0] : (ko == OP_GRAD_NEG ? P.dd_neg[0] : P.sh_neg[0]);
+    }
+    for (int i = threadIdx.x; i < N0; i += NT) {
+        s_tw[i] = __ldg(tw + i);
+        s_kx2[i] = __ldg(P.k2[0] + i);
+        if (ddx) s_ddx[i] = __ldg(ddx + i);
+    }
+    const SmemTable stw{s_tw};
     for (int l = threadIdx.x; l < NL; l += NT) {
         const int line = min(line0 + l, lines_total - 1);
         const int iy = line % g.N1, iz = line / g.N1;
@@ -248,7 +273,7 @@ __global__ void __launch_bounds__(ks_threads(N0, NL), 3 * kThreads / ks_threads(
     using SH = StageShape<N0, NL, false, RPlan<N0, false>::M - 1, NT>;   // forward last stage
     float2 spec[SH::MAXB][SH::R];
     auto keep = [&](int b, int t, int, int, float2 v) { spec[b][t] = v; };
-    rs_fft<N0, NL, false, false, 0, NT>(sm, tw, ld, keep);
+    rs_fft<N0, NL, false, false, 0, NT>(sm, stw, ld, keep);
 
     // common factor of the operator (kappa, |k|^e or cos), times 1/N
     const int kind0 = pick(ops.kind, f);
@@ -264,7 +289,7 @@ __global__ void __launch_bounds__(ks_threads(N0, NL), 3 * kThreads / ks_threads(
 #pragma unroll
         for (int t = 0; t < SH::R; ++t) {
             const int ix = j + t * NSL;
-            const float k2 = __ldg(P.k2[0] + ix) + ky;
+            const float k2 = s_kx2[ix] + ky;
             float fac;
             if (grad) {
                 fac = P.use_kspace ? sinc_series(P.kappa_a * P.kappa_a * k2) : 1.f;
@@ -290,13 +315,14 @@ __global__ void __launch_bounds__(ks_threads(N0, NL), 3 * kThreads / ks_threads(
         float2 *out = pick(bufs.p, oi) + (long long)line0 * N0;
         auto ld2 = [&](int b, int t, int l, int i) -> float2 {
             if (!mul_dd) return spec[b][t];
+            if (axis == 0 && dd == ddx) return cmul(spec[b][t], s_ddx[i]);
             const int idx = axis == 0 ? i : (axis == 1 ? liy[l] : liz[l]);
             return cmul(spec[b][t], __ldg(dd + idx));
         };
         auto st2 = [&](int, int, int l, int i, float2 v) {
             if (line0 + l < lines_total) out[l * N0 + i] = v;
         };
-        rs_fft<N0, NL, false, true, 0, NT>(sm, tw, ld2, st2);
+        rs_fft<N0, NL, false, true, 0, NT>(sm, stw, ld2, st2);
     }
 }
 
