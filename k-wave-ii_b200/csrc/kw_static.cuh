@@ -222,7 +222,10 @@ __global__ void __launch_bounds__(ks_threads(N1, TY), (4 * kThreads + ks_threads
     auto st = [&](int, int, int l, int i, float2 v) {
         if (x0 + l < N0) buf[base + (long long)i * N0 + l] = v;
     };
-    rs_fft<N1, TY, true, INV, 0, NT>(sm, tw, ld, st);
+    // twiddles from shared memory (first read after the first stage's barrier)
+    __shared__ float2 s_tw[N1];
+    for (int i = threadIdx.x; i < N1; i += NT) s_tw[i] = __ldg(tw + i);
+    rs_fft<N1, TY, true, INV, 0, NT>(sm, SmemTable{s_tw}, ld, st);
 }
 
 // ---------------------------------------------------------------------------
