@@ -180,6 +180,15 @@ def make_case(name):
         med = {"sound_speed": c, "density": rho, "alpha_coeff": 0.5, "alpha_power": 1.5}
         return 3, shape, dx, 60, 0.3 * dx / c.max(), med, {"p0": disc_p0(shape, 4)}, \
             {"mask": pts, "record": ["p", "p_rms", "I_avg"], "frequency_response": [1.5e6, 60.0]}, {"PMLSize": 5}
+    if name == "2d_full_mask_odd":
+        # every cell is a sensor and the cell count (1575) is not a multiple
+        # of 4: the index-free gather of the scalar sensor kernel
+        shape = (45, 35)
+        c, rho = blob_medium(shape, rng)
+        return 2, shape, dx, 90, 0.3 * dx / c.max(), {"sound_speed": c, "density": rho, "alpha_coeff": 0.5,
+                                                      "alpha_power": 1.5}, \
+            {"p0": disc_p0(shape, 4)}, {"mask": np.ones(shape), "record": ["p", "p_max", "p_rms", "u_max"]}, \
+            {"PMLSize": 6}
     if name == "3d_layered_full_volume":
         # the large layered recipe at 64^3: rough interfaces, per-cell alpha_coeff
         # and BonA, a focused phased plane source (one signal per point),
@@ -193,7 +202,8 @@ def make_case(name):
 CASES = ["2d_homog_p0", "2d_hetero_abs_nl", "2d_stokes_dirichlet", "2d_nocorr_multi", "2d_u_additive",
          "2d_u_dirichlet", "2d_odd_sizes", "2d_pml_outside", "3d_hetero_abs_nl_plane", "3d_multi_signal_additive",
          "3d_p0_u", "2d_time_reversal", "3d_time_reversal_abs", "3d_static_mixed_radix", "3d_static_128",
-         "2d_intensity", "3d_intensity_static", "2d_cart_linear", "3d_cart_linear", "3d_layered_full_volume"]
+         "2d_intensity", "3d_intensity_static", "2d_cart_linear", "3d_cart_linear", "3d_layered_full_volume",
+         "2d_full_mask_odd"]
 
 
 def adjoint_problem(shape, Nt, seed=0, dx=1e-4):
