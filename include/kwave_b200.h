@@ -286,8 +286,10 @@ kw_status kw_server_destroy(kw_server *server);
  * Tile widths of the compile-time transform kernels (lines per block of the
  * z-stages, the y-pass and the x-pass; 0 for a class that runs the runtime
  * kernels).  Plan creation picks them by rule and then by timing (the
- * autotuner; environment variable KW_AUTOTUNE=0 turns it off).  kw_set_tiles
- * accepts, per class, the full width or the narrow one (a quarter) and
+ * autotuner, which may give the three z-stages different widths;
+ * environment variable KW_AUTOTUNE=0 turns it off).  kw_plan_tiles reports
+ * the momentum stage's z width.  kw_set_tiles accepts, per class, the full
+ * width or the narrow one (a quarter), sets every z-stage to tiles[0] and
  * rejects anything else; results do not depend on the choice.
  */
 kw_status kw_plan_tiles(const kw_plan *plan, int32_t tiles[3]);

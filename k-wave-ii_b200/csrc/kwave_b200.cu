@@ -1075,15 +1075,18 @@ void plan_tiles(kw_plan *P) {
 // keeps what is faster, once per grid shape and tile-relevant structure per
 // process.  Tile widths change how lines are grouped into blocks, never the
 // arithmetic of a line, so results are identical whichever is chosen.
+// z-tile widths of stages U, R and P (each chooses its own), y and x widths
 struct TileChoice {
-    int PL, TY, NL;
+    int PLu, PLr, PLp, TY, NL;
 };
 std::mutex g_tune_mu;
 std::map<std::array<int, 5>, TileChoice> g_tune;
 
-TileChoice tiles_of(const kw_plan *P) { return TileChoice{P->PL_z, P->TY, P->NL}; }
+TileChoice tiles_of(const kw_plan *P) { return TileChoice{P->PL_u, P->PL_r, P->PL_p, P->TY, P->NL}; }
 void set_tiles(kw_plan *P, const TileChoice &c) {
-    P->PL_u = P->PL_z = P->PL_p = P->PL_r = c.PL;
+    P->PL_u = P->PL_z = c.PLu;
+    P->PL_r = c.PLr;
+    P->PL_p = c.PLp;
     P->TY = c.TY;
     P->NL = c.NL;
 }
@@ -1138,11 +1141,15 @@ kw_status autotune_tiles(kw_plan *P) {
     float best_ms = 0.f;
     kw_status st = time_steps(P, 2, &best_ms);
     auto flip = [](int v, int full, int narrow) { return v == full ? narrow : full; };
-    for (int cls = 0; cls < 3 && st == KW_OK; ++cls) {
+    // one width at a time: stage U, stage R, stage P, y-pass, x-pass
+    for (int cls = 0; cls < 5 && st == KW_OK; ++cls) {
         TileChoice c = best;
-        if (cls == 0 && tune_z) c.PL = flip(c.PL, ks_lines(g.N2), ks_narrow(g.N2));
-        else if (cls == 1 && tune_y) c.TY = flip(c.TY, ks_lines(g.N1), ks_narrow(g.N1));
-        else if (cls == 2 && tune_x) c.NL = flip(c.NL, ks_xlines(g.N0), ks_xnarrow(g.N0));
+        const int zf = ks_lines(g.N2), zn = ks_narrow(g.N2);
+        if (cls == 0 && tune_z) c.PLu = flip(c.PLu, zf, zn);
+        else if (cls == 1 && tune_z) c.PLr = flip(c.PLr, zf, zn);
+        else if (cls == 2 && tune_z) c.PLp = flip(c.PLp, zf, zn);
+        else if (cls == 3 && tune_y) c.TY = flip(c.TY, ks_lines(g.N1), ks_narrow(g.N1));
+        else if (cls == 4 && tune_x) c.NL = flip(c.NL, ks_xlines(g.N0), ks_xnarrow(g.N0));
         else continue;
         set_tiles(P, c);
         float ms = 0.f;
@@ -2084,7 +2091,7 @@ kw_status kw_set_tiles(kw_plan *P, const int32_t tiles[3]) {
     KW_TRY(use_device(P));
     KW_CUDA(cudaStreamSynchronize(P->stream));
     TileChoice c = tiles_of(P);
-    if (P->static_z) c.PL = tiles[0];
+    if (P->static_z) c.PLu = c.PLr = c.PLp = tiles[0];
     if (P->static_y) c.TY = tiles[1];
     if (P->static_x) c.NL = tiles[2];
     set_tiles(P, c);
