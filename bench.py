@@ -551,7 +551,7 @@ def large_section(kw, device, N=512, Nt=200, seed=11):
             "us_per_time_step": classes}
 
 
-def adjoint_section(kw, device, Nt=3000, n_shots=16, fd_cells=32, seed=4, tr=True, workers=4):
+def adjoint_section(kw, device, Nt=3000, n_shots=16, fd_cells=32, seed=4, tr=True, workers=8):
     """Gradient of J = 1/2 sum over shots of |p(ring) - d|^2 at the homogeneous
     starting model (16 shots, Nt steps, sqrt(Nt) checkpointing), timed per
     shot, and central finite differences of J for shot 0 at fd_cells random
@@ -650,6 +650,7 @@ def main():
     ap.add_argument("--serve-requests", type=int, default=48, help="0 skips the served-stream section")
     ap.add_argument("--adjoint-shots", type=int, default=16, help="0 skips the adjoint section")
     ap.add_argument("--adjoint-fd", type=int, default=32, help="finite-difference cells of the adjoint check")
+    ap.add_argument("--adjoint-workers", type=int, default=8, help="adjoint shots in flight at once")
     ap.add_argument("--large-Nt", type=int, default=200, help="time steps of the 512^3 layered run (0 skips it)")
     args = ap.parse_args()
     ws, rank, local = dist_setup()
@@ -735,7 +736,8 @@ def main():
 
     adjoint = None
     if args.adjoint_shots > 0:
-        adjoint = adjoint_section(kw, local, n_shots=args.adjoint_shots, fd_cells=args.adjoint_fd, seed=4 + rank)
+        adjoint = adjoint_section(kw, local, n_shots=args.adjoint_shots, fd_cells=args.adjoint_fd, seed=4 + rank,
+                                  workers=args.adjoint_workers)
 
     large = None
     if args.large_Nt > 0:
