@@ -29,6 +29,7 @@ import math
 import os
 import subprocess
 import sys
+import tempfile
 import time
 
 import numpy as np
@@ -673,8 +674,11 @@ def main():
     sim.run_timed(max(args.warmup, 0)) if args.warmup > 0 else None
 
     # timed region: K complete simulations, device events on the library stream
-    os.makedirs(os.path.join(ROOT, "gpurun_out"), exist_ok=True)
-    clk = Clocks(local, os.path.join(ROOT, "gpurun_out", "clocks_rank%d.csv" % rank))
+    # raw clock samples go to KW_CLOCKS_DIR (default: the system temp dir);
+    # the bench line carries their summary
+    clk_dir = os.environ.get("KW_CLOCKS_DIR") or tempfile.gettempdir()
+    os.makedirs(clk_dir, exist_ok=True)
+    clk = Clocks(local, os.path.join(clk_dir, "clocks_rank%d.csv" % rank))
     l0 = sim.launch_count()
     dist_barrier(ws)
     ms = sim.run_timed(args.steps)
