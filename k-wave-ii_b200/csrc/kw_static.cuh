@@ -659,7 +659,8 @@ __global__ void __launch_bounds__(ks_threads(N2, PL), 2 * kThreads / ks_threads(
         }
 #pragma unroll 1
     // commit groups, oldest first: {srho, rho_0, rows_0}, then per component
-    // {rows_i+1} before its physics and {rho_i+1} after it
+    // {rows_i+1} before its physics and {rho_i+1} after it; after the last
+    // component's physics {c0, B/A} for the equation of state
     for (int i = 0; i < D; ++i) {
         float2 hold[SH::MAXB][SH::R];
         if (i == 0) cp_async_wait_all();
