@@ -1667,7 +1667,7 @@ struct SeriesOut {
 kw_status run_streamed(kw_plan *P, const std::vector<SeriesOut> &ser) {
     const size_t M = (size_t)P->M, S = ser.size();
     const int C = (int)std::max<size_t>(1, kStreamChunkBytes / (S * M * sizeof(float)));
-    const size_t half = S * M * (size_t)C;   // floats per ring half
+    const size_t half = kStreamChunkBytes / sizeof(float);   // floats per ring half (holds C steps)
     if (!P->copy_stream) KW_CUDA(cudaStreamCreateWithFlags(&P->copy_stream, cudaStreamNonBlocking));
     for (int k = 0; k < 2; ++k) {
         if (!P->ev_comp[k]) KW_CUDA(cudaEventCreateWithFlags(&P->ev_comp[k], cudaEventDisableTiming));
@@ -1675,7 +1675,7 @@ kw_status run_streamed(kw_plan *P, const std::vector<SeriesOut> &ser) {
     }
     void *ring_v = nullptr;
     size_t ring_bytes = 0;
-    KW_TRY(pinned_get(2 * half * sizeof(float), &ring_v, &ring_bytes));
+    KW_TRY(pinned_get(2 * kStreamChunkBytes, &ring_v, &ring_bytes));
     float *ring = (float *)ring_v;
     // drain chunk [c0, c1) from ring half `slot` into the caller's buffers
     auto drain = [&](int slot, int c0, int c1) -> kw_status {
@@ -1863,11 +1863,23 @@ kw_status kw_run(kw_plan *P, kw_outputs *o) {
             if (o->u_non_staggered[i] && P->o_uns[i]) ser.push_back({o->u_non_staggered[i], P->o_uns[i]});
         }
     }
-    const size_t ser_bytes = ser.size() * (size_t)P->M * P->num_rec * sizeof(float);
-    if (ser_bytes < kStreamMinBytes) {
+    const size_t col_bytes = ser.size() * (size_t)P->M * sizeof(float);   // one recorded step
+    const size_t ser_bytes = col_bytes * P->num_rec;
+    // stream when the series are large and one recorded step fits a chunk
+    // (the ring is two chunks); otherwise, or when no pinned ring can be had,
+    // copy after the loop
+    void *ring = nullptr;
+    size_t ring_bytes = 0;
+    bool stream = ser_bytes >= kStreamMinBytes && col_bytes <= kStreamChunkBytes;
+    if (stream && pinned_get(2 * kStreamChunkBytes, &ring, &ring_bytes) != KW_OK) {
+        g_err.clear();   // not an error: the copy after the loop needs no pinned memory
+        stream = false;
+    }
+    if (!stream) {
         KW_TRY(kw_run_device(P));
         return kw_copy_outputs(P, o);
     }
+    pinned_put(ring, ring_bytes);   // run_streamed takes it back from the pool
     if (P->t != 1 || P->started) KW_TRY(zero_state(P));
     KW_TRY(run_streamed(P, ser));
     KW_CUDA(cudaStreamSynchronize(P->stream));
