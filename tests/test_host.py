@@ -194,3 +194,29 @@ def test_cart_linear_weights(shape):
     assert np.array_equal(tri, t2) and np.allclose(bc, b2, rtol=0, atol=1e-15)
     with pytest.raises(ValueError, match="within the k-space grid"):
         cartLinearWeights(shape, [1e-4] * dim, pts + 1.0)
+
+
+def test_layered_workload_recipe():
+    """The large layered benchmark's inputs (built at 64^3): four layers
+    along x at the recipe's speeds, rough interfaces of 3-cell RMS, B/A in
+    5..9 per layer, one delayed burst per plane-source point (the element
+    farthest from the focus fires first, delay 0) and every cell a sensor."""
+    import bench
+    rng = np.random.default_rng(0)
+    h = bench.rough_surface(128, 96, rng)
+    assert h.shape == (128, 96) and np.isclose(h.std(), 3.0) and abs(h.mean()) < 1.0
+    w = bench.layered_workload(seed=3, N=64, Nt=60, pml=6, f0=2e6, cycles=3, focus=20, src=16, amp=1e5)
+    med = w["medium"]
+    assert set(np.unique(med["sound_speed"])) <= set(bench.LAYER_C)
+    assert np.allclose(med["density"], 1000.0 + 0.6 * (med["sound_speed"] - 1500.0))
+    assert med["BonA"].min() >= 5 and med["BonA"].max() <= 9 and med["alpha_power"] == 1.1
+    # the first layer fills the x = 0 plane, the last the far plane
+    assert np.all(med["sound_speed"][0] == bench.LAYER_C[0]) and np.all(med["sound_speed"][-1] == bench.LAYER_C[3])
+    pm, sig = w["source"]["p_mask"], w["source"]["p"]
+    assert pm.sum() == 16 * 16 and pm[6].sum() == 16 * 16          # every source point on the plane x = 6
+    assert sig.shape == (256, w["src_len"]) and w["src_len"] <= w["Nt"]
+    # corner elements are farthest from the focus: they start first (nonzero at sample 1)
+    first = (np.abs(sig) > 0).argmax(axis=1)
+    assert first.min() <= 1 and first[0] == first.min() and np.all(first >= 0)
+    assert w["sensor"]["mask"].all() and w["sensor"]["record"] == ["p_max", "p_rms"]
+    assert w["dt"] == pytest.approx(0.3 * 1e-4 / 2800.0)
