@@ -21,20 +21,22 @@
 #include <mutex>
 #include <vector>
 
-#include "kw_kernels.cuh"
+#include "kw_plan.cuh"
+#include "kw_aux.cuh"
 #include "kw_static.cuh"
 #include <chrono>
 #include <condition_variable>
 #include <deque>
 #include <memory>
 #include <thread>
-#include "../../include/kwave_b200.h"
 
 using namespace kw;
 
 namespace {
-
 thread_local std::string g_err;
+}  // namespace
+
+namespace kw {
 
 kw_status fail(kw_status s, const char *fmt, ...) {
     char buf[1024];
@@ -46,21 +48,21 @@ kw_status fail(kw_status s, const char *fmt, ...) {
     return s;
 }
 
-#define KW_CUDA(call)                                                                          \
-    do {                                                                                       \
-        cudaError_t e_ = (call);                                                               \
-        if (e_ != cudaSuccess) {                                                               \
-            return fail(e_ == cudaErrorMemoryAllocation ? KW_ERR_NOMEM : KW_ERR_CUDA,          \
-                        "CUDA error %s at %s:%d (%s)", cudaGetErrorName(e_), __FILE__, __LINE__, \
-                        cudaGetErrorString(e_));                                               \
-        }                                                                                      \
-    } while (0)
+kw_status set_smem(const void *fn, size_t bytes) {
+    if (bytes > 48 * 1024) KW_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+    return KW_OK;
+}
 
-#define KW_TRY(call)                   \
-    do {                               \
-        kw_status s_ = (call);         \
-        if (s_ != KW_OK) return s_;    \
-    } while (0)
+kw_status launched(kw_plan *P) {
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return fail(KW_ERR_CUDA, "kernel launch failed: %s", cudaGetErrorString(e));
+    P->launches += 1;
+    return KW_OK;
+}
+
+}  // namespace kw
+
+namespace {
 
 // --------------------------------------------------------------------------
 // FP64 host precompute
@@ -107,120 +109,8 @@ double db2neper(double a, double y) { return 100.0 * a * std::pow(1e-6 / (2 * M_
 }  // namespace
 
 // --------------------------------------------------------------------------
-// the plan
+// plan memory (the plan itself is defined in kw_plan.cuh)
 // --------------------------------------------------------------------------
-struct SourceDev {
-    bool present = false;
-    int mode = 0;
-    int T[3] = {0, 0, 0};
-    int nsig = 0;
-    int npts = 0;
-    bool dense_fast = false;      // additive, one signal: rho += s(t) F
-    bool dense_general = false;   // additive, several signals: F_t each step
-    float *sig[3] = {nullptr, nullptr, nullptr};
-    long long *pos = nullptr;     // 0-based linear indices
-    int *row = nullptr;           // 0-based signal row per point
-    float *F = nullptr;           // filtered mask (fast path)
-    float *Ft[3] = {nullptr, nullptr, nullptr};  // filtered source of this step (general path)
-    float *scratch = nullptr;     // zero field holding the scattered source (general path)
-    int *csr_off = nullptr, *csr_cell = nullptr, *csr_row = nullptr;  // sparse modes
-};
-
-struct TimerRec {
-    cudaEvent_t a, b;
-    int cls;
-};
-
-struct kw_plan {
-    kw_problem prob;               // scalars (pointers are not retained)
-    int D = 3;
-    Geom g{};
-    int N[3] = {1, 1, 1};          // internal shape
-    double d[3] = {1, 1, 1};       // internal spacing
-    int comp_axis[3] = {0, 1, 2};
-    int Nt = 0, index_end = 0, record_start = 1, num_rec = 0;
-    bool time_rev = false, p0 = false, absorbing = false, has_tau = false, has_eta = false;
-    cudaStream_t stream = nullptr;
-
-    AxisFFT fft[3]{};
-    float2 *tw[3] = {nullptr, nullptr, nullptr};
-    float2 *dd_pos[3] = {nullptr, nullptr, nullptr}, *dd_neg[3] = {nullptr, nullptr, nullptr};
-    float2 *sh_neg[3] = {nullptr, nullptr, nullptr};
-    float *k2[3] = {nullptr, nullptr, nullptr};
-    float *pml[3] = {nullptr, nullptr, nullptr}, *pml_sg[3] = {nullptr, nullptr, nullptr};
-    OpParams op{};
-
-    // fields
-    float *p = nullptr, *rho[3] = {nullptr, nullptr, nullptr}, *u[3] = {nullptr, nullptr, nullptr};
-    float *rho_b[3] = {nullptr, nullptr, nullptr};   // second rho buffer (Stage R writes it, then they swap)
-    float *u_b[3] = {nullptr, nullptr, nullptr};     // second velocity buffer (Stage U writes it, then they swap)
-    float *srho = nullptr;                           // nonlinear mass coefficient q = 2 sum(rho) + rho0
-    float2 *spec[4] = {nullptr, nullptr, nullptr, nullptr};
-    float *p0_dev = nullptr;
-    int *d_t = nullptr;
-
-    // medium
-    float *c0_arr = nullptr, *rho0_arr = nullptr, *rsi_arr[3] = {nullptr, nullptr, nullptr};
-    float *bona_arr = nullptr;
-    Med c0{}, rho0{}, rsi[3]{}, bona{};
-    float *c2tau_arr = nullptr, *c2eta_arr = nullptr;
-    Med c2tau{}, c2eta{};           // c0^2 * absorb_tau, c0^2 * absorb_eta
-
-    SourceDev psrc, usrc;
-
-    // tiles
-    int PL_u = 1, PL_r = 1, PL_p = 1, PL_z = 1, TY = 1, NL = 1;
-    bool static_x = false, static_y = false, static_z = false;
-    int kz_chunks = 1;               // kz chunks of the y / x / y groups (L2 reuse)
-
-    // sensors / outputs
-    int M = 0;
-    int K = 1;                     // grid cells per sensor point (interpolated points: K > 1)
-    long long *sidx = nullptr;     // [M x K] column-major
-    bool sidx_all = false;         // the mask holds every cell (sidx[m] == m): gathers read cell m directly
-    float *sw = nullptr;           // [M x K] weights (K > 1)
-    float *tr_data = nullptr;
-    int *tr_off = nullptr, *tr_cell = nullptr, *tr_row = nullptr;
-    uint32_t rec = 0;
-    float *o_series[4] = {nullptr, nullptr, nullptr, nullptr};
-    float *o_max[4] = {nullptr, nullptr, nullptr, nullptr}, *o_min[4] = {nullptr, nullptr, nullptr, nullptr};
-    float *o_sq[4] = {nullptr, nullptr, nullptr, nullptr};
-    float *o_amax[4] = {nullptr, nullptr, nullptr, nullptr}, *o_amin[4] = {nullptr, nullptr, nullptr, nullptr};
-    float *o_tmp = nullptr;        // crop / rms staging
-    float *o_uns[3] = {nullptr, nullptr, nullptr};   // u_non_staggered series
-    float *ush = nullptr;          // one unstaggered velocity component
-    int in_lo[3] = {0, 0, 0}, in_n[3] = {1, 1, 1};
-    long long in_count = 1;
-
-    int t = 1;                     // next step to run (1-based)
-    bool started = false;
-    bool no_record = false;        // steps re-run by the gradient do not record
-
-    // timing
-    uint32_t timing_mask = 0;
-    std::vector<TimerRec> timers;
-    double t_ms[KW_KCLASS_COUNT] = {0};
-    uint64_t t_count[KW_KCLASS_COUNT] = {0};
-
-    // CUDA graphs of steady-state steps, keyed by the step's structure
-    struct GraphEntry {
-        cudaGraphExec_t exec = nullptr;
-        uint64_t launches = 0;
-        int seen = 0;
-    };
-    std::map<uint32_t, GraphEntry> graphs;
-    bool use_graphs = true;
-    float *rho_first = nullptr, *u_first = nullptr;   // buffer identity for the key
-
-    // streamed series outputs of kw_run: copy stream and per-slot events
-    cudaStream_t copy_stream = nullptr;
-    cudaEvent_t ev_comp[2] = {nullptr, nullptr}, ev_copy[2] = {nullptr, nullptr};
-
-    std::vector<void *> allocs;
-    size_t bytes = 0;
-    uint64_t launches = 0;
-    int device = 0;
-};
 
 namespace {
 
@@ -316,23 +206,7 @@ struct Scope {
     }
 };
 
-kw_status set_smem(const void *fn, size_t bytes) {
-    if (bytes > 48 * 1024) KW_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
-    return KW_OK;
-}
 
-kw_status launched(kw_plan *P) {
-    cudaError_t e = cudaGetLastError();
-    if (e != cudaSuccess) return fail(KW_ERR_CUDA, "kernel launch failed: %s", cudaGetErrorString(e));
-    P->launches += 1;
-    return KW_OK;
-}
-
-// ---- transform passes -----------------------------------------------------
-// ---- compile-time tile shapes --------------------------------------------
-// Axis lengths with compile-time kernels; every other length uses the
-// runtime-radix kernels.  Tile shapes of both are shared with the planner.
-#define KW_STATIC_SIZES(X) X(64) X(96) X(128) X(160) X(192) X(256) X(320) X(384) X(512)
 bool is_static(int n) {
     switch (n) {
 #define KW_CASE(N) case N:
@@ -353,38 +227,6 @@ kw_status dispatch(int n, A... args) {
 }
 
 // ---- transform passes -----------------------------------------------------
-template <int N> struct YLaunch {
-    template <int TY>
-    static kw_status go(kw_plan *P, bool inv, Spec4 bufs, dim3 grid, int kz0) {
-        constexpr int NT = ks_threads(N, TY);
-        constexpr size_t sh = (size_t)N * TY * sizeof(float2);
-        if (inv) {
-            KW_TRY(set_smem((const void *)ks_ypass<true, N, TY>, sh));
-            ks_ypass<true, N, TY><<<grid, NT, sh, P->stream>>>(bufs, P->g, P->tw[1], kz0);
-        } else {
-            KW_TRY(set_smem((const void *)ks_ypass<false, N, TY>, sh));
-            ks_ypass<false, N, TY><<<grid, NT, sh, P->stream>>>(bufs, P->g, P->tw[1], kz0);
-        }
-        return KW_OK;
-    }
-    static kw_status run(kw_plan *P, bool inv, Spec4 bufs, int nf, int kz0, int nkz) {
-        dim3 grid((P->g.N0 + P->TY - 1) / P->TY, N > 0 ? nkz : P->g.N2h, nf);
-        if constexpr (N > 0) {
-            if (P->TY == ks_lines(N)) KW_TRY(go<ks_lines(N)>(P, inv, bufs, grid, kz0));
-            else KW_TRY(go<ks_narrow(N)>(P, inv, bufs, grid, kz0));
-        } else {
-            size_t sh = (size_t)P->TY * P->g.N1 * sizeof(float2);
-            if (inv) {
-                KW_TRY(set_smem((const void *)k_ypass<true, 0, 0>, sh));
-                k_ypass<true, 0, 0><<<grid, kThreads, sh, P->stream>>>(bufs, P->g, P->fft[1], P->TY);
-            } else {
-                KW_TRY(set_smem((const void *)k_ypass<false, 0, 0>, sh));
-                k_ypass<false, 0, 0><<<grid, kThreads, sh, P->stream>>>(bufs, P->g, P->fft[1], P->TY);
-            }
-        }
-        return launched(P);
-    }
-};
 
 // kz planes [kz0, kz0 + nkz) only (static kernels); the runtime kernels
 // always take every plane and must be called with the full range
@@ -396,25 +238,6 @@ kw_status ypass(kw_plan *P, bool inv, Spec4 bufs, int nf, int kz0 = 0, int nkz =
     return dispatch<YLaunch>(P->static_y ? P->g.N1 : 0, P, inv, bufs, nf, kz0, nkz);
 }
 
-template <int N> struct XLaunch {
-    static kw_status run(kw_plan *P, Spec4 bufs, OpSet ops, int fanout, int nf, int kz0, int nkz) {
-        const int lines = P->g.N1 * (N > 0 ? nkz : P->g.N2h);
-        dim3 grid((lines + P->NL - 1) / P->NL, 1, fanout ? 1 : nf);
-        if constexpr (N > 0) {
-            if (P->NL == ks_xlines(N))
-                ks_xpass<N, ks_xlines(N)><<<grid, ks_threads(N, ks_xlines(N)), 0, P->stream>>>(bufs, P->g, P->tw[0], P->op,
-                                                                                            ops, fanout, kz0, nkz);
-            else
-                ks_xpass<N, ks_xnarrow(N)><<<grid, ks_threads(N, ks_xnarrow(N)), 0, P->stream>>>(bufs, P->g, P->tw[0],
-                                                                                              P->op, ops, fanout, kz0, nkz);
-        } else {
-            size_t sh = (size_t)(fanout ? 2 : 1) * P->NL * P->g.N0 * sizeof(float2);
-            KW_TRY(set_smem((const void *)k_xpass<0, 0>, sh));
-            k_xpass<0, 0><<<grid, kThreads, sh, P->stream>>>(bufs, P->g, P->fft[0], P->NL, P->op, ops, fanout);
-        }
-        return launched(P);
-    }
-};
 
 kw_status xpass(kw_plan *P, Spec4 bufs, OpSet ops, int fanout, int nf, int kz0 = 0, int nkz = -1) {
     if (P->static_x && !P->tw[0]) return fail(KW_ERR_INVALID, "internal: axis-0 twiddle table missing");
@@ -440,48 +263,6 @@ kw_status yxy_group(kw_plan *P, Spec4 bufs, int n, OpSet ops, bool fanout) {
     return KW_OK;
 }
 
-template <int N> struct ZR2CLaunch {
-    template <int PL>
-    static kw_status go(kw_plan *P, const float *R, float2 *H, dim3 grid) {
-        constexpr size_t sh = (size_t)N * PL * sizeof(float2);
-        KW_TRY(set_smem((const void *)ks_zr2c<N, PL>, sh));
-        ks_zr2c<N, PL><<<grid, ks_threads(N, PL), sh, P->stream>>>(R, H, P->g, P->tw[2]);
-        return KW_OK;
-    }
-    static kw_status run(kw_plan *P, const float *R, float2 *H) {
-        dim3 grid((P->g.N0 + 2 * P->PL_z - 1) / (2 * P->PL_z), P->g.N1, 1);
-        if constexpr (N > 0) {
-            if (P->PL_z == ks_lines(N)) KW_TRY(go<ks_lines(N)>(P, R, H, grid));
-            else KW_TRY(go<ks_narrow(N)>(P, R, H, grid));
-        } else {
-            size_t sh = (size_t)P->PL_z * P->g.N2 * sizeof(float2);
-            KW_TRY(set_smem((const void *)k_zr2c<0, 0>, sh));
-            k_zr2c<0, 0><<<grid, kThreads, sh, P->stream>>>(R, H, P->g, P->fft[2], P->PL_z);
-        }
-        return launched(P);
-    }
-};
-template <int N> struct ZC2RLaunch {
-    template <int PL>
-    static kw_status go(kw_plan *P, const float2 *H, float *R, dim3 grid) {
-        constexpr size_t sh = (size_t)N * PL * sizeof(float2);
-        KW_TRY(set_smem((const void *)ks_zc2r<N, PL>, sh));
-        ks_zc2r<N, PL><<<grid, ks_threads(N, PL), sh, P->stream>>>(H, R, P->g, P->tw[2]);
-        return KW_OK;
-    }
-    static kw_status run(kw_plan *P, const float2 *H, float *R) {
-        dim3 grid((P->g.N0 + 2 * P->PL_z - 1) / (2 * P->PL_z), P->g.N1, 1);
-        if constexpr (N > 0) {
-            if (P->PL_z == ks_lines(N)) KW_TRY(go<ks_lines(N)>(P, H, R, grid));
-            else KW_TRY(go<ks_narrow(N)>(P, H, R, grid));
-        } else {
-            size_t sh = (size_t)P->PL_z * P->g.N2 * sizeof(float2);
-            KW_TRY(set_smem((const void *)k_zc2r<0, 0>, sh));
-            k_zc2r<0, 0><<<grid, kThreads, sh, P->stream>>>(H, R, P->g, P->fft[2], P->PL_z);
-        }
-        return launched(P);
-    }
-};
 
 kw_status zr2c(kw_plan *P, const float *R, float2 *H) {
     if (P->static_z && !P->tw[2]) return fail(KW_ERR_INVALID, "internal: axis-2 twiddle table missing");
@@ -580,72 +361,6 @@ TRSrc tr_of(kw_plan *P) {
     return r;
 }
 
-template <int N> struct ULaunch {
-    template <int PL>
-    static kw_status go(kw_plan *P, const StageU &a, dim3 grid) {
-        using Z = ZStage<N, PL>;
-        const size_t sh = (size_t)(Z::TILE + 2 * Z::SLICE) * sizeof(float2);
-        KW_TRY(set_smem((const void *)ks_stage_u<N, PL>, sh));
-        ks_stage_u<N, PL><<<grid, Z::NT, sh, P->stream>>>(a, P->tw[2]);
-        return KW_OK;
-    }
-    static kw_status run(kw_plan *P, StageU a) {
-        dim3 grid((P->g.N0 + 2 * a.PL - 1) / (2 * a.PL), P->g.N1, P->D);
-        if constexpr (N > 0) {
-            if (a.PL == ks_lines(N)) KW_TRY(go<ks_lines(N)>(P, a, grid));
-            else KW_TRY(go<ks_narrow(N)>(P, a, grid));
-        } else {
-            size_t sh = (size_t)a.PL * P->g.N2 * sizeof(float2);
-            KW_TRY(set_smem((const void *)k_stage_u<0, 0>, sh));
-            k_stage_u<0, 0><<<grid, kThreads, sh, P->stream>>>(a);
-        }
-        return launched(P);
-    }
-};
-template <int N> struct RLaunch {
-    template <int PL>
-    static kw_status go(kw_plan *P, const StageR &a, dim3 grid) {
-        using Z = ZStage<N, PL>;
-        const size_t sh = (size_t)(Z::TILE + 2 * Z::SLICE) * sizeof(float2);
-        KW_TRY(set_smem((const void *)ks_stage_r<N, PL>, sh));
-        ks_stage_r<N, PL><<<grid, Z::NT, sh, P->stream>>>(a, P->tw[2]);
-        return KW_OK;
-    }
-    static kw_status run(kw_plan *P, StageR a) {
-        dim3 grid((P->g.N0 + 2 * a.PL - 1) / (2 * a.PL), P->g.N1, 1);
-        if constexpr (N > 0) {
-            if (a.PL == ks_lines(N)) KW_TRY(go<ks_lines(N)>(P, a, grid));
-            else KW_TRY(go<ks_narrow(N)>(P, a, grid));
-        } else {
-            size_t sh = (size_t)4 * a.PL * P->g.N2 * sizeof(float2);
-            KW_TRY(set_smem((const void *)k_stage_r<0, 0>, sh));
-            k_stage_r<0, 0><<<grid, kThreads, sh, P->stream>>>(a);
-        }
-        return launched(P);
-    }
-};
-template <int N> struct PLaunch {
-    template <int PL>
-    static kw_status go(kw_plan *P, const StageP &a, dim3 grid) {
-        using Z = ZStage<N, PL>;
-        const size_t sh = (size_t)(Z::TILE + 2 * Z::SLICE) * sizeof(float2);
-        KW_TRY(set_smem((const void *)ks_stage_p<N, PL>, sh));
-        ks_stage_p<N, PL><<<grid, Z::NT, sh, P->stream>>>(a, P->tw[2]);
-        return KW_OK;
-    }
-    static kw_status run(kw_plan *P, StageP a) {
-        dim3 grid((P->g.N0 + 2 * a.PL - 1) / (2 * a.PL), P->g.N1, 1);
-        if constexpr (N > 0) {
-            if (a.PL == ks_lines(N)) KW_TRY(go<ks_lines(N)>(P, a, grid));
-            else KW_TRY(go<ks_narrow(N)>(P, a, grid));
-        } else {
-            size_t sh = (size_t)2 * a.PL * P->g.N2 * sizeof(float2);
-            KW_TRY(set_smem((const void *)k_stage_p<0, 0>, sh));
-            k_stage_p<0, 0><<<grid, kThreads, sh, P->stream>>>(a);
-        }
-        return launched(P);
-    }
-};
 
 kw_status stage_u(kw_plan *P, int init, int t) {
     StageU a{};
