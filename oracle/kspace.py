@@ -424,6 +424,151 @@ def tone_burst_hann(sample_freq, signal_freq, num_cycles):
 # the solver
 # ---------------------------------------------------------------------------
 
+
+# ---------------------------------------------------------------------------
+# Array backends of the time loop.  The set-up always runs in NumPy; the loop
+# runs on NumPy (the default) or, as a fast FP64 oracle for full-size checks,
+# on torch.float64 tensors (CPU or CUDA, torch.fft).  Both execute the same
+# statements in the same order; only the array library differs.  Flat
+# indices handed to a backend are C-order (row-major) indices of arrays
+# indexed a[x, y, z], converted once from MATLAB's column-major ones.
+# ---------------------------------------------------------------------------
+
+class _NumpyBackend:
+    name = "numpy"
+
+    def put(self, a):
+        return a
+
+    def fftn(self, a):
+        return fftn(a)
+
+    def ifftn(self, a):
+        return ifftn(a)
+
+    def fft(self, a, axis):
+        return np.fft.fft(a, axis=axis)
+
+    def ifft(self, a, axis):
+        return np.fft.ifft(a, axis=axis)
+
+    real = staticmethod(np.real)
+    maximum = staticmethod(np.maximum)
+    minimum = staticmethod(np.minimum)
+    sqrt = staticmethod(np.sqrt)
+
+    def zeros(self, shape, complex_=False):
+        return np.zeros(shape, dtype=complex if complex_ else np.float64)
+
+    def full(self, v, shape):
+        return np.broadcast_to(v, shape).copy()
+
+    def copy(self, a):
+        return a.copy()
+
+    def take(self, field, idx):
+        return np.ascontiguousarray(field).reshape(-1)[idx]
+
+    def scatter_set(self, field, idx, vals):
+        f = np.array(field, dtype=np.float64, copy=True)
+        f.reshape(-1)[idx] = vals
+        return f
+
+    def scatter_add(self, field, idx, vals):
+        f = np.array(field, dtype=np.float64, copy=True)
+        f.reshape(-1)[idx] += vals
+        return f
+
+    def numpy(self, a):
+        return np.asarray(a)
+
+
+class _TorchBackend:
+    """The loop on torch.float64 / complex128 tensors (``device``: "cpu" or "cuda")."""
+    name = "torch"
+
+    def __init__(self, device):
+        import torch
+        self.t = torch
+        self.device = torch.device(device)
+
+    def put(self, a):
+        if a is None:
+            return None
+        if isinstance(a, (int, float, complex)):
+            return a
+        a = np.asarray(a)
+        if a.ndim == 0 or a.size == 1 and a.ndim == 0:
+            return complex(a) if np.iscomplexobj(a) else float(a)
+        if a.dtype.kind in "iu":
+            return self.t.as_tensor(np.ascontiguousarray(a, dtype=np.int64), device=self.device)
+        dt = self.t.complex128 if np.iscomplexobj(a) else self.t.float64
+        return self.t.as_tensor(np.ascontiguousarray(a), dtype=dt, device=self.device)
+
+    def fftn(self, a):
+        return self.t.fft.fftn(a)
+
+    def ifftn(self, a):
+        return self.t.fft.ifftn(a)
+
+    def fft(self, a, axis):
+        return self.t.fft.fft(a, dim=axis)
+
+    def ifft(self, a, axis):
+        return self.t.fft.ifft(a, dim=axis)
+
+    def real(self, a):
+        return a.real
+
+    def maximum(self, a, b):
+        return self.t.maximum(a, b)
+
+    def minimum(self, a, b):
+        return self.t.minimum(a, b)
+
+    def sqrt(self, a):
+        return self.t.sqrt(a)
+
+    def zeros(self, shape, complex_=False):
+        return self.t.zeros(shape, dtype=self.t.complex128 if complex_ else self.t.float64, device=self.device)
+
+    def full(self, v, shape):
+        if isinstance(v, self.t.Tensor):
+            return v.expand(shape).clone()
+        return self.t.full(shape, float(v), dtype=self.t.float64, device=self.device)
+
+    def copy(self, a):
+        return a.clone()
+
+    def take(self, field, idx):
+        return field.reshape(-1)[idx]
+
+    def scatter_set(self, field, idx, vals):
+        f = field.clone()
+        f.view(-1)[idx] = vals
+        return f
+
+    def scatter_add(self, field, idx, vals):
+        f = field.clone()
+        f.view(-1)[idx] += vals
+        return f
+
+    def numpy(self, a):
+        if isinstance(a, self.t.Tensor):
+            return a.detach().cpu().numpy()
+        return np.asarray(a)
+
+
+def _backend(device):
+    return _NumpyBackend() if device is None else _TorchBackend(device)
+
+
+def _f2c(idx, shape):
+    """MATLAB column-major linear indices -> C-order flat indices of a[x, y, z]."""
+    idx = np.asarray(idx, dtype=np.int64)
+    return np.ravel_multi_index(np.unravel_index(idx, shape, order="F"), shape).astype(np.int64)
+
+
 RECORD_FLAGS = ("p", "p_max", "p_min", "p_rms", "p_max_all", "p_min_all", "p_final",
                 "u", "u_max", "u_min", "u_rms", "u_max_all", "u_min_all", "u_final",
                 "u_non_staggered", "I", "I_avg")
@@ -452,9 +597,12 @@ def kspace_first_order(kgrid, medium, source, sensor, **opts):
 
     ``StepCallback`` (not a reference option) is called as f(t, p) with the
     pressure field after every time step t, for tests that need the field
-    history.
+    history.  ``Device`` (not a reference option) runs the loop on
+    torch.float64 tensors on that device ("cpu" or "cuda") instead of NumPy:
+    the fast FP64 oracle of the full-size checks.
     """
     step_callback = opts.pop("StepCallback", None)
+    device = opts.pop("Device", None)
     dim = kgrid.dim
     if dim not in (2, 3):
         raise ValueError("only 2D and 3D are restated")
@@ -613,27 +761,7 @@ def kspace_first_order(kgrid, medium, source, sensor, **opts):
     def find(m):
         return np.flatnonzero(np.asarray(m).ravel(order="F") != 0)
 
-    def gather(field, idx):
-        return field.ravel(order="F")[idx]
-
     sensor_interp = cart_linear(kgrid, cart_points) if cart_points is not None else None
-
-    def gather_s(field):
-        """the recorded value at every sensor point (extractSensorData.m:63-100, 301-352)"""
-        if sensor_interp is None:
-            return gather(field, sensor_idx)
-        tri, bc = sensor_interp
-        return (field.ravel(order="F")[tri] * bc).sum(axis=1)
-
-    def scatter_set(field, idx, vals):
-        f = field.ravel(order="F").copy()
-        f[idx] = vals
-        return f.reshape(shape, order="F")
-
-    def scatter_add(field, idx, vals):
-        f = field.ravel(order="F").copy()
-        f[idx] = f[idx] + vals
-        return f.reshape(shape, order="F")
 
     sensor_idx = find(mask) if mask is not None else None
 
@@ -753,28 +881,30 @@ def kspace_first_order(kgrid, medium, source, sensor, **opts):
         source_kappa = 1.0
 
     # ---- storage (createStorageVariables.m) ----
+    xp = _backend(device)
+    X = xp.put
     num_rec = Nt - record_start + 1
     out = {}
     M = sensor_idx.size if sensor_idx is not None else (cart_points.shape[1] if cart_points is not None else 0)
     if "p" in record:
-        out["p"] = np.zeros((M, num_rec))
+        out["p"] = xp.zeros((M, num_rec))
     if "p_rms" in record:
-        out["p_rms"] = np.zeros(M)
+        out["p_rms"] = xp.zeros(M)
     if "u" in record:
         for i in range(dim):
-            out[u_comps[i]] = np.zeros((M, num_rec))
+            out[u_comps[i]] = xp.zeros((M, num_rec))
     if "u_non_staggered" in record:
         for i in range(dim):
-            out[u_comps[i] + "_non_staggered"] = np.zeros((M, num_rec))
+            out[u_comps[i] + "_non_staggered"] = xp.zeros((M, num_rec))
     if "u_rms" in record:
         for i in range(dim):
-            out[u_comps[i] + "_rms"] = np.zeros(M)
+            out[u_comps[i] + "_rms"] = xp.zeros(M)
     shift_neg = None
     if "u_non_staggered" in record:
         shift_neg = []
         for a, kv in enumerate(kgrid.k_vecs()):
             s = ifftshift(np.exp(-1j * kv * kgrid.spacing[a] / 2)) if use_sg else np.ones(shape[a])
-            shift_neg.append(s)
+            shift_neg.append(X(_axis(s, a, dim)))
 
     # ---- time reversal data ----
     if time_rev:
@@ -782,72 +912,103 @@ def kspace_first_order(kgrid, medium, source, sensor, **opts):
         if reorder_index is not None:
             # inputChecking.m:640-648: rows re-sorted into find(mask) order
             trd = trd[np.argsort(order_index, kind="stable")]
-        trd = trd[:, ::-1]
+        trd = X(np.ascontiguousarray(trd[:, ::-1]))
         index_end = Nt - 1
     else:
         index_end = Nt
 
+    # ---- loop operands on the backend ----
+    sidx = X(_f2c(sensor_idx, shape)) if sensor_idx is not None else None
+    if sensor_interp is not None:
+        tri_c = X(_f2c(sensor_interp[0].ravel(order="C"), shape).reshape(sensor_interp[0].shape))
+        bc_x = X(sensor_interp[1])
+
+    def gather_s(field):
+        """the recorded value at every sensor point (extractSensorData.m:63-100, 301-352)"""
+        if sensor_interp is None:
+            return xp.take(field, sidx)
+        return (xp.take(field, tri_c) * bc_x).sum(1)
+
+    if source_p:
+        p_pos_x, p_sig_x, sp_x = X(_f2c(p_pos, shape)), X(p_sig), X(sp)
+    if any(source_u):
+        u_pos_x, u_sig_x = X(_f2c(u_pos, shape)), X(u_sig)
+        su_x = [X(v) for v in su]
+        u_row0 = X(np.zeros_like(u_sig))
+    pml, pml_sg = [X(v) for v in pml], [X(v) for v in pml_sg]
+    rho_sg_inv = [X(v) for v in rho_sg_inv]
+    dd_pos, dd_neg = [X(v) for v in dd_pos], [X(v) for v in dd_neg]
+    kappa, source_kappa = X(kappa), X(source_kappa)
+    if eos == "absorbing":
+        nabla1, nabla2, tau, eta = X(nabla1), X(nabla2), X(tau), X(eta)
+    elif eos == "stokes":
+        tau = X(tau)
+    rho0_x = X(rho0)
+    BonA_x = X(BonA) if nonlinear else None
+    if source_p0:
+        p0_x = X(p0)
+
     # ---- loop ----
-    p = np.zeros(shape)
-    rho = [np.zeros(shape) for _ in range(dim)]
-    u = [np.zeros(shape) for _ in range(dim)]
-    p_k = np.zeros(shape, dtype=complex)
-    c2 = c0 ** 2
+    p = xp.zeros(shape)
+    rho = [xp.zeros(shape) for _ in range(dim)]
+    u = [xp.zeros(shape) for _ in range(dim)]
+    p_k = xp.zeros(shape, complex_=True)
+    c2 = X(c0 ** 2)
 
     import time as _time
     _t0 = _time.perf_counter()
     for t in range(1, index_end + 1):
         if time_rev:
-            p = scatter_set(p, sensor_idx, trd[:, t - 1])
-            p_k = fftn(p)
+            p = xp.scatter_set(p, sidx, trd[:, t - 1])
+            p_k = xp.fftn(p)
             rmod = p / (dim * c2) if dim == 3 else 0.5 * p / c2
-            rmod = np.broadcast_to(rmod, shape)
+            rmod = xp.full(rmod, shape)
             for i in range(dim):
-                rho[i] = scatter_set(rho[i], sensor_idx, gather(np.ascontiguousarray(rmod), sensor_idx))
+                rho[i] = xp.scatter_set(rho[i], sidx, xp.take(rmod, sidx))
 
         # momentum (kspaceFirstOrder3D.m:792-803)
         for i in range(dim):
-            u[i] = pml_sg[i] * (pml_sg[i] * u[i] - dt * rho_sg_inv[i] * np.real(ifftn(dd_pos[i] * kappa * p_k)))
+            u[i] = pml_sg[i] * (pml_sg[i] * u[i] - dt * rho_sg_inv[i] * xp.real(xp.ifftn(dd_pos[i] * kappa * p_k)))
 
         # velocity sources (kspaceFirstOrder3D.m:806-886)
         for i in range(dim):
             if source_u[i] >= t:
-                rows = u_sig if su[i].shape[0] > 1 else np.zeros_like(u_sig)
-                vals = su[i][rows, t - 1]
+                rows = u_sig_x if su[i].shape[0] > 1 else u_row0
+                vals = su_x[i][rows, t - 1]
                 if u_mode == "dirichlet":
-                    u[i] = scatter_set(u[i], u_pos, vals)
+                    u[i] = xp.scatter_set(u[i], u_pos_x, vals)
                 elif u_mode == "additive":
-                    smat = scatter_set(np.zeros(shape), u_pos, vals)
-                    u[i] = u[i] + np.real(ifftn(source_kappa * fftn(smat)))
+                    smat = xp.scatter_set(xp.zeros(shape), u_pos_x, vals)
+                    u[i] = u[i] + xp.real(xp.ifftn(source_kappa * xp.fftn(smat)))
                 else:
-                    u[i] = scatter_add(u[i], u_pos, vals)
+                    u[i] = xp.scatter_add(u[i], u_pos_x, vals)
 
         # divergence (kspaceFirstOrder3D.m:907-909)
-        du = [np.real(ifftn(dd_neg[i] * kappa * fftn(u[i]))) for i in range(dim)]
+        du = [xp.real(xp.ifftn(dd_neg[i] * kappa * xp.fftn(u[i]))) for i in range(dim)]
 
         # mass conservation (kspaceFirstOrder3D.m:912-927)
         if not nonlinear:
             for i in range(dim):
-                rho[i] = pml[i] * (pml[i] * rho[i] - dt * rho0 * du[i])
+                rho[i] = pml[i] * (pml[i] * rho[i] - dt * rho0_x * du[i])
         else:
-            r0pr = 2 * sum(rho) + rho0
+            r0pr = 2 * sum(rho) + rho0_x
             for i in range(dim):
                 rho[i] = pml[i] * (pml[i] * rho[i] - dt * r0pr * du[i])
 
         # pressure sources (kspaceFirstOrder3D.m:930-962)
         if source_p >= t:
-            vals = sp[p_sig, t - 1]
+            vals = sp_x[p_sig_x, t - 1]
             if p_mode == "dirichlet":
                 for i in range(dim):
-                    rho[i] = scatter_set(rho[i], p_pos, vals)
+                    rho[i] = xp.scatter_set(rho[i], p_pos_x, vals)
             elif p_mode == "additive":
-                smat = scatter_set(np.zeros(shape), p_pos, vals)
-                smat = np.real(ifftn(source_kappa * fftn(smat)))
+                smat = xp.scatter_set(xp.zeros(shape), p_pos_x, vals)
+                smat = xp.real(xp.ifftn(source_kappa * xp.fftn(smat)))
                 for i in range(dim):
                     rho[i] = rho[i] + smat
             else:
                 for i in range(dim):
-                    rho[i] = scatter_add(rho[i], p_pos, vals)
+                    rho[i] = xp.scatter_add(rho[i], p_pos_x, vals)
 
         # equation of state (kspaceFirstOrder3D.m:965-1019)
         srho = sum(rho)
@@ -855,25 +1016,25 @@ def kspace_first_order(kgrid, medium, source, sensor, **opts):
         if eos == "lossless":
             p = c2 * srho
         elif eos == "absorbing":
-            p = c2 * (srho + tau * np.real(ifftn(nabla1 * fftn(rho0 * sdu)))
-                      - eta * np.real(ifftn(nabla2 * fftn(srho))))
+            p = c2 * (srho + tau * xp.real(xp.ifftn(nabla1 * xp.fftn(rho0_x * sdu)))
+                      - eta * xp.real(xp.ifftn(nabla2 * xp.fftn(srho))))
         else:
-            p = c2 * (srho + tau * rho0 * sdu)
+            p = c2 * (srho + tau * rho0_x * sdu)
         if nonlinear:
-            p = p + c2 * BonA * srho ** 2 / (2 * rho0)
-        p = np.broadcast_to(p, shape).copy()
+            p = p + c2 * BonA_x * srho ** 2 / (2 * rho0_x)
+        p = xp.full(p, shape)
 
         # p0 initial condition (kspaceFirstOrder3D.m:1023-1037)
         if t == 1 and source_p0:
-            p = p0.copy()
+            p = xp.copy(p0_x)
             for i in range(dim):
-                rho[i] = np.broadcast_to(p0 / (dim * c2), shape).copy()
-            pk0 = fftn(p)
+                rho[i] = xp.full(p0_x / (dim * c2), shape)
+            pk0 = xp.fftn(p)
             for i in range(dim):
-                u[i] = dt * rho_sg_inv[i] * np.real(ifftn(dd_pos[i] * kappa * pk0)) / 2
-                u[i] = np.broadcast_to(u[i], shape).copy()
+                u[i] = dt * rho_sg_inv[i] * xp.real(xp.ifftn(dd_pos[i] * kappa * pk0)) / 2
+                u[i] = xp.full(u[i], shape)
 
-        p_k = fftn(p)
+        p_k = xp.fftn(p)
         if step_callback is not None:
             step_callback(t, p)
 
@@ -885,48 +1046,49 @@ def kspace_first_order(kgrid, medium, source, sensor, **opts):
                 if "p" in record:
                     out["p"][:, fi - 1] = ps
                 if "p_max" in record:
-                    out["p_max"] = ps.copy() if fi == 1 else np.maximum(out["p_max"], ps)
+                    out["p_max"] = xp.copy(ps) if fi == 1 else xp.maximum(out["p_max"], ps)
                 if "p_min" in record:
-                    out["p_min"] = ps.copy() if fi == 1 else np.minimum(out["p_min"], ps)
+                    out["p_min"] = xp.copy(ps) if fi == 1 else xp.minimum(out["p_min"], ps)
                 if "p_rms" in record:
-                    out["p_rms"] = np.sqrt((out["p_rms"] ** 2 * (fi - 1) + ps ** 2) / fi)
+                    out["p_rms"] = xp.sqrt((out["p_rms"] ** 2 * (fi - 1) + ps ** 2) / fi)
                 for i in range(dim):
                     us = gather_s(u[i])
                     n = u_comps[i]
                     if "u" in record:
                         out[n][:, fi - 1] = us
                     if "u_max" in record:
-                        out[n + "_max"] = us.copy() if fi == 1 else np.maximum(out[n + "_max"], us)
+                        out[n + "_max"] = xp.copy(us) if fi == 1 else xp.maximum(out[n + "_max"], us)
                     if "u_min" in record:
-                        out[n + "_min"] = us.copy() if fi == 1 else np.minimum(out[n + "_min"], us)
+                        out[n + "_min"] = xp.copy(us) if fi == 1 else xp.minimum(out[n + "_min"], us)
                     if "u_rms" in record:
-                        out[n + "_rms"] = np.sqrt((out[n + "_rms"] ** 2 * (fi - 1) + us ** 2) / fi)
+                        out[n + "_rms"] = xp.sqrt((out[n + "_rms"] ** 2 * (fi - 1) + us ** 2) / fi)
                     if "u_non_staggered" in record:
-                        ush = np.real(np.fft.ifft(_axis(shift_neg[i], i, dim) * np.fft.fft(u[i], axis=i), axis=i))
+                        ush = xp.real(xp.ifft(shift_neg[i] * xp.fft(u[i], i), i))
                         out[n + "_non_staggered"][:, fi - 1] = gather_s(ush)
             ins = tuple(inside)
             if "p_max_all" in record:
-                out["p_max_all"] = p[ins].copy() if fi == 1 else np.maximum(out["p_max_all"], p[ins])
+                out["p_max_all"] = xp.copy(p[ins]) if fi == 1 else xp.maximum(out["p_max_all"], p[ins])
             if "p_min_all" in record:
-                out["p_min_all"] = p[ins].copy() if fi == 1 else np.minimum(out["p_min_all"], p[ins])
+                out["p_min_all"] = xp.copy(p[ins]) if fi == 1 else xp.minimum(out["p_min_all"], p[ins])
             for i in range(dim):
                 n = u_comps[i]
                 if "u_max_all" in record:
-                    out[n + "_max_all"] = u[i][ins].copy() if fi == 1 else np.maximum(out[n + "_max_all"], u[i][ins])
+                    out[n + "_max_all"] = xp.copy(u[i][ins]) if fi == 1 else xp.maximum(out[n + "_max_all"], u[i][ins])
                 if "u_min_all" in record:
-                    out[n + "_min_all"] = u[i][ins].copy() if fi == 1 else np.minimum(out[n + "_min_all"], u[i][ins])
+                    out[n + "_min_all"] = xp.copy(u[i][ins]) if fi == 1 else xp.minimum(out[n + "_min_all"], u[i][ins])
 
     global LAST_LOOP_SECONDS
     LAST_LOOP_SECONDS = _time.perf_counter() - _t0
     if time_rev:
-        p = scatter_set(p, sensor_idx, trd[:, index_end])
+        p = xp.scatter_set(p, sidx, trd[:, index_end])
         record.add("p_final")
     ins = tuple(inside)
     if "p_final" in record:
-        out["p_final"] = p[ins].copy()
+        out["p_final"] = xp.copy(p[ins])
     if "u_final" in record:
         for i in range(dim):
-            out[u_comps[i] + "_final"] = u[i][ins].copy()
+            out[u_comps[i] + "_final"] = xp.copy(u[i][ins])
+    out = {k: np.array(xp.numpy(v), dtype=np.float64) for k, v in out.items()}
 
     # intensity (kspaceFirstOrder_saveIntensity.m): u_non_staggered shifted
     # forward in time by dt/2, times p; I_avg is its time average
