@@ -36,9 +36,9 @@ typedef int kw_status;
 #define KW_ERR_CUDA        2   /* CUDA runtime failure */
 #define KW_ERR_NOMEM       3   /* device allocation failed */
 #define KW_ERR_UNSUPPORTED 4   /* valid reference input this build does not handle */
-#define KW_ERR_TIMEOUT     5   /* a bounded device wait gave up */
+#define KW_ERR_TIMEOUT     5   /* a bounded wait gave up, or a served request passed its deadline */
 
-#define KW_ABI_VERSION 2
+#define KW_ABI_VERSION 3
 
 /* sensor.record bit mask (inputChecking.m:340-400 list of record flags) */
 #define KW_REC_P               (1u << 0)
@@ -93,6 +93,22 @@ typedef struct kw_source {
     const float *input;          /* [num_signals x num_time_samples], already scaled
                                     by scaleSourceTerms.m */
 } kw_source;
+
+/*
+ * The velocity source of a transducer (kWaveTransducer as `source`):
+ * kspaceFirstOrder_inputChecking.m:1160-1209 and the loop hook of
+ * kspaceFirstOrder3D.m:888-904.  While t <= signal_length - max(delay),
+ * ux at point i gains apodization[i] * input_signal[delay[i] + t - 1]
+ * (additive, no k-space correction).  3-D only; excludes u_source.
+ */
+typedef struct kw_transducer_source {
+    uint64_t num_points;         /* active element grid points, 0 = none */
+    const uint64_t *index;       /* [num_points] 1-based, increasing: find(active_elements_mask) */
+    const uint64_t *delay;       /* [num_points] beamforming delay in samples (delay_mask, 0-based) */
+    const float *apodization;    /* [num_points] transmit apodization, or NULL ('Rectangular') */
+    uint64_t signal_length;      /* samples of input_signal */
+    const float *input_signal;   /* already scaled by 2 c0 dt / dx (scaleSourceTerms.m:377-390) */
+} kw_transducer_source;
 
 typedef struct kw_problem {
     uint32_t abi_version;        /* KW_ABI_VERSION */
@@ -163,6 +179,15 @@ typedef struct kw_problem {
        1-based in any order.  Time reversal and the gradient need K <= 1. */
     uint32_t sensor_vertices;
     const float *sensor_weights;
+
+    /* medium.alpha_filter (createAbsorptionVariables.m:56-76): N values in
+       natural (fftshift-ed) wavenumber order, laid out like the other grid
+       arrays (array_order), multiplying both absorption operators; NULL when
+       absent.  Power-law absorption only (absorbing_flag KW_ABSORBING). */
+    const float *alpha_filter;
+
+    /* transducer velocity source; num_points 0 when absent */
+    kw_transducer_source transducer_source;
 } kw_problem;
 
 /* Output sizes (createStorageVariables.m:58-88). */
@@ -260,6 +285,11 @@ typedef struct kw_server_config {
     uint64_t hbm_budget_bytes;   /* admission budget; 0 = 80% of free memory */
     int32_t  max_active;         /* simulations resident at once; 0 = 32 */
     int32_t  steps_per_slice;    /* steps issued per simulation per round; 0 = 32 */
+    /* Watchdog: a request still running this many milliseconds after its
+       admission is stopped -- no further steps are issued, the work already
+       issued drains, its memory and slot are released -- and its waiter gets
+       KW_ERR_TIMEOUT.  0 = no deadline. */
+    uint32_t request_timeout_ms;
 } kw_server_config;
 
 typedef struct kw_server_stats {
@@ -278,6 +308,11 @@ kw_status kw_server_create(const kw_server_config *config, kw_server **server);
 kw_status kw_server_submit(kw_server *server, const kw_problem *problem, uint64_t *ticket);
 /* Blocks until the request is done; copies its outputs (like kw_copy_outputs). */
 kw_status kw_server_wait(kw_server *server, uint64_t ticket, kw_outputs *out, double *latency_ms);
+/* kw_server_wait bounded by timeout_ms of host time: returns KW_ERR_TIMEOUT
+   if the request has not finished by then; the ticket stays valid and a
+   later wait returns its result. */
+kw_status kw_server_wait_for(kw_server *server, uint64_t ticket, uint32_t timeout_ms, kw_outputs *out,
+                             double *latency_ms);
 kw_status kw_server_get_stats(kw_server *server, kw_server_stats *stats);
 /* Stops the worker after the admitted and pending requests finish. */
 kw_status kw_server_destroy(kw_server *server);
@@ -339,12 +374,17 @@ kw_status kw_adjoint_gradient(kw_plan *plan, const float *residual, uint32_t che
  *
  * It calls no cudaMalloc or cudaFree.  Its only other device memory is one
  * file-scope array of 32 MiB, held by every GPU that loads the library until
- * the process exits; grids whose spectrum and operator tables do not fit
- * (above about 4.1 million cells) are rejected with KW_ERR_UNSUPPORTED.  The
- * first call on each device looks up the array's device address with that
- * device current; make that first call before any stream capture.  Every call
- * shares the array, so calls that overlap on the GPU (other host threads,
- * other streams) race; issue them one at a time.
+ * the process exits.  The array holds the half spectrum, shape[0] *
+ * shape[1] * (floor(shape[2] / 2) + 1) complex FP32 values in 3-D
+ * (shape[0] * (floor(shape[1] / 2) + 1) in 2-D), plus a few kilobytes of
+ * operator tables, so grids of up to about 8.3 million cells fit: 200^3 is
+ * accepted, 256 x 256 x 128 is rejected with KW_ERR_UNSUPPORTED.  The first
+ * call on each device looks up the array's device address with that device
+ * current; make that first call before any stream capture.  The address is
+ * kept for the life of the process: after cudaDeviceReset it is stale, so do
+ * not call this entry point again in a process that has reset the device.
+ * Every call shares the array, so calls that overlap on the GPU (other host
+ * threads, other streams) race; issue them one at a time.
  */
 kw_status kw_gradient_noalloc(int32_t dim, const uint64_t shape[3], const double spacing[3], int32_t axis,
                               int32_t shift_sign, double c_ref, double dt, int32_t use_kspace,

@@ -8,7 +8,8 @@
 // radix stages in shared memory and writes it back once.
 //
 // Algorithm: the Stockham autosort formulation (natural-order input and
-// output, no bit reversal), radices 2/3/4/5/7.  Stage with radix R and
+// output, no bit reversal), radices 2/3/4/5/7 in registers and any other
+// prime factor as a direct sum (fft_stage_any).  Stage with radix R and
 // current sub-transform length Ns: butterfly j reads x[j + t*n/R]
 // (t = 0..R-1), multiplies by w^(t*k) with k = j mod Ns and
 // w = exp(-2 pi i / (Ns R)), runs an R-point DFT and writes
@@ -274,6 +275,56 @@ __device__ __forceinline__ void fft_stage(float2 *s, int n, int Ns, int nl, int 
     __syncthreads();
 }
 
+// One Stockham stage of any radix R (the prime factors above 7): every output
+// is a direct R-term sum.  Output q of butterfly j (k = j mod Ns) is
+//   sum_t x[j + t n/R] w^(t k) w_R^(t q) = sum_t x[j + t n/R] tw[t e mod n],
+// e = k n/(Ns R) + q n/R, written to (j / Ns) Ns R + k + q Ns.  The sums run
+// in FP64 (R can be in the thousands); a thread owns at most kVPT outputs of
+// the tile, held in registers until every thread has read its inputs.
+template <bool INV>
+__device__ __noinline__ void fft_stage_any(float2 *s, int n, int R, int Ns, int nl, int es, int ls,
+                                           const float2 *__restrict__ tw) {
+    const int nb = n / R;
+    const int total = n * nl;
+    const int twstride = n / (Ns * R);
+    float2 out[kVPT];
+#pragma unroll
+    for (int b = 0; b < kVPT; ++b) {
+        const int g = threadIdx.x + b * kThreads;
+        if (g < total) {
+            const int l = g / n, r = g % n;
+            const int j = r % nb, q = r / nb;
+            const int k = j % Ns;
+            const int e = (int)(((long long)k * twstride + (long long)q * nb) % n);
+            const float2 *line = s + l * ls;
+            double re = 0.0, im = 0.0;
+            int m = 0;
+            for (int t = 0; t < R; ++t) {
+                const float2 x = line[(j + t * nb) * es];
+                float2 w = __ldg(tw + m);
+                if (INV) w.y = -w.y;
+                re = fma((double)x.x, (double)w.x, fma(-(double)x.y, (double)w.y, re));
+                im = fma((double)x.x, (double)w.y, fma((double)x.y, (double)w.x, im));
+                m += e;
+                if (m >= n) m -= n;
+            }
+            out[b] = make_float2((float)re, (float)im);
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int b = 0; b < kVPT; ++b) {
+        const int g = threadIdx.x + b * kThreads;
+        if (g < total) {
+            const int l = g / n, r = g % n;
+            const int j = r % nb, q = r / nb;
+            const int k = j % Ns;
+            s[l * ls + ((j / Ns) * Ns * R + k + q * Ns) * es] = out[b];
+        }
+    }
+    __syncthreads();
+}
+
 // Full transform of every line of the tile (unnormalised in both directions).
 // Must be called by all threads of the block; the caller synchronises before.
 template <bool INV>
@@ -287,7 +338,7 @@ __device__ void fft_tile(float2 *s, const AxisFFT &ax, int nl, int es, int ls, b
             case 3: fft_stage<3, INV>(s, ax.n, Ns, nl, es, ls, lines_fast, ax.tw); break;
             case 5: fft_stage<5, INV>(s, ax.n, Ns, nl, es, ls, lines_fast, ax.tw); break;
             case 7: fft_stage<7, INV>(s, ax.n, Ns, nl, es, ls, lines_fast, ax.tw); break;
-            default: break;
+            default: fft_stage_any<INV>(s, ax.n, R, Ns, nl, es, ls, ax.tw); break;
         }
         Ns *= R;
     }

@@ -92,6 +92,11 @@ struct OpParams {
     int use_kspace;
     float nabla1_exp, nabla2_exp;  // alpha_power - 2, alpha_power - 1
     float scale;               // 1 / (N0 N1 N2)
+    // medium.alpha_filter on the z-half spectrum (Hermitian part, FFT order,
+    // element (x, y, kz) at x + N0 (y + N1 kz)) multiplying both absorption
+    // operators; NULL when absent
+    const float *filt;
+    int n0, n1;
 };
 
 struct OpSet {
@@ -143,8 +148,12 @@ __device__ __forceinline__ float2 eval_op(const OpParams &P, int kind, int axis,
             const int i = axis == 0 ? ix : (axis == 1 ? iy : iz);
             return cscale(__ldg(P.sh_neg[axis] + i), P.scale);
         }
-        case OP_NABLA1: return make_float2(pow_k(km, P.nabla1_exp) * P.scale, 0.f);
-        case OP_NABLA2: return make_float2(pow_k(km, P.nabla2_exp) * P.scale, 0.f);
+        case OP_NABLA1:
+        case OP_NABLA2: {
+            float v = pow_k(km, kind == OP_NABLA1 ? P.nabla1_exp : P.nabla2_exp) * P.scale;
+            if (P.filt) v *= __ldg(P.filt + ix + (long long)P.n0 * (iy + (long long)P.n1 * iz));
+            return make_float2(v, 0.f);
+        }
         case OP_SRC_KAPPA: {
             const float c = P.use_kspace ? cosf(P.kappa_a * km) : 1.f;
             return make_float2(c * P.scale, 0.f);

@@ -299,6 +299,7 @@ __global__ void __launch_bounds__(ks_threads(N0, NL), 3 * kThreads / ks_threads(
             } else if (kind0 == OP_NABLA1 || kind0 == OP_NABLA2) {
                 const float e = kind0 == OP_NABLA1 ? P.nabla1_exp : P.nabla2_exp;
                 fac = k2 == 0.f ? (e > 0.f ? 0.f : (e == 0.f ? 1.f : 0.f)) : pow_pos(k2, 0.5f * e);
+                if (P.filt) fac *= __ldg(P.filt + (long long)min(line0 + l, lines_total - 1) * N0 + ix);
             } else if (kind0 == OP_SRC_KAPPA) {
                 fac = P.use_kspace ? cos_series(P.kappa_a * P.kappa_a * k2) : 1.f;
             } else {

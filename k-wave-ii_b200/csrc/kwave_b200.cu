@@ -74,7 +74,11 @@ bool factorize(int n, std::vector<int> &radix) {
     const int primes[3] = {3, 5, 7};
     for (int p : primes)
         while (n % p == 0) { radix.push_back(p); n /= p; }
-    return n == 1 && radix.size() <= (size_t)kMaxStages;
+    // any other prime factor: a direct-sum stage (fft_stage_any)
+    for (int p = 11; n > 1 && (long long)p * p <= n; p += 2)
+        while (n % p == 0) { radix.push_back(p); n /= p; }
+    if (n > 1) radix.push_back(n);
+    return radix.size() <= (size_t)kMaxStages;
 }
 
 // kWaveGrid.makeDim (kWaveGrid.m:779-797) in FFT order (ifftshift applied)
@@ -660,7 +664,12 @@ kw_status setup_source(kw_plan *P, SourceDev &S, const kw_source *src, int ncomp
         if (i > 0 && v <= s0.index[i - 1]) return fail(KW_ERR_INVALID, "source indices must be increasing (find(mask) order)");
         pos[i] = (long long)v - 1;
     }
-    S.nsig = (int)s0.num_signals;
+    // components may differ in row count when the mask is binary: one row
+    // drives every point (MATLAB's source.ux(':', t) scalar expansion), or one
+    // row per point (kspaceFirstOrder_inputChecking.m:966-984)
+    S.nsig = 1;
+    for (int c = 0; c < ncomp; ++c)
+        if (src[c].num_time_samples > 0) S.nsig = std::max(S.nsig, (int)src[c].num_signals);
     std::vector<int> row(S.npts);
     for (int i = 0; i < S.npts; ++i) {
         if (s0.signal_index) {
@@ -680,17 +689,24 @@ kw_status setup_source(kw_plan *P, SourceDev &S, const kw_source *src, int ncomp
     const bool fast = S.mode == KW_SOURCE_ADDITIVE && one_row;
     for (int c = 0; c < ncomp; ++c) {
         if (src[c].num_time_samples == 0) continue;
-        if (src[c].num_signals != s0.num_signals || !src[c].input)
+        const int ns = (int)src[c].num_signals;
+        if (!src[c].input || (ns != S.nsig && (ns != 1 || s0.signal_index)))
             return fail(KW_ERR_INVALID, "velocity source components must share the mask and the number of signals");
         S.T[c] = (int)std::min<uint64_t>(src[c].num_time_samples, (uint64_t)P->Nt);
+        const size_t len = src[c].num_time_samples;
         if (fast) {
             // one signal drives every point: keep that row only
             std::vector<float> h(S.T[c]);
-            for (int tt = 0; tt < S.T[c]; ++tt) h[tt] = src[c].input[row[0] + (size_t)S.nsig * tt];
+            for (int tt = 0; tt < S.T[c]; ++tt) h[tt] = src[c].input[(ns == 1 ? 0 : row[0]) + (size_t)ns * tt];
             KW_TRY(pupload(P, &S.sig[c], h.data(), h.size()));
+        } else if (ns == S.nsig) {
+            KW_TRY(pupload(P, &S.sig[c], src[c].input, (size_t)S.nsig * len));
         } else {
-            const size_t cnt = (size_t)S.nsig * src[c].num_time_samples;
-            KW_TRY(pupload(P, &S.sig[c], src[c].input, cnt));
+            // a one-row component beside per-point ones: the row for every point
+            std::vector<float> h((size_t)S.nsig * len);
+            for (size_t tt = 0; tt < len; ++tt)
+                for (int r = 0; r < S.nsig; ++r) h[r + (size_t)S.nsig * tt] = src[c].input[tt];
+            KW_TRY(pupload(P, &S.sig[c], h.data(), h.size()));
         }
     }
     KW_TRY(pupload(P, &S.pos, pos.data(), pos.size()));
@@ -882,6 +898,83 @@ kw_status autotune_tiles(kw_plan *P) {
     return KW_OK;
 }
 
+// medium.alpha_filter multiplies both absorption operators in natural
+// wavenumber order: nabla <- ifftshift(fftshift(nabla) .* alpha_filter)
+// (createAbsorptionVariables.m:56-76), i.e. the operator in FFT order times
+// ifftshift(alpha_filter).  real(ifftn(op X)) of a real field sees only the
+// Hermitian part of a real op, (f(k) + f(-k)) / 2, which is tabulated on the
+// z-half spectrum (element (x, y, kz) at x + N0 (y + N1 kz)) in FP64 and
+// stored FP32.
+kw_status build_alpha_filter(kw_plan *P, const kw_problem &q, const int *phys_of_int) {
+    const Geom &g = P->g;
+    const uint64_t dims[3] = {q.Nx, q.Ny, q.dim == 3 ? q.Nz : 1};
+    // user array element at physical (x, y, z), natural order
+    auto at = [&](long long x, long long y, long long z) -> double {
+        long long i;
+        if (q.array_order == KW_ROW_MAJOR)
+            i = q.dim == 3 ? z + (long long)dims[2] * (y + (long long)dims[1] * x) : y + (long long)dims[1] * x;
+        else
+            i = x + (long long)dims[0] * (y + (long long)dims[1] * z);
+        return (double)q.alpha_filter[i];
+    };
+    const int n[3] = {g.N0, g.N1, g.N2};
+    std::vector<float> h((size_t)g.Nh);
+    for (int i2 = 0; i2 < g.N2h; ++i2)
+        for (int i1 = 0; i1 < g.N1; ++i1)
+            for (int i0 = 0; i0 < g.N0; ++i0) {
+                const int fi[3] = {i0, i1, i2};
+                long long pos[3] = {0, 0, 0}, neg[3] = {0, 0, 0};   // physical (x, y, z), natural order
+                for (int a = 0; a < 3; ++a) {
+                    const int pa = phys_of_int[a];
+                    if (pa < 0) continue;
+                    pos[pa] = (fi[a] + n[a] / 2) % n[a];
+                    neg[pa] = ((n[a] - fi[a]) % n[a] + n[a] / 2) % n[a];
+                }
+                const double v = 0.5 * (at(pos[0], pos[1], pos[2]) + at(neg[0], neg[1], neg[2]));
+                h[(size_t)i0 + (size_t)g.N0 * (i1 + (size_t)g.N1 * i2)] = (float)v;
+            }
+    float *d = nullptr;
+    KW_TRY(pupload(P, &d, h.data(), h.size()));
+    P->op.filt = d;
+    P->op.n0 = g.N0;
+    P->op.n1 = g.N1;
+    return KW_OK;
+}
+
+// The transducer's delayed, apodised drive (kspaceFirstOrder3D.m:888-904):
+// point i adds apodization[i] * s[delay[i] + t - 1] to ux while
+// t <= L - max(delay), which is an additive-no-correction ux source whose
+// row i is that delayed series; the rows are formed here and run through
+// the sparse source path of the momentum stage.
+kw_status transducer_as_source(kw_plan *P, const kw_problem &q, kw_source us[3], std::vector<float> &sig) {
+    const kw_transducer_source &ts = q.transducer_source;
+    for (int c = 0; c < 3; ++c) us[c] = kw_source{};
+    if (q.dim != 3) return fail(KW_ERR_INVALID, "Transducer inputs are only compatible with 3D simulations.");
+    for (int c = 0; c < 3; ++c)
+        if (q.u_source[c].num_time_samples)
+            return fail(KW_ERR_INVALID, "a transducer source excludes source.ux / uy / uz");
+    if (!ts.index || !ts.delay || !ts.input_signal || ts.signal_length == 0)
+        return fail(KW_ERR_INVALID, "transducer source: index, delay and input_signal must be given");
+    uint64_t dmax = 0;
+    for (uint64_t i = 0; i < ts.num_points; ++i) dmax = std::max(dmax, ts.delay[i]);
+    if (dmax >= ts.signal_length) return KW_OK;   // never active (flags.transducer_source <= 0)
+    const uint64_t T = std::min<uint64_t>(ts.signal_length - dmax, (uint64_t)P->Nt);
+    const uint64_t n = ts.num_points;
+    sig.assign((size_t)(n * T), 0.f);
+    for (uint64_t t = 0; t < T; ++t)
+        for (uint64_t i = 0; i < n; ++i)
+            sig[i + n * t] = (ts.apodization ? ts.apodization[i] : 1.f) * ts.input_signal[ts.delay[i] + t];
+    us[0].num_time_samples = T;
+    us[0].mode = KW_SOURCE_ADDITIVE_NO_CORRECTION;
+    us[0].num_points = n;
+    us[0].index = ts.index;
+    us[0].num_signals = n;
+    us[0].signal_index = nullptr;
+    us[0].input = sig.data();
+    (void)P;
+    return KW_OK;
+}
+
 kw_status create(const kw_problem *pr, kw_plan *P) {
     if (!pr) return fail(KW_ERR_INVALID, "problem is NULL");
     if (pr->abi_version != KW_ABI_VERSION) return fail(KW_ERR_INVALID, "abi_version %u, library expects %d", pr->abi_version, KW_ABI_VERSION);
@@ -957,7 +1050,7 @@ kw_status create(const kw_problem *pr, kw_plan *P) {
     for (int a = 0; a < 3; ++a) {
         const int n = P->N[a];
         std::vector<int> rad;
-        if (!factorize(n, rad)) return fail(KW_ERR_UNSUPPORTED, "grid size %d has a prime factor above 7", n);
+        if (!factorize(n, rad)) return fail(KW_ERR_UNSUPPORTED, "grid size %d needs more than %d transform stages", n, kMaxStages);
         AxisFFT &f = P->fft[a];
         f.n = n;
         f.nstages = (int)rad.size();
@@ -1153,6 +1246,12 @@ kw_status create(const kw_problem *pr, kw_plan *P) {
             P->c2eta.val = (float)(c * c * eta * sg1);
         }
     }
+    if (q.alpha_filter) {
+        if (q.absorbing_flag != KW_ABSORBING)
+            return fail(KW_ERR_INVALID, "Input option medium.alpha_filter is not supported with medium.alpha_mode = 'stokes' "
+                        "or without absorption.");
+        KW_TRY(build_alpha_filter(P, q, phys_of_int));
+    }
     if (P->p0) KW_TRY(upload_grid(&P->p0_dev, q.p0_source_input));
     {
         int hf = 0;
@@ -1164,7 +1263,14 @@ kw_status create(const kw_problem *pr, kw_plan *P) {
 
     // sources
     KW_TRY(setup_source(P, P->psrc, &q.p_source, 1, P->PL_r));
-    KW_TRY(setup_source(P, P->usrc, q.u_source, P->D, P->PL_u));
+    if (q.transducer_source.num_points) {
+        kw_source us[3];
+        std::vector<float> sig;
+        KW_TRY(transducer_as_source(P, q, us, sig));
+        KW_TRY(setup_source(P, P->usrc, us, P->D, P->PL_u));
+    } else {
+        KW_TRY(setup_source(P, P->usrc, q.u_source, P->D, P->PL_u));
+    }
 
     // sensors
     P->rec = q.record;
@@ -1723,7 +1829,7 @@ kw_status kw_gradient_noalloc(int32_t dim, const uint64_t shape[3], const double
     const size_t o_dd = off; off = align256(off + (size_t)n[iaxis] * sizeof(float2));
     if (off > KW_NOALLOC_SCRATCH_BYTES)
         return fail(KW_ERR_UNSUPPORTED, "grid needs %zu bytes of scratch; kw_gradient_noalloc is limited to %zu bytes "
-                    "(about 4.1 million cells)", off, (size_t)KW_NOALLOC_SCRATCH_BYTES);
+                    "(the half spectrum of about 8.3 million cells)", off, (size_t)KW_NOALLOC_SCRATCH_BYTES);
 
     int dev = 0;
     KW_CUDA(cudaGetDevice(&dev));
@@ -1734,7 +1840,7 @@ kw_status kw_gradient_noalloc(int32_t dim, const uint64_t shape[3], const double
 
     for (int a = 0; a < 3; ++a) {
         std::vector<int> rad;
-        if (!factorize(n[a], rad)) return fail(KW_ERR_UNSUPPORTED, "grid size %d has a prime factor above 7", n[a]);
+        if (!factorize(n[a], rad)) return fail(KW_ERR_UNSUPPORTED, "grid size %d needs more than %d transform stages", n[a], kMaxStages);
         AxisFFT &f = P.fft[a];
         f.n = n[a];
         f.nstages = (int)rad.size();

@@ -8,12 +8,13 @@ the in-tree C-ABI library ``libkwave_b200.so`` (include/kwave_b200.h); there
 is no CPU fallback.
 """
 from .kgrid import kWaveGrid
-from .helpers import makeDisc, makeBall, makeCartCircle, cart2grid, smooth, getWin, reorderBinarySensorData
+from .helpers import (makeDisc, makeBall, makeCartCircle, cart2grid, smooth, getWin, reorderBinarySensorData,
+                      TransducerSource)
 from .solver import Simulation, Server, kspaceFirstOrder2D, kspaceFirstOrder3D, KWaveInputError
 from ._abi import KWaveError, load_library, LIB_PATH
 
 __all__ = [
     "kWaveGrid", "makeDisc", "makeBall", "makeCartCircle", "cart2grid", "smooth", "getWin",
-    "reorderBinarySensorData", "Simulation", "Server", "kspaceFirstOrder2D", "kspaceFirstOrder3D",
+    "reorderBinarySensorData", "TransducerSource", "Simulation", "Server", "kspaceFirstOrder2D", "kspaceFirstOrder3D",
     "KWaveInputError", "KWaveError", "load_library", "LIB_PATH",
 ]

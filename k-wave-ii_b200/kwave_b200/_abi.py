@@ -14,7 +14,7 @@ import numpy as np
 LIB_NAME = "libkwave_b200.so"
 LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), LIB_NAME)
 
-KW_ABI_VERSION = 2
+KW_ABI_VERSION = 3
 
 KW_OK = 0
 KW_ERR_INVALID = 1
@@ -60,6 +60,11 @@ class kw_source(C.Structure):
     ]
 
 
+class kw_transducer_source(C.Structure):
+    _fields_ = [("num_points", C.c_uint64), ("index", u64p), ("delay", u64p), ("apodization", f32p),
+                ("signal_length", C.c_uint64), ("input_signal", f32p)]
+
+
 class kw_problem(C.Structure):
     _fields_ = [
         ("abi_version", C.c_uint32),
@@ -97,6 +102,8 @@ class kw_problem(C.Structure):
         ("derive_rho0_sg", C.c_int32),
         ("sensor_vertices", C.c_uint32),
         ("sensor_weights", f32p),
+        ("alpha_filter", f32p),
+        ("transducer_source", kw_transducer_source),
     ]
 
 
@@ -122,7 +129,7 @@ class kw_outputs(C.Structure):
 # every symbol the header declares, with its signature
 class kw_server_config(C.Structure):
     _fields_ = [("device", C.c_int32), ("hbm_budget_bytes", C.c_uint64), ("max_active", C.c_int32),
-                ("steps_per_slice", C.c_int32)]
+                ("steps_per_slice", C.c_int32), ("request_timeout_ms", C.c_uint32)]
 
 
 class kw_server_stats(C.Structure):
@@ -159,6 +166,8 @@ SYMBOLS = {
     "kw_server_create": (C.c_int, [C.POINTER(kw_server_config), C.POINTER(C.c_void_p)]),
     "kw_server_submit": (C.c_int, [C.c_void_p, C.POINTER(kw_problem), C.POINTER(C.c_uint64)]),
     "kw_server_wait": (C.c_int, [C.c_void_p, C.c_uint64, C.POINTER(kw_outputs), C.POINTER(C.c_double)]),
+    "kw_server_wait_for": (C.c_int, [C.c_void_p, C.c_uint64, C.c_uint32, C.POINTER(kw_outputs),
+                                     C.POINTER(C.c_double)]),
     "kw_server_get_stats": (C.c_int, [C.c_void_p, C.POINTER(kw_server_stats)]),
     "kw_server_destroy": (C.c_int, [C.c_void_p]),
 }

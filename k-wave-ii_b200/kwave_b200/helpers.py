@@ -196,3 +196,26 @@ def cartLinearWeights(shape, spacing, cart_data):
         tri[:, k + 1] = np.ravel_multi_index(tuple(v), tuple(shape), order="F")
         bc[:, k + 1] = fs[k] - (fs[k + 1] if k + 1 < dim else 0.0)
     return tri, bc
+
+
+class TransducerSource:
+    """The transmit side of a kWaveTransducer used as ``source``: the
+    properties the reference's setup reads for the loop's transducer hook
+    (kspaceFirstOrder_inputChecking.m:1160-1209, kspaceFirstOrder3D.m:888-904).
+
+    ``active_elements_mask``: grid of the active elements' points;
+    ``delay_mask``: per-point beamforming delay in samples (0 = the first
+    sample of ``input_signal``); ``input_signal``: the one drive series;
+    ``transmit_apodization``: 'Rectangular' or anything else, in which case
+    ``transmit_apodization_mask`` holds the per-point weights.  Building the
+    masks from element geometry (kWaveTransducer itself) is outside this
+    library.
+    """
+
+    def __init__(self, active_elements_mask, delay_mask, input_signal, transmit_apodization="Rectangular",
+                 transmit_apodization_mask=None):
+        self.active_elements_mask = active_elements_mask
+        self.delay_mask = delay_mask
+        self.input_signal = input_signal
+        self.transmit_apodization = transmit_apodization
+        self.transmit_apodization_mask = transmit_apodization_mask

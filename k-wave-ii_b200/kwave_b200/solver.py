@@ -227,10 +227,19 @@ def _prepare(dim, kgrid, medium, source, sensor, options):
                                       "for medium.alpha_power = 1.")
         if _any(lambda x: x < 0, alpha_coeff):
             raise KWaveInputError("medium.alpha_coeff must be non-negative and real.")
-        if _has(medium, "alpha_filter"):
-            raise KWaveInputError("medium.alpha_filter is not supported by this solver.")
     else:
         eos = "lossless"
+    # absorption filter in natural wavenumber order (createAbsorptionVariables.m:56-76)
+    alpha_filter = None
+    if _has(medium, "alpha_filter"):
+        if eos == "stokes":
+            raise KWaveInputError("Input option medium.alpha_filter is not supported with the axisymmetric code or "
+                                  "medium.alpha_mode = 'stokes'.")
+        alpha_filter = np.asarray(_field(medium, "alpha_filter"), dtype=np.float64)
+        if alpha_filter.shape != kgrid.shape:
+            raise KWaveInputError("medium.alpha_filter must be the same size as the computational grid.")
+        if eos == "lossless":
+            alpha_filter = None     # no absorption operators to filter
     alpha_sign = [1.0, 1.0]
     if _has(medium, "alpha_sign"):
         s = np.asarray(_field(medium, "alpha_sign"), dtype=np.float64).ravel()
@@ -344,9 +353,13 @@ def _prepare(dim, kgrid, medium, source, sensor, options):
         if mode not in _abi.SOURCE_MODES:
             raise KWaveInputError("source.p_mode must be set to 'additive', 'additive-no-correction', or 'dirichlet'.")
         sig = np.atleast_2d(np.asarray(_field(source, "p"), dtype=np.float64))
-        if _has(source, "p_frequency_ref"):
-            raise KWaveInputError("source.p_frequency_ref is not supported by this solver.")
-        psrc = dict(mask=pm, mode=mode, sig=sig)
+        freq_ref = _frequency_ref(source, "p_frequency_ref", kgrid, c0)
+        if freq_ref is not None:
+            # the k-space source correction as a function of w instead of k
+            # (inputChecking.m:820-836): the source is injected without the
+            # spatial correction
+            mode = "additive-no-correction"
+        psrc = dict(mask=pm, mode=mode, sig=sig, freq_ref=freq_ref)
     usrc = None
     ucomp = ["ux", "uy", "uz"][:dim]
     if any(_has(source, n) for n in ucomp) or _has(source, "u_mask"):
@@ -360,12 +373,32 @@ def _prepare(dim, kgrid, medium, source, sensor, options):
         mode = _field(source, "u_mode", "additive")
         if mode not in _abi.SOURCE_MODES:
             raise KWaveInputError("source.u_mode must be set to 'additive', 'additive-no-correction', or 'dirichlet'.")
-        if _has(source, "u_frequency_ref"):
-            raise KWaveInputError("source.u_frequency_ref is not supported by this solver.")
+        freq_ref = _frequency_ref(source, "u_frequency_ref", kgrid, c0)
+        if freq_ref is not None:
+            mode = "additive-no-correction"   # inputChecking.m:923-939
         sigs = [np.atleast_2d(np.asarray(_field(source, n), dtype=np.float64)) if _has(source, n) else None
                 for n in ucomp]
-        usrc = dict(mask=um, mode=mode, sigs=sigs)
-    if not user_density and (usrc is not None or record & {"u", "u_max", "u_rms"}):
+        usrc = dict(mask=um, mode=mode, sigs=sigs, freq_ref=freq_ref)
+    # a transducer as the source (kspaceFirstOrder_inputChecking.m:1160-1209):
+    # any object exposing active_elements_mask, delay_mask, input_signal and
+    # transmit_apodization(_mask), as kWaveTransducer does
+    tsrc = None
+    if _has(source, "active_elements_mask") and _has(source, "input_signal"):
+        if dim != 3:
+            raise KWaveInputError("Transducer inputs are only compatible with 3D simulations.")
+        if psrc is not None or usrc is not None or source_p0:
+            raise KWaveInputError("A transducer source cannot be combined with source.p, source.u or source.p0.")
+        am = np.asarray(_field(source, "active_elements_mask")) != 0
+        dm = np.asarray(_field(source, "delay_mask"))
+        if am.shape != kgrid.shape or dm.shape != kgrid.shape:
+            raise KWaveInputError("The transducer masks must be the same size as the computational grid.")
+        apod = None
+        ta = _field(source, "transmit_apodization", "Rectangular")
+        if not (isinstance(ta, str) and ta == "Rectangular"):
+            apod = np.asarray(_field(source, "transmit_apodization_mask"), dtype=np.float64)
+        tsrc = dict(mask=am, delay=dm, apod=apod,
+                    sig=np.asarray(_field(source, "input_signal"), dtype=np.float64).ravel())
+    if not user_density and (usrc is not None or tsrc is not None or record & {"u", "u_max", "u_rms"}):
         raise KWaveInputError("medium.density must be explicitly defined if velocity inputs or outputs are used, "
                               "even in homogeneous media.")
     if not user_density and nonlinear:
@@ -406,6 +439,8 @@ def _prepare(dim, kgrid, medium, source, sensor, options):
             rho0 = grow(rho0, True)
         if alpha_coeff is not None and alpha_coeff.size > 1:
             alpha_coeff = grow(alpha_coeff, True)
+        if alpha_filter is not None:
+            alpha_filter = grow(alpha_filter, False)     # expandGridMatrices.m:165-168, zeros
         if nonlinear and BonA.size > 1:
             BonA = grow(BonA, True)
         if source_p0:
@@ -414,6 +449,12 @@ def _prepare(dim, kgrid, medium, source, sensor, options):
             psrc["mask"] = grow(psrc["mask"], False)
         if usrc is not None:
             usrc["mask"] = grow(usrc["mask"], False)
+        if tsrc is not None:
+            # the delays stay as they are (inputChecking.m:1196-1198)
+            tsrc["mask"] = grow(tsrc["mask"], False)
+            tsrc["delay"] = grow(tsrc["delay"], False)
+            if tsrc["apod"] is not None:
+                tsrc["apod"] = grow(tsrc["apod"], False)
         if mask is not None:
             mask = grow(mask, False)
         inside = [(pml_size[a] + 1, shape[a] - pml_size[a]) for a in range(dim)]
@@ -454,6 +495,8 @@ def _prepare(dim, kgrid, medium, source, sensor, options):
         sig = psrc["sig"].copy()
         rows = _signal_rows(labels, sig.shape[0], pos.size, "source.p", "source.p_mask")
         cpos = _at(c0, pos[:sig.shape[0]]) if hetero_c else None
+        if scale_source_terms and psrc["freq_ref"] is not None:
+            sig = sig * math.cos(2 * math.pi * psrc["freq_ref"] * dt / 2)   # scaleSourceTerms.m:43-45
         if scale_source_terms:
             if psrc["mode"] == "dirichlet":
                 for r in range(sig.shape[0]):
@@ -471,6 +514,9 @@ def _prepare(dim, kgrid, medium, source, sensor, options):
         nrows = max(s.shape[0] for s in sigs if s is not None) if any(s is not None for s in sigs) else 1
         rows = _signal_rows(labels, nrows, pos.size, "source.ux (etc)", "source.u_mask")
         cpos = _at(c0, pos[:nrows]) if hetero_c else None
+        if scale_source_terms and usrc["freq_ref"] is not None:
+            w = math.cos(2 * math.pi * usrc["freq_ref"] * dt / 2)          # scaleSourceTerms.m:272-282
+            sigs = [None if s_ is None else s_ * w for s_ in sigs]
         if scale_source_terms and usrc["mode"] != "dirichlet":
             for i, s in enumerate(sigs):
                 if s is None:
@@ -480,6 +526,19 @@ def _prepare(dim, kgrid, medium, source, sensor, options):
                     cc = c0 if cpos is None else cpos[r]
                     s[r] = s[r] * (2.0 * cc * dt / d)
         src_struct.append(("u", usrc["mode"], pos, rows, sigs))
+
+    if tsrc is not None:
+        pos = _find(tsrc["mask"])
+        tsrc["pos"] = pos
+        tsrc["delay_pts"] = np.rint(_at(tsrc["delay"], pos)).astype(np.uint64)
+        tsrc["apod_pts"] = None if tsrc["apod"] is None else _at(tsrc["apod"], pos)
+        sig = tsrc["sig"]
+        if scale_source_terms:
+            # scaleSourceTerms.m:377-390: one drive signal, scaled with the
+            # mean sound speed over the transducer's points
+            cc = float(c0) if c0.size == 1 else float(np.mean(_at(c0, pos)))
+            sig = sig * (2.0 * cc * dt / kgrid.dx)
+        tsrc["sig_scaled"] = sig
 
     # ---- staggered density (kspaceFirstOrder3D.m:585-607) ----
     # the midpoint averages are formed on the device from rho0
@@ -546,12 +605,28 @@ def _prepare(dim, kgrid, medium, source, sensor, options):
         else:
             pr.alpha_coeff_scalar = float(alpha_coeff)
     pr.alpha_power = alpha_power
+    if tsrc is not None:
+        ts = pr.transducer_source
+        ts.num_points = tsrc["pos"].size
+        ts.index = idx_arr(tsrc["pos"])
+        d = np.ascontiguousarray(tsrc["delay_pts"], dtype=np.uint64)
+        keep.append(d)
+        ts.delay = _abi.uptr(d)
+        ts.apodization = arr(tsrc["apod_pts"]) if tsrc["apod_pts"] is not None else _abi.f32p()
+        ts.signal_length = tsrc["sig_scaled"].size
+        ts.input_signal = arr(tsrc["sig_scaled"])
+    if alpha_filter is not None:
+        pr.alpha_filter = grid_arr(alpha_filter)
     pr.alpha_mode = _abi.ALPHA_MODES.get(alpha_mode if alpha_mode != "stokes" else None, 0)
     pr.alpha_sign[0], pr.alpha_sign[1] = alpha_sign
     for kind, mode, pos, rows, sigs in src_struct:
         targets = [pr.p_source] if kind == "p" else [pr.u_source[i] for i in range(dim)]
         pos_p = idx_arr(pos)
-        row_p = idx_arr(rows)
+        # a binary mask (one row for every point, or row i for point i) passes
+        # no signal index, so a one-row component can sit beside per-point
+        # ones (MATLAB's source.ux(':', t) with one row drives every point)
+        binary = bool(np.all(rows == 0)) or bool(np.array_equal(rows, np.arange(pos.size)))
+        row_p = _abi.u64p() if binary else idx_arr(rows)
         for tgt, s in zip(targets, sigs):
             if s is None:
                 continue
@@ -785,10 +860,10 @@ class Server:
     plain call returns for the same inputs.
     """
 
-    def __init__(self, device=0, hbm_budget_bytes=0, max_active=0, steps_per_slice=0):
+    def __init__(self, device=0, hbm_budget_bytes=0, max_active=0, steps_per_slice=0, request_timeout_ms=0):
         self._lib = _abi.load_library()
         cfg = _abi.kw_server_config(device=device, hbm_budget_bytes=hbm_budget_bytes, max_active=max_active,
-                                    steps_per_slice=steps_per_slice)
+                                    steps_per_slice=steps_per_slice, request_timeout_ms=request_timeout_ms)
         h = C.c_void_p()
         _abi.check(self._lib.kw_server_create(C.byref(cfg), C.byref(h)))
         self.handle = h
@@ -808,11 +883,20 @@ class Server:
         self._preps[t.value] = prep
         return t.value
 
-    def result(self, ticket, with_latency=False):
-        prep = self._preps.pop(ticket)
+    def result(self, ticket, with_latency=False, timeout_ms=None):
+        """What the plain call returns for this request.  timeout_ms bounds
+        the wait (KWaveError with status KW_ERR_TIMEOUT when the request has
+        not finished by then; the ticket stays valid)."""
+        prep = self._preps[ticket]
         o, host = _alloc_outputs(prep)
         ms = C.c_double()
-        _abi.check(self._lib.kw_server_wait(self.handle, ticket, C.byref(o), C.byref(ms)))
+        if timeout_ms is None:
+            st = self._lib.kw_server_wait(self.handle, ticket, C.byref(o), C.byref(ms))
+        else:
+            st = self._lib.kw_server_wait_for(self.handle, ticket, int(timeout_ms), C.byref(o), C.byref(ms))
+        if st != _abi.KW_ERR_TIMEOUT or timeout_ms is None:
+            self._preps.pop(ticket)
+        _abi.check(st)
         out = _finish(prep, host)
         return (out, ms.value) if with_latency else out
 
@@ -930,6 +1014,20 @@ def _finish(P, host):
     return out
 
 
+def _frequency_ref(source, name, kgrid, c0):
+    """source.p_frequency_ref / u_frequency_ref checked as
+    kspaceFirstOrder_inputChecking.m:820-836 / 923-939 does; None if unset."""
+    if not _has(source, name):
+        return None
+    f = np.asarray(_field(source, name), dtype=np.float64)
+    if f.size != 1 or not np.isfinite(f).all() or float(f.ravel()[0]) < 0:
+        raise KWaveInputError("Expected input source.%s to be a nonnegative scalar." % name)
+    f = float(f.ravel()[0])
+    if f > kgrid.k_max * float(np.min(c0)) / (2 * math.pi):
+        raise KWaveInputError("source.%s is higher than the maximum frequency supported by the spatial grid." % name)
+    return f
+
+
 def _cuboids(P, out):
     """Per-cuboid outputs shaped [X, Y, (Z,) T] (reorderCuboidCorners.m)."""
     all_idx = _find_union(P.cuboid_rows)
@@ -943,7 +1041,9 @@ def _cuboids(P, out):
         d = {}
         for k, v in out.items():
             if k.endswith("_all") or k.endswith("_final"):
-                d[k] = v
+                # whole-grid outputs belong to the first cuboid only
+                if c == 0:
+                    d[k] = v
             elif v.ndim == 2:
                 d[k] = v[sel].reshape(size + (v.shape[1],), order="F")
             else:

@@ -435,9 +435,17 @@ def tone_burst_hann(sample_freq, signal_freq, num_cycles):
 # ---------------------------------------------------------------------------
 
 class _NumpyBackend:
+    """``single``: the loop in FP32 / complex64 (scipy.fft keeps single
+    precision), the FP32 variant of the CPU baseline."""
     name = "numpy"
 
+    def __init__(self, single=False):
+        self.f = np.float32 if single else np.float64
+        self.c = np.complex64 if single else np.complex128
+
     def put(self, a):
+        if isinstance(a, np.ndarray) and a.ndim > 0 and a.dtype.kind in "fc":
+            return a.astype(self.c if a.dtype.kind == "c" else self.f, copy=False)
         return a
 
     def fftn(self, a):
@@ -458,10 +466,10 @@ class _NumpyBackend:
     sqrt = staticmethod(np.sqrt)
 
     def zeros(self, shape, complex_=False):
-        return np.zeros(shape, dtype=complex if complex_ else np.float64)
+        return np.zeros(shape, dtype=self.c if complex_ else self.f)
 
     def full(self, v, shape):
-        return np.broadcast_to(v, shape).copy()
+        return np.array(np.broadcast_to(v, shape), dtype=self.f)
 
     def copy(self, a):
         return a.copy()
@@ -470,12 +478,12 @@ class _NumpyBackend:
         return np.ascontiguousarray(field).reshape(-1)[idx]
 
     def scatter_set(self, field, idx, vals):
-        f = np.array(field, dtype=np.float64, copy=True)
+        f = np.array(field, dtype=self.f, copy=True)
         f.reshape(-1)[idx] = vals
         return f
 
     def scatter_add(self, field, idx, vals):
-        f = np.array(field, dtype=np.float64, copy=True)
+        f = np.array(field, dtype=self.f, copy=True)
         f.reshape(-1)[idx] += vals
         return f
 
@@ -559,8 +567,8 @@ class _TorchBackend:
         return np.asarray(a)
 
 
-def _backend(device):
-    return _NumpyBackend() if device is None else _TorchBackend(device)
+def _backend(device, single=False):
+    return _NumpyBackend(single) if device is None else _TorchBackend(device)
 
 
 def _f2c(idx, shape):
@@ -599,10 +607,13 @@ def kspace_first_order(kgrid, medium, source, sensor, **opts):
     pressure field after every time step t, for tests that need the field
     history.  ``Device`` (not a reference option) runs the loop on
     torch.float64 tensors on that device ("cpu" or "cuda") instead of NumPy:
-    the fast FP64 oracle of the full-size checks.
+    the fast FP64 oracle of the full-size checks.  ``Single`` (not a
+    reference option, NumPy only) runs the loop in FP32: the reference's
+    ``DataCast = 'single'``, used as the FP32 CPU baseline.
     """
     step_callback = opts.pop("StepCallback", None)
     device = opts.pop("Device", None)
+    single = bool(opts.pop("Single", False))
     dim = kgrid.dim
     if dim not in (2, 3):
         raise ValueError("only 2D and 3D are restated")
@@ -642,6 +653,9 @@ def kspace_first_order(kgrid, medium, source, sensor, **opts):
         eos = "lossless"
     nonlinear = _has(medium, "BonA")
     BonA = np.asarray(_get(medium, "BonA"), dtype=np.float64) if nonlinear else None
+    alpha_filter = None
+    if eos == "absorbing" and _has(medium, "alpha_filter"):
+        alpha_filter = np.asarray(_get(medium, "alpha_filter"), dtype=np.float64)
 
     # c_ref (setSoundSpeedRef.m:30-49)
     cref_opt = _get(medium, "sound_speed_ref")
@@ -680,10 +694,21 @@ def kspace_first_order(kgrid, medium, source, sensor, **opts):
     reorder_index = None
     mask = None
     cart_points = None
+    cuboids = None
     if use_sensor and not blank_sensor:
         m = np.asarray(_get(sensor, "mask"), dtype=np.float64)
         if m.shape == kgrid.shape:
             mask = m
+        elif m.ndim == 2 and m.shape[0] == 2 * dim:
+            # cuboid corners [x1, y1, (z1,) x2, y2, (z2)] per column, 1-based
+            # (inputChecking.m:517-575)
+            if np.any(np.mod(m, 1) != 0):
+                raise ValueError("sensor.mask cuboid corner indices must be integers.")
+            if np.any(m[dim:] - m[:dim] < 0):
+                raise ValueError("sensor.mask cuboid corners must be defined with x2 => x1, etc.")
+            if np.any(m < 1) or any(np.any(m[[a, a + dim]] > kgrid.shape[a]) for a in range(dim)):
+                raise ValueError("sensor.mask cuboid corners must be within the grid.")
+            cuboids = m.astype(np.int64)
         elif m.ndim == 2 and m.shape[0] == dim:
             if cart_interp == "linear" and not time_rev:
                 # recorded by barycentric interpolation (createStorageVariables.m:376-400)
@@ -699,10 +724,15 @@ def kspace_first_order(kgrid, medium, source, sensor, **opts):
     if source_p0:
         p0 = np.asarray(p0, dtype=np.float64)
     source_p = 0
+    p_freq_ref = u_freq_ref = None
     if _has(source, "p"):
         sp = np.atleast_2d(np.asarray(_get(source, "p"), dtype=np.float64))
         p_mask = np.asarray(_get(source, "p_mask"))
         p_mode = _get(source, "p_mode", "additive")
+        p_freq_ref = _get(source, "p_frequency_ref")
+        if p_freq_ref is not None:
+            # inputChecking.m:820-836: the k-space correction as a function of w
+            p_mode = "additive-no-correction"
         source_p = sp.shape[1]
         if source_p0:
             raise ValueError("source.p0 and source.p can't be defined in the same simulation.")
@@ -712,10 +742,24 @@ def kspace_first_order(kgrid, medium, source, sensor, **opts):
     if any(_has(source, n) for n in u_comps) or _has(source, "u_mask"):
         u_mask = np.asarray(_get(source, "u_mask"))
         u_mode = _get(source, "u_mode", "additive")
+        u_freq_ref = _get(source, "u_frequency_ref")
+        if u_freq_ref is not None:
+            # inputChecking.m:923-939
+            u_mode = "additive-no-correction"
         for i, n in enumerate(u_comps):
             if _has(source, n):
                 su[i] = np.atleast_2d(np.asarray(_get(source, n), dtype=np.float64))
                 source_u[i] = su[i].shape[1]
+
+    # transducer source (inputChecking.m:1160-1209)
+    tr_src = None
+    if _has(source, "active_elements_mask") and _has(source, "input_signal"):
+        ta = _get(source, "transmit_apodization", "Rectangular")
+        tr_src = dict(mask=np.asarray(_get(source, "active_elements_mask"), dtype=np.float64),
+                      delay=np.asarray(_get(source, "delay_mask"), dtype=np.float64),
+                      apod=None if (isinstance(ta, str) and ta == "Rectangular")
+                      else np.asarray(_get(source, "transmit_apodization_mask"), dtype=np.float64),
+                      sig=np.asarray(_get(source, "input_signal"), dtype=np.float64).ravel())
 
     # ---- time (inputChecking.m:1227-1268) ----
     if kgrid.Nt is None:
@@ -745,14 +789,21 @@ def kspace_first_order(kgrid, medium, source, sensor, **opts):
             alpha_coeff = expand_matrix(alpha_coeff, pml_size)
         if nonlinear and BonA.size > 1:
             BonA = expand_matrix(BonA, pml_size)
+        if alpha_filter is not None:
+            alpha_filter = expand_matrix(alpha_filter, pml_size, 0)
         if source_p0:
             p0 = expand_matrix(p0, pml_size, 0)
         if source_p:
             p_mask = expand_matrix(p_mask, pml_size, 0)
         if any(source_u):
             u_mask = expand_matrix(u_mask, pml_size, 0)
+        if tr_src is not None:
+            for key in ("mask", "delay") + (("apod",) if tr_src["apod"] is not None else ()):
+                tr_src[key] = expand_matrix(tr_src[key], pml_size, 0)
         if mask is not None:
             mask = expand_matrix(mask, pml_size, 0)
+        if cuboids is not None:
+            cuboids = cuboids + np.array(pml_size * 2, dtype=np.int64)[:, None]
         inside = [slice(pml_size[a], kgrid.shape[a] - pml_size[a]) for a in range(dim)]
     else:
         inside = [slice(0, kgrid.shape[a]) for a in range(dim)]
@@ -764,6 +815,14 @@ def kspace_first_order(kgrid, medium, source, sensor, **opts):
     sensor_interp = cart_linear(kgrid, cart_points) if cart_points is not None else None
 
     sensor_idx = find(mask) if mask is not None else None
+    if cuboids is not None:
+        # concatenation of every cuboid's find() (inputChecking.m:1610-1633)
+        parts = []
+        for ci in range(cuboids.shape[1]):
+            tm = np.zeros(shape)
+            tm[tuple(slice(cuboids[a, ci] - 1, cuboids[a + dim, ci]) for a in range(dim))] = 1
+            parts.append(find(tm))
+        sensor_idx = np.concatenate(parts)
 
     # source indices / labels
     def sig_index(msk, nrows):
@@ -804,6 +863,10 @@ def kspace_first_order(kgrid, medium, source, sensor, **opts):
             eta = 2 * a_np * c ** alpha_power * np.tan(np.pi * alpha_power / 2)
         else:
             nabla2, eta = 0.0, 0.0
+        if alpha_filter is not None:
+            # createAbsorptionVariables.m:56-76: filter in natural order
+            nabla1 = np.fft.ifftshift(np.fft.fftshift(np.broadcast_to(nabla1, shape)) * alpha_filter)
+            nabla2 = np.fft.ifftshift(np.fft.fftshift(np.broadcast_to(nabla2, shape)) * alpha_filter)
         if _has(medium, "alpha_sign"):
             sgn = np.asarray(_get(medium, "alpha_sign"), dtype=np.float64)
             tau = np.sign(sgn[0]) * tau
@@ -815,21 +878,29 @@ def kspace_first_order(kgrid, medium, source, sensor, **opts):
             tau = np.sign(np.asarray(_get(medium, "alpha_sign"))[0]) * tau
 
     c0 = c
+    # c0 in column-major (find) order, for the per-point source scaling
+    c0f = c0.ravel(order="F") if c0.size > 1 else None
     # ---- source scaling (scaleSourceTerms.m) ----
     if source_p:
         sp = sp.copy()
+        if p_freq_ref is not None:
+            # scaleSourceTerms.m:43-45
+            sp = sp * np.cos(2 * np.pi * float(p_freq_ref) * dt / 2)
         if p_mode == "dirichlet":
             if c0.size == 1:
                 sp = sp / (dim * c0 ** 2)
             else:
                 for r in range(sp.shape[0]):
-                    sp[r] = sp[r] / (dim * c0.ravel(order="F")[p_pos[r]] ** 2)
+                    sp[r] = sp[r] / (dim * c0f[p_pos[r]] ** 2)
         else:
             if c0.size == 1:
                 sp = sp * (2 * dt / (dim * c0 * kgrid.dx))
             else:
                 for r in range(sp.shape[0]):
-                    sp[r] = sp[r] * (2 * dt / (dim * c0.ravel(order="F")[p_pos[r]] * kgrid.dx))
+                    sp[r] = sp[r] * (2 * dt / (dim * c0f[p_pos[r]] * kgrid.dx))
+    if any(source_u) and u_freq_ref is not None:
+        # scaleSourceTerms.m:272-282
+        su = [None if v is None else v * np.cos(2 * np.pi * float(u_freq_ref) * dt / 2) for v in su]
     if any(source_u) and u_mode != "dirichlet":
         for i in range(dim):
             if su[i] is None:
@@ -840,7 +911,20 @@ def kspace_first_order(kgrid, medium, source, sensor, **opts):
                 su[i] = su[i] * (2 * c0 * dt / d)
             else:
                 for r in range(su[i].shape[0]):
-                    su[i][r] = su[i][r] * (2 * c0.ravel(order="F")[u_pos[r]] * dt / d)
+                    su[i][r] = su[i][r] * (2 * c0f[u_pos[r]] * dt / d)
+
+    # transducer drive: points, delays and apodization in find() order, the
+    # signal scaled by 2 c0 dt / dx with c0 averaged over the points
+    # (scaleSourceTerms.m:377-390); active while t <= length - max(delay)
+    if tr_src is not None:
+        tr_pos = find(tr_src["mask"])
+        tr_delay = np.rint(tr_src["delay"].ravel(order="F")[tr_pos]).astype(np.int64)
+        tr_apod = np.ones(tr_pos.size) if tr_src["apod"] is None else tr_src["apod"].ravel(order="F")[tr_pos]
+        cmean = float(c0) if c0.size == 1 else float(np.mean(c0f[tr_pos]))
+        tr_sig = tr_src["sig"] * (2 * cmean * dt / kgrid.dx)
+        tr_steps = tr_sig.size - int(tr_delay.max())
+    else:
+        tr_steps = 0
 
     # ---- staggered density (kspaceFirstOrder3D.m:585-607) ----
     rho_sg_inv = []
@@ -881,7 +965,7 @@ def kspace_first_order(kgrid, medium, source, sensor, **opts):
         source_kappa = 1.0
 
     # ---- storage (createStorageVariables.m) ----
-    xp = _backend(device)
+    xp = _backend(device, single)
     X = xp.put
     num_rec = Nt - record_start + 1
     out = {}
@@ -931,6 +1015,8 @@ def kspace_first_order(kgrid, medium, source, sensor, **opts):
 
     if source_p:
         p_pos_x, p_sig_x, sp_x = X(_f2c(p_pos, shape)), X(p_sig), X(sp)
+    if tr_steps > 0:
+        tr_pos_x, tr_delay_x, tr_apod_x, tr_sig_x = X(_f2c(tr_pos, shape)), X(tr_delay), X(tr_apod), X(tr_sig)
     if any(source_u):
         u_pos_x, u_sig_x = X(_f2c(u_pos, shape)), X(u_sig)
         su_x = [X(v) for v in su]
@@ -982,6 +1068,10 @@ def kspace_first_order(kgrid, medium, source, sensor, **opts):
                     u[i] = u[i] + xp.real(xp.ifftn(source_kappa * xp.fftn(smat)))
                 else:
                     u[i] = xp.scatter_add(u[i], u_pos_x, vals)
+
+        # transducer source (kspaceFirstOrder3D.m:888-904)
+        if tr_steps >= t:
+            u[0] = xp.scatter_add(u[0], tr_pos_x, tr_apod_x * tr_sig_x[tr_delay_x + (t - 1)])
 
         # divergence (kspaceFirstOrder3D.m:907-909)
         du = [xp.real(xp.ifftn(dd_neg[i] * kappa * xp.fftn(u[i]))) for i in range(dim)]
@@ -1118,13 +1208,39 @@ def kspace_first_order(kgrid, medium, source, sensor, **opts):
         fr = np.asarray(_get(sensor, "frequency_response"), dtype=np.float64).ravel()
         out["p"] = gaussian_filter(out["p"], 1.0 / dt, fr[0], fr[1])
 
+    if cuboids is not None and not time_rev:
+        out = _reorder_cuboids(out, cuboids, dim)
+
     if not use_sensor:
         return None
     if time_rev:
         return out["p_final"]
-    if not record_given:
+    if not record_given and cuboids is None:
         return out["p"]
     return out
+
+
+def _reorder_cuboids(out, cuboids, dim):
+    """kspaceFirstOrder_reorderCuboidCorners.m: one dict per cuboid, its
+    rows of every sensor output reshaped to [X, Y, (Z,) T] (column-major);
+    the _final and _all outputs go to the first cuboid only."""
+    res = []
+    start = 0
+    for ci in range(cuboids.shape[1]):
+        size = tuple(int(cuboids[a + dim, ci] - cuboids[a, ci] + 1) for a in range(dim))
+        n = int(np.prod(size))
+        d = {}
+        for k, v in out.items():
+            if k.endswith("_all") or k.endswith("_final"):
+                if ci == 0:
+                    d[k] = v
+            elif v.ndim == 2:
+                d[k] = v[start:start + n].reshape(size + (v.shape[1],), order="F")
+            else:
+                d[k] = v[start:start + n].reshape(size, order="F")
+        res.append(d)
+        start += n
+    return res
 
 
 def rel_l2(a, b):

@@ -62,7 +62,8 @@ def test_struct_layout_matches_header():
               "alpha_sign", "p_source", "u_source", "p0_source_input", "sensor_num", "record",
               "time_reversal_input", "inside_hi"]
     prog = ['#include <stdio.h>', '#include <stddef.h>', '#include "kwave_b200.h"', 'int main(void){',
-            'printf("%zu %zu %zu %zu\\n", sizeof(kw_problem), sizeof(kw_source), sizeof(kw_outputs), sizeof(kw_output_desc));']
+            'printf("%zu %zu %zu %zu %zu %zu\\n", sizeof(kw_problem), sizeof(kw_source), sizeof(kw_outputs), '
+            'sizeof(kw_output_desc), sizeof(kw_server_config), sizeof(kw_server_stats));']
     for f in fields:
         prog.append('printf("%%zu\\n", offsetof(kw_problem, %s));' % f)
     prog.append("return 0;}")
@@ -72,8 +73,9 @@ def test_struct_layout_matches_header():
         exe = os.path.join(d, "probe")
         subprocess.run([cc, "-I", os.path.join(ROOT, "include"), c, "-o", exe], check=True)
         out = subprocess.run([exe], check=True, capture_output=True, text=True).stdout.split()
-    sizes = [int(v) for v in out[:4]]
+    sizes = [int(v) for v in out[:6]]
     assert sizes == [ctypes.sizeof(_abi.kw_problem), ctypes.sizeof(_abi.kw_source),
-                     ctypes.sizeof(_abi.kw_outputs), ctypes.sizeof(_abi.kw_output_desc)]
-    offs = [int(v) for v in out[4:]]
+                     ctypes.sizeof(_abi.kw_outputs), ctypes.sizeof(_abi.kw_output_desc),
+                     ctypes.sizeof(_abi.kw_server_config), ctypes.sizeof(_abi.kw_server_stats)]
+    offs = [int(v) for v in out[6:]]
     assert offs == [getattr(_abi.kw_problem, f).offset for f in fields]

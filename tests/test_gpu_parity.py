@@ -36,7 +36,17 @@ def test_parity(name):
     run = kw.kspaceFirstOrder2D if dim == 2 else kw.kspaceFirstOrder3D
     gpu = run(_grid(kw, shape, dx, Nt, dt), med, src, sen, **opts)
     ref = oracle.kspace_first_order(_grid(oracle, shape, dx, Nt, dt), med, src, sen, **opts)
-    if isinstance(ref, dict):
+    _compare_outputs(name, gpu, ref)
+
+
+def _compare_outputs(name, gpu, ref):
+    """Same output structure (matrix, dict of outputs, or one dict per
+    cuboid) and every output within TOL."""
+    if isinstance(ref, list):
+        assert isinstance(gpu, list) and len(gpu) == len(ref)
+        for i, (g, r) in enumerate(zip(gpu, ref)):
+            _compare_outputs("%s[cuboid %d]" % (name, i), g, r)
+    elif isinstance(ref, dict):
         assert set(gpu) == set(ref), (sorted(gpu), sorted(ref))
         for k in ref:
             assert gpu[k].shape == ref[k].shape, k

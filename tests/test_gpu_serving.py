@@ -83,21 +83,56 @@ def test_mix_equals_alone(max_active, slice_steps, budget):
 
 @pytest.mark.gpu
 def test_failed_request_does_not_disturb_others():
-    """A request the library rejects at admission (a prime factor of 11 in
-    the grid size) fails alone; the runs around it finish unchanged."""
+    """A request the library rejects at admission (an axis of 4100 points,
+    above the 4096-point line of one transform tile) fails alone; the runs
+    around it finish unchanged."""
     import kwave_b200 as kw
     name = "2d_hetero_abs_nl"
     ref = _alone(kw, name)
-    bad = kw.kWaveGrid(22, 1e-4, 22, 1e-4)
+    bad = kw.kWaveGrid(22, 1e-4, 4100, 1e-4)
     bad.setTime(10, 2e-8)
     with kw.Server(max_active=2, steps_per_slice=3) as srv:
         t0 = _submit(kw, srv, name)
-        tb = srv.submit(2, bad, {"sound_speed": 1500.0}, {"p0": np.ones((22, 22))}, {"mask": np.ones((22, 22))},
+        tb = srv.submit(2, bad, {"sound_speed": 1500.0}, {"p0": np.ones((22, 4100))}, {"mask": np.ones((22, 4100))},
                         PMLSize=2)
         t1 = _submit(kw, srv, name)
-        with pytest.raises(kw.KWaveError, match="prime factor"):
+        with pytest.raises(kw.KWaveError, match="outside 2..4096"):
             srv.result(tb)
         _compare(name, srv.result(t0), ref)
         _compare(name, srv.result(t1), ref)
         st = srv.stats()
     assert st["completed"] == 2 and st["failed"] == 1
+
+
+@pytest.mark.gpu
+def test_deadline_watchdog_and_bounded_wait():
+    """The serving watchdog: a request still running request_timeout_ms after
+    its admission gets no further steps, drains and fails with KW_ERR_TIMEOUT,
+    while the run beside it finishes unchanged; a bounded wait on an
+    unfinished request returns KW_ERR_TIMEOUT and leaves its ticket valid.
+    The stall is a host-side one (a run far longer than the deadline); no
+    device wait is involved."""
+    import kwave_b200 as kw
+    from kwave_b200 import _abi
+    name = "2d_hetero_abs_nl"
+    ref = _alone(kw, name)
+    N = 512
+    long_grid = kw.kWaveGrid(N, 1e-4, N, 1e-4)
+    long_grid.setTime(200000, 2e-8)      # tens of seconds alone
+    mask = np.zeros((N, N))
+    mask[40, :] = 1
+    with kw.Server(max_active=4, steps_per_slice=16, request_timeout_ms=2000) as srv:
+        t_long = srv.submit(2, long_grid, {"sound_speed": 1500.0, "density": 1000.0},
+                            {"p0": kw.makeDisc(N, N, N // 2, N // 2, 8)}, {"mask": mask, "record": ["p_max"]},
+                            PMLSize=10)
+        t0 = _submit(kw, srv, name)
+        with pytest.raises(kw.KWaveError) as e:
+            srv.result(t_long, timeout_ms=5)
+        assert e.value.status == _abi.KW_ERR_TIMEOUT
+        _compare(name, srv.result(t0), ref)
+        with pytest.raises(kw.KWaveError, match="deadline") as e:
+            srv.result(t_long)
+        assert e.value.status == _abi.KW_ERR_TIMEOUT
+        st = srv.stats()
+    assert st["completed"] == 1 and st["failed"] == 1
+    assert st["active"] == 0 and st["pending"] == 0

@@ -72,12 +72,40 @@ def test_noalloc_gradient_matches_allocating_path(shape):
 
 
 @pytest.mark.gpu
-def test_noalloc_rejects_grids_above_the_scratch_limit():
+def test_noalloc_at_the_scratch_limit():
+    """200^3 (a 32.3 MB half spectrum) is the largest cube that fits the
+    32 MiB scratch: the spectrum's end and the operator tables sit at the top
+    of the array.  Checked against the allocating path on a smooth field."""
+    torch = pytest.importorskip("torch")
+    import kwave_b200 as kw
+    from kwave_b200 import _abi
+    lib = _abi.load_library()
+    shape = (200, 200, 200)
+    dx, c, rho = 1e-4, 1500.0, 1000.0
+    dt = 0.3 * dx / c
+    ax = [np.arange(n) - n / 2 for n in shape]
+    f = np.exp(-(ax[0][:, None, None] ** 2 + ax[1][None, :, None] ** 2 + ax[2][None, None, :] ** 2) / (2 * 12.0 ** 2))
+    ref = _reference_gradients(kw, f, dx, dt, c, rho)
+    f_dev = torch.tensor(f.ravel(order="F"), dtype=torch.float32, device="cuda")
+    for axis in (0, 2):
+        out_dev = torch.full_like(f_dev, float("nan"))
+        torch.cuda.synchronize()
+        assert _noalloc(lib, f_dev, out_dev, shape, dx, axis, c, dt) == 0, lib.kw_last_error()
+        got = out_dev.cpu().numpy().reshape(shape, order="F")
+        e = _rel(got, ref[axis])
+        assert e <= TOL, "axis %d rel-L2 %.3e" % (axis, e)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("shape", [(256, 256, 256), (256, 256, 128)])
+def test_noalloc_rejects_grids_above_the_scratch_limit(shape):
+    """256 x 256 x 128 (a 34.1 MB half spectrum) is the first such shape
+    rejected; nothing is launched for it."""
     torch = pytest.importorskip("torch")
     from kwave_b200 import _abi
     lib = _abi.load_library()
     f = torch.zeros(8, device="cuda")
-    shp = (C.c_uint64 * 3)(256, 256, 256)
+    shp = (C.c_uint64 * 3)(*shape)
     sp = (C.c_double * 3)(1e-4, 1e-4, 1e-4)
     st = lib.kw_gradient_noalloc(3, shp, sp, 0, 1, 1500.0, 1e-8, 1, C.c_void_p(f.data_ptr()),
                                  C.c_void_p(f.data_ptr()), None)
