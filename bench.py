@@ -232,20 +232,67 @@ class Clocks:
                 "samples": len(sm)}
 
 
-def cpu_baseline(w, steps):
-    """The FP64 oracle (NumPy/SciPy, all host cores) on a bounded sample of the
-    same workload: the first ``steps`` time steps."""
+def cpu_baseline(w, steps, single=False):
+    """The oracle (NumPy/SciPy, all host cores) on a bounded sample of the
+    same workload: the first ``steps`` time steps, in FP64 (the reference's
+    default) or FP32 (its DataCast 'single')."""
     sys.path.insert(0, ROOT)
     from oracle import kspace as oracle
     g = oracle.KWaveGrid(w["shape"][0], w["dx"], w["shape"][1], w["dx"], w["shape"][2], w["dx"])
     g.setTime(steps, w["dt"])
-    oracle.kspace_first_order(g, w["medium"], w["source"], w["sensor"], **w["options"])
+    oracle.kspace_first_order(g, w["medium"], w["source"], w["sensor"], Single=single, **w["options"])
     secs = oracle.LAST_LOOP_SECONDS
     cells = float(np.prod(w["shape"]))
     return {"value": cells * steps / secs / 1e9, "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
-            "sample": "first %d of %d time steps of the 256^3 workload, FP64 NumPy/SciPy oracle "
-                      "(scipy.fft workers=%d); loop time only" % (steps, w["Nt"], os.cpu_count()),
+            "sample": "first %d of %d time steps of the %s workload, %s NumPy/SciPy oracle "
+                      "(scipy.fft workers=%d); loop time only"
+                      % (steps, w["Nt"], "x".join(str(n) for n in w["shape"]), "FP32" if single else "FP64",
+                         os.cpu_count()),
             "seconds": secs}
+
+
+def cfg1_workload(N=128, dx=0.1e-3, c=1500.0, pml=20):
+    """The 2-D homogeneous lossless case: 128^2, dx 0.1 mm, disc p0 of radius
+    5 at the centre (smoothed), PML 20 / alpha 2, CFL 0.3, t_end = 1.2 x the
+    grid diagonal / c (Nt = 725), 64 points on a circle of radius 40 cells
+    mapped to the grid by nearest neighbour, recording p."""
+    import kwave_b200 as kw
+    t_end = 1.2 * math.sqrt(2) * N * dx / c
+    g = kw.kWaveGrid(N, dx, N, dx)
+    g.makeTime(c, 0.3, t_end)
+    return dict(shape=(N, N), dx=dx, Nt=g.Nt, dt=g.dt, t_end=t_end, medium={"sound_speed": c, "density": 1000.0},
+                source={"p0": kw.makeDisc(N, N, N // 2 + 1, N // 2 + 1, 5)},
+                sensor={"mask": kw.makeCartCircle(40 * dx, 64)},
+                options={"PMLSize": pml, "PMLAlpha": 2.0, "CartInterp": "nearest"})
+
+
+def cfg1_section(kw, device, runs=20, cpu=True):
+    """The 2-D case as specified, device-resident on the GPU (runs complete
+    simulations timed with CUDA events) and the FP64 oracle at its full Nt on
+    the host cores; rel-L2 of the GPU p against the oracle's."""
+    w = cfg1_workload()
+    cells = float(np.prod(w["shape"]))
+    g = kw.kWaveGrid(w["shape"][0], w["dx"], w["shape"][1], w["dx"])
+    g.setTime(w["Nt"], w["dt"])
+    with kw.Simulation(2, g, w["medium"], w["source"], w["sensor"], **dict(w["options"], DeviceNum=device)) as sim:
+        p = sim.run()
+        sim.run_timed(2)
+        ms = sim.run_timed(runs)
+    out = {"workload": "kspaceFirstOrder2D 128^2 homogeneous lossless, disc p0 r=5, PML 20, Nt=%d, "
+                       "64-point circle r=40 (nearest), record p" % w["Nt"],
+           "gpu": {"value": cells * w["Nt"] * runs / (ms / 1e3) / 1e9, "unit": UNIT,
+                   "ms_per_simulation": ms / runs, "note": "launch-bound: 16 384 cells per step"}}
+    if cpu:
+        sys.path.insert(0, ROOT)
+        from oracle import kspace as oracle
+        og = oracle.KWaveGrid(w["shape"][0], w["dx"], w["shape"][1], w["dx"])
+        og.setTime(w["Nt"], w["dt"])
+        ref = oracle.kspace_first_order(og, w["medium"], w["source"], w["sensor"], **w["options"])
+        secs = oracle.LAST_LOOP_SECONDS
+        out["cpu_fp64"] = {"value": cells * w["Nt"] / secs / 1e9, "unit": UNIT, "cores": os.cpu_count(),
+                           "kind": "port", "sample": "the full run (Nt=%d), loop time only" % w["Nt"]}
+        out["rel_l2_gpu_vs_oracle"] = _rel_l2(p, ref)
+    return out
 
 
 def dist_setup(backend=None):
@@ -321,12 +368,6 @@ def run_reference(args, ws, rank):
     print(json.dumps(line), flush=True)
 
 
-# Request mix of the served stream: (kind, size, Nt, weight).  Sizes are the
-# small-to-medium runs a service sees next to the 256^3 headline run.
-SERVE_MIX = [("2d", 256, 500, 0.30), ("2d", 512, 800, 0.15), ("3d", 64, 300, 0.30), ("3d", 96, 400, 0.15),
-             ("3d", 128, 500, 0.10)]
-
-
 def _latency_stats(lat_ms):
     v = np.sort(np.asarray(lat_ms, dtype=np.float64))
     return {"p50_ms": float(np.percentile(v, 50)), "p99_ms": float(np.percentile(v, 99)), "mean_ms": float(v.mean())}
@@ -341,30 +382,63 @@ def _rel_l2(a, b):
     return float(np.linalg.norm(a - b) / (d if d > 0 else 1.0))
 
 
-def served_section(kw, device, n_req=48, seed=7, load=0.9):
+SERVE_EDGES = (64, 96, 128, 160, 192, 256, 320, 384)
+
+
+def served_request(rng, dx=0.2e-3, nt_scale=1.0, pml=10):
+    """One request of the served stream: a 3-D simulation whose edge along
+    each axis is drawn log-uniformly from SERVE_EDGES (so grids are
+    anisotropic), a blob medium as in the headline workload (absorbing,
+    BonA 6), a point pressure source at a random interior position driven by
+    a Hann-windowed 3-cycle tone burst of 0.5-2 MHz at 1 MPa, Nt uniform in
+    500-2000 (times nt_scale), FP32; p recorded at 32 random points and p_max
+    on the central xy-plane."""
+    logs = np.log(SERVE_EDGES)
+    shape = tuple(int(SERVE_EDGES[int(np.argmin(np.abs(logs - rng.uniform(logs[0], logs[-1]))))]) for _ in range(3))
+    Nt = max(1, int(round(rng.integers(500, 2001) * nt_scale)))
+    c = blob_speed(shape, rng, pml=pml)
+    medium = {"sound_speed": c, "density": 1000.0 + 0.6 * (c - 1500.0), "alpha_coeff": 0.75, "alpha_power": 1.5,
+              "BonA": 6.0}
+    dt = 0.3 * dx / c.max()
+    pm = np.zeros(shape, dtype=bool)
+    pm[tuple(int(rng.integers(pml + 2, n - pml - 2)) for n in shape)] = True
+    f0 = rng.uniform(0.5e6, 2e6)
+    sig = hann_burst(dt, f0=f0, cycles=3, amp=1e6)
+    sm = np.zeros(shape, dtype=bool)
+    sm[:, :, shape[2] // 2] = True
+    pts = np.zeros(shape, dtype=bool)
+    for _ in range(32):
+        pts[tuple(int(rng.integers(pml, n - pml)) for n in shape)] = True
+    return dict(shape=shape, dx=dx, Nt=Nt, dt=dt, medium=medium, source={"p_mask": pm, "p": sig[None, :]},
+                sensor={"mask": sm | pts, "record": ["p", "p_max"]}, options={"PMLSize": pml},
+                src_len=len(sig), f0=f0)
+
+
+def served_section(kw, device, n_req=40, seed=7, load=0.8, nt_scale=0.2):
     """Continuous batching against the plain path on the same request stream.
 
-    Two passes per path over the same n_req requests drawn from SERVE_MIX:
+    The stream is the served-stream recipe (3-D requests, per-axis edges
+    log-uniform over 64..384, blob media, point sources of 0.5-2 MHz,
+    Nt uniform in 500-2000) as a time-scaled subset: n_req requests with Nt
+    scaled by nt_scale.  Two passes per path over the same requests:
     'saturated' submits everything at t = 0 (aggregate Gcell-steps/s =
     cell-steps / makespan); 'poisson' submits at Poisson arrival times whose
     rate is `load` x the plain path's capacity (p50 / p99 of submit->result
     latency).  The plain path runs the requests one after another through
     the drop-in call on a prepared problem (plan, loop, outputs to host);
     the served path hands them to kwave_b200.Server.  Host setup (input
-    checking, smoothing) is done beforehand for both.  Every served result
-    is compared with the plain result of the same request.
+    checking) is done beforehand for both.  Every served result is compared
+    with the plain result of the same request.
     """
     rng = np.random.default_rng(seed)
-    kinds = [m[:3] for m in SERVE_MIX]
-    wts = np.array([m[3] for m in SERVE_MIX])
-    picks = rng.choice(len(kinds), size=n_req, p=wts / wts.sum())
-    preps, cells = {}, {}
-    for i, (kind, n, nt) in enumerate(kinds):
-        w = workload2d(seed=i, N=n, Nt=nt) if kind == "2d" else workload(seed=i, N=n, Nt=nt)
-        dim = 2 if kind == "2d" else 3
-        preps[i] = kw.Server.prepare(dim, make_grid(kw, w), w["medium"], w["source"], w["sensor"],
+    preps, cells, reqs = {}, {}, []
+    for i in range(n_req):
+        w = served_request(rng, nt_scale=nt_scale)
+        preps[i] = kw.Server.prepare(3, make_grid(kw, w), w["medium"], w["source"], w["sensor"],
                                      **dict(w["options"], DeviceNum=device))
-        cells[i] = float(np.prod(w["shape"])) * nt
+        cells[i] = float(np.prod(w["shape"])) * w["Nt"]
+        reqs.append((w["shape"], w["Nt"]))
+    picks = np.arange(n_req)
     work = float(sum(cells[k] for k in picks))
 
     def plain(arrivals):
@@ -408,9 +482,15 @@ def served_section(kw, device, n_req=48, seed=7, load=0.9):
     pp_span, pp_lat, _ = plain(arrivals)
     sp_span, sp_lat, sp_outs, _ = served(arrivals)
     err = max(err, max(_rel_l2(a, b) for a, b in zip(sp_outs, p_outs)))
-    mix = ["%s %s Nt=%d x%d" % (kind, "x".join([str(n)] * (2 if kind == "2d" else 3)), nt, int((picks == i).sum()))
-           for i, (kind, n, nt) in enumerate(kinds)]
+    edges = [s for shp, _ in reqs for s in shp]
+    mix = {"requests": n_req, "nt_scale": nt_scale, "Nt_range": [min(n for _, n in reqs), max(n for _, n in reqs)],
+           "cells_range": [min(int(np.prod(s)) for s, _ in reqs), max(int(np.prod(s)) for s, _ in reqs)],
+           "edge_counts": {str(e): edges.count(e) for e in SERVE_EDGES},
+           "anisotropic": sum(len(set(s)) > 1 for s, _ in reqs)}
     return {
+        "stream": "3-D requests, per-axis edges log-uniform over %s, blob media, point source 0.5-2 MHz, "
+                  "Nt uniform 500-2000 x %g (time-scaled subset of the 2000-request stream)"
+                  % (list(SERVE_EDGES), nt_scale),
         "requests": n_req, "mix": mix, "cell_steps": work,
         "saturated": {"served_gcell_steps_per_s": work / s_span / 1e9, "plain_gcell_steps_per_s": work / p_span / 1e9,
                       "served_makespan_s": s_span, "plain_makespan_s": p_span, "served_worker_seconds": s_worker},
@@ -519,34 +599,53 @@ def tr_check(kw, N=256, n_elem=128, radius=110, Nt=1500, dx=0.1e-3, seed=5):
 LARGE_BYTES_PER_CELL_STEP = 164.0   # 4 B x (6 + 7 state + 8 medium + 2 x 8 spectral + 4 full-volume accumulators)
 
 
-def large_section(kw, device, N=512, Nt=200, seed=11):
-    """The large layered simulation (512^3, full-volume p_max / p_rms) at a
-    reduced number of time steps: one warm-up and one timed simulation with
-    every input resident, per-class device times from a third run."""
+def large_section(kw, device, N=512, Nt=2000, seed=11):
+    """The large layered simulation (512^3, full-volume p_max / p_rms) at its
+    full Nt with every input resident.  Warm-up: the first source_steps + 8
+    steps (every step structure is captured); then one whole simulation,
+    stepped as its source-active part and its quiet part (each call returns
+    when its steps are done), so the two kinds of step are timed apart;
+    per-class device times from the first 200 steps of a further run."""
     t0 = time.perf_counter()
     w = layered_workload(seed=seed, N=N, Nt=Nt)
     cells = float(np.prod(w["shape"]))
+    src_steps = min(w["src_len"], Nt)
     with kw.Simulation(3, make_grid(kw, w), w["medium"], w["source"], w["sensor"], **dict(w["options"], DeviceNum=device)) as sim:
         setup_s = time.perf_counter() - t0
         dev_gb = sim.device_bytes() / 1e9
-        sim.run_timed(1)
-        ms = sim.run_timed(1)
+        sim.step(min(Nt, src_steps + 8))
+        sim.reset()
+        ta = time.perf_counter()
+        sim.step(src_steps)
+        tb = time.perf_counter()
+        if Nt > src_steps:
+            sim.step(Nt - src_steps)
+        tc = time.perf_counter()
+        ms = (tc - ta) * 1e3
         classes = {}
+        n_cls = min(Nt, 200)
+        sim.reset()
         sim.set_timing(["zstage_u", "zstage_r", "zstage_p", "ypass", "xpass", "sensor", "source"])
-        sim.run_device()
+        sim.step(n_cls)
         for c in ("zstage_u", "zstage_r", "zstage_p", "ypass", "xpass", "sensor", "source"):
-            classes[c] = round(sim.timing(c)[0] / Nt * 1e3, 1)
+            classes[c] = round(sim.timing(c)[0] / n_cls * 1e3, 1)
         sim.set_timing([])
     peak, peak_kind = measured_peak()
-    src_steps = min(w["src_len"], Nt)
     alg = cells * (LARGE_BYTES_PER_CELL_STEP * Nt + BYTES_PER_CELL_SRC_STEP * src_steps)
     achieved = alg / (ms / 1e3) / 1e9
+    phases = {"source_active": {"steps": src_steps, "ms_per_step": (tb - ta) * 1e3 / src_steps,
+                                "gcell_steps_per_s": cells * src_steps / (tb - ta) / 1e9}}
+    if Nt > src_steps:
+        phases["quiet"] = {"steps": Nt - src_steps, "ms_per_step": (tc - tb) * 1e3 / (Nt - src_steps),
+                           "gcell_steps_per_s": cells * (Nt - src_steps) / (tc - tb) / 1e9}
     return {"workload": "kspaceFirstOrder3D %d^3 layered 1480/1560/2800/1560 m/s (rough interfaces, 3-cell RMS), "
                         "alpha_power 1.1, per-layer alpha_coeff %s dB/(MHz^y cm) and BonA 5..9, 128x128 phased plane "
                         "p source focused 300 cells deep, 500 kHz 5-cycle burst, PML 20, full-volume p_max + p_rms"
                         % (N, "/".join("%g" % a for a in LAYER_ALPHA)),
             "Nt": Nt, "source_steps": src_steps, "value": cells * Nt / (ms / 1e3) / 1e9, "unit": UNIT,
             "ms_per_time_step": ms / Nt, "device_gb": round(dev_gb, 2), "host_setup_s": round(setup_s, 1),
+            "phases": phases, "timing": "wall clock around synchronous step calls (graph-replayed steps)",
+            "class_us_per_step_over": "first %d steps" % min(Nt, 200),
             "roofline": {"achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                          "peak_source": peak_kind, "alg_bytes_per_cell_step": LARGE_BYTES_PER_CELL_STEP},
             "us_per_time_step": classes}
@@ -614,7 +713,14 @@ def adjoint_section(kw, device, Nt=3000, n_shots=16, fd_cells=32, seed=4, tr=Tru
         ad.append(float(g0[x, yy]))
     fd, ad = np.array(fd), np.array(ad)
     big = np.abs(fd) > 0.05 * np.abs(fd).max()
-    tr_cos = [{"elements": ne, "cosine_with_adjoint_gradient": tr_check(kw, n_elem=ne)} for ne in (512, 128)] if tr else None
+    tr_cos = None
+    if tr:
+        # the inversion case's own ring (512^2, 256 elements, radius 230,
+        # Nt 3000) and, for contrast, a dense and a sparse ring on 256^2
+        tr_cos = [{"grid": 512, "elements": 256, "radius": 230, "Nt": Nt,
+                   "cosine_with_adjoint_gradient": tr_check(kw, N=512, n_elem=256, radius=230, Nt=Nt, seed=seed)}]
+        tr_cos += [{"grid": 256, "elements": ne, "radius": 110, "Nt": 1500,
+                    "cosine_with_adjoint_gradient": tr_check(kw, n_elem=ne)} for ne in (512, 128)]
     return {
         "workload": "2D %dx%d ring array of %d elements (radius %d cells), %d shots, 1 MHz Ricker, Nt=%d, "
                     "homogeneous 1500 m/s start, blob true medium" % (w["N"], w["N"], w["n_elem"], w["radius"],
@@ -630,10 +736,9 @@ def adjoint_section(kw, device, Nt=3000, n_shots=16, fd_cells=32, seed=4, tr=Tru
                      "median_rel_err_where_fd_above_5pct": float(np.median(np.abs(ad[big] - fd[big]) / np.abs(fd[big])))},
         "time_reversal_check": None if tr_cos is None else {
             "rings": tr_cos,
-            "case": "256x256, ring of radius 110 cells, shot 0, Nt=1500: image sum_t (2/c) dp/dt q of the forward "
-                    "field p and the field q of the time-reversal run fed the residual, inside 0.8 x radius; the "
-                    "time-reversal mode pins p at the sensor cells, so sparse rings scatter and the image departs "
-                    "from the exact gradient"},
+            "case": "shot 0 of each ring: image sum_t (2/c) dp/dt q of the forward field p and the field q of the "
+                    "time-reversal run fed the residual, inside 0.8 x radius; the time-reversal mode pins p at the "
+                    "sensor cells, so sparse rings scatter and the image departs from the exact gradient"},
     }
 
 
@@ -643,16 +748,18 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--cpu-steps", type=int, default=3)
+    ap.add_argument("--cpu-steps", type=int, default=5)
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--Nt", type=int, default=1000)
     ap.add_argument("--N", type=int, default=256)
-    ap.add_argument("--serve-requests", type=int, default=48, help="0 skips the served-stream section")
+    ap.add_argument("--serve-requests", type=int, default=40, help="0 skips the served-stream section")
+    ap.add_argument("--serve-nt-scale", type=float, default=0.2, help="Nt scale of the served-stream subset")
+    ap.add_argument("--cfg1-runs", type=int, default=20, help="0 skips the 2-D 128^2 section")
     ap.add_argument("--adjoint-shots", type=int, default=16, help="0 skips the adjoint section")
     ap.add_argument("--adjoint-fd", type=int, default=32, help="finite-difference cells of the adjoint check")
     ap.add_argument("--adjoint-workers", type=int, default=8, help="adjoint shots in flight at once")
-    ap.add_argument("--large-Nt", type=int, default=200, help="time steps of the 512^3 layered run (0 skips it)")
+    ap.add_argument("--large-Nt", type=int, default=2000, help="time steps of the 512^3 layered run (0 skips it)")
     args = ap.parse_args()
     ws, rank, local = dist_setup()
     if args.impl == "reference":
@@ -736,7 +843,11 @@ def main():
 
     served = None
     if args.serve_requests > 0:
-        served = served_section(kw, local, n_req=args.serve_requests, seed=7 + rank)
+        served = served_section(kw, local, n_req=args.serve_requests, seed=7 + rank, nt_scale=args.serve_nt_scale)
+
+    cfg1 = None
+    if args.cfg1_runs > 0:
+        cfg1 = cfg1_section(kw, local, runs=args.cfg1_runs, cpu=(rank == 0 and not args.no_cpu))
 
     adjoint = None
     if args.adjoint_shots > 0:
@@ -752,6 +863,9 @@ def main():
         try:
             cpu = cpu_baseline(w, args.cpu_steps)
             cpu.pop("seconds", None)
+            c32 = cpu_baseline(w, args.cpu_steps, single=True)
+            c32.pop("seconds", None)
+            cpu["fp32"] = c32
         except Exception as e:  # the baseline is reported, not required
             cpu = {"error": str(e)}
 
@@ -768,7 +882,7 @@ def main():
                            "parallelism": "replicas x%d" % ws},
                 "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
                 "clocks": clocks, "kernel_classes": classes, "served": served, "adjoint": adjoint,
-                "large_512": large}
+                "large_512": large, "cfg1_2d": cfg1}
         print(json.dumps(line), flush=True)
     if ws > 1:
         import torch.distributed as dist
