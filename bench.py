@@ -812,15 +812,21 @@ def main():
     src_steps = min(w["src_len"], Nt)
     alg_bytes_per_sim = cells * (BYTES_PER_CELL_STEP * Nt + BYTES_PER_CELL_SRC_STEP * src_steps)
     achieved = alg_bytes_per_sim / (ms / args.steps / 1e3) / 1e9
-    traffic = None
+    # DRAM bytes of one time step, per-kernel ncu captures of the 256^3
+    # workload (profiles/traffic_256cube_per_kernel.md); ncu runs each launch
+    # with cold caches, so this is an upper bound on the warm traffic
+    traffic, traffic_src = None, None
     tf = os.path.join(ROOT, "profiles", "step_traffic_256.json")
-    if os.path.exists(tf):
+    if os.path.exists(tf) and args.N == 256:
         try:
-            traffic = json.load(open(tf)).get("dram_bytes_per_step")
+            tj = json.load(open(tf))
+            traffic = tj.get("dram_bytes_per_step")
+            traffic_src = {"file": "profiles/step_traffic_256.json", "measured_at_commit": tj.get("measured_at_commit"),
+                           "method": tj.get("method"), "caveat": tj.get("caveat")}
         except Exception:
             traffic = None
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                "traffic": traffic, "peak_source": peak_kind,
+                "traffic": traffic, "traffic_source": traffic_src, "peak_source": peak_kind,
                 "kernel": "one time step of the loop (all its launches)",
                 "alg_bytes_per_cell_step": BYTES_PER_CELL_STEP}
     sim.close()
