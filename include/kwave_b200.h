@@ -188,6 +188,18 @@ typedef struct kw_problem {
 
     /* transducer velocity source; num_points 0 when absent */
     kw_transducer_source transducer_source;
+
+    /* 'StreamToDisk' (kspaceFirstOrder3D.m:1101-1146, 1235-1295): 0 = off;
+       otherwise the p time series is recorded through a device buffer of
+       this many time steps, and kw_run writes each filled buffer out during
+       the loop -- appended to stream_to_disk_file (FP32, column-major
+       sensor_num x steps blocks, as fwrite writes them), which is read back
+       into out->p after the loop and deleted, or, with no file, straight
+       into out->p.  3-D forward runs recording p only.  The device holds
+       sensor_num x stream_to_disk values of the series instead of the whole
+       record; kw_copy_outputs cannot return a streamed p. */
+    uint64_t stream_to_disk;
+    const char *stream_to_disk_file;
 } kw_problem;
 
 /* Output sizes (createStorageVariables.m:58-88). */
@@ -290,6 +302,11 @@ typedef struct kw_server_config {
        issued drains, its memory and slot are released -- and its waiter gets
        KW_ERR_TIMEOUT.  0 = no deadline. */
     uint32_t request_timeout_ms;
+    /* Grid cells that fill the GPU: a resident request of this many cells
+       or more has its slices issued alone, smaller ones share the device in
+       proportion to their size (in-flight cells summed up to this); the
+       oldest waiting request goes first.  0 = 4 Mi cells. */
+    uint64_t fill_cells;
 } kw_server_config;
 
 typedef struct kw_server_stats {

@@ -24,6 +24,7 @@ struct SensorArgs {
     float *vmax[4], *vmin[4], *vsq[4];
     int nfield;
     int record_start;
+    int ring;                  // > 0: the series hold `ring` columns, column = step mod ring
     const int *d_t;
 };
 
@@ -48,7 +49,7 @@ __global__ void k_sensor(SensorArgs a) {
     for (int f = 0; f < 4; ++f) {
         if (f >= a.nfield || !a.field[f]) continue;
         const float v = sensor_value(a.field[f], a.idx, a.w, a.M, a.K, m);
-        if (a.series[f]) a.series[f][m + (long long)a.M * fi] = v;
+        if (a.series[f]) a.series[f][m + (long long)a.M * (a.ring ? fi % a.ring : fi)] = v;
         if (a.vmax[f]) a.vmax[f][m] = fi == 0 ? v : fmaxf(a.vmax[f][m], v);
         if (a.vmin[f]) a.vmin[f][m] = fi == 0 ? v : fminf(a.vmin[f][m], v);
         if (a.vsq[f]) a.vsq[f][m] = fi == 0 ? v * v : fmaf(v, v, a.vsq[f][m]);
@@ -69,7 +70,7 @@ __global__ void k_sensor_all(SensorArgs a) {
     for (int f = 0; f < 4; ++f) {
         if (f >= a.nfield || !a.field[f]) continue;
         const float4 v = *reinterpret_cast<const float4 *>(a.field[f] + m);
-        if (a.series[f]) *reinterpret_cast<float4 *>(a.series[f] + m + (long long)a.M * fi) = v;
+        if (a.series[f]) *reinterpret_cast<float4 *>(a.series[f] + m + (long long)a.M * (a.ring ? fi % a.ring : fi)) = v;
         if (a.vmax[f]) {
             float4 *q = reinterpret_cast<float4 *>(a.vmax[f] + m);
             if (fi == 0) *q = v;

@@ -126,6 +126,7 @@ struct kw_plan {
     float *o_uns[3] = {nullptr, nullptr, nullptr};   // u_non_staggered series
     float *ush = nullptr;          // one unstaggered velocity component
     int in_lo[3] = {0, 0, 0}, in_n[3] = {1, 1, 1};
+    int stream_cols = 0;           // StreamToDisk: columns of the p series ring (0: whole record)
     long long in_count = 1;
 
     int t = 1;                     // next step to run (1-based)

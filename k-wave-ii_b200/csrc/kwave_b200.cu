@@ -477,6 +477,7 @@ kw_status sensors(kw_plan *P, int t) {
         if (any) {
             Scope s(P, KW_KCLASS_SENSOR);
             a.record_start = P->record_start;
+            a.ring = P->stream_cols;
             a.d_t = P->d_t;
             if (P->sidx_all && P->M % 4 == 0)
                 k_sensor_all<<<(P->M / 4 + 255) / 256, 256, 0, P->stream>>>(a);
@@ -1321,8 +1322,20 @@ kw_status create(const kw_problem *pr, kw_plan *P) {
     }
     const bool tr = P->time_rev;
     const size_t ser = (size_t)P->M * P->num_rec;
+    if (q.stream_to_disk) {
+        // kspaceFirstOrder_inputChecking.m:1369-1375, checkOptionalInputs.m:353-374
+        if (q.dim != 3) return fail(KW_ERR_INVALID, "Optional input 'StreamToDisk' is currently only compatible with 3D fluid simulations.");
+        if (tr || P->M == 0)
+            return fail(KW_ERR_INVALID, "The optional input 'StreamToDisk' is currently only compatible with forward "
+                        "simulations using a non-zero sensor mask.");
+        if (P->rec != KW_REC_P)
+            return fail(KW_ERR_INVALID, "The optional input 'StreamToDisk' is currently only compatible with sensor.record = {'p'} (the default).");
+        if (q.sensor_vertices > 1)
+            return fail(KW_ERR_UNSUPPORTED, "StreamToDisk needs a binary (or nearest-neighbour Cartesian) sensor mask");
+        P->stream_cols = (int)std::min<uint64_t>(q.stream_to_disk, (uint64_t)P->num_rec);
+    }
     if (!tr && P->M > 0) {
-        if (P->rec & KW_REC_P) KW_TRY(palloc(P, &P->o_series[0], ser));
+        if (P->rec & KW_REC_P) KW_TRY(palloc(P, &P->o_series[0], P->stream_cols ? (size_t)P->M * P->stream_cols : ser));
         if (P->rec & KW_REC_P_MAX) KW_TRY(palloc(P, &P->o_max[0], P->M));
         if (P->rec & KW_REC_P_MIN) KW_TRY(palloc(P, &P->o_min[0], P->M));
         if (P->rec & KW_REC_P_RMS) KW_TRY(palloc(P, &P->o_sq[0], P->M));
@@ -1540,6 +1553,97 @@ kw_status run_streamed(kw_plan *P, const std::vector<SeriesOut> &ser) {
     return st;
 }
 
+// StreamToDisk (kspaceFirstOrder3D.m:1101-1146, 1235-1295): the loop runs in
+// chunks of stream_cols recorded steps; after each chunk the ring of p
+// columns is copied to pinned host memory and appended to the file (FP32,
+// column-major, as MATLAB's fwrite) -- or copied into out->p when no file is
+// named -- while the next chunk computes.  After the loop the file is read
+// back into out->p and deleted, and the other outputs are copied.
+kw_status run_to_disk(kw_plan *P, kw_outputs *o) {
+    const size_t M = (size_t)P->M, C = (size_t)P->stream_cols;
+    const char *path = P->prob.stream_to_disk_file;
+    if (P->t != 1 || P->started) KW_TRY(zero_state(P));
+    if (!P->copy_stream) KW_CUDA(cudaStreamCreateWithFlags(&P->copy_stream, cudaStreamNonBlocking));
+    for (int k = 0; k < 2; ++k) {
+        if (!P->ev_comp[k]) KW_CUDA(cudaEventCreateWithFlags(&P->ev_comp[k], cudaEventDisableTiming));
+        if (!P->ev_copy[k]) KW_CUDA(cudaEventCreateWithFlags(&P->ev_copy[k], cudaEventDisableTiming));
+    }
+    std::FILE *fp = nullptr;
+    if (path) {
+        fp = std::fopen(path, "w+b");
+        if (!fp) return fail(KW_ERR_INVALID, "Error in writing file using 'StreamToDisk': cannot open %s", path);
+    }
+    float *host = nullptr;
+    if (cudaMallocHost((void **)&host, 2 * M * C * sizeof(float)) != cudaSuccess) {
+        if (fp) {
+            std::fclose(fp);
+            std::remove(path);
+        }
+        return fail(KW_ERR_NOMEM, "StreamToDisk: pinned host buffer of %zu bytes failed", 2 * M * C * sizeof(float));
+    }
+    kw_status st = KW_OK;
+    // write chunk [c0, c1) held in ring half `slot`
+    auto drain = [&](int slot, int c0, int c1) -> kw_status {
+        KW_CUDA(cudaEventSynchronize(P->ev_copy[slot]));
+        const float *h = host + (size_t)slot * M * C;
+        const size_t n = M * (size_t)(c1 - c0);
+        if (fp) {
+            if (std::fwrite(h, sizeof(float), n, fp) != n)
+                return fail(KW_ERR_INVALID, "Error in writing file using 'StreamToDisk'");
+        } else if (o->p) {
+            std::memcpy(o->p + M * (size_t)c0, h, n * sizeof(float));
+        }
+        return KW_OK;
+    };
+    int prev = -1, pc0 = 0, pc1 = 0, k = 0;
+    for (int c0 = 0; c0 < P->num_rec && st == KW_OK; c0 += (int)C, ++k) {
+        const int c1 = std::min(P->num_rec, c0 + (int)C);
+        const int slot = k & 1;
+        const long long target = (long long)P->record_start + c1;   // next step after the chunk
+        if (target > P->t) st = run_steps(P, (uint64_t)(target - P->t));
+        if (st != KW_OK) break;
+        // columns c0 .. c1-1 sit at ring columns 0 .. c1-c0-1 (c0 is a multiple of C)
+        cudaError_t e = cudaEventRecord(P->ev_comp[slot], P->stream);
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(P->copy_stream, P->ev_comp[slot], 0);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(host + (size_t)slot * M * C, P->o_series[0], M * (size_t)(c1 - c0) * sizeof(float),
+                                cudaMemcpyDeviceToHost, P->copy_stream);
+        if (e == cudaSuccess) e = cudaEventRecord(P->ev_copy[slot], P->copy_stream);
+        // the compute stream may overwrite this half's device columns only
+        // after the copy: the next chunk waits for it
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(P->stream, P->ev_copy[slot], 0);
+        if (e != cudaSuccess) {
+            st = fail(KW_ERR_CUDA, "streamed output copy failed: %s", cudaGetErrorString(e));
+            break;
+        }
+        if (prev >= 0) st = drain(prev, pc0, pc1);
+        prev = slot;
+        pc0 = c0;
+        pc1 = c1;
+    }
+    if (st == KW_OK && prev >= 0) st = drain(prev, pc0, pc1);
+    if (st == KW_OK && P->t <= P->index_end) st = run_steps(P, (uint64_t)P->index_end);
+    cudaStreamSynchronize(P->copy_stream);
+    cudaStreamSynchronize(P->stream);
+    cudaFreeHost(host);
+    if (fp) {
+        // reload the complete streamed series and remove the file
+        if (st == KW_OK && o->p) {
+            std::fflush(fp);
+            std::rewind(fp);
+            const size_t n = M * (size_t)P->num_rec;
+            if (std::fread(o->p, sizeof(float), n, fp) != n)
+                st = fail(KW_ERR_INVALID, "StreamToDisk: short read of %s", path);
+        }
+        std::fclose(fp);
+        std::remove(path);
+    }
+    KW_TRY(st);
+    kw_outputs rest = *o;
+    rest.p = nullptr;
+    return kw_copy_outputs(P, &rest);
+}
+
 }  // namespace
 
 // --------------------------------------------------------------------------
@@ -1650,6 +1754,8 @@ kw_status kw_run_device(kw_plan *P) {
 kw_status kw_copy_outputs(kw_plan *P, kw_outputs *o) {
     if (!P || !o) return fail(KW_ERR_INVALID, "NULL argument");
     KW_TRY(use_device(P));
+    if (P->stream_cols && o->p)
+        return fail(KW_ERR_UNSUPPORTED, "the p series of a StreamToDisk plan is written out by kw_run only");
     const size_t ser = (size_t)P->M * P->num_rec;
     KW_TRY(copy_dev(P, o->p, P->o_series[0], ser));
     KW_TRY(copy_dev(P, o->p_max, P->o_max[0], P->M));
@@ -1675,6 +1781,7 @@ kw_status kw_copy_outputs(kw_plan *P, kw_outputs *o) {
 kw_status kw_run(kw_plan *P, kw_outputs *o) {
     if (!P || !o) return fail(KW_ERR_INVALID, "NULL argument");
     KW_TRY(use_device(P));
+    if (P->stream_cols) return run_to_disk(P, o);
     // time series large enough to be worth streaming to the host during the loop
     std::vector<SeriesOut> ser;
     if (!P->time_rev && P->M > 0) {

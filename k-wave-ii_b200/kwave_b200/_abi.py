@@ -104,6 +104,8 @@ class kw_problem(C.Structure):
         ("sensor_weights", f32p),
         ("alpha_filter", f32p),
         ("transducer_source", kw_transducer_source),
+        ("stream_to_disk", C.c_uint64),
+        ("stream_to_disk_file", C.c_char_p),
     ]
 
 
@@ -129,7 +131,7 @@ class kw_outputs(C.Structure):
 # every symbol the header declares, with its signature
 class kw_server_config(C.Structure):
     _fields_ = [("device", C.c_int32), ("hbm_budget_bytes", C.c_uint64), ("max_active", C.c_int32),
-                ("steps_per_slice", C.c_int32), ("request_timeout_ms", C.c_uint32)]
+                ("steps_per_slice", C.c_int32), ("request_timeout_ms", C.c_uint32), ("fill_cells", C.c_uint64)]
 
 
 class kw_server_stats(C.Structure):

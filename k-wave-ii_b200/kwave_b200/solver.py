@@ -39,6 +39,9 @@ _KNOWN_OPTIONS = {
     "Smooth", "UsekSpace", "UseSG", "StreamToDisk", "SaveToDisk", "SaveToDiskExit",
     "HDFCompressionLevel", "MultiAxialPMLRatio", "PMLRange", "RadialSymmetry", "UseFD", "DeviceNum",
 }
+# kspaceFirstOrder_setDefaults.m:181, 197
+STREAM_TO_DISK_STEPS_DEF = 200
+STREAM_TO_DISK_FILENAME = "temp_sensor_data.bin"
 _DATA_CASTS = {"off", "double", "single", "gsingle", "gdouble", "GPUsingle", "GPUdouble",
                "gpuArray-single", "gpuArray-double"}
 
@@ -159,9 +162,23 @@ def _prepare(dim, kgrid, medium, source, sensor, options):
     P.dim = dim
 
     # ---- optional inputs (setDefaults.m:151-170, checkOptionalInputs.m) ----
-    for o in ("StreamToDisk", "SaveToDisk", "SaveToDiskExit", "HDFCompressionLevel"):
+    for o in ("SaveToDisk", "SaveToDiskExit", "HDFCompressionLevel"):
         if options.get(o) not in (None, False):
-            raise KWaveInputError("Optional input %r (HDF5 / disk streaming) is not supported by this solver." % o)
+            raise KWaveInputError("Optional input %r (the HDF5 input file of the native binaries) is not supported by "
+                                  "this solver: no HDF5 library." % o)
+    # StreamToDisk (checkOptionalInputs.m:353-374): true -> 200 steps; the
+    # series goes through a file named as the reference names it
+    stream = options.get("StreamToDisk", False)
+    if stream is not False and stream is not None:
+        if dim != 3:
+            raise KWaveInputError("Optional input 'StreamToDisk' is currently only compatible with 3D fluid simulations.")
+        if isinstance(stream, (bool, np.bool_)):
+            stream = STREAM_TO_DISK_STEPS_DEF if stream else 0
+        elif np.size(stream) != 1 or not np.isfinite(stream) or stream < 0:
+            raise KWaveInputError("Optional input 'StreamToDisk' must be a single scalar or Boolean value.")
+        stream = int(stream)
+    else:
+        stream = 0
     for o in ("MultiAxialPMLRatio", "PMLRange", "RadialSymmetry", "UseFD"):
         if o in options:
             raise KWaveInputError("Optional input %r is not valid for kspaceFirstOrder%dD." % (o, dim))
@@ -657,6 +674,18 @@ def _prepare(dim, kgrid, medium, source, sensor, options):
         if r in _abi.REC_BITS:
             bits |= 1 << _abi.REC_BITS[r]
     pr.record = bits
+    if stream:
+        # inputChecking.m:1369-1375
+        if not use_sensor or time_rev or mask is None and getattr(P, "cart_points", None) is None:
+            raise KWaveInputError("The optional input 'StreamToDisk' is currently only compatible with forward "
+                                  "simulations using a non-zero sensor mask.")
+        if record_given and set(record) != {"p"}:
+            raise KWaveInputError("The optional input 'StreamToDisk' is currently only compatible with sensor.record "
+                                  "= {'p'} (the default).")
+        pr.stream_to_disk = stream
+        fname = STREAM_TO_DISK_FILENAME.encode()
+        keep.append(fname)
+        pr.stream_to_disk_file = fname
     if time_rev:
         trd = np.atleast_2d(np.asarray(_field(sensor, "time_reversal_boundary_data"), dtype=np.float64))
         if P.reorder_index is None and getattr(P, "order_index", None) is not None:
@@ -672,7 +701,7 @@ def _prepare(dim, kgrid, medium, source, sensor, options):
     pr.device = int(options.get("DeviceNum", 0))
     P.problem = pr
     P.keep = keep
-    P.h2d_bytes = int(sum(a.nbytes for a in keep))
+    P.h2d_bytes = int(sum(a.nbytes for a in keep if isinstance(a, np.ndarray)))
     P.record = record
     P.record_given = record_given
     P.time_rev = time_rev
@@ -860,10 +889,12 @@ class Server:
     plain call returns for the same inputs.
     """
 
-    def __init__(self, device=0, hbm_budget_bytes=0, max_active=0, steps_per_slice=0, request_timeout_ms=0):
+    def __init__(self, device=0, hbm_budget_bytes=0, max_active=0, steps_per_slice=0, request_timeout_ms=0,
+                 fill_cells=0):
         self._lib = _abi.load_library()
         cfg = _abi.kw_server_config(device=device, hbm_budget_bytes=hbm_budget_bytes, max_active=max_active,
-                                    steps_per_slice=steps_per_slice, request_timeout_ms=request_timeout_ms)
+                                    steps_per_slice=steps_per_slice, request_timeout_ms=request_timeout_ms,
+                                    fill_cells=fill_cells)
         h = C.c_void_p()
         _abi.check(self._lib.kw_server_create(C.byref(cfg), C.byref(h)))
         self.handle = h

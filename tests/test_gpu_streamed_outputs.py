@@ -38,3 +38,31 @@ def test_streamed_series_equal_split_copy():
         assert np.array_equal(again[k], split[k]), k
     assert streamed["p"].shape == (512 * 64, 500)
     assert np.abs(streamed["p"]).max() > 0
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("steps", [True, 7])
+def test_stream_to_disk_equals_plain_run(tmp_path, monkeypatch, steps):
+    """StreamToDisk: the p series goes through a device buffer of `steps`
+    columns and the reference's temp_sensor_data.bin in the working
+    directory, and comes back identical to the plain run; the file is gone
+    afterwards (kspaceFirstOrder3D.m:1101-1146, 1235-1295).  7 does not divide
+    the 160 recorded steps, so the last chunk is partial."""
+    import kwave_b200 as kw
+    monkeypatch.chdir(tmp_path)
+    N = 48
+    kg = kw.kWaveGrid(N, 1e-4, N, 1e-4, N, 1e-4)
+    kg.setTime(180, 0.3 * 1e-4 / 1600.0)
+    ax = np.arange(N)
+    c = 1500.0 + 100.0 * np.exp(-((ax[:, None, None] - 20) ** 2 + (ax[None, :, None] - 24) ** 2
+                                  + (ax[None, None, :] - 28) ** 2) / (2 * 6.0 ** 2))
+    med = {"sound_speed": c, "density": 1000.0, "alpha_coeff": 0.5, "alpha_power": 1.5}
+    mask = np.zeros((N, N, N))
+    mask[30, :, :] = 1
+    src = {"p0": kw.makeBall(N, N, N, 24, 24, 24, 4)}
+    sen = {"mask": mask, "record_start_index": 21}
+    plain = kw.kspaceFirstOrder3D(kg, med, src, sen, PMLSize=6)
+    streamed = kw.kspaceFirstOrder3D(kg, med, src, sen, PMLSize=6, StreamToDisk=steps)
+    assert streamed.shape == plain.shape == (N * N, 160)
+    assert np.array_equal(streamed, plain)
+    assert not (tmp_path / "temp_sensor_data.bin").exists()

@@ -220,3 +220,25 @@ def test_layered_workload_recipe():
     assert first.min() <= 1 and first[0] == first.min() and np.all(first >= 0)
     assert w["sensor"]["mask"].all() and w["sensor"]["record"] == ["p_max", "p_rms"]
     assert w["dt"] == pytest.approx(0.3 * 1e-4 / 2800.0)
+
+
+def test_stream_to_disk_setup():
+    """StreamToDisk (checkOptionalInputs.m:353-374, inputChecking.m:1369-1375):
+    3-D only, p only; true means 200 steps; the series file is the
+    reference's temp_sensor_data.bin."""
+    g3 = kw.kWaveGrid(16, 1e-4, 16, 1e-4, 16, 1e-4)
+    g3.setTime(10, 2e-8)
+    med = {"sound_speed": 1500.0}
+    src = {"p0": np.ones((16, 16, 16))}
+    mask = np.zeros((16, 16, 16))
+    mask[4, :, :] = 1
+    P = _prepare(3, g3, med, src, {"mask": mask}, {"StreamToDisk": True, "PMLSize": 4})
+    assert P.problem.stream_to_disk == 200 and P.problem.stream_to_disk_file == b"temp_sensor_data.bin"
+    assert _prepare(3, g3, med, src, {"mask": mask}, {"StreamToDisk": 7, "PMLSize": 4}).problem.stream_to_disk == 7
+    assert _prepare(3, g3, med, src, {"mask": mask}, {"PMLSize": 4}).problem.stream_to_disk == 0
+    with pytest.raises(KWaveInputError, match="sensor.record"):
+        _prepare(3, g3, med, src, {"mask": mask, "record": ["p", "p_max"]}, {"StreamToDisk": 5, "PMLSize": 4})
+    g2 = kw.kWaveGrid(16, 1e-4, 16, 1e-4)
+    g2.setTime(10, 2e-8)
+    with pytest.raises(KWaveInputError, match="3D fluid"):
+        _prepare(2, g2, med, {"p0": np.ones((16, 16))}, {"mask": np.ones((16, 16))}, {"StreamToDisk": True})
