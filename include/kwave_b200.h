@@ -341,7 +341,7 @@ kw_status kw_server_destroy(kw_server *server);
  * autotuner, which may give the three z-stages different widths;
  * environment variable KW_AUTOTUNE=0 turns it off).  kw_plan_tiles reports
  * the momentum stage's z width.  kw_set_tiles accepts, per class, the full
- * width or the narrow one (a quarter), sets every z-stage to tiles[0] and
+ * width, half of it or a quarter of it, sets every z-stage to tiles[0] and
  * rejects anything else; results do not depend on the choice.
  */
 kw_status kw_plan_tiles(const kw_plan *plan, int32_t tiles[3]);

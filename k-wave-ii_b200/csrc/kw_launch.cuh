@@ -1,8 +1,8 @@
 // kw_launch.cuh -- kernel launchers of one axis length.
 //
 // Each launcher picks the kernel of its length and tile width (full tiles of
-// ks_lines(N) lines or narrow ones of ks_narrow(N)), sets its shared-memory
-// limit and launches it on the plan's stream.  N = 0 selects the
+// ks_lines(N) lines, half ones of ks_half(N) or narrow ones of ks_narrow(N)),
+// sets its shared-memory limit and launches it on the plan's stream.  N = 0 selects the
 // runtime-radix kernels of kw_kernels.cuh, which take any supported length.
 // Included by kw_inst.cu only.
 #pragma once
@@ -77,6 +77,7 @@ kw_status YLaunch<N>::run(kw_plan *P, bool inv, Spec4 bufs, int nf, int kz0, int
     dim3 grid((P->g.N0 + P->TY - 1) / P->TY, N > 0 ? nkz : P->g.N2h, nf);
     if constexpr (N > 0) {
         if (P->TY == ks_lines(N)) KW_TRY((launch::ypass<N, ks_lines(N)>(P, inv, bufs, grid, kz0)));
+        else if (P->TY == ks_half(N)) KW_TRY((launch::ypass<N, ks_half(N)>(P, inv, bufs, grid, kz0)));
         else KW_TRY((launch::ypass<N, ks_narrow(N)>(P, inv, bufs, grid, kz0)));
     } else {
         size_t sh = (size_t)P->TY * P->g.N1 * sizeof(float2);
@@ -99,6 +100,9 @@ kw_status XLaunch<N>::run(kw_plan *P, Spec4 bufs, OpSet ops, int fanout, int nf,
         if (P->NL == ks_xlines(N))
             ks_xpass<N, ks_xlines(N)><<<grid, ks_threads(N, ks_xlines(N)), 0, P->stream>>>(bufs, P->g, P->tw[0], P->op,
                                                                                         ops, fanout, kz0, nkz);
+        else if (P->NL == ks_xhalf(N))
+            ks_xpass<N, ks_xhalf(N)><<<grid, ks_threads(N, ks_xhalf(N)), 0, P->stream>>>(bufs, P->g, P->tw[0], P->op,
+                                                                                      ops, fanout, kz0, nkz);
         else
             ks_xpass<N, ks_xnarrow(N)><<<grid, ks_threads(N, ks_xnarrow(N)), 0, P->stream>>>(bufs, P->g, P->tw[0],
                                                                                           P->op, ops, fanout, kz0, nkz);
@@ -115,6 +119,7 @@ kw_status ZR2CLaunch<N>::run(kw_plan *P, const float *R, float2 *H) {
     dim3 grid((P->g.N0 + 2 * P->PL_z - 1) / (2 * P->PL_z), P->g.N1, 1);
     if constexpr (N > 0) {
         if (P->PL_z == ks_lines(N)) KW_TRY((launch::zr2c<N, ks_lines(N)>(P, R, H, grid)));
+        else if (P->PL_z == ks_half(N)) KW_TRY((launch::zr2c<N, ks_half(N)>(P, R, H, grid)));
         else KW_TRY((launch::zr2c<N, ks_narrow(N)>(P, R, H, grid)));
     } else {
         size_t sh = (size_t)P->PL_z * P->g.N2 * sizeof(float2);
@@ -129,6 +134,7 @@ kw_status ZC2RLaunch<N>::run(kw_plan *P, const float2 *H, float *R) {
     dim3 grid((P->g.N0 + 2 * P->PL_z - 1) / (2 * P->PL_z), P->g.N1, 1);
     if constexpr (N > 0) {
         if (P->PL_z == ks_lines(N)) KW_TRY((launch::zc2r<N, ks_lines(N)>(P, H, R, grid)));
+        else if (P->PL_z == ks_half(N)) KW_TRY((launch::zc2r<N, ks_half(N)>(P, H, R, grid)));
         else KW_TRY((launch::zc2r<N, ks_narrow(N)>(P, H, R, grid)));
     } else {
         size_t sh = (size_t)P->PL_z * P->g.N2 * sizeof(float2);
@@ -143,6 +149,7 @@ kw_status ULaunch<N>::run(kw_plan *P, StageU a) {
     dim3 grid((P->g.N0 + 2 * a.PL - 1) / (2 * a.PL), P->g.N1, P->D);
     if constexpr (N > 0) {
         if (a.PL == ks_lines(N)) KW_TRY((launch::stage_u<N, ks_lines(N)>(P, a, grid)));
+        else if (a.PL == ks_half(N)) KW_TRY((launch::stage_u<N, ks_half(N)>(P, a, grid)));
         else KW_TRY((launch::stage_u<N, ks_narrow(N)>(P, a, grid)));
     } else {
         size_t sh = (size_t)a.PL * P->g.N2 * sizeof(float2);
@@ -157,6 +164,7 @@ kw_status RLaunch<N>::run(kw_plan *P, StageR a) {
     dim3 grid((P->g.N0 + 2 * a.PL - 1) / (2 * a.PL), P->g.N1, 1);
     if constexpr (N > 0) {
         if (a.PL == ks_lines(N)) KW_TRY((launch::stage_r<N, ks_lines(N)>(P, a, grid)));
+        else if (a.PL == ks_half(N)) KW_TRY((launch::stage_r<N, ks_half(N)>(P, a, grid)));
         else KW_TRY((launch::stage_r<N, ks_narrow(N)>(P, a, grid)));
     } else {
         size_t sh = (size_t)4 * a.PL * P->g.N2 * sizeof(float2);
@@ -171,6 +179,7 @@ kw_status PLaunch<N>::run(kw_plan *P, StageP a) {
     dim3 grid((P->g.N0 + 2 * a.PL - 1) / (2 * a.PL), P->g.N1, 1);
     if constexpr (N > 0) {
         if (a.PL == ks_lines(N)) KW_TRY((launch::stage_p<N, ks_lines(N)>(P, a, grid)));
+        else if (a.PL == ks_half(N)) KW_TRY((launch::stage_p<N, ks_half(N)>(P, a, grid)));
         else KW_TRY((launch::stage_p<N, ks_narrow(N)>(P, a, grid)));
     } else {
         size_t sh = (size_t)2 * a.PL * P->g.N2 * sizeof(float2);

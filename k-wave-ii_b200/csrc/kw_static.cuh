@@ -199,6 +199,10 @@ __host__ __device__ constexpr int ks_threads(int n, int pl) { return kThreads * 
 // the narrow tile widths used when full tiles give less than one wave of blocks
 __host__ __device__ constexpr int ks_narrow(int n) { return ks_lines(n) / 4; }
 __host__ __device__ constexpr int ks_xnarrow(int n) { return ks_xlines(n) / 4; }
+// half-width tiles, between the two: a choice of the autotuner for grids
+// whose full tiles leave a ragged last wave of blocks
+__host__ __device__ constexpr int ks_half(int n) { return ks_lines(n) / 2; }
+__host__ __device__ constexpr int ks_xhalf(int n) { return ks_xlines(n) / 2; }
 
 // ---------------------------------------------------------------------------
 // y-pass (C2C along axis 1, in place).  grid = (ceil(N0/TY), N2h, nfields),

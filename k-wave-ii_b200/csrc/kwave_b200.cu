@@ -801,11 +801,11 @@ void plan_tiles(kw_plan *P) {
 
 // ---- tile autotuner ------------------------------------------------------
 // The compile-time kernels of each pass class (z-stages, y-pass, x-pass)
-// exist with a full tile (ks_lines(n) lines) and a narrow one (ks_narrow(n)).
-// plan_tiles picks by a rule (narrow when full tiles give fewer blocks than
-// SMs); the autotuner then times a few steps with each class flipped and
-// keeps what is faster, once per grid shape and tile-relevant structure per
-// process.  Tile widths change how lines are grouped into blocks, never the
+// exist with a full tile (ks_lines(n) lines), a half one (ks_half(n)) and a
+// narrow one (ks_narrow(n), a quarter).  plan_tiles picks by a rule (narrow
+// when full tiles give fewer blocks than SMs); the autotuner then times a few
+// steps with each other width of one class at a time and keeps what is
+// faster, once per grid shape and tile-relevant structure per process.  Tile widths change how lines are grouped into blocks, never the
 // arithmetic of a line, so results are identical whichever is chosen.
 // z-tile widths of stages U, R and P (each chooses its own), y and x widths
 struct TileChoice {
@@ -872,23 +872,36 @@ kw_status autotune_tiles(kw_plan *P) {
     TileChoice best = tiles_of(P);
     float best_ms = 0.f;
     kw_status st = time_steps(P, 2, &best_ms);
-    auto flip = [](int v, int full, int narrow) { return v == full ? narrow : full; };
-    // one width at a time: stage U, stage R, stage P, y-pass, x-pass
+    // the other widths of one class at a time (full, half, quarter): stage U,
+    // stage R, stage P, y-pass, x-pass
     for (int cls = 0; cls < 5 && st == KW_OK; ++cls) {
-        TileChoice c = best;
-        const int zf = ks_lines(g.N2), zn = ks_narrow(g.N2);
-        if (cls == 0 && tune_z) c.PLu = flip(c.PLu, zf, zn);
-        else if (cls == 1 && tune_z) c.PLr = flip(c.PLr, zf, zn);
-        else if (cls == 2 && tune_z) c.PLp = flip(c.PLp, zf, zn);
-        else if (cls == 3 && tune_y) c.TY = flip(c.TY, ks_lines(g.N1), ks_narrow(g.N1));
-        else if (cls == 4 && tune_x) c.NL = flip(c.NL, ks_xlines(g.N0), ks_xnarrow(g.N0));
-        else continue;
-        set_tiles(P, c);
-        float ms = 0.f;
-        st = time_steps(P, 2, &ms);
-        if (st == KW_OK && ms < 0.97f * best_ms) {
-            best = c;
-            best_ms = ms;
+        int widths[3];
+        int *slot = nullptr;
+        TileChoice base = best;
+        if (cls <= 2 && tune_z) {
+            widths[0] = ks_lines(g.N2); widths[1] = ks_half(g.N2); widths[2] = ks_narrow(g.N2);
+            slot = cls == 0 ? &base.PLu : (cls == 1 ? &base.PLr : &base.PLp);
+        } else if (cls == 3 && tune_y) {
+            widths[0] = ks_lines(g.N1); widths[1] = ks_half(g.N1); widths[2] = ks_narrow(g.N1);
+            slot = &base.TY;
+        } else if (cls == 4 && tune_x) {
+            widths[0] = ks_xlines(g.N0); widths[1] = ks_xhalf(g.N0); widths[2] = ks_xnarrow(g.N0);
+            slot = &base.NL;
+        } else {
+            continue;
+        }
+        const int current = *slot;
+        for (int w : widths) {
+            if (w == current || st != KW_OK) continue;
+            TileChoice c = base;
+            *(cls == 0 ? &c.PLu : cls == 1 ? &c.PLr : cls == 2 ? &c.PLp : cls == 3 ? &c.TY : &c.NL) = w;
+            set_tiles(P, c);
+            float ms = 0.f;
+            st = time_steps(P, 2, &ms);
+            if (st == KW_OK && ms < 0.97f * best_ms) {
+                best = c;
+                best_ms = ms;
+            }
         }
     }
     set_tiles(P, best);
@@ -2019,11 +2032,13 @@ kw_status kw_plan_tiles(const kw_plan *P, int32_t tiles[3]) {
 kw_status kw_set_tiles(kw_plan *P, const int32_t tiles[3]) {
     if (!P || !tiles) return fail(KW_ERR_INVALID, "NULL argument");
     const Geom &g = P->g;
-    auto ok = [](int v, int n) { return v == ks_lines(n) || v == ks_narrow(n); };
-    if (P->static_z && !ok(tiles[0], g.N2)) return fail(KW_ERR_INVALID, "z tile width must be %d or %d", ks_lines(g.N2), ks_narrow(g.N2));
-    if (P->static_y && !ok(tiles[1], g.N1)) return fail(KW_ERR_INVALID, "y tile width must be %d or %d", ks_lines(g.N1), ks_narrow(g.N1));
-    if (P->static_x && tiles[2] != ks_xlines(g.N0) && tiles[2] != ks_xnarrow(g.N0))
-        return fail(KW_ERR_INVALID, "x tile width must be %d or %d", ks_xlines(g.N0), ks_xnarrow(g.N0));
+    auto ok = [](int v, int n) { return v == ks_lines(n) || v == ks_half(n) || v == ks_narrow(n); };
+    if (P->static_z && !ok(tiles[0], g.N2))
+        return fail(KW_ERR_INVALID, "z tile width must be %d, %d or %d", ks_lines(g.N2), ks_half(g.N2), ks_narrow(g.N2));
+    if (P->static_y && !ok(tiles[1], g.N1))
+        return fail(KW_ERR_INVALID, "y tile width must be %d, %d or %d", ks_lines(g.N1), ks_half(g.N1), ks_narrow(g.N1));
+    if (P->static_x && tiles[2] != ks_xlines(g.N0) && tiles[2] != ks_xhalf(g.N0) && tiles[2] != ks_xnarrow(g.N0))
+        return fail(KW_ERR_INVALID, "x tile width must be %d, %d or %d", ks_xlines(g.N0), ks_xhalf(g.N0), ks_xnarrow(g.N0));
     const bool z_fixed = P->time_rev || (P->psrc.present && !P->psrc.dense_fast && !P->psrc.dense_general) ||
                          (P->usrc.present && !P->usrc.dense_fast && !P->usrc.dense_general);
     if (P->static_z && z_fixed && tiles[0] != P->PL_z)

@@ -154,7 +154,7 @@ def test_column_major_abi_matches_row_major(name):
 @pytest.mark.gpu
 @pytest.mark.parametrize("name", ["3d_intensity_static", "3d_static_mixed_radix", "2d_homog_p0"])
 def test_tile_widths_do_not_change_results(name):
-    """Every choice of full or narrow tiles the autotuner may make gives
+    """Every choice of full, half or quarter tiles the autotuner may make gives
     bit-identical outputs (tile widths group lines into blocks; the
     arithmetic of a line does not depend on them)."""
     import itertools
@@ -170,7 +170,7 @@ def test_tile_widths_do_not_change_results(name):
             options.append([0])
         else:
             full = min(64, 1 << int(np.floor(np.log2(4096 // n))))
-            options.append([full, full // 4])
+            options.append([full, full // 2, full // 4])
     for tiles in itertools.product(*options):
         sim.set_tiles(tiles)
         out = sim.run()
