@@ -21,6 +21,8 @@
 // is a full complex transform.
 #pragma once
 
+#include <cuda.h>   // CUtensorMap (the type only; maps are encoded through the runtime's driver entry point)
+
 #include "kw_fft.cuh"
 
 namespace kw {
@@ -531,6 +533,21 @@ struct StageR {
     TRSrc tr;
     int write_spec;
     const int *d_t;
+};
+
+// Tensor maps of one stage R launch with TMA staging, filled per launch by
+// the host (rho[] name the current input buffers).  Real fields: 3-D FP32
+// maps of (N0, N1, N2) with a (TX, 1, zbox) box; spectra: 3-D 8-byte maps
+// of (N0, N1, N2/2+1) with a (TX, 1, N2/2+1) box.
+struct StageRMaps {
+    CUtensorMap rho[3];    // staged rho_i
+    CUtensorMap coef;      // mass coefficient: q (nonlinear) or rho0 (linear)
+    CUtensorMap rho0;      // rho0 for the equation of state (nonlinear)
+    CUtensorMap c0;
+    CUtensorMap bona;
+    CUtensorMap spec[3];   // spectra (rows prefetch)
+    int zbox;              // z extent of a real-field box (N2 / zbox boxes per field)
+    int *err;              // bit 1: a staged copy did not arrive in time
 };
 
 __device__ __forceinline__ void apply_tr(float2 *sm, const TRSrc &tr, const Geom &g, int PL, int x0, int y, int t,

@@ -56,8 +56,23 @@ template <int N, int PL>
 kw_status stage_r(kw_plan *P, const StageR &a, dim3 grid) {
     using Z = ZStage<N, PL>;
     const size_t sh = (size_t)(Z::TILE + 2 * Z::SLICE) * sizeof(float2);
-    KW_TRY(set_smem((const void *)ks_stage_r<N, PL>, sh));
-    ks_stage_r<N, PL><<<grid, Z::NT, sh, P->stream>>>(a, P->tw[2]);
+    StageRMaps m;
+    bool tma = false;
+    KW_TRY(stage_r_maps(P, a, Z::TX, &m, &tma));
+    // TMA boxes hold at most 256 rows: the half spectrum's N/2 + 1 rows fit
+    // for N <= 384
+    if constexpr (N <= 384) {
+        if (tma) {
+            // 128 bytes of slack for the kernel to align its TMA destinations
+            KW_TRY(set_smem((const void *)ks_stage_r<N, PL, true>, sh + 128));
+            ks_stage_r<N, PL, true><<<grid, Z::NT, sh + 128, P->stream>>>(a, P->tw[2], m);
+            return KW_OK;
+        }
+    }
+    {
+        KW_TRY(set_smem((const void *)ks_stage_r<N, PL, false>, sh));
+        ks_stage_r<N, PL, false><<<grid, Z::NT, sh, P->stream>>>(a, P->tw[2], m);
+    }
     return KW_OK;
 }
 

@@ -127,6 +127,12 @@ struct kw_plan {
     float *ush = nullptr;          // one unstaggered velocity component
     int in_lo[3] = {0, 0, 0}, in_n[3] = {1, 1, 1};
     int stream_cols = 0;           // StreamToDisk: columns of the p series ring (0: whole record)
+
+    // TMA staging of stage R: usable for this plan's shapes, tensor maps by
+    // (device pointer, box width), device error word of bounded waits
+    bool tma_r = false;
+    std::map<std::pair<const void *, int>, CUtensorMap> tmaps;
+    int *d_err = nullptr;
     long long in_count = 1;
 
     int t = 1;                     // next step to run (1-based)
@@ -163,6 +169,9 @@ namespace kw {
 
 // raise the dynamic shared-memory limit of a kernel when it needs more than 48 KB
 kw_status set_smem(const void *fn, size_t bytes);
+// tensor maps of a stage R launch with tile width TX; *use is false when
+// the plan stages with cp.async instead
+kw_status stage_r_maps(kw_plan *P, const StageR &a, int TX, StageRMaps *m, bool *use);
 // check the last launch and count it in the plan
 kw_status launched(kw_plan *P);
 

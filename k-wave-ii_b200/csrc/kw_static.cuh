@@ -443,13 +443,74 @@ __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wai
 template <int N>
 __device__ __forceinline__ void cp_async_wait_group() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
 
+// ---------------------------------------------------------------------------
+// Tensor-memory-accelerator (TMA) staging: one thread issues a bulk tensor
+// copy of a whole tile (a real field's TX x N2 cells at one y, or the N2/2+1
+// half-spectrum rows of TX columns) into shared memory; the block waits on
+// an mbarrier for the bytes to land.  The copy takes no registers, address
+// arithmetic or load instructions from the other threads.  Tensor maps
+// cover this GPU's own memory only; no multicast.
+//
+// Every wait is bounded: after kTmaSpinLimit polls it gives up, sets bit 1
+// of *err (the host turns that into KW_ERR_TIMEOUT) and lets the block run
+// on, so the kernel always finishes.
+// ---------------------------------------------------------------------------
+constexpr unsigned kTmaSpinLimit = 1u << 22;
+
+__device__ __forceinline__ unsigned smem_u32(const void *p) { return (unsigned)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void mbar_init(uint64_t *bar, unsigned count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_fence_init() { asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory"); }
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, unsigned bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+// generic-proxy accesses of a shared-memory region, ordered before an
+// async-proxy (TMA) write of it
+__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory"); }
+__device__ __forceinline__ void tma_load_3d(void *dst, const CUtensorMap *map, int x, int y, int z, uint64_t *bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];\n" ::"r"(
+            smem_u32(dst)),
+        "l"((unsigned long long)map), "r"(x), "r"(y), "r"(z), "r"(smem_u32(bar))
+        : "memory");
+}
+// wait for phase `phase` of *bar to complete, at most kTmaSpinLimit polls
+__device__ __forceinline__ void mbar_wait(uint64_t *bar, unsigned phase, int *err) {
+    const unsigned a = smem_u32(bar);
+    for (unsigned i = 0; i < kTmaSpinLimit; ++i) {
+        unsigned done;
+        asm volatile(
+            "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+            : "=r"(done)
+            : "r"(a), "r"(phase)
+            : "memory");
+        if (done) return;
+    }
+    if (err) atomicOr(err, 2);
+}
+// one real field's tile (TX x N2 cells at row y) into dst, [z][x] order
+template <int N2, int TX>
+__device__ __forceinline__ void tma_field(float2 *dst, const CUtensorMap *map, int zbox, int x0, int y, uint64_t *bar) {
+    mbar_expect_tx(bar, (unsigned)(TX * N2 * sizeof(float)));
+    for (int z = 0; z < N2; z += zbox) tma_load_3d(reinterpret_cast<float *>(dst) + z * TX, map, x0, y, z, bar);
+}
+// half-spectrum rows kz = 0 .. N2/2 of TX columns at row y into dst, [kz][x]
+template <int N2, int TX>
+__device__ __forceinline__ void tma_rows(float2 *dst, const CUtensorMap *map, int x0, int y, uint64_t *bar) {
+    mbar_expect_tx(bar, (unsigned)(TX * (N2 / 2 + 1) * sizeof(float2)));
+    tma_load_3d(dst, map, x0, y, 0, bar);
+}
+
 template <int N2, int PL_> struct ZStage {
     using ZT = ZTile<N2, PL_>;
     using SH = typename ZT::SH;
     static constexpr int PL = ZT::PL, TX = ZT::TX, NT = ZT::NT;
     // float2 of the transform tile; it also holds the raw half-spectrum rows of
-    // a prefetched input, (N2/2 + 1) rows of TX values
-    static constexpr int TILE = N2 * PL + 2 * PL;
+    // a prefetched input, (N2/2 + 1) rows of TX values.  Rounded up to 128
+    // bytes, so the slices after it can be TMA destinations (128-byte
+    // aligned shared-memory addresses).
+    static constexpr int TILE = (N2 * PL + 2 * PL + 15) / 16 * 16;
     static constexpr int SLICE = SH::MAXB * SH::R * NT;   // float2 of one staged field
     static __device__ __forceinline__ int sidx(int b, int t) { return (b * SH::R + t) * NT + threadIdx.x; }
 };
@@ -615,15 +676,22 @@ __global__ void __launch_bounds__(ks_threads(N2, PL), 2 * kThreads / ks_threads(
 // rho of every component is staged into shared memory at the start; the
 // nonlinear coefficient 2 sum(rho_old) + rho0 is formed from the staged values
 // during component 0 and kept in component 0's slice.
+// TMA: the staged fields and the spectrum rows are brought in by bulk tensor
+// copies that one thread issues (slices then hold cells in [z][x] order);
+// otherwise by per-thread cp.async into thread-private slots.
 // grid = (ceil(N0/TX), N1, 1); dynamic shared memory: tile + D staged fields.
 // ---------------------------------------------------------------------------
-template <int N2, int PL>
+template <int N2, int PL, bool TMA>
 __global__ void __launch_bounds__(ks_threads(N2, PL), 2 * kThreads / ks_threads(N2, PL))
-    ks_stage_r(StageR a, const float2 *__restrict__ tw) {
+    ks_stage_r(StageR a, const float2 *__restrict__ tw, const __grid_constant__ StageRMaps m) {
     using Z = ZStage<N2, PL>;
     using SH = typename Z::SH;
     constexpr int TX = Z::TX, NT = Z::NT;
-    extern __shared__ float2 dsm[];
+    extern __shared__ __align__(128) float2 dsm_raw[];
+    // TMA destinations must be 128-byte aligned: the dynamic shared memory
+    // carries 128 bytes of slack (ZStage launch size) for this
+    float2 *dsm = TMA ? reinterpret_cast<float2 *>(dsm_raw + ((128u - (smem_u32(dsm_raw) & 127u)) & 127u) / 8)
+                      : dsm_raw;
     float2 *sm = dsm;
     float2 *s_c = dsm + Z::TILE;        // staged mass coefficient (q or rho0)
     float2 *s_a = s_c + Z::SLICE;       // staged rho_old of the current component
@@ -632,13 +700,45 @@ __global__ void __launch_bounds__(ks_threads(N2, PL), 2 * kThreads / ks_threads(
     const int t = *a.d_t;
     const int D = a.D;
     const bool r0arr = a.rho0.arr != nullptr;
+    // TMA layout invariants: the tile and each slice are whole 128-byte
+    // units, a real-field box set fits a slice and the tile, the spectrum rows
+    // fit the tile, and every box row is a multiple of 16 bytes
+    static_assert(!TMA || ((Z::TILE * 8) % 128 == 0 && (Z::SLICE * 8) % 128 == 0 && TX * N2 / 2 <= Z::SLICE &&
+                           TX * N2 / 2 <= Z::TILE && TX * (N2 / 2 + 1) <= Z::TILE && (TX * 4) % 16 == 0),
+                  "TMA staging layout");
+    // slot of this thread's cell (l, z) in a staged slice
+    auto slot = [&](int b, int tt, int l, int z) -> int { return TMA ? z * PL + l : Z::sidx(b, tt); };
+    // TMA barriers: tile (spectrum rows, rho0), slice a, slice c; phases
+    __shared__ __align__(8) uint64_t bars[3];
+    unsigned ph_t = 0, ph_a = 0, ph_c = 0;
+    const bool lead = threadIdx.x == 0;
+    const bool coef_staged = a.nonlinear || r0arr;
     // mass coefficient: q = 2 sum(rho_old) + rho0, carried between steps
     // (nonlinear), or rho0 (linear)
-    if (a.nonlinear) stage_field<N2, PL>(s_c, a.srho, g, x0, y);
-    else if (r0arr) stage_field<N2, PL>(s_c, a.rho0.arr, g, x0, y);
-    stage_field<N2, PL>(s_a, a.rho[0], g, x0, y);
-    zraw_prefetch<N2, PL>(sm, a.spec.p[0], g, x0, y);
-    cp_async_commit();
+    if constexpr (TMA) {
+        // self-check of the alignment every TMA destination needs; a block
+        // that fails it records bit 2 of *err and returns without copying
+        __shared__ int misaligned;
+        if (lead) {
+            misaligned = ((smem_u32(sm) | smem_u32(s_c) | smem_u32(s_a)) & 127u) != 0;
+            if (misaligned && m.err) atomicOr(m.err, 4);
+            for (int k = 0; k < 3; ++k) mbar_init(&bars[k], 1);
+            mbar_fence_init();
+        }
+        __syncthreads();
+        if (misaligned) return;
+        if (lead) {
+            if (coef_staged) tma_field<N2, TX>(s_c, &m.coef, m.zbox, x0, y, &bars[2]);
+            tma_field<N2, TX>(s_a, &m.rho[0], m.zbox, x0, y, &bars[1]);
+            tma_rows<N2, TX>(sm, &m.spec[0], x0, y, &bars[0]);
+        }
+    } else {
+        if (a.nonlinear) stage_field<N2, PL>(s_c, a.srho, g, x0, y);
+        else if (r0arr) stage_field<N2, PL>(s_c, a.rho0.arr, g, x0, y);
+        stage_field<N2, PL>(s_a, a.rho[0], g, x0, y);
+        zraw_prefetch<N2, PL>(sm, a.spec.p[0], g, x0, y);
+        cp_async_commit();
+    }
     float dscale = 0.f;
     const bool dense = dense_active(a.dense, t, dscale);
     int e0 = 0, e1 = 0;
@@ -668,21 +768,49 @@ __global__ void __launch_bounds__(ks_threads(N2, PL), 2 * kThreads / ks_threads(
     // component's physics {c0, B/A} for the equation of state
     for (int i = 0; i < D; ++i) {
         float2 hold[SH::MAXB][SH::R];
-        if (i == 0) cp_async_wait_all();
-        else cp_async_wait_group<1>();   // rows_i landed; rho_i may be in flight
-        __syncthreads();                 // the prefetched rows of every thread are in the tile
+        if constexpr (TMA) {
+            mbar_wait(&bars[0], ph_t, m.err);   // rows_i in the tile
+            ph_t ^= 1;
+            if (i == 0 && coef_staged) {
+                mbar_wait(&bars[2], ph_c, m.err);
+                ph_c ^= 1;
+            }
+        } else {
+            if (i == 0) cp_async_wait_all();
+            else cp_async_wait_group<1>();   // rows_i landed; rho_i may be in flight
+            __syncthreads();                 // the prefetched rows of every thread are in the tile
+        }
         auto ld = [&](int, int, int l, int z) -> float2 { return zpack_raw<N2, PL>(sm, g, x0, l, z); };
         auto st = [&](int b, int tt, int, int, float2 v) { hold[b][tt] = v; };
         rs_fft<N2, PL, true, true, 0, NT>(sm, tw, ld, st);
-        cp_async_wait_all();             // staged rho_i (this thread's own slots)
+        if constexpr (TMA) {
+            mbar_wait(&bars[1], ph_a, m.err);   // rho_i in slice a
+            ph_a ^= 1;
+        } else {
+            cp_async_wait_all();             // staged rho_i (this thread's own slots)
+        }
         if (i + 1 < D) {
             __syncthreads();   // every thread has read the tile
-            zraw_prefetch<N2, PL>(sm, a.spec.p[i + 1], g, x0, y);
-            cp_async_commit();
+            if constexpr (TMA) {
+                if (lead) {
+                    fence_proxy_async();
+                    tma_rows<N2, TX>(sm, &m.spec[i + 1], x0, y, &bars[0]);
+                }
+            } else {
+                zraw_prefetch<N2, PL>(sm, a.spec.p[i + 1], g, x0, y);
+                cp_async_commit();
+            }
         } else if (r0_tile) {
             __syncthreads();   // every thread has read the tile
-            stage_field<N2, PL>(sm, a.rho0.arr, g, x0, y);
-            cp_async_commit();
+            if constexpr (TMA) {
+                if (lead) {
+                    fence_proxy_async();
+                    tma_field<N2, TX>(sm, &m.rho0, m.zbox, x0, y, &bars[0]);
+                }
+            } else {
+                stage_field<N2, PL>(sm, a.rho0.arr, g, x0, y);
+                cp_async_commit();
+            }
         }
         const int ax = a.comp_axis[i];
         const float *pmlv = a.pml[ax];
@@ -697,7 +825,7 @@ __global__ void __launch_bounds__(ks_threads(N2, PL), 2 * kThreads / ks_threads(
                 const int xa = x0 + 2 * l;
                 if (xa >= g.N0) continue;
                 const long long gi = xa + (long long)g.N0 * (y + (long long)g.N1 * z);
-                const int si = Z::sidx(b, tt);
+                const int si = slot(b, tt, l, z);
                 const float2 du = hold[b][tt];
                 const float2 ro = s_a[si];
                 const float2 coef = (a.nonlinear || r0arr) ? s_c[si] : make_float2(a.rho0.val, a.rho0.val);
@@ -719,17 +847,32 @@ __global__ void __launch_bounds__(ks_threads(N2, PL), 2 * kThreads / ks_threads(
                 acc_d[b][tt].x += du.x;
                 acc_d[b][tt].y += du.y;
             }
-        // every thread reads only its own slots, so the next component (or,
-        // after the last one, c0 for the equation of state) can be staged
-        // into the same slice right away
-        if (i + 1 < D) {
-            stage_field<N2, PL>(s_a, a.rho[i + 1], g, x0, y);
-            cp_async_commit();
+        // cp.async: every thread reads only its own slots, so the next
+        // component (or, after the last one, c0 for the equation of state) is
+        // staged into the same slice right away; TMA rewrites the whole slice,
+        // so it waits until every thread has read it
+        if constexpr (TMA) {
+            if (i + 1 < D || c0_staged || bona_staged) __syncthreads();
+            if (lead) {
+                fence_proxy_async();
+                if (i + 1 < D) {
+                    tma_field<N2, TX>(s_a, &m.rho[i + 1], m.zbox, x0, y, &bars[1]);
+                } else {
+                    if (c0_staged) tma_field<N2, TX>(s_a, &m.c0, m.zbox, x0, y, &bars[1]);
+                    // q is read by the mass updates only: its slice takes B/A
+                    if (bona_staged) tma_field<N2, TX>(s_c, &m.bona, m.zbox, x0, y, &bars[2]);
+                }
+            }
         } else {
-            if (c0_staged) stage_field<N2, PL>(s_a, a.c0.arr, g, x0, y);
-            // q is read by the mass updates only: its slice takes B/A
-            if (bona_staged) stage_field<N2, PL>(s_c, a.BonA.arr, g, x0, y);
-            cp_async_commit();
+            if (i + 1 < D) {
+                stage_field<N2, PL>(s_a, a.rho[i + 1], g, x0, y);
+                cp_async_commit();
+            } else {
+                if (c0_staged) stage_field<N2, PL>(s_a, a.c0.arr, g, x0, y);
+                // q is read by the mass updates only: its slice takes B/A
+                if (bona_staged) stage_field<N2, PL>(s_c, a.BonA.arr, g, x0, y);
+                cp_async_commit();
+            }
         }
     }
     // sparse pressure sources act on every rho component (:930-962)
@@ -758,7 +901,13 @@ __global__ void __launch_bounds__(ks_threads(N2, PL), 2 * kThreads / ks_threads(
     // equation of state (c0^2 applied to the non-spectral terms here; the
     // absorbing terms are finished in Stage P)
     const bool absorbing = a.eos == 1;
-    if (r0_tile || c0_staged || bona_staged) cp_async_wait_all();
+    if constexpr (TMA) {
+        if (r0_tile) mbar_wait(&bars[0], ph_t, m.err);
+        if (c0_staged) mbar_wait(&bars[1], ph_a, m.err);
+        if (bona_staged) mbar_wait(&bars[2], ph_c, m.err);
+    } else {
+        if (r0_tile || c0_staged || bona_staged) cp_async_wait_all();
+    }
     auto r0_at = [&](int si, long long gi) -> float2 {
         if (r0_tile) return sm[si];
         if (!a.nonlinear && r0arr) return s_c[si];
@@ -775,7 +924,7 @@ __global__ void __launch_bounds__(ks_threads(N2, PL), 2 * kThreads / ks_threads(
             float2 rd = make_float2(0.f, 0.f);
             if (xa < g.N0) {
                 const long long gi = xa + (long long)g.N0 * (y + (long long)g.N1 * z);
-                const int si = Z::sidx(b, tt);
+                const int si = slot(b, tt, l, z);
                 const float2 sr = acc_r[b][tt];
                 const float2 c = c0_staged ? s_a[si] : med2(a.c0, gi, true, true);
                 pv = sr;
@@ -824,7 +973,11 @@ __global__ void __launch_bounds__(ks_threads(N2, PL), 2 * kThreads / ks_threads(
 #pragma unroll
     for (int b = 0; b < SH::MAXB; ++b)
 #pragma unroll
-        for (int tt = 0; tt < SH::R; ++tt) s_a[Z::sidx(b, tt)] = acc_r[b][tt];
+        for (int tt = 0; tt < SH::R; ++tt) {
+            int l = 0, z = 0;
+            if (TMA && !hand_pos<N2, PL, true, NT>(b, tt, l, z)) continue;
+            s_a[slot(b, tt, l, z)] = acc_r[b][tt];
+        }
     int out = 0;
 #pragma unroll 1
     for (int term = 0; term < 2; ++term) {
@@ -833,7 +986,11 @@ __global__ void __launch_bounds__(ks_threads(N2, PL), 2 * kThreads / ks_threads(
 #pragma unroll
         for (int b = 0; b < SH::MAXB; ++b)
 #pragma unroll
-            for (int tt = 0; tt < SH::R; ++tt) src[b][tt] = term == 0 ? acc_d[b][tt] : s_a[Z::sidx(b, tt)];
+            for (int tt = 0; tt < SH::R; ++tt) {
+                int l = 0, z = 0;
+                if (TMA && !hand_pos<N2, PL, true, NT>(b, tt, l, z)) { src[b][tt] = make_float2(0.f, 0.f); continue; }
+                src[b][tt] = term == 0 ? acc_d[b][tt] : s_a[slot(b, tt, l, z)];
+            }
         zforward_store<N2, PL>(sm, tw, src, pick(a.spec.p, out++), g, x0, y);
     }
 }

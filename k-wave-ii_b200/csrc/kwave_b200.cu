@@ -21,6 +21,8 @@
 #include <mutex>
 #include <vector>
 
+#include <cudaTypedefs.h>
+
 #include "kw_plan.cuh"
 #include "kw_aux.cuh"
 #include "kw_static.cuh"
@@ -57,6 +59,78 @@ kw_status launched(kw_plan *P) {
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return fail(KW_ERR_CUDA, "kernel launch failed: %s", cudaGetErrorString(e));
     P->launches += 1;
+    return KW_OK;
+}
+
+}  // namespace kw
+
+namespace {
+
+// cuTensorMapEncodeTiled from the driver, through the runtime's entry-point
+// query (no link-time dependency on the driver library)
+PFN_cuTensorMapEncodeTiled_v12000 g_encode_tiled = nullptr;
+std::once_flag g_encode_once;
+bool have_encode_tiled() {
+    std::call_once(g_encode_once, [] {
+        void *fn = nullptr;
+        cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            g_encode_tiled = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+        cudaGetLastError();
+    });
+    return g_encode_tiled != nullptr;
+}
+
+// 3-D tensor map of a grid array of (d0, d1, d2) elements of `elem` bytes
+// (4: a real field, 8: a half spectrum), x fastest, box (b0, 1, b2)
+kw_status encode_map(CUtensorMap *m, const void *base, int elem, int d0, int d1, int d2, int b0, int b2) {
+    const cuuint64_t dims[3] = {(cuuint64_t)d0, (cuuint64_t)d1, (cuuint64_t)d2};
+    const cuuint64_t strides[2] = {(cuuint64_t)d0 * elem, (cuuint64_t)d0 * d1 * elem};
+    const cuuint32_t box[3] = {(cuuint32_t)b0, 1u, (cuuint32_t)b2};
+    const cuuint32_t es[3] = {1u, 1u, 1u};
+    const CUresult r = g_encode_tiled(m, elem == 4 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_UINT64, 3,
+                                      const_cast<void *>(base), dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                                      CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                                      CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) return fail(KW_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d)", (int)r);
+    return KW_OK;
+}
+
+}  // namespace
+
+namespace kw {
+
+kw_status stage_r_maps(kw_plan *P, const StageR &a, int TX, StageRMaps *m, bool *use) {
+    *use = P->tma_r;
+    if (!*use) return KW_OK;
+    const Geom &g = P->g;
+    const int zbox = g.N2 <= 256 ? g.N2 : g.N2 / 2;
+    // cached per (buffer, box width); buffers never move during a plan's life
+    auto map_of = [&](const void *ptr, int elem, CUtensorMap *dst) -> kw_status {
+        if (!ptr) return KW_OK;
+        const auto key = std::make_pair(ptr, TX * elem);
+        auto it = P->tmaps.find(key);
+        if (it == P->tmaps.end()) {
+            CUtensorMap t;
+            if (elem == 4) KW_TRY(encode_map(&t, ptr, 4, g.N0, g.N1, g.N2, TX, zbox));
+            else KW_TRY(encode_map(&t, ptr, 8, g.N0, g.N1, g.N2h, TX, g.N2h));
+            it = P->tmaps.emplace(key, t).first;
+        }
+        *dst = it->second;
+        return KW_OK;
+    };
+    std::memset(m, 0, sizeof(*m));
+    for (int i = 0; i < a.D; ++i) {
+        KW_TRY(map_of(a.rho[i], 4, &m->rho[i]));
+        KW_TRY(map_of(a.spec.p[i], 8, &m->spec[i]));
+    }
+    KW_TRY(map_of(a.nonlinear ? (const void *)a.srho : (const void *)a.rho0.arr, 4, &m->coef));
+    KW_TRY(map_of(a.rho0.arr, 4, &m->rho0));
+    KW_TRY(map_of(a.c0.arr, 4, &m->c0));
+    KW_TRY(map_of(a.nonlinear ? a.BonA.arr : nullptr, 4, &m->bona));
+    m->zbox = zbox;
+    m->err = P->d_err;
     return KW_OK;
 }
 
@@ -1138,6 +1212,14 @@ kw_status create(const kw_problem *pr, kw_plan *P) {
     if (g.N2 > kCap / 2) return fail(KW_ERR_UNSUPPORTED, "axis length %d above %d", g.N2, kCap / 2);
     const size_t N = (size_t)g.N, Nh = (size_t)g.Nh;
     KW_TRY(palloc(P, &P->d_t, 1));
+    KW_TRY(palloc(P, &P->d_err, 1));
+    // stage R stages its fields with TMA when the boxes fit the rules: FP32
+    // rows of 16-byte multiples (N0 % 4), at most 256 rows of half spectrum
+    // (N2 <= 384); KW_TMA=0 keeps the cp.async path
+    {
+        const char *e = getenv("KW_TMA");
+        P->tma_r = P->static_z && g.N2 <= 384 && g.N0 % 4 == 0 && !(e && atoi(e) == 0) && have_encode_tiled();
+    }
     KW_TRY(palloc(P, &P->p, N));
     for (int i = 0; i < P->D; ++i) {
         KW_TRY(palloc(P, &P->rho[i], N));
@@ -1566,6 +1648,21 @@ kw_status run_streamed(kw_plan *P, const std::vector<SeriesOut> &ser) {
     return st;
 }
 
+// The device error word: bit 1, a TMA-staged copy of stage R did not land
+// within its poll limit (KW_ERR_TIMEOUT); bit 2, a TMA destination was not
+// 128-byte aligned and the block skipped its work (KW_ERR_CUDA).  The word is
+// cleared for the next call.
+kw_status check_dev_err(kw_plan *P) {
+    if (!P->d_err) return KW_OK;
+    int e = 0;
+    KW_CUDA(cudaMemcpyAsync(&e, P->d_err, sizeof(int), cudaMemcpyDeviceToHost, P->stream));
+    KW_CUDA(cudaStreamSynchronize(P->stream));
+    if (e == 0) return KW_OK;
+    cudaMemsetAsync(P->d_err, 0, sizeof(int), P->stream);
+    if (e & 4) return fail(KW_ERR_CUDA, "internal: a TMA staging buffer was misaligned (device error word %d)", e);
+    return fail(KW_ERR_TIMEOUT, "a staged tensor copy did not complete within its wait limit (device error word %d)", e);
+}
+
 // StreamToDisk (kspaceFirstOrder3D.m:1101-1146, 1235-1295): the loop runs in
 // chunks of stream_cols recorded steps; after each chunk the ring of p
 // columns is copied to pinned host memory and appended to the file (FP32,
@@ -1752,7 +1849,7 @@ kw_status kw_step(kw_plan *P, uint64_t n) {
     KW_TRY(use_device(P));
     KW_TRY(run_steps(P, n));
     KW_CUDA(cudaStreamSynchronize(P->stream));
-    return KW_OK;
+    return check_dev_err(P);
 }
 
 kw_status kw_run_device(kw_plan *P) {
@@ -1761,7 +1858,7 @@ kw_status kw_run_device(kw_plan *P) {
     if (P->t != 1 || P->started) KW_TRY(zero_state(P));
     KW_TRY(run_steps(P, (uint64_t)P->index_end));
     KW_CUDA(cudaStreamSynchronize(P->stream));
-    return KW_OK;
+    return check_dev_err(P);
 }
 
 kw_status kw_copy_outputs(kw_plan *P, kw_outputs *o) {
@@ -1794,7 +1891,10 @@ kw_status kw_copy_outputs(kw_plan *P, kw_outputs *o) {
 kw_status kw_run(kw_plan *P, kw_outputs *o) {
     if (!P || !o) return fail(KW_ERR_INVALID, "NULL argument");
     KW_TRY(use_device(P));
-    if (P->stream_cols) return run_to_disk(P, o);
+    if (P->stream_cols) {
+        KW_TRY(run_to_disk(P, o));
+        return check_dev_err(P);
+    }
     // time series large enough to be worth streaming to the host during the loop
     std::vector<SeriesOut> ser;
     if (!P->time_rev && P->M > 0) {
@@ -1824,6 +1924,7 @@ kw_status kw_run(kw_plan *P, kw_outputs *o) {
     if (P->t != 1 || P->started) KW_TRY(zero_state(P));
     KW_TRY(run_streamed(P, ser));
     KW_CUDA(cudaStreamSynchronize(P->stream));
+    KW_TRY(check_dev_err(P));
     // the remaining (non-series) outputs after the loop
     kw_outputs rest = *o;
     rest.p = nullptr;
@@ -1897,7 +1998,7 @@ kw_status kw_run_timed(kw_plan *P, uint32_t n, double *device_ms) {
     KW_TRY(st);
     KW_CUDA(cudaGetLastError());
     *device_ms = ms;
-    return KW_OK;
+    return check_dev_err(P);
 }
 
 kw_status kw_launch_count(const kw_plan *P, uint64_t *launches) {
