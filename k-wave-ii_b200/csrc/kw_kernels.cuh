@@ -535,6 +535,26 @@ struct StageR {
     const int *d_t;
 };
 
+// Tensor maps of one stage U launch with TMA staging (component f = the
+// block's z index): the current velocity, 1 / rho_sg and the spectrum of
+// each component.
+struct StageUMaps {
+    CUtensorMap u[3];
+    CUtensorMap rsi[3];
+    CUtensorMap spec[3];
+    int zbox;
+    int *err;
+};
+
+// Tensor maps of one stage P launch with TMA staging: the term weights
+// (c0^2 tau, c0^2 eta), p and the terms' spectra.
+struct StagePMaps {
+    CUtensorMap w0, w1, p;
+    CUtensorMap spec[2];
+    int zbox;
+    int *err;
+};
+
 // Tensor maps of one stage R launch with TMA staging, filled per launch by
 // the host (rho[] name the current input buffers).  Real fields: 3-D FP32
 // maps of (N0, N1, N2) with a (TX, 1, zbox) box; spectra: 3-D 8-byte maps

@@ -47,8 +47,19 @@ template <int N, int PL>
 kw_status stage_u(kw_plan *P, const StageU &a, dim3 grid) {
     using Z = ZStage<N, PL>;
     const size_t sh = (size_t)(Z::TILE + 2 * Z::SLICE) * sizeof(float2);
-    KW_TRY(set_smem((const void *)ks_stage_u<N, PL>, sh));
-    ks_stage_u<N, PL><<<grid, Z::NT, sh, P->stream>>>(a, P->tw[2]);
+    StageUMaps m;
+    bool tma = false;
+    KW_TRY(stage_u_maps(P, a, Z::TX, &m, &tma));
+    if constexpr (N <= 384) {
+        if (tma) {
+            // 128 bytes of slack for the kernel to align its TMA destinations
+            KW_TRY(set_smem((const void *)ks_stage_u<N, PL, true>, sh + 128));
+            ks_stage_u<N, PL, true><<<grid, Z::NT, sh + 128, P->stream>>>(a, P->tw[2], m);
+            return KW_OK;
+        }
+    }
+    KW_TRY(set_smem((const void *)ks_stage_u<N, PL, false>, sh));
+    ks_stage_u<N, PL, false><<<grid, Z::NT, sh, P->stream>>>(a, P->tw[2], m);
     return KW_OK;
 }
 
@@ -80,8 +91,19 @@ template <int N, int PL>
 kw_status stage_p(kw_plan *P, const StageP &a, dim3 grid) {
     using Z = ZStage<N, PL>;
     const size_t sh = (size_t)(Z::TILE + 2 * Z::SLICE) * sizeof(float2);
-    KW_TRY(set_smem((const void *)ks_stage_p<N, PL>, sh));
-    ks_stage_p<N, PL><<<grid, Z::NT, sh, P->stream>>>(a, P->tw[2]);
+    StagePMaps m;
+    bool tma = false;
+    KW_TRY(stage_p_maps(P, a, Z::TX, &m, &tma));
+    if constexpr (N <= 384) {
+        if (tma) {
+            // 128 bytes of slack for the kernel to align its TMA destinations
+            KW_TRY(set_smem((const void *)ks_stage_p<N, PL, true>, sh + 128));
+            ks_stage_p<N, PL, true><<<grid, Z::NT, sh + 128, P->stream>>>(a, P->tw[2], m);
+            return KW_OK;
+        }
+    }
+    KW_TRY(set_smem((const void *)ks_stage_p<N, PL, false>, sh));
+    ks_stage_p<N, PL, false><<<grid, Z::NT, sh, P->stream>>>(a, P->tw[2], m);
     return KW_OK;
 }
 

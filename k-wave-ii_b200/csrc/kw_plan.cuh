@@ -172,6 +172,8 @@ kw_status set_smem(const void *fn, size_t bytes);
 // tensor maps of a stage R launch with tile width TX; *use is false when
 // the plan stages with cp.async instead
 kw_status stage_r_maps(kw_plan *P, const StageR &a, int TX, StageRMaps *m, bool *use);
+kw_status stage_u_maps(kw_plan *P, const StageU &a, int TX, StageUMaps *m, bool *use);
+kw_status stage_p_maps(kw_plan *P, const StageP &a, int TX, StagePMaps *m, bool *use);
 // check the last launch and count it in the plan
 kw_status launched(kw_plan *P);
 

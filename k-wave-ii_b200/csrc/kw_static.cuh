@@ -568,14 +568,20 @@ __device__ __forceinline__ float2 zpack_raw(const float2 *raw, const Geom &g, in
 // u is double-buffered (read a.u, write a.u_out).  grid = (ceil(N0/TX), N1, D);
 // dynamic shared memory: tile + 2 staged fields.
 // ---------------------------------------------------------------------------
-template <int N2, int PL>
+template <int N2, int PL, bool TMA>
 __global__ void __launch_bounds__(ks_threads(N2, PL), 2 * kThreads / ks_threads(N2, PL))
-    ks_stage_u(StageU a, const float2 *__restrict__ tw) {
+    ks_stage_u(StageU a, const float2 *__restrict__ tw, const __grid_constant__ StageUMaps m) {
     using Z = ZStage<N2, PL>;
     using SH = typename Z::SH;
     constexpr int TX = Z::TX, NT = Z::NT;
     static_assert(RPlan<N2, false>::M >= 2, "z-stages need two stages");
-    extern __shared__ float2 dsm[];
+    static_assert(!TMA || ((Z::TILE * 8) % 128 == 0 && (Z::SLICE * 8) % 128 == 0 && TX * N2 / 2 <= Z::SLICE &&
+                           TX * (N2 / 2 + 1) <= Z::TILE && (TX * 4) % 16 == 0),
+                  "TMA staging layout");
+    extern __shared__ __align__(128) float2 dsm_raw[];
+    // TMA destinations must be 128-byte aligned (128 bytes of launch slack)
+    float2 *dsm = TMA ? reinterpret_cast<float2 *>(dsm_raw + ((128u - (smem_u32(dsm_raw) & 127u)) & 127u) / 8)
+                      : dsm_raw;
     float2 *sm = dsm;
     float2 *s_u = dsm + Z::TILE;
     float2 *s_r = s_u + Z::SLICE;
@@ -588,29 +594,66 @@ __global__ void __launch_bounds__(ks_threads(N2, PL), 2 * kThreads / ks_threads(
     const float *pmlv = a.pml_sg[ax];
     const float2 *H = a.spec.p[f];
     const Med rsi = a.rho_sg_inv[f];
-
-    // the first transform stage's inputs are loaded before the per-cell
-    // staging is issued, so they are not queued behind it
-    using S0 = StageShape<N2, PL, true, 0, NT>;
-    float2 in0[S0::MAXB][S0::R];
-#pragma unroll
-    for (int b = 0; b < S0::MAXB; ++b) {
-        const int gg = threadIdx.x + b * NT;
-        if (!(S0::TOT % NT == 0 || gg < S0::TOT)) continue;
-        int l, j;
-        bmap<S0::NB, PL, true>(gg, l, j);
-#pragma unroll
-        for (int tt = 0; tt < S0::R; ++tt) in0[b][tt] = zpack_load<N2>(H, g, x0, y, l, j + tt * S0::NB);
-    }
-    if (!a.init) stage_field<N2, PL>(s_u, a.u[f], g, x0, y);
-    if (rsi.arr) stage_field<N2, PL>(s_r, rsi.arr, g, x0, y);
-    cp_async_commit();
+    auto slot = [&](int b, int tt, int l, int z) -> int { return TMA ? z * PL + l : Z::sidx(b, tt); };
 
     float2 hold[SH::MAXB][SH::R];
-    auto ld = [&](int b, int tt, int, int) -> float2 { return in0[b][tt]; };
-    auto st = [&](int b, int tt, int, int, float2 v) { hold[b][tt] = v; };
-    rs_fft<N2, PL, true, true, 0, NT>(sm, tw, ld, st);
-    cp_async_wait_all();
+    if constexpr (TMA) {
+        // spectrum rows into the tile, old u and 1/rho_sg into their slices:
+        // three bulk copies issued by one thread; the transform reads the rows
+        // from shared memory.  A block whose destinations fail the 128-byte
+        // alignment self-check records bit 2 of *err and returns.
+        __shared__ __align__(8) uint64_t bars[2];
+        __shared__ int misaligned;
+        const bool lead = threadIdx.x == 0;
+        if (lead) {
+            misaligned = ((smem_u32(sm) | smem_u32(s_u) | smem_u32(s_r)) & 127u) != 0;
+            if (misaligned && m.err) atomicOr(m.err, 4);
+            mbar_init(&bars[0], 1);
+            mbar_init(&bars[1], 1);
+            mbar_fence_init();
+        }
+        __syncthreads();
+        if (misaligned) return;
+        const bool any_field = !a.init || rsi.arr;
+        if (lead) {
+            tma_rows<N2, TX>(sm, &m.spec[0] + f, x0, y, &bars[0]);
+            if (any_field) {
+                // one barrier for both slices: their bytes are expected together
+                const unsigned bytes = (unsigned)(TX * N2 * sizeof(float)) * ((!a.init ? 1u : 0u) + (rsi.arr ? 1u : 0u));
+                mbar_expect_tx(&bars[1], bytes);
+                for (int z = 0; z < N2; z += m.zbox) {
+                    if (!a.init) tma_load_3d(reinterpret_cast<float *>(s_u) + z * TX, &m.u[0] + f, x0, y, z, &bars[1]);
+                    if (rsi.arr) tma_load_3d(reinterpret_cast<float *>(s_r) + z * TX, &m.rsi[0] + f, x0, y, z, &bars[1]);
+                }
+            }
+        }
+        mbar_wait(&bars[0], 0, m.err);
+        auto ld = [&](int, int, int l, int z) -> float2 { return zpack_raw<N2, PL>(sm, g, x0, l, z); };
+        auto st = [&](int b, int tt, int, int, float2 v) { hold[b][tt] = v; };
+        rs_fft<N2, PL, true, true, 0, NT>(sm, tw, ld, st);
+        if (any_field) mbar_wait(&bars[1], 0, m.err);
+    } else {
+        // the first transform stage's inputs are loaded before the per-cell
+        // staging is issued, so they are not queued behind it
+        using S0 = StageShape<N2, PL, true, 0, NT>;
+        float2 in0[S0::MAXB][S0::R];
+#pragma unroll
+        for (int b = 0; b < S0::MAXB; ++b) {
+            const int gg = threadIdx.x + b * NT;
+            if (!(S0::TOT % NT == 0 || gg < S0::TOT)) continue;
+            int l, j;
+            bmap<S0::NB, PL, true>(gg, l, j);
+#pragma unroll
+            for (int tt = 0; tt < S0::R; ++tt) in0[b][tt] = zpack_load<N2>(H, g, x0, y, l, j + tt * S0::NB);
+        }
+        if (!a.init) stage_field<N2, PL>(s_u, a.u[f], g, x0, y);
+        if (rsi.arr) stage_field<N2, PL>(s_r, rsi.arr, g, x0, y);
+        cp_async_commit();
+        auto ld = [&](int b, int tt, int, int) -> float2 { return in0[b][tt]; };
+        auto st = [&](int b, int tt, int, int, float2 v) { hold[b][tt] = v; };
+        rs_fft<N2, PL, true, true, 0, NT>(sm, tw, ld, st);
+        cp_async_wait_all();
+    }
 
     float dscale = 0.f;
     const bool dense = dense_active(a.dense[f], t, dscale);
@@ -625,7 +668,7 @@ __global__ void __launch_bounds__(ks_threads(N2, PL), 2 * kThreads / ks_threads(
             if (xa >= g.N0) { hold[b][tt] = make_float2(0.f, 0.f); continue; }
             const long long gi = xa + (long long)g.N0 * (y + (long long)g.N1 * z);
             const float2 gr = hold[b][tt];
-            const float2 ri = rsi.arr ? s_r[Z::sidx(b, tt)] : make_float2(rsi.val, rsi.val);
+            const float2 ri = rsi.arr ? s_r[slot(b, tt, l, z)] : make_float2(rsi.val, rsi.val);
             float2 un;
             if (a.init) {
                 un = make_float2(0.5f * a.dt * ri.x * gr.x, 0.5f * a.dt * ri.y * gr.y);
@@ -634,7 +677,7 @@ __global__ void __launch_bounds__(ks_threads(N2, PL), 2 * kThreads / ks_threads(
                 if (ax == 0) pm = make_float2(__ldg(pmlv + xa), __ldg(pmlv + xa + 1));
                 else if (ax == 1) pm = make_float2(pml_y, pml_y);
                 else { const float q = __ldg(pmlv + z); pm = make_float2(q, q); }
-                const float2 uo = s_u[Z::sidx(b, tt)];
+                const float2 uo = s_u[slot(b, tt, l, z)];
                 un.x = pm.x * (pm.x * uo.x - a.dt * ri.x * gr.x);
                 un.y = pm.y * (pm.y * uo.y - a.dt * ri.y * gr.y);
                 if (dense) {
@@ -998,18 +1041,30 @@ __global__ void __launch_bounds__(ks_threads(N2, PL), 2 * kThreads / ks_threads(
 // ---------------------------------------------------------------------------
 // Stage P: p = p_partial + c0^2 tau A1 - c0^2 eta A2, time reversal, forward z of p.
 // ---------------------------------------------------------------------------
-template <int N2, int PL>
+template <int N2, int PL, bool TMA>
 __global__ void __launch_bounds__(ks_threads(N2, PL), 2 * kThreads / ks_threads(N2, PL))
-    ks_stage_p(StageP a, const float2 *__restrict__ tw) {
+    ks_stage_p(StageP a, const float2 *__restrict__ tw, const __grid_constant__ StagePMaps m) {
     using Z = ZStage<N2, PL>;
     using SH = typename Z::SH;
     constexpr int TX = Z::TX, NT = Z::NT;
-    extern __shared__ float2 dsm[];
+    static_assert(!TMA || ((Z::TILE * 8) % 128 == 0 && (Z::SLICE * 8) % 128 == 0 && TX * N2 / 2 <= Z::SLICE &&
+                           TX * (N2 / 2 + 1) <= Z::TILE && (TX * 4) % 16 == 0),
+                  "TMA staging layout");
+    extern __shared__ __align__(128) float2 dsm_raw[];
+    // TMA destinations must be 128-byte aligned (128 bytes of launch slack)
+    float2 *dsm = TMA ? reinterpret_cast<float2 *>(dsm_raw + ((128u - (smem_u32(dsm_raw) & 127u)) & 127u) / 8)
+                      : dsm_raw;
     float2 *sm = dsm;
     float2 *const s_w0 = dsm + Z::TILE, *const s_w1 = dsm + Z::TILE + Z::SLICE;
     const Geom &g = a.g;
     const int x0 = blockIdx.x * TX, y = blockIdx.y;
     const int t = *a.d_t;
+    auto slot = [&](int b, int tt, int l, int z) -> int { return TMA ? z * PL + l : Z::sidx(b, tt); };
+    // TMA barriers: tile rows, slice 0, slice 1, and their phases
+    __shared__ __align__(8) uint64_t bars[3];
+    __shared__ int misaligned;
+    unsigned ph_t = 0, ph_0 = 0, ph_1 = 0;
+    const bool lead = threadIdx.x == 0;
     // the terms' spectra are spec[0 .. nterm-1]; term k's per-cell weight
     // (c0^2 tau or c0^2 eta) is staged into slice k at the start, its rows
     // are prefetched into the tile while term k-1 is applied, and p is staged
@@ -1018,12 +1073,31 @@ __global__ void __launch_bounds__(ks_threads(N2, PL), 2 * kThreads / ks_threads(
     // s_w1 (selects, not arrays, so nothing is indexed at run time)
     const int nterm = (a.has_tau ? 1 : 0) + (a.has_eta ? 1 : 0);
     const Med w0 = a.has_tau ? a.c2tau : a.c2eta, w1 = a.c2eta;
-    if (nterm > 0 && w0.arr) stage_field<N2, PL>(s_w0, w0.arr, g, x0, y);
-    if (nterm > 1 && w1.arr) stage_field<N2, PL>(s_w1, w1.arr, g, x0, y);
     float2 *s_p = nterm == 2 ? s_w0 : s_w1;
-    if (nterm < 2) stage_field<N2, PL>(s_p, a.p, g, x0, y);
-    if (nterm > 0) zraw_prefetch<N2, PL>(sm, a.spec.p[0], g, x0, y);
-    cp_async_commit();
+    if constexpr (TMA) {
+        // a block whose destinations fail the 128-byte alignment self-check
+        // records bit 2 of *err and returns
+        if (lead) {
+            misaligned = ((smem_u32(sm) | smem_u32(s_w0) | smem_u32(s_w1)) & 127u) != 0;
+            if (misaligned && m.err) atomicOr(m.err, 4);
+            for (int k = 0; k < 3; ++k) mbar_init(&bars[k], 1);
+            mbar_fence_init();
+        }
+        __syncthreads();
+        if (misaligned) return;
+        if (lead) {
+            if (nterm > 0 && w0.arr) tma_field<N2, TX>(s_w0, &m.w0, m.zbox, x0, y, &bars[1]);
+            if (nterm > 1 && w1.arr) tma_field<N2, TX>(s_w1, &m.w1, m.zbox, x0, y, &bars[2]);
+            if (nterm < 2) tma_field<N2, TX>(s_p, &m.p, m.zbox, x0, y, &bars[2]);
+            if (nterm > 0) tma_rows<N2, TX>(sm, &m.spec[0], x0, y, &bars[0]);
+        }
+    } else {
+        if (nterm > 0 && w0.arr) stage_field<N2, PL>(s_w0, w0.arr, g, x0, y);
+        if (nterm > 1 && w1.arr) stage_field<N2, PL>(s_w1, w1.arr, g, x0, y);
+        if (nterm < 2) stage_field<N2, PL>(s_p, a.p, g, x0, y);
+        if (nterm > 0) zraw_prefetch<N2, PL>(sm, a.spec.p[0], g, x0, y);
+        cp_async_commit();
+    }
     float2 acc[SH::MAXB][SH::R];
 #pragma unroll
     for (int b = 0; b < SH::MAXB; ++b)
@@ -1035,16 +1109,33 @@ __global__ void __launch_bounds__(ks_threads(N2, PL), 2 * kThreads / ks_threads(
     for (int k = 0; k < nterm; ++k) {
         const int term = (k == 0 && a.has_tau) ? 0 : 1;
         float2 hold[SH::MAXB][SH::R];
-        if (k == 0) cp_async_wait_all();
-        else cp_async_wait_group<1>();   // rows_1 landed; p may be in flight
-        __syncthreads();                 // the prefetched rows of every thread are in the tile
+        if constexpr (TMA) {
+            mbar_wait(&bars[0], ph_t, m.err);   // rows_k in the tile
+            ph_t ^= 1;
+        } else {
+            if (k == 0) cp_async_wait_all();
+            else cp_async_wait_group<1>();   // rows_1 landed; p may be in flight
+            __syncthreads();                 // the prefetched rows of every thread are in the tile
+        }
         auto ld = [&](int, int, int l, int z) -> float2 { return zpack_raw<N2, PL>(sm, g, x0, l, z); };
         auto st = [&](int b, int tt, int, int, float2 v) { hold[b][tt] = v; };
         rs_fft<N2, PL, true, true, 0, NT>(sm, tw, ld, st);
         if (k + 1 < nterm) {
             __syncthreads();   // every thread has read the tile
-            zraw_prefetch<N2, PL>(sm, a.spec.p[k + 1], g, x0, y);
-            cp_async_commit();
+            if constexpr (TMA) {
+                if (lead) {
+                    fence_proxy_async();
+                    tma_rows<N2, TX>(sm, &m.spec[1], x0, y, &bars[0]);
+                }
+            } else {
+                zraw_prefetch<N2, PL>(sm, a.spec.p[k + 1], g, x0, y);
+                cp_async_commit();
+            }
+        }
+        if constexpr (TMA) {
+            // term k's weights in slice k
+            if (k == 0 && w0.arr) { mbar_wait(&bars[1], ph_0, m.err); ph_0 ^= 1; }
+            if (k == 1 && w1.arr) { mbar_wait(&bars[2], ph_1, m.err); ph_1 ^= 1; }
         }
         const Med w = k == 0 ? w0 : w1;
         const float2 *sw = k == 0 ? s_w0 : s_w1;
@@ -1057,17 +1148,31 @@ __global__ void __launch_bounds__(ks_threads(N2, PL), 2 * kThreads / ks_threads(
                 if (!hand_pos<N2, PL, true, NT>(b, tt, l, z)) continue;
                 const int xa = x0 + 2 * l;
                 if (xa >= g.N0) continue;
-                const float2 wv = w.arr ? sw[Z::sidx(b, tt)] : make_float2(w.val, w.val);
+                const float2 wv = w.arr ? sw[slot(b, tt, l, z)] : make_float2(w.val, w.val);
                 acc[b][tt].x = fmaf(sg * wv.x, hold[b][tt].x, acc[b][tt].x);
                 acc[b][tt].y = fmaf(sg * wv.y, hold[b][tt].y, acc[b][tt].y);
             }
         if (k == 0 && nterm == 2) {
-            // slice 0's weights are consumed (this thread's own slots): p goes there
-            stage_field<N2, PL>(s_p, a.p, g, x0, y);
-            cp_async_commit();
+            if constexpr (TMA) {
+                // slice 0's weights are consumed by every thread: p goes there
+                __syncthreads();
+                if (lead) {
+                    fence_proxy_async();
+                    tma_field<N2, TX>(s_p, &m.p, m.zbox, x0, y, &bars[1]);
+                }
+            } else {
+                // slice 0's weights are consumed (this thread's own slots): p goes there
+                stage_field<N2, PL>(s_p, a.p, g, x0, y);
+                cp_async_commit();
+            }
         }
     }
-    cp_async_wait_all();
+    if constexpr (TMA) {
+        if (nterm == 2) mbar_wait(&bars[1], ph_0, m.err);
+        else mbar_wait(&bars[2], ph_1, m.err);
+    } else {
+        cp_async_wait_all();
+    }
 #pragma unroll
     for (int b = 0; b < SH::MAXB; ++b)
 #pragma unroll
@@ -1078,7 +1183,7 @@ __global__ void __launch_bounds__(ks_threads(N2, PL), 2 * kThreads / ks_threads(
             float2 pv = make_float2(0.f, 0.f);
             if (xa < g.N0) {
                 const long long gi = xa + (long long)g.N0 * (y + (long long)g.N1 * z);
-                const float2 pp = s_p[Z::sidx(b, tt)];
+                const float2 pp = s_p[slot(b, tt, l, z)];
                 pv.x = pp.x + acc[b][tt].x;
                 pv.y = pp.y + acc[b][tt].y;
                 *reinterpret_cast<float2 *>(a.p + gi) = pv;

@@ -101,25 +101,59 @@ kw_status encode_map(CUtensorMap *m, const void *base, int elem, int d0, int d1,
 
 namespace kw {
 
+// tensor map of a plan buffer (elem 4: a real field, 8: a half spectrum) for
+// tiles TX wide, cached per (buffer, box width); buffers never move during a
+// plan's life
+kw_status plan_map(kw_plan *P, const void *ptr, int elem, int TX, CUtensorMap *dst) {
+    if (!ptr) return KW_OK;
+    const Geom &g = P->g;
+    const auto key = std::make_pair(ptr, TX * elem);
+    auto it = P->tmaps.find(key);
+    if (it == P->tmaps.end()) {
+        CUtensorMap t;
+        if (elem == 4) KW_TRY(encode_map(&t, ptr, 4, g.N0, g.N1, g.N2, TX, g.N2 <= 256 ? g.N2 : g.N2 / 2));
+        else KW_TRY(encode_map(&t, ptr, 8, g.N0, g.N1, g.N2h, TX, g.N2h));
+        it = P->tmaps.emplace(key, t).first;
+    }
+    *dst = it->second;
+    return KW_OK;
+}
+
+kw_status stage_u_maps(kw_plan *P, const StageU &a, int TX, StageUMaps *m, bool *use) {
+    *use = P->tma_r;
+    if (!*use) return KW_OK;
+    std::memset(m, 0, sizeof(*m));
+    for (int i = 0; i < P->D; ++i) {
+        KW_TRY(plan_map(P, a.u[i], 4, TX, &m->u[i]));
+        KW_TRY(plan_map(P, a.rho_sg_inv[i].arr, 4, TX, &m->rsi[i]));
+        KW_TRY(plan_map(P, a.spec.p[i], 8, TX, &m->spec[i]));
+    }
+    m->zbox = P->g.N2 <= 256 ? P->g.N2 : P->g.N2 / 2;
+    m->err = P->d_err;
+    return KW_OK;
+}
+
+kw_status stage_p_maps(kw_plan *P, const StageP &a, int TX, StagePMaps *m, bool *use) {
+    *use = P->tma_r;
+    if (!*use) return KW_OK;
+    std::memset(m, 0, sizeof(*m));
+    const int nterm = (a.has_tau ? 1 : 0) + (a.has_eta ? 1 : 0);
+    const Med w0 = a.has_tau ? a.c2tau : a.c2eta;
+    KW_TRY(plan_map(P, nterm > 0 ? w0.arr : nullptr, 4, TX, &m->w0));
+    KW_TRY(plan_map(P, nterm > 1 ? a.c2eta.arr : nullptr, 4, TX, &m->w1));
+    KW_TRY(plan_map(P, a.p, 4, TX, &m->p));
+    for (int k = 0; k < nterm && k < 2; ++k) KW_TRY(plan_map(P, a.spec.p[k], 8, TX, &m->spec[k]));
+    m->zbox = P->g.N2 <= 256 ? P->g.N2 : P->g.N2 / 2;
+    m->err = P->d_err;
+    return KW_OK;
+}
+
 kw_status stage_r_maps(kw_plan *P, const StageR &a, int TX, StageRMaps *m, bool *use) {
     *use = P->tma_r;
     if (!*use) return KW_OK;
     const Geom &g = P->g;
     const int zbox = g.N2 <= 256 ? g.N2 : g.N2 / 2;
-    // cached per (buffer, box width); buffers never move during a plan's life
-    auto map_of = [&](const void *ptr, int elem, CUtensorMap *dst) -> kw_status {
-        if (!ptr) return KW_OK;
-        const auto key = std::make_pair(ptr, TX * elem);
-        auto it = P->tmaps.find(key);
-        if (it == P->tmaps.end()) {
-            CUtensorMap t;
-            if (elem == 4) KW_TRY(encode_map(&t, ptr, 4, g.N0, g.N1, g.N2, TX, zbox));
-            else KW_TRY(encode_map(&t, ptr, 8, g.N0, g.N1, g.N2h, TX, g.N2h));
-            it = P->tmaps.emplace(key, t).first;
-        }
-        *dst = it->second;
-        return KW_OK;
-    };
+    auto map_of = [&](const void *ptr, int elem, CUtensorMap *dst) -> kw_status { return plan_map(P, ptr, elem, TX, dst); };
     std::memset(m, 0, sizeof(*m));
     for (int i = 0; i < a.D; ++i) {
         KW_TRY(map_of(a.rho[i], 4, &m->rho[i]));
