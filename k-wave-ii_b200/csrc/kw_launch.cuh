@@ -27,6 +27,15 @@ kw_status ypass(kw_plan *P, bool inv, Spec4 bufs, dim3 grid, int kz0) {
     return KW_OK;
 }
 
+template <int N, int TY>
+kw_status ypass_fan(kw_plan *P, Spec4 bufs, dim3 grid, int kz0, const float2 *ddy, const float2 *ddz) {
+    constexpr int NT = ks_threads(N, TY);
+    constexpr size_t sh = (size_t)N * TY * sizeof(float2);
+    KW_TRY(set_smem((const void *)ks_ypass_fan<N, TY>, sh));
+    ks_ypass_fan<N, TY><<<grid, NT, sh, P->stream>>>(bufs, P->g, P->tw[1], kz0, ddy, ddz);
+    return KW_OK;
+}
+
 template <int N, int PL>
 kw_status zr2c(kw_plan *P, const float *R, float2 *H, dim3 grid) {
     constexpr size_t sh = (size_t)N * PL * sizeof(float2);
@@ -127,6 +136,19 @@ kw_status YLaunch<N>::run(kw_plan *P, bool inv, Spec4 bufs, int nf, int kz0, int
         }
     }
     return launched(P);
+}
+
+template <int N>
+kw_status YLaunch<N>::run_fan(kw_plan *P, Spec4 bufs, int kz0, int nkz, const float2 *ddy, const float2 *ddz) {
+    if constexpr (N > 0) {
+        dim3 grid((P->g.N0 + P->TY - 1) / P->TY, nkz, 2);
+        if (P->TY == ks_lines(N)) KW_TRY((launch::ypass_fan<N, ks_lines(N)>(P, bufs, grid, kz0, ddy, ddz)));
+        else if (P->TY == ks_half(N)) KW_TRY((launch::ypass_fan<N, ks_half(N)>(P, bufs, grid, kz0, ddy, ddz)));
+        else KW_TRY((launch::ypass_fan<N, ks_narrow(N)>(P, bufs, grid, kz0, ddy, ddz)));
+        return launched(P);
+    } else {
+        return fail(KW_ERR_INVALID, "internal: the gradient fan-out y-pass needs a compile-time axis length");
+    }
 }
 
 template <int N>

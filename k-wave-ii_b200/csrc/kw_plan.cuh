@@ -185,6 +185,8 @@ kw_status launched(kw_plan *P);
 // Defined in kw_launch.cuh and instantiated per length in kw_inst.cu.
 template <int N> struct YLaunch {
     static kw_status run(kw_plan *P, bool inv, Spec4 bufs, int nf, int kz0, int nkz);
+    // inverse y-pass of the 3-D gradient fan-out (ks_ypass_fan); N > 0 only
+    static kw_status run_fan(kw_plan *P, Spec4 bufs, int kz0, int nkz, const float2 *ddy, const float2 *ddz);
 };
 template <int N> struct XLaunch {
     static kw_status run(kw_plan *P, Spec4 bufs, OpSet ops, int fanout, int nf, int kz0, int nkz);

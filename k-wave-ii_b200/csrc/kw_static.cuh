@@ -233,6 +233,64 @@ __global__ void __launch_bounds__(ks_threads(N1, TY), (4 * kThreads + ks_threads
 }
 
 // ---------------------------------------------------------------------------
+// Inverse y-pass of the 3-D gradient fan-out.  The x-pass left the axis-0
+// output in bufs.p[0] and, in bufs.p[1], the inverse x-transform B shared by
+// the axis-1 and axis-2 outputs, whose multipliers dd_y(k_y) and dd_z(k_z)
+// are constant along x.  blockIdx.z = 0 transforms bufs.p[0] in place;
+// blockIdx.z = 1 reads B twice (the second time from L2) and writes
+// dd_z(k_z) IFFT_y(B) to bufs.p[2], then IFFT_y(dd_y(k_y) B) in place to
+// bufs.p[1].  One read of B replaces the x-pass's write and this pass's read
+// of a third field.  grid = (ceil(N0/TY), N2h, 2).
+// ---------------------------------------------------------------------------
+template <int N1, int TY>
+__global__ void __launch_bounds__(ks_threads(N1, TY), (4 * kThreads + ks_threads(N1, TY) - 1) / ks_threads(N1, TY))
+    ks_ypass_fan(Spec4 bufs, Geom g, const float2 *__restrict__ tw, int kz0, const float2 *__restrict__ ddy,
+                 const float2 *__restrict__ ddz) {
+    constexpr int NT = ks_threads(N1, TY);
+    static_assert(RPlan<N1, false>::M >= 2, "in-place pass needs two stages");
+    extern __shared__ float2 sm[];   // N1 * TY
+    const int x0 = blockIdx.x * TY;
+    const int kz = blockIdx.y + kz0;
+    const long long base = (long long)kz * N1 * g.N0 + x0;
+    const int N0 = g.N0;
+    __shared__ float2 s_tw[N1], s_dy[N1];
+    for (int i = threadIdx.x; i < N1; i += NT) {
+        s_tw[i] = __ldg(tw + i);
+        s_dy[i] = __ldg(ddy + i);
+    }
+    const SmemTable stw{s_tw};
+    if (blockIdx.z == 0) {
+        float2 *buf = bufs.p[0];
+        auto ld = [&](int, int, int l, int i) -> float2 {
+            return x0 + l < N0 ? buf[base + (long long)i * N0 + l] : make_float2(0.f, 0.f);
+        };
+        auto st = [&](int, int, int l, int i, float2 v) {
+            if (x0 + l < N0) buf[base + (long long)i * N0 + l] = v;
+        };
+        rs_fft<N1, TY, true, true, 0, NT>(sm, stw, ld, st);
+        return;
+    }
+    float2 *B = bufs.p[1], *out_z = bufs.p[2];
+    const float2 mz = __ldg(ddz + kz);
+    auto ldb = [&](int, int, int l, int i) -> float2 {
+        return x0 + l < N0 ? B[base + (long long)i * N0 + l] : make_float2(0.f, 0.f);
+    };
+    auto stz = [&](int, int, int l, int i, float2 v) {
+        if (x0 + l < N0) out_z[base + (long long)i * N0 + l] = cmul(v, mz);
+    };
+    rs_fft<N1, TY, true, true, 0, NT>(sm, stw, ldb, stz);
+    // the first stage's loads of the second transform come after every
+    // thread's loads of the first (its stores went to out_z, not B)
+    auto ldy = [&](int, int, int l, int i) -> float2 {
+        return x0 + l < N0 ? cmul(B[base + (long long)i * N0 + l], s_dy[i]) : make_float2(0.f, 0.f);
+    };
+    auto sty = [&](int, int, int l, int i, float2 v) {
+        if (x0 + l < N0) B[base + (long long)i * N0 + l] = v;
+    };
+    rs_fft<N1, TY, true, true, 0, NT>(sm, stw, ldy, sty);
+}
+
+// ---------------------------------------------------------------------------
 // x-pass: forward C2C along axis 0, operator, inverse C2C, in place.
 // grid = (ceil(N1*N2h/NL), 1, fanout ? 1 : nfields), ks_threads(N0, NL) threads
 // ---------------------------------------------------------------------------
@@ -243,7 +301,9 @@ __global__ void __launch_bounds__(ks_threads(N0, NL), 3 * kThreads / ks_threads(
     static_assert(RPlan<N0, false>::M >= 2, "in-place pass needs two stages");
     __shared__ float2 sm[NL * Padded<N0>::LS];
     __shared__ float kyz2[NL];
-    __shared__ int liy[NL], liz[NL];
+    // per-line multiplier of each output whose operator table runs along y
+    // or z (constant along an x line); 1 for the others
+    __shared__ float2 s_lm[3][NL];
     // per-x tables read on the transforms' dependency chains, kept in shared
     // memory: twiddles, k_x^2 and the x-derivative table of an axis-0 output
     __shared__ float2 s_tw[N0], s_ddx[N0];
@@ -268,9 +328,18 @@ __global__ void __launch_bounds__(ks_threads(N0, NL), 3 * kThreads / ks_threads(
     for (int l = threadIdx.x; l < NL; l += NT) {
         const int line = min(line0 + l, lines_total - 1);
         const int iy = line % g.N1, iz = line / g.N1;
-        liy[l] = iy;
-        liz[l] = iz;
         kyz2[l] = __ldg(P.k2[1] + iy) + __ldg(P.k2[2] + iz);
+#pragma unroll
+        for (int o = 0; o < 3; ++o) {
+            float2 m = make_float2(1.f, 0.f);
+            if (o < ops.n && ops.axis[o] != 0) {
+                const int ko = ops.kind[o], ax = ops.axis[o];
+                const float2 *dd = ko == OP_GRAD_POS ? pick(P.dd_pos, ax)
+                                                     : (ko == OP_GRAD_NEG ? pick(P.dd_neg, ax) : pick(P.sh_neg, ax));
+                if (ko == OP_GRAD_POS || ko == OP_GRAD_NEG || ko == OP_SHIFT_NEG) m = __ldg(dd + (ax == 1 ? iy : iz));
+            }
+            s_lm[o][l] = m;
+        }
     }
     __syncthreads();
     const float2 *in = pick(bufs.p, f) + (long long)line0 * N0;
@@ -312,7 +381,12 @@ __global__ void __launch_bounds__(ks_threads(N0, NL), 3 * kThreads / ks_threads(
             spec[b][t] = cscale(spec[b][t], fac * P.scale);
         }
     }
+    // An output whose operator table runs along x gets its own inverse
+    // transform.  Every other output is the inverse transform of spec times a
+    // constant per x line (s_lm), so in fan-out mode they share one inverse
+    // transform and are scaled as they are stored.
     const int nout = fanout ? ops.n : 1;
+    int shared_mask = 0;
     for (int o = 0; o < nout; ++o) {
         const int oi = fanout ? o : f;
         const int axis = pick(ops.axis, oi);
@@ -320,17 +394,39 @@ __global__ void __launch_bounds__(ks_threads(N0, NL), 3 * kThreads / ks_threads(
         const float2 *dd = ko == OP_GRAD_POS ? pick(P.dd_pos, axis)
                                              : (ko == OP_GRAD_NEG ? pick(P.dd_neg, axis) : pick(P.sh_neg, axis));
         const bool mul_dd = ko == OP_GRAD_POS || ko == OP_GRAD_NEG || ko == OP_SHIFT_NEG;
+        if (fanout && !(mul_dd && axis == 0)) {
+            shared_mask |= 1 << o;
+            continue;
+        }
         float2 *out = pick(bufs.p, oi) + (long long)line0 * N0;
         auto ld2 = [&](int b, int t, int l, int i) -> float2 {
             if (!mul_dd) return spec[b][t];
-            if (axis == 0 && dd == ddx) return cmul(spec[b][t], s_ddx[i]);
-            const int idx = axis == 0 ? i : (axis == 1 ? liy[l] : liz[l]);
-            return cmul(spec[b][t], __ldg(dd + idx));
+            if (axis != 0) return cmul(spec[b][t], s_lm[oi][l]);
+            return cmul(spec[b][t], dd == ddx ? s_ddx[i] : __ldg(dd + i));
         };
         auto st2 = [&](int, int, int l, int i, float2 v) {
             if (line0 + l < lines_total) out[l * N0 + i] = v;
         };
         rs_fft<N0, NL, false, true, 0, NT>(sm, stw, ld2, st2);
+    }
+    if (shared_mask) {
+        // fanout == 2 (the 3-D gradient ahead of ks_ypass_fan): the shared
+        // transform is stored once, unscaled, to the first shared output; the
+        // inverse y-pass applies the y and z multipliers
+        const int first = __ffs(shared_mask) - 1;
+        auto ld3 = [&](int b, int t, int, int) -> float2 { return spec[b][t]; };
+        auto st3 = [&](int, int, int l, int i, float2 v) {
+            if (line0 + l >= lines_total) return;
+            if (fanout == 2) {
+                (pick(bufs.p, first) + (long long)line0 * N0)[l * N0 + i] = v;
+                return;
+            }
+#pragma unroll
+            for (int o = 0; o < 3; ++o)
+                if (shared_mask & (1 << o))
+                    (bufs.p[o] + (long long)line0 * N0)[l * N0 + i] = cmul(v, s_lm[o][l]);
+        };
+        rs_fft<N0, NL, false, true, 0, NT>(sm, stw, ld3, st3);
     }
 }
 

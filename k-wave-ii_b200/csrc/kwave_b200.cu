@@ -398,11 +398,33 @@ Spec4 specs(kw_plan *P, int a, int b = -1, int c = -1) {
 // gradient spectra of p for the next momentum update: spec[0] holds the
 // z-half spectrum of p on entry; spec[0..D-1] hold dd_pos_i kappa p_k after
 // the inverse x and y passes on exit.
+template <int N> struct YFan {
+    static kw_status run(kw_plan *P, Spec4 bufs, int kz0, int nkz) {
+        return YLaunch<N>::run_fan(P, bufs, kz0, nkz, P->dd_pos[1], P->dd_pos[2]);
+    }
+};
+
 kw_status grad_group(kw_plan *P) {
     OpSet ops{};
     ops.n = P->D;
     for (int i = 0; i < P->D; ++i) { ops.kind[i] = OP_GRAD_POS; ops.axis[i] = P->comp_axis[i]; }
-    return yxy_group(P, specs(P, 0, 1, 2), P->D, ops, true);
+    const bool fan3 = P->static_x && P->static_y && P->g.N1 > 1 && P->D == 3 && P->comp_axis[0] == 0 &&
+                      P->comp_axis[1] == 1 && P->comp_axis[2] == 2 && P->tw[0] && P->tw[1];
+    if (!fan3) return yxy_group(P, specs(P, 0, 1, 2), P->D, ops, true);
+    // 3-D: the y and z outputs share one inverse x-transform (their
+    // multipliers are constant along x) and one read of it in the inverse
+    // y-pass (ks_ypass_fan)
+    const Spec4 bufs = specs(P, 0, 1, 2);
+    const int nch = P->kz_chunks;
+    const int N2h = P->g.N2h;
+    for (int c = 0; c < nch; ++c) {
+        const int kz0 = (int)((long long)N2h * c / nch), kz1 = (int)((long long)N2h * (c + 1) / nch);
+        KW_TRY(ypass(P, false, bufs, 1, kz0, kz1 - kz0));
+        KW_TRY(xpass(P, bufs, ops, 2, 1, kz0, kz1 - kz0));
+        Scope s(P, KW_KCLASS_YPASS);
+        KW_TRY(dispatch<YFan>(P->g.N1, P, bufs, kz0, kz1 - kz0));
+    }
+    return KW_OK;
 }
 
 // real(ifftn(source_kappa .* fftn(field))) into out, via spec[3]
