@@ -35,6 +35,12 @@ template <int N, bool INV> struct RPlan {
         for (int k = 0; k < s; ++k) p *= R(k);
         return p;
     }
+    // every stage has the same radix (e.g. 256 = 16 x 16)
+    __host__ __device__ static constexpr bool uniform() {
+        for (int s = 1; s < M; ++s)
+            if (R(s) != R(0)) return false;
+        return true;
+    }
 };
 
 // element (l, i) of a tile: interleaved lines (i*NL + l) or padded rows
@@ -78,6 +84,11 @@ __device__ __forceinline__ void rs_stage(float2 *sm, const TW &tw, Ld &ld, St &s
     constexpr int M = P::M, R = SH::R, NS = P::NS(S), NB = SH::NB;
     constexpr int TOT = SH::TOT, MAXB = SH::MAXB;
     constexpr int TWS = N / (NS * R);
+    // Contiguous lines whose every stage has the same radix, with at most 32
+    // butterflies per line and one butterfly per thread: thread g keeps line
+    // g / NB in every stage, so a line is exchanged within one warp and a
+    // warp barrier orders the exchange (no block barrier).
+    constexpr bool WL = !IL && P::uniform() && 32 % NB == 0 && TOT <= NT && NT % 32 == 0;
     float2 v[MAXB][R];
 #pragma unroll
     for (int b = 0; b < MAXB; ++b) {
@@ -116,7 +127,9 @@ __device__ __forceinline__ void rs_stage(float2 *sm, const TW &tw, Ld &ld, St &s
             }
         }
     } else {
-        __syncthreads();   // earlier readers of the tile are done
+        // earlier readers of the tile are done
+        if constexpr (WL) __syncwarp();
+        else __syncthreads();
 #pragma unroll
         for (int b = 0; b < MAXB; ++b) {
             const int g = threadIdx.x + b * NT;
@@ -128,7 +141,8 @@ __device__ __forceinline__ void rs_stage(float2 *sm, const TW &tw, Ld &ld, St &s
                 for (int t = 0; t < R; ++t) sm[tat<N, NL, IL>(l, base + t * NS)] = v[b][t];
             }
         }
-        __syncthreads();
+        if constexpr (WL) __syncwarp();
+        else __syncthreads();
     }
 }
 
