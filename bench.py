@@ -814,7 +814,7 @@ def main():
     achieved = alg_bytes_per_sim / (ms / args.steps / 1e3) / 1e9
     # DRAM bytes of one time step, per-kernel ncu captures of the 256^3
     # workload (profiles/traffic_256cube_per_kernel.md); ncu runs each launch
-    # with cold caches, so this is an upper bound on the warm traffic
+    # with cold caches (the file also gives the figure without the flush)
     traffic, traffic_src = None, None
     tf = os.path.join(ROOT, "profiles", "step_traffic_256.json")
     if os.path.exists(tf) and args.N == 256:
