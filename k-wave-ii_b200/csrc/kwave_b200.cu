@@ -1265,7 +1265,9 @@ kw_status create(const kw_problem *pr, kw_plan *P) {
     P->op.scale = (float)(1.0 / (double)g.N);
 
     plan_tiles(P);
-    if (g.N2 > kCap / 2) return fail(KW_ERR_UNSUPPORTED, "axis length %d above %d", g.N2, kCap / 2);
+    // one packed line of the real-to-complex axis fills at most one transform
+    // tile (the runtime stage R then holds four such tiles, 128 KB)
+    if (g.N2 > kCap) return fail(KW_ERR_UNSUPPORTED, "axis length %d above %d", g.N2, kCap);
     const size_t N = (size_t)g.N, Nh = (size_t)g.Nh;
     KW_TRY(palloc(P, &P->d_t, 1));
     KW_TRY(palloc(P, &P->d_err, 1));

@@ -220,6 +220,24 @@ def make_case(name):
         mask = np.zeros(shape); mask[900, :] = 1; mask[:, 18] = 1
         return 2, shape, dx, 160, dt, {"sound_speed": c, "density": rho, "alpha_coeff": 0.5, "alpha_power": 1.3}, \
             {"p_mask": pm, "p": 1e4 * tone(dt, 1.5e6, 3, 160)}, {"mask": mask, "record": ["p", "p_max"]}, {"PMLSize": 10}
+    if name == "2d_long_y_4096":
+        # the real-to-complex axis at its 4096-point limit (2-D y maps to it)
+        shape = (24, 4096)
+        c, rho = blob_medium(shape, rng)
+        dt = 0.3 * dx / c.max()
+        pm = np.zeros(shape); pm[6:18, 300] = 1
+        mask = np.zeros(shape); mask[12, :] = 1; mask[:, 3900] = 1
+        return 2, shape, dx, 120, dt, {"sound_speed": c, "density": rho, "alpha_coeff": 0.5, "alpha_power": 1.5,
+                                       "BonA": 5.0}, \
+            {"p_mask": pm, "p": 1e5 * tone(dt, 2e6, 3, 120)}, {"mask": mask, "record": ["p", "p_max"]}, {"PMLSize": 8}
+    if name == "3d_long_z_3000":
+        # a 3000-point real-to-complex axis (8 x 3 x 5^3), runtime-radix kernels
+        shape = (20, 16, 3000)
+        c, rho = blob_medium(shape, rng)
+        mask = np.zeros(shape); mask[10, 8, :] = 1
+        return 3, shape, dx, 60, 0.3 * dx / c.max(), {"sound_speed": c, "density": rho, "alpha_coeff": 0.75,
+                                                      "alpha_power": 1.5}, \
+            {"p0": disc_p0(shape, 3)}, {"mask": mask, "record": ["p", "p_max", "u"]}, {"PMLSize": 4}
     # ---- operator options (kspaceFirstOrder3D.m:629-661) ----
     if name == "2d_no_sg":
         shape = (60, 52)
@@ -405,7 +423,8 @@ CASES = ["2d_homog_p0", "2d_hetero_abs_nl", "2d_stokes_dirichlet", "2d_nocorr_mu
          "3d_p0_u", "2d_time_reversal", "3d_time_reversal_abs", "3d_static_mixed_radix", "3d_static_128",
          "2d_intensity", "3d_intensity_static", "2d_cart_linear", "3d_cart_linear", "3d_layered_full_volume",
          "2d_full_mask_odd",
-         "2d_prime_22x26", "3d_prime_26x22x34", "2d_long_axis_1030", "2d_no_sg", "3d_no_kspace",
+         "2d_prime_22x26", "3d_prime_26x22x34", "2d_long_axis_1030", "2d_long_y_4096", "3d_long_z_3000", "2d_no_sg",
+         "3d_no_kspace",
          "2d_no_absorption_sign", "2d_alpha_sign", "2d_stokes_sign", "2d_cref_min", "3d_cref_mean", "2d_cref_value",
          "2d_smooth_all", "2d_record_start", "2d_u_nocorr", "3d_u_additive", "3d_u_dirichlet", "2d_p_freq_ref",
          "3d_u_freq_ref", "3d_cuboids", "2d_cuboids_pml_outside", "legacy_abs_2dx", "legacy_abs_2dy",
