@@ -36,6 +36,15 @@ kw_status ypass_fan(kw_plan *P, Spec4 bufs, dim3 grid, int kz0, const float2 *dd
     return KW_OK;
 }
 
+template <int N, int NL>
+kw_status xpass(kw_plan *P, Spec4 bufs, OpSet ops, int fanout, int kz0, int nkz, dim3 grid) {
+    if (fanout)
+        ks_xpass<N, NL, true><<<grid, ks_threads(N, NL), 0, P->stream>>>(bufs, P->g, P->tw[0], P->op, ops, fanout, kz0, nkz);
+    else
+        ks_xpass<N, NL, false><<<grid, ks_threads(N, NL), 0, P->stream>>>(bufs, P->g, P->tw[0], P->op, ops, 0, kz0, nkz);
+    return KW_OK;
+}
+
 template <int N, int PL>
 kw_status zr2c(kw_plan *P, const float *R, float2 *H, dim3 grid) {
     constexpr size_t sh = (size_t)N * PL * sizeof(float2);
@@ -156,15 +165,9 @@ kw_status XLaunch<N>::run(kw_plan *P, Spec4 bufs, OpSet ops, int fanout, int nf,
     const int lines = P->g.N1 * (N > 0 ? nkz : P->g.N2h);
     dim3 grid((lines + P->NL - 1) / P->NL, 1, fanout ? 1 : nf);
     if constexpr (N > 0) {
-        if (P->NL == ks_xlines(N))
-            ks_xpass<N, ks_xlines(N)><<<grid, ks_threads(N, ks_xlines(N)), 0, P->stream>>>(bufs, P->g, P->tw[0], P->op,
-                                                                                        ops, fanout, kz0, nkz);
-        else if (P->NL == ks_xhalf(N))
-            ks_xpass<N, ks_xhalf(N)><<<grid, ks_threads(N, ks_xhalf(N)), 0, P->stream>>>(bufs, P->g, P->tw[0], P->op,
-                                                                                      ops, fanout, kz0, nkz);
-        else
-            ks_xpass<N, ks_xnarrow(N)><<<grid, ks_threads(N, ks_xnarrow(N)), 0, P->stream>>>(bufs, P->g, P->tw[0],
-                                                                                          P->op, ops, fanout, kz0, nkz);
+        if (P->NL == ks_xlines(N)) KW_TRY((launch::xpass<N, ks_xlines(N)>(P, bufs, ops, fanout, kz0, nkz, grid)));
+        else if (P->NL == ks_xhalf(N)) KW_TRY((launch::xpass<N, ks_xhalf(N)>(P, bufs, ops, fanout, kz0, nkz, grid)));
+        else KW_TRY((launch::xpass<N, ks_xnarrow(N)>(P, bufs, ops, fanout, kz0, nkz, grid)));
     } else {
         size_t sh = (size_t)(fanout ? 2 : 1) * P->NL * P->g.N0 * sizeof(float2);
         KW_TRY(set_smem((const void *)k_xpass<0, 0>, sh));

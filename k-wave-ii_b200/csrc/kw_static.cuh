@@ -306,12 +306,17 @@ __global__ void __launch_bounds__(ks_threads(N1, TY), (4 * kThreads + ks_threads
 
 // ---------------------------------------------------------------------------
 // x-pass: forward C2C along axis 0, operator, inverse C2C, in place.
-// grid = (ceil(N1*N2h/NL), 1, fanout ? 1 : nfields), ks_threads(N0, NL) threads
+// grid = (ceil(N1*N2h/NL), 1, fanout ? 1 : nfields), ks_threads(N0, NL) threads.
+// FAN: the fan-out variant (fanout 1 or 2), which keeps the forward spectrum
+// in registers across two or more inverse transforms, at three blocks per SM;
+// the single-output variant (fanout 0) fits four.
 // ---------------------------------------------------------------------------
-template <int N0, int NL>
-__global__ void __launch_bounds__(ks_threads(N0, NL), 3 * kThreads / ks_threads(N0, NL))
-    ks_xpass(Spec4 bufs, Geom g, const float2 *__restrict__ tw, OpParams P, OpSet ops, int fanout, int kz0, int nkz) {
+template <int N0, int NL, bool FAN>
+__global__ void __launch_bounds__(ks_threads(N0, NL), (FAN ? 3 : 4) * kThreads / ks_threads(N0, NL))
+    ks_xpass(Spec4 bufs, Geom g, const float2 *__restrict__ tw, OpParams P, OpSet ops, int fanout_arg, int kz0,
+             int nkz) {
     constexpr int NT = ks_threads(N0, NL);
+    const int fanout = FAN ? fanout_arg : 0;
     static_assert(RPlan<N0, false>::M >= 2, "in-place pass needs two stages");
     __shared__ float2 sm[NL * Padded<N0>::LS];
     __shared__ float kyz2[NL];
