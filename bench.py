@@ -666,6 +666,7 @@ def adjoint_section(kw, device, Nt=3000, n_shots=16, fd_cells=32, seed=4, tr=Tru
             data.append(sim.run())
     def one_shot(s):
         with kw.Simulation.from_prepared(_adjoint_problem(kw, w, w["c_start"], s, cells)) as sim:
+            sim.keep_checkpoints()   # the misfit's forward run is the gradient's checkpointing run
             y = sim.run()
             r = y.astype(np.float64) - data[s]
             gc, _ = sim.adjoint_gradient(r)

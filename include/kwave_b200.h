@@ -372,6 +372,20 @@ kw_status kw_adjoint_gradient(kw_plan *plan, const float *residual, uint32_t che
                               double *grad_rho);
 
 /*
+ * Keep the adjoint's checkpoints from the plan's own runs.  No counterpart in
+ * the reference.  With enable != 0, every later complete run of the loop
+ * (kw_run, kw_run_device, or kw_step up to Nt from a fresh start) also keeps
+ * the state after every checkpoint_interval-th step (0: round(sqrt(Nt))), so
+ * a kw_adjoint_gradient that follows it with the same interval skips its own
+ * forward pass: the misfit's forward run is the checkpointing run.  The
+ * states are the ones kw_adjoint_gradient would compute, so its result is
+ * unchanged.  Costs (Nt / K - 1) (2 D + 1) N floats of device memory, held
+ * until enable = 0 or kw_plan_destroy; any reset, or an incomplete run,
+ * discards the kept states.  Time reversal plans: KW_ERR_UNSUPPORTED.
+ */
+kw_status kw_keep_checkpoints(kw_plan *plan, int32_t enable, uint32_t checkpoint_interval);
+
+/*
  * Allocation-free staggered spectral gradient.  No counterpart in the
  * reference: it exists for callers that must not have this library allocate
  * device memory -- a MEX function working on gpuArray data owned by MATLAB's

@@ -133,6 +133,11 @@ struct kw_plan {
     bool tma_r = false;
     std::map<std::pair<const void *, int>, CUtensorMap> tmaps;
     int *d_err = nullptr;
+    // adjoint checkpoints kept by the plan's own runs (kw_keep_checkpoints):
+    // the state after steps K, 2K, ..., (nseg - 1) K; valid after a complete run
+    float *ck_buf = nullptr;
+    int ck_K = 0, ck_nseg = 0, ck_saved = 0;
+    bool ck_on = false, ck_valid = false;
     long long in_count = 1;
 
     int t = 1;                     // next step to run (1-based)

@@ -684,8 +684,12 @@ kw_status zero_state(kw_plan *P) {
     KW_CUDA(cudaMemcpyAsync(P->d_t, &one, sizeof(int), cudaMemcpyHostToDevice, P->stream));
     P->t = 1;
     P->started = false;
+    P->ck_saved = 0;
+    P->ck_valid = false;
     return KW_OK;
 }
+
+kw_status save_state(kw_plan *P, float *dst);
 
 kw_status start(kw_plan *P) {
     if (P->time_rev) {
@@ -1597,7 +1601,19 @@ kw_status run_step_graphed(kw_plan *P) {
 
 kw_status run_steps(kw_plan *P, uint64_t n) {
     if (!P->started) KW_TRY(start(P));
-    for (uint64_t k = 0; k < n && P->t <= P->index_end; ++k) KW_TRY(run_step_graphed(P));
+    for (uint64_t k = 0; k < n && P->t <= P->index_end; ++k) {
+        KW_TRY(run_step_graphed(P));
+        if (P->ck_on) {
+            // kept adjoint checkpoints: the state after step done = j K
+            const int done = P->t - 1;
+            if (done % P->ck_K == 0 && done / P->ck_K == P->ck_saved + 1 && P->ck_saved + 1 < P->ck_nseg) {
+                const size_t snap = (size_t)(2 * P->D + 1) * (size_t)P->g.N;
+                KW_TRY(save_state(P, P->ck_buf + (size_t)P->ck_saved * snap));
+                P->ck_saved += 1;
+            }
+            P->ck_valid = P->t > P->Nt && P->ck_saved + 1 == P->ck_nseg;
+        }
+    }
     if (P->time_rev && P->t > P->index_end) {
         k_tr_final<<<(P->M + 255) / 256, 256, 0, P->stream>>>(P->sidx, P->M, P->tr_data, P->p);
         KW_TRY(launched(P));

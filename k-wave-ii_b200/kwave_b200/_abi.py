@@ -165,6 +165,7 @@ SYMBOLS = {
     "kw_plan_tiles": (C.c_int, [C.c_void_p, C.POINTER(C.c_int32)]),
     "kw_set_tiles": (C.c_int, [C.c_void_p, C.POINTER(C.c_int32)]),
     "kw_adjoint_gradient": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p]),
+    "kw_keep_checkpoints": (C.c_int, [C.c_void_p, C.c_int32, C.c_uint32]),
     "kw_server_create": (C.c_int, [C.POINTER(kw_server_config), C.POINTER(C.c_void_p)]),
     "kw_server_submit": (C.c_int, [C.c_void_p, C.POINTER(kw_problem), C.POINTER(C.c_uint64)]),
     "kw_server_wait": (C.c_int, [C.c_void_p, C.c_uint64, C.POINTER(kw_outputs), C.POINTER(C.c_double)]),

@@ -835,6 +835,13 @@ class Simulation:
         return b.value
 
     # -- adjoint -----------------------------------------------------------------
+    def keep_checkpoints(self, enable=True, checkpoint_interval=0):
+        """Let the next complete run keep the adjoint's checkpoints (the
+        state after every checkpoint_interval-th step, 0: round(sqrt(Nt))), so
+        that an ``adjoint_gradient`` with the same interval after it skips its
+        own forward pass (kw_keep_checkpoints).  The gradient is unchanged."""
+        _abi.check(self._lib.kw_keep_checkpoints(self.handle, 1 if enable else 0, int(checkpoint_interval)))
+
     def adjoint_gradient(self, residual, checkpoint_interval=0, density=True):
         """Gradient of a sensor misfit J with respect to the sound speed and
         the density at every grid cell (the library's discrete adjoint of this

@@ -61,6 +61,43 @@ def test_gradient_matches_oracle_adjoint(shape, Nt):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("shape,Nt,K", [((32, 28), 60, 0), ((64, 64), 120, 11), ((12, 14, 10), 25, 4)])
+def test_kept_checkpoints_give_the_same_gradient(shape, Nt, K):
+    """kw_keep_checkpoints: the misfit's own run keeps the states the
+    adjoint would recompute, so the gradient that follows skips its forward
+    pass (fewer launches) and is bit-identical; an incomplete run or a reset
+    discards them (the gradient then runs its own forward pass)."""
+    import kwave_b200 as kw
+    shape, dx, Nt, dt, c, rho, pm, sig, sm = adjoint_problem(shape, Nt)
+    dim = len(shape)
+    medium = {"sound_speed": c, "density": rho, "sound_speed_ref": 1700.0}
+    with kw.Simulation(dim, _grid(kw, shape, dx, Nt, dt), medium, {"p_mask": pm, "p": sig[None, :]},
+                       {"mask": sm}, PMLSize=4, Smooth=False) as sim:
+        y = sim.run()
+        r = 0.1 * y.astype(np.float64)
+        gc, gr = sim.adjoint_gradient(r, checkpoint_interval=K)
+        n0 = sim.launch_count()
+        gc_again, _ = sim.adjoint_gradient(r, checkpoint_interval=K)
+        plain_launches = sim.launch_count() - n0
+        assert np.array_equal(gc_again, gc)
+        sim.keep_checkpoints(True, K)
+        assert np.array_equal(sim.run(), y)      # recording is unchanged
+        n1 = sim.launch_count()
+        gc2, gr2 = sim.adjoint_gradient(r, checkpoint_interval=K)
+        kept_launches = sim.launch_count() - n1
+        assert np.array_equal(gc2, gc) and np.array_equal(gr2, gr)
+        assert kept_launches < plain_launches    # the forward pass was skipped
+        # a partial run keeps nothing usable: the gradient recomputes, same result
+        sim.reset()
+        sim.step(Nt // 2)
+        gc3, _ = sim.adjoint_gradient(r, checkpoint_interval=K)
+        assert np.array_equal(gc3, gc)
+        sim.keep_checkpoints(False)
+        gc4, _ = sim.adjoint_gradient(r, checkpoint_interval=K)
+        assert np.array_equal(gc4, gc)
+
+
+@pytest.mark.gpu
 def test_gradient_rejects_unsupported_media():
     import kwave_b200 as kw
     shape, dx, Nt, dt, c, rho, pm, sig, sm = adjoint_problem((32, 28), 20)
