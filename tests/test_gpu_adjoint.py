@@ -30,7 +30,8 @@ def _grid(mod, shape, dx, Nt, dt):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("shape,Nt", [((32, 28), 60), ((64, 64), 120), ((12, 14, 10), 25), ((32, 64, 48), 40)])
+@pytest.mark.parametrize("shape,Nt", [((32, 28), 60), ((64, 64), 120), ((12, 14, 10), 25), ((32, 64, 48), 40),
+                                      ((32, 48, 64), 40)])
 def test_gradient_matches_oracle_adjoint(shape, Nt):
     import kwave_b200 as kw
     from oracle import adjoint as adj
