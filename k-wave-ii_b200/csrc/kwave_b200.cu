@@ -1554,11 +1554,11 @@ kw_status rms_out(kw_plan *P, float *dst, const float *sq) {
 // general (filtered) source is active, whether sensors record, and whether
 // the next step's gradient is needed.  Each combination is captured once as a
 // CUDA graph (on its second occurrence; the first runs directly) and replayed.
-kw_status run_step_graphed(kw_plan *P) {
-    const int t = P->t;
-    if (!P->use_graphs || P->timing_mask || (t == 1 && P->p0)) return run_step(P);
+// structure of step t as the graph cache sees it: buffer parity, general
+// source activity, recording, next-step gradient
+uint32_t step_key(const kw_plan *P, int t, bool parity_first) {
     uint32_t key = 0;
-    key |= (P->rho[0] == P->rho_first) ? 1u : 0u;
+    key |= parity_first ? 1u : 0u;
     key |= (P->u[0] == P->u_first) ? 2u : 0u;
     bool usrc = false;
     for (int c = 0; c < P->D; ++c) usrc = usrc || (P->usrc.dense_general && P->usrc.sig[c] && t <= P->usrc.T[c]);
@@ -1566,6 +1566,13 @@ kw_status run_step_graphed(kw_plan *P) {
     key |= (P->psrc.dense_general && t <= P->psrc.T[0]) ? 8u : 0u;
     key |= (!P->no_record && !P->time_rev && t >= P->record_start) ? 16u : 0u;
     key |= (t < P->index_end) ? 32u : 0u;
+    return key;
+}
+
+kw_status run_step_graphed(kw_plan *P) {
+    const int t = P->t;
+    if (!P->use_graphs || P->timing_mask || (t == 1 && P->p0)) return run_step(P);
+    const uint32_t key = step_key(P, t, P->rho[0] == P->rho_first);
     kw_plan::GraphEntry &e = P->graphs[key];
     if (e.exec) {
         KW_CUDA(cudaGraphLaunch(e.exec, P->stream));
@@ -1599,9 +1606,67 @@ kw_status run_step_graphed(kw_plan *P) {
     return KW_OK;
 }
 
+// Small grids: kBlockSteps consecutive steps of one structure (an even
+// number, so the double buffers end where they started) captured as one
+// graph, which removes the gaps between per-step graph launches.  Used when a
+// step moves fewer than kBlockCells cells; larger grids gain nothing from it.
+constexpr int kBlockSteps = 8;
+constexpr long long kBlockCells = 1LL << 20;
+
+// kBlockSteps if steps t .. t + kBlockSteps - 1 can run as one block graph
+int block_steps(const kw_plan *P, uint64_t remaining) {
+    if (!P->use_graphs || P->timing_mask || P->ck_on || P->g.N > kBlockCells || remaining < (uint64_t)kBlockSteps)
+        return 0;
+    const int t = P->t, G = kBlockSteps;
+    if ((t == 1 && P->p0) || t + G - 1 >= P->index_end) return 0;
+    // every step of the block has the structure of the first (parity aside)
+    const uint32_t k0 = step_key(P, t, true) & ~1u;
+    for (int s = 1; s < G; ++s)
+        if ((step_key(P, t + s, true) & ~1u) != k0) return 0;
+    return G;
+}
+
+kw_status run_block_graphed(kw_plan *P, int G) {
+    const uint32_t key = step_key(P, P->t, P->rho[0] == P->rho_first) | ((uint32_t)G << 8);
+    kw_plan::GraphEntry &e = P->graphs[key];
+    if (e.exec) {
+        KW_CUDA(cudaGraphLaunch(e.exec, P->stream));   // G even: the buffers end where they started
+        P->launches += e.launches;
+        P->t += G;
+        return KW_OK;
+    }
+    if (e.seen == 0) {
+        e.seen = 1;
+        for (int s = 0; s < G; ++s) KW_TRY(run_step_graphed(P));
+        return KW_OK;
+    }
+    const uint64_t l0 = P->launches;
+    KW_CUDA(cudaStreamBeginCapture(P->stream, cudaStreamCaptureModeThreadLocal));
+    kw_status st = KW_OK;
+    for (int s = 0; s < G && st == KW_OK; ++s) st = run_step(P);
+    cudaGraph_t graph = nullptr;
+    const cudaError_t ce = cudaStreamEndCapture(P->stream, &graph);
+    if (st != KW_OK) {
+        if (graph) cudaGraphDestroy(graph);
+        return st;
+    }
+    if (ce != cudaSuccess) return fail(KW_ERR_CUDA, "step block capture failed: %s", cudaGetErrorString(ce));
+    const cudaError_t ie = cudaGraphInstantiate(&e.exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (ie != cudaSuccess) return fail(KW_ERR_CUDA, "graph instantiation failed: %s", cudaGetErrorString(ie));
+    e.launches = P->launches - l0;
+    KW_CUDA(cudaGraphLaunch(e.exec, P->stream));   // the captured steps have not run yet
+    return KW_OK;
+}
+
 kw_status run_steps(kw_plan *P, uint64_t n) {
     if (!P->started) KW_TRY(start(P));
     for (uint64_t k = 0; k < n && P->t <= P->index_end; ++k) {
+        if (const int G = block_steps(P, n - k)) {
+            KW_TRY(run_block_graphed(P, G));
+            k += G - 1;
+            continue;
+        }
         KW_TRY(run_step_graphed(P));
         if (P->ck_on) {
             // kept adjoint checkpoints: the state after step done = j K
