@@ -35,12 +35,6 @@ template <int N, bool INV> struct RPlan {
         for (int k = 0; k < s; ++k) p *= R(k);
         return p;
     }
-    // every stage has the same radix (e.g. 256 = 16 x 16)
-    __host__ __device__ static constexpr bool uniform() {
-        for (int s = 1; s < M; ++s)
-            if (R(s) != R(0)) return false;
-        return true;
-    }
 };
 
 // element (l, i) of a tile: interleaved lines (i*NL + l) or padded rows
@@ -55,6 +49,39 @@ template <int NB, int NL, bool IL>
 __device__ __forceinline__ void bmap(int g, int &l, int &j) {
     if constexpr (IL) { l = g % NL; j = g / NL; }
     else { j = g % NB; l = g / NB; }
+}
+
+// Contiguous lines (not interleaved) with NT / NL threads per line, a divisor
+// of 32, and every stage's butterflies per line a multiple of it: thread u of
+// line l (l = tid / T, u = tid % T) takes butterflies u, u + T, ... of its
+// line in every stage, so a line never leaves its warp and the exchanges
+// between stages need only warp barriers (N = 64, 128, 256, 512 x-passes).
+template <int N, int NL, int NT, bool IL>
+__host__ __device__ constexpr bool line_in_warp() {
+    if (IL || NL <= 0 || NT % NL != 0) return false;
+    constexpr int T = NT / NL;
+    if (T <= 0 || 32 % T != 0) return false;
+    int n = N;
+    while (n > 1) {
+        const int r = plan_next(n);
+        if (r == 0 || (N / r) % T != 0) return false;
+        n /= r;
+    }
+    return true;
+}
+
+// butterfly slot b of this thread at a stage with NB butterflies per line ->
+// (line, butterfly): the line-in-warp map, or butterfly g = tid + b NT of
+// the tile in the order of bmap
+template <int NB, int NL, bool IL, int NT, bool LW>
+__device__ __forceinline__ void bslot(int b, int &l, int &j) {
+    if constexpr (LW) {
+        constexpr int T = NT / NL;
+        l = threadIdx.x / T;
+        j = threadIdx.x % T + T * b;
+    } else {
+        bmap<NB, NL, IL>(threadIdx.x + b * NT, l, j);
+    }
 }
 
 // Registers a thread owns after stage S of plan (N, INV) in a block of NT
@@ -84,18 +111,16 @@ __device__ __forceinline__ void rs_stage(float2 *sm, const TW &tw, Ld &ld, St &s
     constexpr int M = P::M, R = SH::R, NS = P::NS(S), NB = SH::NB;
     constexpr int TOT = SH::TOT, MAXB = SH::MAXB;
     constexpr int TWS = N / (NS * R);
-    // Contiguous lines whose every stage has the same radix, with at most 32
-    // butterflies per line and one butterfly per thread: thread g keeps line
-    // g / NB in every stage, so a line is exchanged within one warp and a
-    // warp barrier orders the exchange (no block barrier).
-    constexpr bool WL = !IL && P::uniform() && 32 % NB == 0 && TOT <= NT && NT % 32 == 0;
+    // a line that stays in one warp through every stage is exchanged under a
+    // warp barrier (no block barrier)
+    constexpr bool WL = line_in_warp<N, NL, NT, IL>();
     float2 v[MAXB][R];
 #pragma unroll
     for (int b = 0; b < MAXB; ++b) {
         const int g = threadIdx.x + b * NT;
-        if (TOT % NT == 0 || g < TOT) {
+        if (WL || TOT % NT == 0 || g < TOT) {
             int l, j;
-            bmap<NB, NL, IL>(g, l, j);
+            bslot<NB, NL, IL, NT, WL>(b, l, j);
 #pragma unroll
             for (int t = 0; t < R; ++t) {
                 const int i = j + t * NB;
@@ -118,9 +143,9 @@ __device__ __forceinline__ void rs_stage(float2 *sm, const TW &tw, Ld &ld, St &s
 #pragma unroll
         for (int b = 0; b < MAXB; ++b) {
             const int g = threadIdx.x + b * NT;
-            if (TOT % NT == 0 || g < TOT) {
+            if (WL || TOT % NT == 0 || g < TOT) {
                 int l, j;
-                bmap<NB, NL, IL>(g, l, j);
+                bslot<NB, NL, IL, NT, WL>(b, l, j);
                 const int base = (j / NS) * NS * R + j % NS;
 #pragma unroll
                 for (int t = 0; t < R; ++t) st(b, t, l, base + t * NS, v[b][t]);
@@ -133,9 +158,9 @@ __device__ __forceinline__ void rs_stage(float2 *sm, const TW &tw, Ld &ld, St &s
 #pragma unroll
         for (int b = 0; b < MAXB; ++b) {
             const int g = threadIdx.x + b * NT;
-            if (TOT % NT == 0 || g < TOT) {
+            if (WL || TOT % NT == 0 || g < TOT) {
                 int l, j;
-                bmap<NB, NL, IL>(g, l, j);
+                bslot<NB, NL, IL, NT, WL>(b, l, j);
                 const int base = (j / NS) * NS * R + j % NS;
 #pragma unroll
                 for (int t = 0; t < R; ++t) sm[tat<N, NL, IL>(l, base + t * NS)] = v[b][t];
@@ -375,10 +400,11 @@ __global__ void __launch_bounds__(ks_threads(N0, NL), (FAN ? 3 : 4) * kThreads /
     const bool grad = kind0 == OP_GRAD_POS || kind0 == OP_GRAD_NEG;
 #pragma unroll
     for (int b = 0; b < SH::MAXB; ++b) {
+        constexpr bool LW = line_in_warp<N0, NL, NT, false>();
         const int gg = threadIdx.x + b * NT;
-        if (!(SH::TOT % NT == 0 || gg < SH::TOT)) continue;
+        if (!(LW || SH::TOT % NT == 0 || gg < SH::TOT)) continue;
         int l, j;
-        bmap<SH::NB, NL, false>(gg, l, j);
+        bslot<SH::NB, NL, false, NT, LW>(b, l, j);
         const float ky = kyz2[l];
         constexpr int NSL = RPlan<N0, false>::NS(RPlan<N0, false>::M - 1);
 #pragma unroll
