@@ -158,6 +158,7 @@ struct kw_plan {
     };
     std::map<uint32_t, GraphEntry> graphs;
     bool use_graphs = true;
+    bool block_graphs = true;   // small grids: several steps per graph (run_steps)
     float *rho_first = nullptr, *u_first = nullptr;   // buffer identity for the key
 
     // streamed series outputs of kw_run: copy stream and per-slot events

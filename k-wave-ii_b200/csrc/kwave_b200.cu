@@ -1290,6 +1290,11 @@ kw_status create(const kw_problem *pr, kw_plan *P) {
         KW_TRY(palloc(P, &P->u_b[i], N));
     }
     KW_TRY(palloc(P, &P->srho, N));
+    {
+        // KW_BLOCK_GRAPHS=0: one graph per step on every grid
+        const char *e = getenv("KW_BLOCK_GRAPHS");
+        P->block_graphs = !(e && atoi(e) == 0);
+    }
     P->rho_first = P->rho[0];
     P->u_first = P->u[0];
     if (const char *e = getenv("KW_GRAPHS")) P->use_graphs = atoi(e) != 0;
@@ -1615,7 +1620,7 @@ constexpr long long kBlockCells = 1LL << 20;
 
 // kBlockSteps if steps t .. t + kBlockSteps - 1 can run as one block graph
 int block_steps(const kw_plan *P, uint64_t remaining) {
-    if (!P->use_graphs || P->timing_mask || P->ck_on || P->g.N > kBlockCells || remaining < (uint64_t)kBlockSteps)
+    if (!P->use_graphs || !P->block_graphs || P->timing_mask || P->ck_on || P->g.N > kBlockCells || remaining < (uint64_t)kBlockSteps)
         return 0;
     const int t = P->t, G = kBlockSteps;
     if ((t == 1 && P->p0) || t + G - 1 >= P->index_end) return 0;
