@@ -78,6 +78,15 @@ __device__ __forceinline__ void st2(float *p, long long gi, float2 v, bool two, 
     if (two) p[gi + 1] = v.y;
 }
 
+// TMA copies of half-spectrum rows: a box holds at most 256 rows, so the
+// N2/2 + 1 rows of one z-tile come in tma_row_boxes(N2) boxes of
+// tma_row_box(N2) rows each (the last may reach past the spectrum; its
+// out-of-range rows are filled and never read)
+__host__ __device__ constexpr int tma_row_boxes(int n2) { return (n2 / 2 + 1 + 255) / 256; }
+__host__ __device__ constexpr int tma_row_box(int n2) {
+    return (n2 / 2 + 1 + tma_row_boxes(n2) - 1) / tma_row_boxes(n2);
+}
+
 // ---- spectral operators ----------------------------------------------------
 // OP_SHIFT_NEG: exp(-i k d / 2) along one axis, no kappa -- the shift of a
 // staggered velocity component onto the regular grid

@@ -68,7 +68,7 @@ kw_status stage_u(kw_plan *P, const StageU &a, dim3 grid) {
     StageUMaps m;
     bool tma = false;
     KW_TRY(stage_u_maps(P, a, Z::TX, &m, &tma));
-    if constexpr (N <= 384) {
+    if constexpr (Z::TMA_OK) {
         if (tma) {
             // 128 bytes of slack for the kernel to align its TMA destinations
             KW_TRY(set_smem((const void *)ks_stage_u<N, PL, true>, sh + 128));
@@ -88,9 +88,9 @@ kw_status stage_r(kw_plan *P, const StageR &a, dim3 grid) {
     StageRMaps m;
     bool tma = false;
     KW_TRY(stage_r_maps(P, a, Z::TX, &m, &tma));
-    // TMA boxes hold at most 256 rows: the half spectrum's N/2 + 1 rows fit
-    // for N <= 384
-    if constexpr (N <= 384) {
+    // the spectrum rows come in boxes of at most 256 rows (tma_rows); the
+    // TMA variant exists where every box starts 128-byte aligned
+    if constexpr (Z::TMA_OK) {
         if (tma) {
             // 128 bytes of slack for the kernel to align its TMA destinations
             KW_TRY(set_smem((const void *)ks_stage_r<N, PL, true>, sh + 128));
@@ -112,7 +112,7 @@ kw_status stage_p(kw_plan *P, const StageP &a, dim3 grid) {
     StagePMaps m;
     bool tma = false;
     KW_TRY(stage_p_maps(P, a, Z::TX, &m, &tma));
-    if constexpr (N <= 384) {
+    if constexpr (Z::TMA_OK) {
         if (tma) {
             // 128 bytes of slack for the kernel to align its TMA destinations
             KW_TRY(set_smem((const void *)ks_stage_p<N, PL, true>, sh + 128));

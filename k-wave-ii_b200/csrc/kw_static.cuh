@@ -636,11 +636,14 @@ __device__ __forceinline__ void tma_field(float2 *dst, const CUtensorMap *map, i
     mbar_expect_tx(bar, (unsigned)(TX * N2 * sizeof(float)));
     for (int z = 0; z < N2; z += zbox) tma_load_3d(reinterpret_cast<float *>(dst) + z * TX, map, x0, y, z, bar);
 }
-// half-spectrum rows kz = 0 .. N2/2 of TX columns at row y into dst, [kz][x]
+// half-spectrum rows kz = 0 .. N2/2 of TX columns at row y into dst, [kz][x],
+// in tma_row_boxes(N2) boxes (every box's bytes count, filled rows included)
 template <int N2, int TX>
 __device__ __forceinline__ void tma_rows(float2 *dst, const CUtensorMap *map, int x0, int y, uint64_t *bar) {
-    mbar_expect_tx(bar, (unsigned)(TX * (N2 / 2 + 1) * sizeof(float2)));
-    tma_load_3d(dst, map, x0, y, 0, bar);
+    constexpr int NB = tma_row_boxes(N2), BR = tma_row_box(N2);
+    mbar_expect_tx(bar, (unsigned)(NB * BR * TX * sizeof(float2)));
+#pragma unroll
+    for (int k = 0; k < NB; ++k) tma_load_3d(dst + k * BR * TX, map, x0, y, k * BR, bar);
 }
 
 template <int N2, int PL_> struct ZStage {
@@ -648,10 +651,16 @@ template <int N2, int PL_> struct ZStage {
     using SH = typename ZT::SH;
     static constexpr int PL = ZT::PL, TX = ZT::TX, NT = ZT::NT;
     // float2 of the transform tile; it also holds the raw half-spectrum rows of
-    // a prefetched input, (N2/2 + 1) rows of TX values.  Rounded up to 128
-    // bytes, so the slices after it can be TMA destinations (128-byte
-    // aligned shared-memory addresses).
-    static constexpr int TILE = (N2 * PL + 2 * PL + 15) / 16 * 16;
+    // a prefetched input, (N2/2 + 1) rows of TX values (whole TMA boxes of
+    // rows, tma_row_boxes(N2) x tma_row_box(N2)).  Rounded up to 128 bytes,
+    // so the slices after it can be TMA destinations (128-byte aligned
+    // shared-memory addresses).
+    static constexpr int ROWS = tma_row_boxes(N2) * tma_row_box(N2) > N2 / 2 + 1 ? tma_row_boxes(N2) * tma_row_box(N2)
+                                                                                 : N2 / 2 + 1;
+    static constexpr int TILE = (ROWS * TX + 15) / 16 * 16;
+    // the TMA path: every box of rows starts on a 128-byte boundary
+    static constexpr bool TMA_OK =
+        (tma_row_boxes(N2) == 1 || (tma_row_box(N2) * TX * 8) % 128 == 0) && (TX * 4) % 16 == 0;
     static constexpr int SLICE = SH::MAXB * SH::R * NT;   // float2 of one staged field
     static __device__ __forceinline__ int sidx(int b, int t) { return (b * SH::R + t) * NT + threadIdx.x; }
 };

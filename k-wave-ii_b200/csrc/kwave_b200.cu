@@ -112,7 +112,7 @@ kw_status plan_map(kw_plan *P, const void *ptr, int elem, int TX, CUtensorMap *d
     if (it == P->tmaps.end()) {
         CUtensorMap t;
         if (elem == 4) KW_TRY(encode_map(&t, ptr, 4, g.N0, g.N1, g.N2, TX, g.N2 <= 256 ? g.N2 : g.N2 / 2));
-        else KW_TRY(encode_map(&t, ptr, 8, g.N0, g.N1, g.N2h, TX, g.N2h));
+        else KW_TRY(encode_map(&t, ptr, 8, g.N0, g.N1, g.N2h, TX, tma_row_box(g.N2)));
         it = P->tmaps.emplace(key, t).first;
     }
     *dst = it->second;
@@ -1275,12 +1275,14 @@ kw_status create(const kw_problem *pr, kw_plan *P) {
     const size_t N = (size_t)g.N, Nh = (size_t)g.Nh;
     KW_TRY(palloc(P, &P->d_t, 1));
     KW_TRY(palloc(P, &P->d_err, 1));
-    // stage R stages its fields with TMA when the boxes fit the rules: FP32
-    // rows of 16-byte multiples (N0 % 4), at most 256 rows of half spectrum
-    // (N2 <= 384); KW_TMA=0 keeps the cp.async path
+    // the stage kernels stage their fields with TMA when the boxes fit the
+    // rules: FP32 rows of 16-byte multiples (N0 % 4), a compile-time z length
+    // (the half spectrum's rows come in boxes of at most 256 rows, each
+    // 128-byte aligned: the launchers check that per tile width); KW_TMA=0
+    // keeps the cp.async path
     {
         const char *e = getenv("KW_TMA");
-        P->tma_r = P->static_z && g.N2 <= 384 && g.N0 % 4 == 0 && !(e && atoi(e) == 0) && have_encode_tiled();
+        P->tma_r = P->static_z && g.N2 <= 512 && g.N0 % 4 == 0 && !(e && atoi(e) == 0) && have_encode_tiled();
     }
     KW_TRY(palloc(P, &P->p, N));
     for (int i = 0; i < P->D; ++i) {
