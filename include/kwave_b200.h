@@ -411,7 +411,9 @@ kw_status kw_keep_checkpoints(kw_plan *plan, int32_t enable, uint32_t checkpoint
  * operator tables, so grids of up to about 8.3 million cells fit: 200^3 is
  * accepted, 256 x 256 x 128 is rejected with KW_ERR_UNSUPPORTED.  The first
  * call on each device looks up the array's device address with that device
- * current; make that first call before any stream capture.  The address is
+ * current.  No call may be made while its stream is being captured: each call
+ * copies operator tables from host memory and synchronizes the stream, so a
+ * call on a capturing stream returns KW_ERR_UNSUPPORTED.  The address is
  * kept for the life of the process: after cudaDeviceReset it is stale, so do
  * not call this entry point again in a process that has reset the device.
  * Every call shares the array, so calls that overlap on the GPU (other host

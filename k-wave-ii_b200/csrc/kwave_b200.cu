@@ -2198,6 +2198,13 @@ kw_status kw_gradient_noalloc(int32_t dim, const uint64_t shape[3], const double
         return fail(KW_ERR_UNSUPPORTED, "grid needs %zu bytes of scratch; kw_gradient_noalloc is limited to %zu bytes "
                     "(the half spectrum of about 8.3 million cells)", off, (size_t)KW_NOALLOC_SCRATCH_BYTES);
 
+    // the call copies its tables from host memory and synchronizes the
+    // stream, neither of which a stream capture can record
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    KW_CUDA(cudaStreamIsCapturing((cudaStream_t)stream, &cap));
+    if (cap != cudaStreamCaptureStatusNone)
+        return fail(KW_ERR_UNSUPPORTED, "kw_gradient_noalloc cannot run while its stream is being captured");
+
     int dev = 0;
     KW_CUDA(cudaGetDevice(&dev));
     void *basev = nullptr;

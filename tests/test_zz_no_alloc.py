@@ -111,3 +111,34 @@ def test_noalloc_rejects_grids_above_the_scratch_limit(shape):
                                  C.c_void_p(f.data_ptr()), None)
     assert st == _abi.KW_ERR_UNSUPPORTED
     assert b"limited to" in lib.kw_last_error()
+
+
+@pytest.mark.gpu
+def test_noalloc_refuses_a_capturing_stream():
+    """A call on a stream under capture returns KW_ERR_UNSUPPORTED and
+    enqueues nothing, so the capture stays valid; the same call then runs
+    once the capture has ended."""
+    torch = pytest.importorskip("torch")
+    from kwave_b200 import _abi
+    lib = _abi.load_library()
+    shape = (64, 64)
+    f_dev = torch.ones(int(np.prod(shape)), device="cuda")
+    out_dev = torch.zeros_like(f_dev)
+    shp = (C.c_uint64 * 3)(64, 64, 1)
+    sp = (C.c_double * 3)(1e-4, 1e-4, 1e-4)
+    graph = torch.cuda.CUDAGraph()
+    torch.cuda.synchronize()
+    with torch.cuda.graph(graph):
+        handle = C.c_void_p(torch.cuda.current_stream().cuda_stream)
+        st = lib.kw_gradient_noalloc(2, shp, sp, 0, 1, 1500.0, 2e-8, 1, C.c_void_p(f_dev.data_ptr()),
+                                     C.c_void_p(out_dev.data_ptr()), handle)
+        out_dev.add_(1.0)     # something for the graph to hold
+    assert st == _abi.KW_ERR_UNSUPPORTED
+    assert b"captured" in lib.kw_last_error()
+    del graph
+    st = lib.kw_gradient_noalloc(2, shp, sp, 0, 1, 1500.0, 2e-8, 1, C.c_void_p(f_dev.data_ptr()),
+                                 C.c_void_p(out_dev.data_ptr()), None)
+    assert st == 0, lib.kw_last_error()
+    torch.cuda.synchronize()
+    # the gradient of a constant field is zero
+    assert float(out_dev.abs().max()) < 1e-3
