@@ -13,6 +13,8 @@
 //     and "forward -> operator -> inverse" (x-pass) stay in registers.
 #pragma once
 
+#include <type_traits>
+
 #include "kw_kernels.cuh"
 
 namespace kw {
@@ -104,6 +106,40 @@ struct SmemTable {
 __device__ __forceinline__ float2 tw_at(const float2 *__restrict__ tw, int i) { return __ldg(tw + i); }
 __device__ __forceinline__ float2 tw_at(const SmemTable &tw, int i) { return tw.p[i]; }
 
+// Per-stage twiddle table in shared memory for contiguous-line passes: the
+// multipliers of stage S >= 1 of plan (N, INV) at [off(S) + (t - 1) NS + k]
+// (k = butterfly index within its group of NS, t = 1 .. R-1), conjugated
+// already for an inverse plan.  Threads with consecutive k read consecutive
+// entries, where the shared N-entry table (index t k N / (NS R)) puts them
+// 2 t words apart and so into the same banks for even t.
+struct StageTable {
+    const float2 *p;
+};
+template <int N, bool INV>
+__host__ __device__ constexpr int stage_table_off(int S) {
+    int o = 0;
+    for (int s = 1; s < S; ++s) o += (RPlan<N, INV>::R(s) - 1) * RPlan<N, INV>::NS(s);
+    return o;
+}
+template <int N, bool INV> __host__ __device__ constexpr int stage_table_size() {
+    return stage_table_off<N, INV>(RPlan<N, INV>::M);
+}
+// fill the table of plan (N, INV) from the N-entry forward table tw (block-wide)
+template <int N, bool INV, int NT>
+__device__ __forceinline__ void stage_table_fill(float2 *dst, const float2 *__restrict__ tw) {
+    constexpr int M = RPlan<N, INV>::M;
+    for (int e = threadIdx.x; e < stage_table_size<N, INV>(); e += NT) {
+        int S = 1;
+        while (S + 1 < M && e >= stage_table_off<N, INV>(S + 1)) ++S;
+        const int NS = RPlan<N, INV>::NS(S), R = RPlan<N, INV>::R(S);
+        const int r = e - stage_table_off<N, INV>(S);
+        const int t = r / NS + 1, k = r % NS;
+        float2 w = __ldg(tw + t * k * (N / (NS * R)));
+        if (INV) w.y = -w.y;
+        dst[e] = w;
+    }
+}
+
 template <int N, int NL, bool IL, bool INV, int S, int NT, class TW, class Ld, class St>
 __device__ __forceinline__ void rs_stage(float2 *sm, const TW &tw, Ld &ld, St &st) {
     using P = RPlan<N, INV>;
@@ -131,8 +167,13 @@ __device__ __forceinline__ void rs_stage(float2 *sm, const TW &tw, Ld &ld, St &s
                 const int k = j % NS;
 #pragma unroll
                 for (int t = 1; t < R; ++t) {
-                    float2 w = tw_at(tw, t * k * TWS);
-                    if (INV) w.y = -w.y;
+                    float2 w;
+                    if constexpr (std::is_same<TW, StageTable>::value) {
+                        w = tw.p[stage_table_off<N, INV>(S) + (t - 1) * NS + k];
+                    } else {
+                        w = tw_at(tw, t * k * TWS);
+                        if (INV) w.y = -w.y;
+                    }
                     v[b][t] = cmul(v[b][t], w);
                 }
             }
@@ -350,7 +391,12 @@ __global__ void __launch_bounds__(ks_threads(N0, NL), (FAN ? 3 : 4) * kThreads /
     __shared__ float2 s_lm[3][NL];
     // per-x tables read on the transforms' dependency chains, kept in shared
     // memory: twiddles, k_x^2 and the x-derivative table of an axis-0 output
-    __shared__ float2 s_tw[N0], s_ddx[N0];
+    // stage twiddles: per-stage tables for contiguous lines of up to 256
+    // points (conflict-free reads), else the N0-entry table (512 points would
+    // take the static shared memory past 48 KB)
+    constexpr bool STAB = line_in_warp<N0, NL, NT, false>() && N0 <= 256;
+    __shared__ float2 s_tw[STAB ? 1 : N0], s_ddx[N0];
+    __shared__ float2 s_stf[STAB ? stage_table_size<N0, false>() : 1], s_sti[STAB ? stage_table_size<N0, true>() : 1];
     __shared__ float s_kx2[N0];
     // lines (y, kz) of kz planes kz0 .. kz0+nkz-1
     const int lines_total = (kz0 + nkz) * g.N1;
@@ -364,11 +410,16 @@ __global__ void __launch_bounds__(ks_threads(N0, NL), (FAN ? 3 : 4) * kThreads /
             ddx = ko == OP_GRAD_POS ? P.dd_pos[0] : (ko == OP_GRAD_NEG ? P.dd_neg[0] : P.sh_neg[0]);
     }
     for (int i = threadIdx.x; i < N0; i += NT) {
-        s_tw[i] = __ldg(tw + i);
+        if constexpr (!STAB) s_tw[i] = __ldg(tw + i);
         s_kx2[i] = __ldg(P.k2[0] + i);
         if (ddx) s_ddx[i] = __ldg(ddx + i);
     }
-    const SmemTable stw{s_tw};
+    if constexpr (STAB) {
+        stage_table_fill<N0, false, NT>(s_stf, tw);
+        stage_table_fill<N0, true, NT>(s_sti, tw);
+    }
+    using TT = std::conditional_t<STAB, StageTable, SmemTable>;
+    const TT twf{STAB ? s_stf : s_tw}, twi{STAB ? s_sti : s_tw};
     for (int l = threadIdx.x; l < NL; l += NT) {
         const int line = min(line0 + l, lines_total - 1);
         const int iy = line % g.N1, iz = line / g.N1;
@@ -393,7 +444,7 @@ __global__ void __launch_bounds__(ks_threads(N0, NL), (FAN ? 3 : 4) * kThreads /
     using SH = StageShape<N0, NL, false, RPlan<N0, false>::M - 1, NT>;   // forward last stage
     float2 spec[SH::MAXB][SH::R];
     auto keep = [&](int b, int t, int, int, float2 v) { spec[b][t] = v; };
-    rs_fft<N0, NL, false, false, 0, NT>(sm, stw, ld, keep);
+    rs_fft<N0, NL, false, false, 0, NT>(sm, twf, ld, keep);
 
     // common factor of the operator (kappa, |k|^e or cos), times 1/N
     const int kind0 = pick(ops.kind, f);
@@ -452,7 +503,7 @@ __global__ void __launch_bounds__(ks_threads(N0, NL), (FAN ? 3 : 4) * kThreads /
         auto st2 = [&](int, int, int l, int i, float2 v) {
             if (line0 + l < lines_total) out[l * N0 + i] = v;
         };
-        rs_fft<N0, NL, false, true, 0, NT>(sm, stw, ld2, st2);
+        rs_fft<N0, NL, false, true, 0, NT>(sm, twi, ld2, st2);
     }
     if (shared_mask) {
         // fanout == 2 (the 3-D gradient ahead of ks_ypass_fan): the shared
@@ -471,7 +522,7 @@ __global__ void __launch_bounds__(ks_threads(N0, NL), (FAN ? 3 : 4) * kThreads /
                 if (shared_mask & (1 << o))
                     (bufs.p[o] + (long long)line0 * N0)[l * N0 + i] = cmul(v, s_lm[o][l]);
         };
-        rs_fft<N0, NL, false, true, 0, NT>(sm, stw, ld3, st3);
+        rs_fft<N0, NL, false, true, 0, NT>(sm, twi, ld3, st3);
     }
 }
 
@@ -824,7 +875,7 @@ __global__ void __launch_bounds__(ks_threads(N2, PL), 2 * kThreads / ks_threads(
                 un = make_float2(0.5f * a.dt * ri.x * gr.x, 0.5f * a.dt * ri.y * gr.y);
             } else {
                 float2 pm;
-                if (ax == 0) pm = make_float2(__ldg(pmlv + xa), __ldg(pmlv + xa + 1));
+                if (ax == 0) pm = __ldg(reinterpret_cast<const float2 *>(pmlv + xa));   // xa even, N0 even
                 else if (ax == 1) pm = make_float2(pml_y, pml_y);
                 else { const float q = __ldg(pmlv + z); pm = make_float2(q, q); }
                 const float2 uo = s_u[slot(b, tt, l, z)];
@@ -1023,7 +1074,7 @@ __global__ void __launch_bounds__(ks_threads(N2, PL), 2 * kThreads / ks_threads(
                 const float2 ro = s_a[si];
                 const float2 coef = (a.nonlinear || r0arr) ? s_c[si] : make_float2(a.rho0.val, a.rho0.val);
                 float2 pm;
-                if (ax == 0) pm = make_float2(__ldg(pmlv + xa), __ldg(pmlv + xa + 1));
+                if (ax == 0) pm = __ldg(reinterpret_cast<const float2 *>(pmlv + xa));   // xa even, N0 even
                 else if (ax == 1) pm = make_float2(pml_y, pml_y);
                 else { const float q = __ldg(pmlv + z); pm = make_float2(q, q); }
                 float2 rn;
