@@ -38,10 +38,15 @@ kw_status ypass_fan(kw_plan *P, Spec4 bufs, dim3 grid, int kz0, const float2 *dd
 
 template <int N, int NL>
 kw_status xpass(kw_plan *P, Spec4 bufs, OpSet ops, int fanout, int kz0, int nkz, dim3 grid) {
-    if (fanout)
-        ks_xpass<N, NL, true><<<grid, ks_threads(N, NL), 0, P->stream>>>(bufs, P->g, P->tw[0], P->op, ops, fanout, kz0, nkz);
+    // fanout 2 is the 3-D gradient's (three outputs along x, y, z)
+    if (fanout == 2) {
+        if (!(ops.n == 3 && ops.axis[0] == 0 && ops.axis[1] == 1 && ops.axis[2] == 2))
+            return fail(KW_ERR_INVALID, "internal: the gradient fan-out x-pass needs outputs along x, y and z");
+        ks_xpass<N, NL, 2><<<grid, ks_threads(N, NL), 0, P->stream>>>(bufs, P->g, P->tw[0], P->op, ops, 2, kz0, nkz);
+    } else if (fanout)
+        ks_xpass<N, NL, 1><<<grid, ks_threads(N, NL), 0, P->stream>>>(bufs, P->g, P->tw[0], P->op, ops, fanout, kz0, nkz);
     else
-        ks_xpass<N, NL, false><<<grid, ks_threads(N, NL), 0, P->stream>>>(bufs, P->g, P->tw[0], P->op, ops, 0, kz0, nkz);
+        ks_xpass<N, NL, 0><<<grid, ks_threads(N, NL), 0, P->stream>>>(bufs, P->g, P->tw[0], P->op, ops, 0, kz0, nkz);
     return KW_OK;
 }
 

@@ -373,16 +373,68 @@ __global__ void __launch_bounds__(ks_threads(N1, TY), (4 * kThreads + ks_threads
 // ---------------------------------------------------------------------------
 // x-pass: forward C2C along axis 0, operator, inverse C2C, in place.
 // grid = (ceil(N1*N2h/NL), 1, fanout ? 1 : nfields), ks_threads(N0, NL) threads.
-// FAN: the fan-out variant (fanout 1 or 2), which keeps the forward spectrum
-// in registers across two or more inverse transforms, at three blocks per SM;
-// the single-output variant (fanout 0) fits four.
+// FAN: 0 the single-output variant (four blocks per SM); 1 the general
+// fan-out (ops.n outputs from one forward transform, kept in registers across
+// the inverse transforms); 2 the fan-out of the 3-D gradient ahead of
+// ks_ypass_fan (output 0 along x with its own inverse transform, outputs 1
+// and 2 sharing one stored unscaled in bufs.p[1]).  The fan-out variants run
+// three blocks per SM.  The operator class and, for FAN 0 and 2, the inverse
+// transform's input multiplier are chosen once per block, outside the
+// per-value loops.
 // ---------------------------------------------------------------------------
-template <int N0, int NL, bool FAN>
+
+// operator classes of the x-pass's common factor (times 1/N)
+enum { XOP_ONE = 0, XOP_SINC = 1, XOP_NABLA = 2, XOP_COS = 3 };
+
+__device__ __forceinline__ int xop_class(int kind, int use_kspace) {
+    if (kind == OP_GRAD_POS || kind == OP_GRAD_NEG) return use_kspace ? XOP_SINC : XOP_ONE;
+    if (kind == OP_NABLA1 || kind == OP_NABLA2) return XOP_NABLA;
+    if (kind == OP_SRC_KAPPA) return use_kspace ? XOP_COS : XOP_ONE;
+    return XOP_ONE;
+}
+
+// spec <- spec * fac(k) / N for the values this thread holds after the
+// forward transform's last stage
+template <int N0, int NL, int NT, int CLS, class SPEC>
+__device__ __forceinline__ void xpass_operator(SPEC &spec, const OpParams &P, int kind0, const float *s_kx2,
+                                               const float *kyz2, int line0, int lines_total) {
+    using SH = StageShape<N0, NL, false, RPlan<N0, false>::M - 1, NT>;
+    constexpr bool LW = line_in_warp<N0, NL, NT, false>();
+    constexpr int NSL = RPlan<N0, false>::NS(RPlan<N0, false>::M - 1);
+#pragma unroll
+    for (int b = 0; b < SH::MAXB; ++b) {
+        const int gg = threadIdx.x + b * NT;
+        if (!(LW || SH::TOT % NT == 0 || gg < SH::TOT)) continue;
+        int l, j;
+        bslot<SH::NB, NL, false, NT, LW>(b, l, j);
+        const float ky = kyz2[l];
+#pragma unroll
+        for (int t = 0; t < SH::R; ++t) {
+            const int ix = j + t * NSL;
+            const float k2 = s_kx2[ix] + ky;
+            float fac;
+            if constexpr (CLS == XOP_SINC) {
+                fac = sinc_series(P.kappa_a * P.kappa_a * k2);
+            } else if constexpr (CLS == XOP_NABLA) {
+                const float e = kind0 == OP_NABLA1 ? P.nabla1_exp : P.nabla2_exp;
+                fac = k2 == 0.f ? (e > 0.f ? 0.f : (e == 0.f ? 1.f : 0.f)) : pow_pos(k2, 0.5f * e);
+                if (P.filt) fac *= __ldg(P.filt + (long long)min(line0 + l, lines_total - 1) * N0 + ix);
+            } else if constexpr (CLS == XOP_COS) {
+                fac = cos_series(P.kappa_a * P.kappa_a * k2);
+            } else {
+                fac = 1.f;
+            }
+            spec[b][t] = cscale(spec[b][t], fac * P.scale);
+        }
+    }
+}
+
+template <int N0, int NL, int FAN>
 __global__ void __launch_bounds__(ks_threads(N0, NL), (FAN ? 3 : 4) * kThreads / ks_threads(N0, NL))
     ks_xpass(Spec4 bufs, Geom g, const float2 *__restrict__ tw, OpParams P, OpSet ops, int fanout_arg, int kz0,
              int nkz) {
     constexpr int NT = ks_threads(N0, NL);
-    const int fanout = FAN ? fanout_arg : 0;
+    const int fanout = FAN == 0 ? 0 : (FAN == 2 ? 2 : fanout_arg);
     static_assert(RPlan<N0, false>::M >= 2, "in-place pass needs two stages");
     __shared__ float2 sm[NL * Padded<N0>::LS];
     __shared__ float kyz2[NL];
@@ -390,8 +442,8 @@ __global__ void __launch_bounds__(ks_threads(N0, NL), (FAN ? 3 : 4) * kThreads /
     // or z (constant along an x line); 1 for the others
     __shared__ float2 s_lm[3][NL];
     // per-x tables read on the transforms' dependency chains, kept in shared
-    // memory: twiddles, k_x^2 and the x-derivative table of an axis-0 output
-    // stage twiddles: per-stage tables for contiguous lines of up to 256
+    // memory: twiddles, k_x^2 and the x-derivative table of an axis-0 output.
+    // Stage twiddles: per-stage tables for contiguous lines of up to 256
     // points (conflict-free reads), else the N0-entry table (512 points would
     // take the static shared memory past 48 KB)
     constexpr bool STAB = line_in_warp<N0, NL, NT, false>() && N0 <= 256;
@@ -448,81 +500,79 @@ __global__ void __launch_bounds__(ks_threads(N0, NL), (FAN ? 3 : 4) * kThreads /
 
     // common factor of the operator (kappa, |k|^e or cos), times 1/N
     const int kind0 = pick(ops.kind, f);
-    const bool grad = kind0 == OP_GRAD_POS || kind0 == OP_GRAD_NEG;
-#pragma unroll
-    for (int b = 0; b < SH::MAXB; ++b) {
-        constexpr bool LW = line_in_warp<N0, NL, NT, false>();
-        const int gg = threadIdx.x + b * NT;
-        if (!(LW || SH::TOT % NT == 0 || gg < SH::TOT)) continue;
-        int l, j;
-        bslot<SH::NB, NL, false, NT, LW>(b, l, j);
-        const float ky = kyz2[l];
-        constexpr int NSL = RPlan<N0, false>::NS(RPlan<N0, false>::M - 1);
-#pragma unroll
-        for (int t = 0; t < SH::R; ++t) {
-            const int ix = j + t * NSL;
-            const float k2 = s_kx2[ix] + ky;
-            float fac;
-            if (grad) {
-                fac = P.use_kspace ? sinc_series(P.kappa_a * P.kappa_a * k2) : 1.f;
-            } else if (kind0 == OP_NABLA1 || kind0 == OP_NABLA2) {
-                const float e = kind0 == OP_NABLA1 ? P.nabla1_exp : P.nabla2_exp;
-                fac = k2 == 0.f ? (e > 0.f ? 0.f : (e == 0.f ? 1.f : 0.f)) : pow_pos(k2, 0.5f * e);
-                if (P.filt) fac *= __ldg(P.filt + (long long)min(line0 + l, lines_total - 1) * N0 + ix);
-            } else if (kind0 == OP_SRC_KAPPA) {
-                fac = P.use_kspace ? cos_series(P.kappa_a * P.kappa_a * k2) : 1.f;
-            } else {
-                fac = 1.f;
-            }
-            spec[b][t] = cscale(spec[b][t], fac * P.scale);
-        }
+    switch (xop_class(kind0, P.use_kspace)) {
+    case XOP_SINC: xpass_operator<N0, NL, NT, XOP_SINC>(spec, P, kind0, s_kx2, kyz2, line0, lines_total); break;
+    case XOP_NABLA: xpass_operator<N0, NL, NT, XOP_NABLA>(spec, P, kind0, s_kx2, kyz2, line0, lines_total); break;
+    case XOP_COS: xpass_operator<N0, NL, NT, XOP_COS>(spec, P, kind0, s_kx2, kyz2, line0, lines_total); break;
+    default: xpass_operator<N0, NL, NT, XOP_ONE>(spec, P, kind0, s_kx2, kyz2, line0, lines_total); break;
     }
-    // An output whose operator table runs along x gets its own inverse
-    // transform.  Every other output is the inverse transform of spec times a
-    // constant per x line (s_lm), so in fan-out mode they share one inverse
-    // transform and are scaled as they are stored.
-    const int nout = fanout ? ops.n : 1;
-    int shared_mask = 0;
-    for (int o = 0; o < nout; ++o) {
-        const int oi = fanout ? o : f;
-        const int axis = pick(ops.axis, oi);
-        const int ko = pick(ops.kind, oi);
-        const float2 *dd = ko == OP_GRAD_POS ? pick(P.dd_pos, axis)
-                                             : (ko == OP_GRAD_NEG ? pick(P.dd_neg, axis) : pick(P.sh_neg, axis));
-        const bool mul_dd = ko == OP_GRAD_POS || ko == OP_GRAD_NEG || ko == OP_SHIFT_NEG;
-        if (fanout && !(mul_dd && axis == 0)) {
-            shared_mask |= 1 << o;
-            continue;
-        }
-        float2 *out = pick(bufs.p, oi) + (long long)line0 * N0;
-        auto ld2 = [&](int b, int t, int l, int i) -> float2 {
-            if (!mul_dd) return spec[b][t];
-            if (axis != 0) return cmul(spec[b][t], s_lm[oi][l]);
-            return cmul(spec[b][t], dd == ddx ? s_ddx[i] : __ldg(dd + i));
-        };
-        auto st2 = [&](int, int, int l, int i, float2 v) {
+    auto store_to = [&](float2 *outb) {
+        float2 *out = outb + (long long)line0 * N0;
+        return [=](int, int, int l, int i, float2 v) {
             if (line0 + l < lines_total) out[l * N0 + i] = v;
         };
-        rs_fft<N0, NL, false, true, 0, NT>(sm, twi, ld2, st2);
-    }
-    if (shared_mask) {
-        // fanout == 2 (the 3-D gradient ahead of ks_ypass_fan): the shared
-        // transform is stored once, unscaled, to the first shared output; the
-        // inverse y-pass applies the y and z multipliers
-        const int first = __ffs(shared_mask) - 1;
-        auto ld3 = [&](int b, int t, int, int) -> float2 { return spec[b][t]; };
-        auto st3 = [&](int, int, int l, int i, float2 v) {
-            if (line0 + l >= lines_total) return;
-            if (fanout == 2) {
-                (pick(bufs.p, first) + (long long)line0 * N0)[l * N0 + i] = v;
-                return;
+    };
+    auto plain = [&](int b, int t, int, int) -> float2 { return spec[b][t]; };
+    auto by_ddx = [&](int b, int t, int, int i) -> float2 { return cmul(spec[b][t], s_ddx[i]); };
+
+    if constexpr (FAN == 2) {
+        // output 0: its own inverse transform of spec dd_x(k_x); outputs 1
+        // and 2: one inverse transform of spec, stored unscaled to bufs.p[1]
+        // (the inverse y-pass applies their y and z multipliers)
+        auto st0 = store_to(bufs.p[0]);
+        rs_fft<N0, NL, false, true, 0, NT>(sm, twi, by_ddx, st0);
+        auto st1 = store_to(bufs.p[1]);
+        rs_fft<N0, NL, false, true, 0, NT>(sm, twi, plain, st1);
+    } else if constexpr (FAN == 0) {
+        const int axis = pick(ops.axis, f);
+        const bool mul_dd = kind0 == OP_GRAD_POS || kind0 == OP_GRAD_NEG || kind0 == OP_SHIFT_NEG;
+        auto st = store_to(pick(bufs.p, f));
+        if constexpr (!line_in_warp<N0, NL, NT, false>()) {
+            // other lengths (several butterflies of different lines per
+            // thread) keep one inverse with the choice made per value: their
+            // registers are already near the limit
+            auto ld2 = [&](int b, int t, int l, int i) -> float2 {
+                if (!mul_dd) return spec[b][t];
+                if (axis != 0) return cmul(spec[b][t], s_lm[f][l]);
+                return cmul(spec[b][t], s_ddx[i]);
+            };
+            rs_fft<N0, NL, false, true, 0, NT>(sm, twi, ld2, st);
+        } else if (!mul_dd) {
+            rs_fft<N0, NL, false, true, 0, NT>(sm, twi, plain, st);
+        } else {
+            // multiplier dd_x(k_x) (axis 0) or the line's constant (axis 1, 2)
+            const float2 *tab = axis == 0 ? s_ddx : s_lm[f];
+            const int xs = axis == 0 ? 1 : 0, ls = axis == 0 ? 0 : 1;
+            auto by_tab = [&](int b, int t, int l, int i) -> float2 { return cmul(spec[b][t], tab[i * xs + l * ls]); };
+            rs_fft<N0, NL, false, true, 0, NT>(sm, twi, by_tab, st);
+        }
+    } else {
+        // FAN == 1.  An output whose operator table runs along x gets its own
+        // inverse transform.  Every other output is the inverse transform of
+        // spec times a constant per x line (s_lm): they share one inverse
+        // transform and are scaled as they are stored.
+        int shared_mask = 0;
+        for (int o = 0; o < ops.n; ++o) {
+            const int axis = pick(ops.axis, o);
+            const int ko = pick(ops.kind, o);
+            const bool mul_dd = ko == OP_GRAD_POS || ko == OP_GRAD_NEG || ko == OP_SHIFT_NEG;
+            if (!(mul_dd && axis == 0)) {
+                shared_mask |= 1 << o;
+                continue;
             }
+            auto st2 = store_to(pick(bufs.p, o));
+            rs_fft<N0, NL, false, true, 0, NT>(sm, twi, by_ddx, st2);
+        }
+        if (shared_mask) {
+            auto st3 = [&](int, int, int l, int i, float2 v) {
+                if (line0 + l >= lines_total) return;
 #pragma unroll
-            for (int o = 0; o < 3; ++o)
-                if (shared_mask & (1 << o))
-                    (bufs.p[o] + (long long)line0 * N0)[l * N0 + i] = cmul(v, s_lm[o][l]);
-        };
-        rs_fft<N0, NL, false, true, 0, NT>(sm, twi, ld3, st3);
+                for (int o = 0; o < 3; ++o)
+                    if (shared_mask & (1 << o))
+                        (bufs.p[o] + (long long)line0 * N0)[l * N0 + i] = cmul(v, s_lm[o][l]);
+            };
+            rs_fft<N0, NL, false, true, 0, NT>(sm, twi, plain, st3);
+        }
     }
 }
 
