@@ -611,6 +611,35 @@ __device__ __forceinline__ float2 zpack_load(const float2 *__restrict__ H, const
     return make_float2(A.x - B.y, A.y + B.x);
 }
 
+// Rows kz = 0 .. N2/2 of the z-half spectra of the tile's packed lines
+// (packed layout z*PL + l in s), unpacked into the two real columns' spectra
+// as zstore_r2c does and stored as one 16-byte pair per (row, line).  Thread
+// q keeps line q % PL and takes rows q / PL + it KS (KS = NT / PL rows per
+// sweep), so its column and row stride are fixed and only the last sweep is
+// partial.  N0 is even on this path: a pair is in range whole or not at all.
+template <int N2, int PL>
+__device__ __forceinline__ void zstore_r2c_tile(const float2 *s, float2 *__restrict__ H, const Geom &g, int x0, int y) {
+    constexpr int NT = ZTile<N2, PL>::NT, ROWS = N2 / 2 + 1;
+    static_assert(NT % PL == 0, "whole rows per sweep");
+    constexpr int KS = NT / PL, SWEEPS = (ROWS + KS - 1) / KS;
+    const int l = threadIdx.x % PL, k0 = threadIdx.x / PL;
+    const int xa = x0 + 2 * l;
+    if (xa >= g.N0) return;
+    float2 *h = H + ((long long)k0 * g.N1 + y) * g.N0 + xa;
+    const long long step = (long long)KS * g.N1 * g.N0;
+#pragma unroll
+    for (int it = 0; it < SWEEPS; ++it) {
+        const int k = k0 + it * KS;
+        if ((it + 1) * KS > ROWS && k >= ROWS) break;
+        const float2 Zk = s[k * PL + l];
+        const int nk = k == 0 ? 0 : N2 - k;
+        const float2 Zn = s[nk * PL + l];
+        const float2 A = make_float2(0.5f * (Zk.x + Zn.x), 0.5f * (Zk.y - Zn.y));
+        const float2 B = make_float2(0.5f * (Zk.y + Zn.y), -0.5f * (Zk.x - Zn.x));
+        *reinterpret_cast<float4 *>(h + it * step) = make_float4(A.x, A.y, B.x, B.y);
+    }
+}
+
 // forward transform of the hand-off registers, then unpack and store the
 // z-half spectrum (two real columns per packed line)
 template <int N2, int PL, class Hold>
@@ -636,7 +665,7 @@ __device__ __forceinline__ void zforward_store(float2 *sm, const float2 *__restr
         for (int t = 0; t < SL::R; ++t) sm[outi[b] + t * NSL * PL] = outv[b][t];
     }
     __syncthreads();
-    zstore_r2c<N2, PL>(sm, H, g, x0, y, PL);
+    zstore_r2c_tile<N2, PL>(sm, H, g, x0, y);
 }
 
 // write hand-off registers into the tile (packed layout z*PL + l)
@@ -800,17 +829,26 @@ __device__ __forceinline__ void zraw_prefetch(float2 *raw, const float2 *__restr
     }
 }
 // packed C2R input (as zpack_load) from prefetched raw rows
+// Element z = j + t NB (0 <= j < NB) of the inverse transform's first stage:
+// for all but at most two values of t (constants once the stage loop is
+// unrolled) the row's half and the DC / Nyquist tests are known without z.
 template <int N2, int PL>
-__device__ __forceinline__ float2 zpack_raw(const float2 *raw, const Geom &g, int x0, int l, int z) {
+__device__ __forceinline__ float2 zpack_raw(const float2 *raw, const Geom &g, int x0, int l, int z, int t) {
     constexpr int TX = 2 * PL, N2h = N2 / 2 + 1;
-    int k = z;
-    bool cj = false;
-    if (z >= N2h) { k = N2 - z; cj = true; }
+    constexpr int NB = N2 / RPlan<N2, true>::R(0);
+    const int zlo = t * NB, zhi = t * NB + NB - 1;
+    bool cj;
+    if (zhi < N2h) cj = false;
+    else if (zlo >= N2h) cj = true;
+    else cj = z >= N2h;
+    const int k = cj ? N2 - z : z;
     if (x0 + 2 * l >= g.N0) return make_float2(0.f, 0.f);
     const float4 q = *reinterpret_cast<const float4 *>(raw + k * TX + 2 * l);
     float2 A = make_float2(q.x, q.y), B = make_float2(q.z, q.w);
     if (cj) { A.y = -A.y; B.y = -B.y; }
-    if (k == 0 || 2 * k == N2) { A.y = 0.f; B.y = 0.f; }
+    // k == 0 (z == 0) or 2 k == N2 (z == N2 / 2): the Hermitian part is real
+    const bool edge = (zlo == 0 && z == 0) || (N2 % 2 == 0 && zlo <= N2 / 2 && N2 / 2 <= zhi && z == N2 / 2);
+    if (edge) { A.y = 0.f; B.y = 0.f; }
     return make_float2(A.x - B.y, A.y + B.x);
 }
 
@@ -879,7 +917,7 @@ __global__ void __launch_bounds__(ks_threads(N2, PL), 2 * kThreads / ks_threads(
             }
         }
         mbar_wait(&bars[0], 0, m.err);
-        auto ld = [&](int, int, int l, int z) -> float2 { return zpack_raw<N2, PL>(sm, g, x0, l, z); };
+        auto ld = [&](int, int t, int l, int z) -> float2 { return zpack_raw<N2, PL>(sm, g, x0, l, z, t); };
         auto st = [&](int b, int tt, int, int, float2 v) { hold[b][tt] = v; };
         rs_fft<N2, PL, true, true, 0, NT>(sm, tw, ld, st);
         if (any_field) mbar_wait(&bars[1], 0, m.err);
@@ -1074,7 +1112,7 @@ __global__ void __launch_bounds__(ks_threads(N2, PL), 2 * kThreads / ks_threads(
             else cp_async_wait_group<1>();   // rows_i landed; rho_i may be in flight
             __syncthreads();                 // the prefetched rows of every thread are in the tile
         }
-        auto ld = [&](int, int, int l, int z) -> float2 { return zpack_raw<N2, PL>(sm, g, x0, l, z); };
+        auto ld = [&](int, int t, int l, int z) -> float2 { return zpack_raw<N2, PL>(sm, g, x0, l, z, t); };
         auto st = [&](int b, int tt, int, int, float2 v) { hold[b][tt] = v; };
         rs_fft<N2, PL, true, true, 0, NT>(sm, tw, ld, st);
         if constexpr (TMA) {
@@ -1368,7 +1406,7 @@ __global__ void __launch_bounds__(ks_threads(N2, PL), 2 * kThreads / ks_threads(
             else cp_async_wait_group<1>();   // rows_1 landed; p may be in flight
             __syncthreads();                 // the prefetched rows of every thread are in the tile
         }
-        auto ld = [&](int, int, int l, int z) -> float2 { return zpack_raw<N2, PL>(sm, g, x0, l, z); };
+        auto ld = [&](int, int t, int l, int z) -> float2 { return zpack_raw<N2, PL>(sm, g, x0, l, z, t); };
         auto st = [&](int b, int tt, int, int, float2 v) { hold[b][tt] = v; };
         rs_fft<N2, PL, true, true, 0, NT>(sm, tw, ld, st);
         if (k + 1 < nterm) {
