@@ -296,7 +296,7 @@ typedef struct kw_server_config {
     int32_t  device;             /* CUDA device ordinal */
     uint64_t hbm_budget_bytes;   /* admission budget; 0 = 80% of free memory */
     int32_t  max_active;         /* simulations resident at once; 0 = 32 */
-    int32_t  steps_per_slice;    /* steps issued per simulation per round; 0 = 32 */
+    int32_t  steps_per_slice;    /* steps issued per simulation per round; 0 = 64 */
     /* Watchdog: a request still running this many milliseconds after its
        admission is stopped -- no further steps are issued, the work already
        issued drains, its memory and slot are released -- and its waiter gets

@@ -230,6 +230,17 @@ __device__ __forceinline__ bool hand_pos(int b, int t, int &l, int &i) {
     return true;
 }
 
+// (line, first element) of hand-off slot b: element (b, t) is element
+// j + t * NB of line l (hand_pos)
+template <int N, int NL, bool IL, int NT = kThreads>
+__device__ __forceinline__ bool hand_line(int b, int &l, int &j) {
+    using SH = HandShape<N, NL, NT>;
+    const int g = threadIdx.x + b * NT;
+    if (!(SH::TOT % NT == 0 || g < SH::TOT)) return false;
+    bmap<SH::NB, NL, IL>(g, l, j);
+    return true;
+}
+
 // sinc(a) = sin(a)/a and cos(a) from their Taylor series in a^2 (Horner form).
 // The k-space argument is a = c_ref |k| dt / 2 <= (CFL c_ref / c_max) pi sqrt(3) / 2,
 // below 2.8 for any CFL <= 1; the first omitted terms (a^16/17! and
@@ -947,25 +958,34 @@ __global__ void __launch_bounds__(ks_threads(N2, PL), 2 * kThreads / ks_threads(
     float dscale = 0.f;
     const bool dense = dense_active(a.dense[f], t, dscale);
     const float pml_y = ax == 1 ? __ldg(pmlv + y) : 1.f;
+    // cell index of element (b, t): that of its first row plus t row strides
+    const long long dz = (long long)g.N0 * g.N1 * SH::NB;
 #pragma unroll
-    for (int b = 0; b < SH::MAXB; ++b)
+    for (int b = 0; b < SH::MAXB; ++b) {
+        int l, j;
+        if (!hand_line<N2, PL, true, NT>(b, l, j)) continue;
+        const int xa = x0 + 2 * l;
+        if (xa >= g.N0) {
+#pragma unroll
+            for (int tt = 0; tt < SH::R; ++tt) hold[b][tt] = make_float2(0.f, 0.f);
+            continue;
+        }
+        // the x and y PML factors are constant along this thread's line
+        const float2 pmc = ax == 0 ? __ldg(reinterpret_cast<const float2 *>(pmlv + xa))   // xa even, N0 even
+                                   : make_float2(pml_y, pml_y);
+        const long long gi0 = xa + (long long)g.N0 * (y + (long long)g.N1 * j);
 #pragma unroll
         for (int tt = 0; tt < SH::R; ++tt) {
-            int l, z;
-            if (!hand_pos<N2, PL, true, NT>(b, tt, l, z)) continue;
-            const int xa = x0 + 2 * l;
-            if (xa >= g.N0) { hold[b][tt] = make_float2(0.f, 0.f); continue; }
-            const long long gi = xa + (long long)g.N0 * (y + (long long)g.N1 * z);
+            const int z = j + tt * SH::NB;
+            const long long gi = gi0 + tt * dz;
             const float2 gr = hold[b][tt];
             const float2 ri = rsi.arr ? s_r[slot(b, tt, l, z)] : make_float2(rsi.val, rsi.val);
             float2 un;
             if (a.init) {
                 un = make_float2(0.5f * a.dt * ri.x * gr.x, 0.5f * a.dt * ri.y * gr.y);
             } else {
-                float2 pm;
-                if (ax == 0) pm = __ldg(reinterpret_cast<const float2 *>(pmlv + xa));   // xa even, N0 even
-                else if (ax == 1) pm = make_float2(pml_y, pml_y);
-                else { const float q = __ldg(pmlv + z); pm = make_float2(q, q); }
+                float2 pm = pmc;
+                if (ax == 2) { const float q = __ldg(pmlv + z); pm = make_float2(q, q); }
                 const float2 uo = s_u[slot(b, tt, l, z)];
                 un.x = pm.x * (pm.x * uo.x - a.dt * ri.x * gr.x);
                 un.y = pm.y * (pm.y * uo.y - a.dt * ri.y * gr.y);
@@ -978,6 +998,7 @@ __global__ void __launch_bounds__(ks_threads(N2, PL), 2 * kThreads / ks_threads(
             *reinterpret_cast<float2 *>(uout + gi) = un;
             hold[b][tt] = un;
         }
+    }
     if (a.init || !a.write_spec) return;
     if (a.sparse.off && a.sparse.sig[f] && t <= a.sparse.T[f]) {
         const int tile = blockIdx.x + gridDim.x * blockIdx.y;
@@ -1148,15 +1169,19 @@ __global__ void __launch_bounds__(ks_threads(N2, PL), 2 * kThreads / ks_threads(
         const float *pmlv = a.pml[ax];
         const float pml_y = ax == 1 ? __ldg(pmlv + y) : 1.f;
         float *rout = a.rho_out[i];
+        // cell index of element (b, t): that of its first row plus t row strides
+        const long long dz = (long long)g.N0 * g.N1 * SH::NB;
 #pragma unroll
-        for (int b = 0; b < SH::MAXB; ++b)
+        for (int b = 0; b < SH::MAXB; ++b) {
+            int l, j;
+            if (!hand_line<N2, PL, true, NT>(b, l, j)) continue;
+            const int xa = x0 + 2 * l;
+            if (xa >= g.N0) continue;
+            const long long gi0 = xa + (long long)g.N0 * (y + (long long)g.N1 * j);
 #pragma unroll
             for (int tt = 0; tt < SH::R; ++tt) {
-                int l, z;
-                if (!hand_pos<N2, PL, true, NT>(b, tt, l, z)) continue;
-                const int xa = x0 + 2 * l;
-                if (xa >= g.N0) continue;
-                const long long gi = xa + (long long)g.N0 * (y + (long long)g.N1 * z);
+                const int z = j + tt * SH::NB;
+                const long long gi = gi0 + tt * dz;
                 const int si = slot(b, tt, l, z);
                 const float2 du = hold[b][tt];
                 const float2 ro = s_a[si];
@@ -1179,6 +1204,7 @@ __global__ void __launch_bounds__(ks_threads(N2, PL), 2 * kThreads / ks_threads(
                 acc_d[b][tt].x += du.x;
                 acc_d[b][tt].y += du.y;
             }
+        }
         // cp.async: every thread reads only its own slots, so the next
         // component (or, after the last one, c0 for the equation of state) is
         // staged into the same slice right away; TMA rewrites the whole slice,
