@@ -101,6 +101,9 @@ struct OpParams {
     const float *k2[3];        // k_i^2 per axis, FFT order
     float kappa_a;             // c_ref * dt / 2
     int use_kspace;
+    // kappa_a^2 max |k|^2 <= 1: the k-space series to a^10 are exact to FP32
+    // (first omitted terms a^12 / 13! and a^12 / 12! below 2.1e-9)
+    int short_series;
     float nabla1_exp, nabla2_exp;  // alpha_power - 2, alpha_power - 1
     float scale;               // 1 / (N0 N1 N2)
     // medium.alpha_filter on the z-half spectrum (Hermitian part, FFT order,

@@ -257,6 +257,26 @@ __device__ __forceinline__ float sinc_series(float a2) {
     r = fmaf(r, a2, 1.0f);                        // n = 0
     return r;
 }
+// The same series to a^10, for plans with a^2 <= 1 (OpParams::short_series):
+// the first omitted terms, a^12 / 13! and a^12 / 12!, are then below 2.1e-9.
+__device__ __forceinline__ float sinc_series_short(float a2) {
+    float r = -1.0f / 39916800.0f;                // n = 5: -1/11!
+    r = fmaf(r, a2, 1.0f / 362880.0f);            // n = 4: +1/9!
+    r = fmaf(r, a2, -1.0f / 5040.0f);             // n = 3: -1/7!
+    r = fmaf(r, a2, 1.0f / 120.0f);               // n = 2: +1/5!
+    r = fmaf(r, a2, -1.0f / 6.0f);                // n = 1: -1/3!
+    r = fmaf(r, a2, 1.0f);                        // n = 0
+    return r;
+}
+__device__ __forceinline__ float cos_series_short(float a2) {
+    float r = -1.0f / 3628800.0f;                 // n = 5: -1/10!
+    r = fmaf(r, a2, 1.0f / 40320.0f);             // n = 4: +1/8!
+    r = fmaf(r, a2, -1.0f / 720.0f);              // n = 3: -1/6!
+    r = fmaf(r, a2, 1.0f / 24.0f);                // n = 2: +1/4!
+    r = fmaf(r, a2, -0.5f);                       // n = 1: -1/2!
+    r = fmaf(r, a2, 1.0f);                        // n = 0
+    return r;
+}
 __device__ __forceinline__ float cos_series(float a2) {
     // cos(a) = sum_n (-1)^n a^(2n) / (2n)!, n = 0..8
     float r = 1.0f / 20922789888000.0f;           // n = 8: +1/16!
@@ -394,13 +414,15 @@ __global__ void __launch_bounds__(ks_threads(N1, TY), (4 * kThreads + ks_threads
 // per-value loops.
 // ---------------------------------------------------------------------------
 
-// operator classes of the x-pass's common factor (times 1/N)
-enum { XOP_ONE = 0, XOP_SINC = 1, XOP_NABLA = 2, XOP_COS = 3 };
+// operator classes of the x-pass's common factor (times 1/N); the _SHORT
+// forms take the shorter k-space series (OpParams::short_series)
+enum { XOP_ONE = 0, XOP_SINC = 1, XOP_NABLA = 2, XOP_COS = 3, XOP_SINC_SHORT = 4, XOP_COS_SHORT = 5 };
 
-__device__ __forceinline__ int xop_class(int kind, int use_kspace) {
-    if (kind == OP_GRAD_POS || kind == OP_GRAD_NEG) return use_kspace ? XOP_SINC : XOP_ONE;
+__device__ __forceinline__ int xop_class(int kind, const OpParams &P) {
+    if (kind == OP_GRAD_POS || kind == OP_GRAD_NEG)
+        return P.use_kspace ? (P.short_series ? XOP_SINC_SHORT : XOP_SINC) : XOP_ONE;
     if (kind == OP_NABLA1 || kind == OP_NABLA2) return XOP_NABLA;
-    if (kind == OP_SRC_KAPPA) return use_kspace ? XOP_COS : XOP_ONE;
+    if (kind == OP_SRC_KAPPA) return P.use_kspace ? (P.short_series ? XOP_COS_SHORT : XOP_COS) : XOP_ONE;
     return XOP_ONE;
 }
 
@@ -426,6 +448,10 @@ __device__ __forceinline__ void xpass_operator(SPEC &spec, const OpParams &P, in
             float fac;
             if constexpr (CLS == XOP_SINC) {
                 fac = sinc_series(P.kappa_a * P.kappa_a * k2);
+            } else if constexpr (CLS == XOP_SINC_SHORT) {
+                fac = sinc_series_short(P.kappa_a * P.kappa_a * k2);
+            } else if constexpr (CLS == XOP_COS_SHORT) {
+                fac = cos_series_short(P.kappa_a * P.kappa_a * k2);
             } else if constexpr (CLS == XOP_NABLA) {
                 const float e = kind0 == OP_NABLA1 ? P.nabla1_exp : P.nabla2_exp;
                 fac = k2 == 0.f ? (e > 0.f ? 0.f : (e == 0.f ? 1.f : 0.f)) : pow_pos(k2, 0.5f * e);
@@ -511,8 +537,14 @@ __global__ void __launch_bounds__(ks_threads(N0, NL), (FAN ? 3 : 4) * kThreads /
 
     // common factor of the operator (kappa, |k|^e or cos), times 1/N
     const int kind0 = pick(ops.kind, f);
-    switch (xop_class(kind0, P.use_kspace)) {
+    switch (xop_class(kind0, P)) {
     case XOP_SINC: xpass_operator<N0, NL, NT, XOP_SINC>(spec, P, kind0, s_kx2, kyz2, line0, lines_total); break;
+    case XOP_SINC_SHORT:
+        xpass_operator<N0, NL, NT, XOP_SINC_SHORT>(spec, P, kind0, s_kx2, kyz2, line0, lines_total);
+        break;
+    case XOP_COS_SHORT:
+        xpass_operator<N0, NL, NT, XOP_COS_SHORT>(spec, P, kind0, s_kx2, kyz2, line0, lines_total);
+        break;
     case XOP_NABLA: xpass_operator<N0, NL, NT, XOP_NABLA>(spec, P, kind0, s_kx2, kyz2, line0, lines_total); break;
     case XOP_COS: xpass_operator<N0, NL, NT, XOP_COS>(spec, P, kind0, s_kx2, kyz2, line0, lines_total); break;
     default: xpass_operator<N0, NL, NT, XOP_ONE>(spec, P, kind0, s_kx2, kyz2, line0, lines_total); break;
@@ -1488,23 +1520,26 @@ __global__ void __launch_bounds__(ks_threads(N2, PL), 2 * kThreads / ks_threads(
     } else {
         cp_async_wait_all();
     }
+    const long long dz = (long long)g.N0 * g.N1 * SH::NB;
 #pragma unroll
-    for (int b = 0; b < SH::MAXB; ++b)
+    for (int b = 0; b < SH::MAXB; ++b) {
+        int l, j;
+        if (!hand_line<N2, PL, true, NT>(b, l, j)) continue;
+        const int xa = x0 + 2 * l;
+        const long long gi0 = xa + (long long)g.N0 * (y + (long long)g.N1 * j);
 #pragma unroll
         for (int tt = 0; tt < SH::R; ++tt) {
-            int l, z;
-            if (!hand_pos<N2, PL, true, NT>(b, tt, l, z)) continue;
-            const int xa = x0 + 2 * l;
+            const int z = j + tt * SH::NB;
             float2 pv = make_float2(0.f, 0.f);
             if (xa < g.N0) {
-                const long long gi = xa + (long long)g.N0 * (y + (long long)g.N1 * z);
                 const float2 pp = s_p[slot(b, tt, l, z)];
                 pv.x = pp.x + acc[b][tt].x;
                 pv.y = pp.y + acc[b][tt].y;
-                *reinterpret_cast<float2 *>(a.p + gi) = pv;
+                *reinterpret_cast<float2 *>(a.p + gi0 + tt * dz) = pv;
             }
             acc[b][tt] = pv;
         }
+    }
     if (a.tr.off) {
         __syncthreads();
         hold_to_smem<N2, PL>(sm, acc);

@@ -1264,6 +1264,18 @@ kw_status create(const kw_problem *pr, kw_plan *P) {
     }
     P->op.kappa_a = (float)(q.c_ref * q.dt / 2.0);
     P->op.use_kspace = q.use_kspace ? 1 : 0;
+    {
+        // largest |k|^2 of the grid: the sum of each axis's largest k_i^2
+        double kmax2 = 0.0;
+        for (int a = 0; a < 3; ++a)
+            if (phys_of_int[a] >= 0) {
+                double m = 0.0;
+                for (double k : kvec_fft(P->N[a], P->d[a])) m = std::max(m, k * k);
+                kmax2 += m;
+            }
+        const double ka = q.c_ref * q.dt / 2.0;
+        P->op.short_series = ka * ka * kmax2 <= 1.0 ? 1 : 0;
+    }
     P->op.nabla1_exp = (float)(q.alpha_power - 2.0);
     P->op.nabla2_exp = (float)(q.alpha_power - 1.0);
     P->op.scale = (float)(1.0 / (double)g.N);
